@@ -1,0 +1,935 @@
+// engine.cu — Engine implementation: the substep schedule of mod.rs:264-430 on one
+// CUDA stream, plus the extern "C" entry points of include/coffee_sim.h.
+//
+// Unity build: the kernels are included here so the launches see their definitions.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "engine.h"
+#include "kernels.cu"
+
+namespace cs {
+
+static thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+
+static const int kThreads = 256;
+
+int Engine::check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CS_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return CS_ERR_CUDA;
+}
+
+Engine::Engine(const CsSettings& s) : settings(s) {
+    cells_ = (size_t)s.grid_dims[0] * s.grid_dims[1] * s.grid_dims[2];
+    inflow.angle = s.initial_kettle_angle_deg;
+    inflow.flow_override = s.flow_override_ml_s;
+    inflow.speed_override = s.exit_speed_override;
+}
+
+Engine::~Engine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    free_all();
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Engine::alloc(DeviceBuffer& b, size_t bytes) {
+    b.bytes = bytes;
+    if (bytes == 0) bytes = 16;
+    int rc = check(cudaMalloc(&b.ptr, bytes), "cudaMalloc");
+    if (rc) return rc;
+    owned_.push_back(&b);
+    return check(cudaMemsetAsync(b.ptr, 0, bytes, stream_), "cudaMemsetAsync");
+}
+
+void Engine::free_all() {
+    for (DeviceBuffer* b : owned_) {
+        if (b->ptr) cudaFree(b->ptr);
+        b->ptr = nullptr;
+    }
+    owned_.clear();
+}
+
+int Engine::launch_cells_blocks() const {
+    size_t b = (cells_ + kThreads - 1) / kThreads;
+    return (int)std::min<size_t>(b, (size_t)sms_ * 16);
+}
+int Engine::launch_particle_blocks(uint32_t n) const {
+    size_t b = ((size_t)n + kThreads - 1) / kThreads;
+    return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sms_ * 16));
+}
+
+int Engine::init() {
+    int dev = settings.device;
+    int rc = check(cudaSetDevice(dev), "cudaSetDevice");
+    if (rc) return rc;
+    cudaDeviceProp prop;
+    if ((rc = check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties"))) return rc;
+    sms_ = prop.multiProcessorCount;
+    if ((rc = check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    const size_t mp = settings.max_particles;
+    const size_t f4 = sizeof(float4);
+    DeviceBuffer* bufs[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_, &snap_};
+    for (DeviceBuffer* b : bufs)
+        if ((rc = alloc(*b, mp * f4))) return rc;
+    if ((rc = alloc(render_, mp * 2 * f4))) return rc;
+    if ((rc = alloc(delta_, mp * 4 * sizeof(int32_t)))) return rc;
+    if ((rc = alloc(lanes_, cells_ * 6 * sizeof(int32_t)))) return rc;
+    if ((rc = alloc(lanes64_, settings.p2g_mode == CS_P2G_INT64 ? cells_ * 6 * sizeof(long long) : 0))) return rc;
+    if ((rc = alloc(gvel_, cells_ * f4))) return rc;
+    if ((rc = alloc(pf_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(divf_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(fill_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(lookup_, cells_ * sizeof(int32_t)))) return rc;
+    if ((rc = alloc(sdf_, (size_t)SDF_RES * SDF_RES * SDF_RES * sizeof(float)))) return rc;
+    if ((rc = alloc(cls_, cells_))) return rc;
+    if ((rc = alloc(metrics_, 8 * sizeof(uint32_t)))) return rc;
+    if ((rc = alloc(resid_, 4 * sizeof(double)))) return rc;
+    if ((rc = alloc(d_ctx_, sizeof(Ctx)))) return rc;
+    if ((rc = alloc(staging_, std::max<size_t>(mp * 12 * sizeof(float), cells_ * 6 * sizeof(int32_t))))) return rc;
+
+    ctx_.pos = (float4*)pos_.ptr;
+    ctx_.vel = (float4*)vel_.ptr;
+    ctx_.c0 = (float4*)c0_.ptr;
+    ctx_.c1 = (float4*)c1_.ptr;
+    ctx_.c2 = (float4*)c2_.ptr;
+    ctx_.bedA = (float4*)bedA_.ptr;
+    ctx_.bedB = (float4*)bedB_.ptr;
+    ctx_.render = (float4*)render_.ptr;
+    ctx_.snap = (float4*)snap_.ptr;
+    ctx_.delta = (int32_t*)delta_.ptr;
+    ctx_.lanes = (int32_t*)lanes_.ptr;
+    ctx_.lanes64 = (long long*)lanes64_.ptr;
+    ctx_.gvel = (float4*)gvel_.ptr;
+    ctx_.pf = (float*)pf_.ptr;
+    ctx_.divf = (float*)divf_.ptr;
+    ctx_.fill = (float*)fill_.ptr;
+    ctx_.lookup = (int32_t*)lookup_.ptr;
+    ctx_.sdf = (const float*)sdf_.ptr;
+    ctx_.cls = (const uint8_t*)cls_.ptr;
+    ctx_.metrics = (uint32_t*)metrics_.ptr;
+    ctx_.resid = (double*)resid_.ptr;
+
+    // state.rs:178-182: SDF texture and cell-solid mask, generated on the device
+    SdfSpec spec;
+    std::memset(&spec, 0, sizeof(spec));
+    for (int a = 0; a < 3; ++a) spec.bounds[a] = settings.bounds_size[a];
+    spec.wall_thickness = settings.geom.wall_thickness;
+    spec.count = settings.num_obstacles;
+    for (uint32_t k = 0; k < settings.num_obstacles; ++k) spec.obs[k] = settings.obstacles[k];
+    k_gen_sdf<<<sms_ * 8, kThreads, 0, stream_>>>((float*)sdf_.ptr, spec);
+    fill_params(ctx_.u, 0.0f);
+    if ((rc = upload_ctx())) return rc;
+    k_gen_class<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>((const Ctx*)d_ctx_.ptr);
+    if ((rc = check(cudaGetLastError(), "set-up kernels"))) return rc;
+    sdf_host_.resize((size_t)SDF_RES * SDF_RES * SDF_RES);
+    if ((rc = check(cudaMemcpyAsync(sdf_host_.data(), sdf_.ptr, sdf_.bytes, cudaMemcpyDeviceToHost, stream_), "sdf copy")))
+        return rc;
+    if ((rc = sync())) return rc;
+    return reset();
+}
+
+// mod.rs:222-262 (init_bed) after clearing all particle state (mod.rs:432-446)
+int Engine::reset() {
+    num_water = num_bed = 0;
+    total_time = frame_emitted_mass = total_emitted_mass = 0.0f;
+    frame_dropped = total_dropped = 0;
+    float fo = inflow.flow_override, so = inflow.speed_override;
+    inflow = host::Inflow();
+    inflow.angle = settings.initial_kettle_angle_deg;
+    inflow.flow_override = fo;
+    inflow.speed_override = so;
+    have_prev_p = false;
+    std::memset(&last, 0, sizeof(last));
+    last.last_residual = last.initial_residual = -1.0;
+    DeviceBuffer* zero[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_, &render_, &snap_, &delta_, &lanes_,
+                            &gvel_, &pf_, &divf_, &fill_};
+    int rc;
+    for (DeviceBuffer* b : zero)
+        if ((rc = check(cudaMemsetAsync(b->ptr, 0, b->bytes, stream_), "memset"))) return rc;
+    if ((rc = check(cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_), "memset"))) return rc;
+    if (!settings.has_bed) return sync();
+    host::BedSamples bed = host::init_bed(settings.bed, settings.grid_dims, settings.bounds_size);
+    uint32_t n = std::min(bed.count, settings.max_particles);
+    if (n == 0) return sync();
+    num_bed = n;
+    if ((rc = write_particles(0, 0, n, bed.particles.data()))) return rc;
+    if ((rc = write_particles(1, 0, n, bed.affines.data()))) return rc;
+    if ((rc = write_particles(2, 0, n, bed.extracts.data()))) return rc;
+    if ((rc = check(cudaMemcpyAsync(lookup_.ptr, bed.lookup.data(), cells_ * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    stream_),
+                    "lookup upload")))
+        return rc;
+    return sync();
+}
+
+int Engine::sync() { return check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"); }
+
+// mod.rs:569-670 (write_uniforms), plus the WGSL constants of CsGeometry.
+void Engine::fill_params(Params& u, float dt) const {
+    const CsSettings& s = settings;
+    u.gx = s.grid_dims[0];
+    u.gy = s.grid_dims[1];
+    u.gz = s.grid_dims[2];
+    u.cells = u.gx * u.gy * u.gz;
+    u.num_water = num_water;
+    u.num_bed = num_bed;
+    u.max_p = s.max_particles;
+    u.use_sdf_cache = s.use_sdf_cache ? 1u : 0u;
+    float dx = s.bounds_size[0] / (float)u.gx;
+    float inv_dx = 1.0f / dx;
+    u.dt = dt;
+    u.gravity = s.gravity;
+    u.dx = dx;
+    u.inv_dx = inv_dx;
+    u.ox = -s.bounds_size[0] * 0.5f;
+    u.oy = -s.bounds_size[1] * 0.5f;
+    u.oz = -s.bounds_size[2] * 0.5f;
+    u.bx = s.bounds_size[0] * 0.5f;
+    u.by = s.bounds_size[1] * 0.5f;
+    u.bz = s.bounds_size[2] * 0.5f;
+    u.bulk_K = s.bulk_modulus;
+    u.viscosity = s.viscosity;
+    u.nominal_mass = s.brew.water_mass_units_per_ml / s.brew.water_particles_per_ml;
+    u.p_vol = dx * dx * dx * s.particle_volume_cells;
+    u.vel_cap = s.max_velocity;
+    u.outlet_r = s.brew.dripper_outlet_radius;
+    u.top_r = s.brew.dripper_outlet_radius + s.geom.cone_radius_span;
+    u.friction = s.geom.sdf_friction;
+    u.restitution = s.geom.sdf_restitution;
+    u.contact_offset = s.geom.contact_offset;
+    u.nu_m2s = s.brew.water_kinematic_viscosity_m2_s;
+    u.absorption_rate = s.brew.bed_absorption_rate;
+    u.max_saturation = num_bed > 0 ? s.brew.target_bed_retention_ml * s.brew.water_mass_units_per_ml / (float)num_bed
+                                   : 0.7f;
+    u.min_perm = s.brew.min_bed_permeability_m2;
+    u.extraction_rate = 0.01f;
+    u.compaction_rate = s.brew.bed_compaction_rate;
+    u.bed_damping = 8.5f;
+    u.bed_impact = s.brew.bed_impact_rate;
+    u.pore_capacity_scale = s.brew.bed_pore_capacity_scale;
+    u.pore_overfill_alpha = s.brew.bed_pore_overfill_alpha;
+    u.div_clamp = std::fmin(4.0f * s.max_velocity * inv_dx, FP_VALUE_LIMIT - 1.0f);
+    u.p_clamp = FP_VALUE_LIMIT - 1.0f;
+    u.j_alpha = 32.0f;
+    u.j_expand_alpha = 2.0f;
+    u.max_rest_frac = 1.20f;
+    u.surface_void_scale = s.brew.bed_surface_void_scale;
+    u.water_r_dx = s.brew.water_sample_radius_dx;
+    u.bed_r_dx = s.brew.bed_sample_radius_dx;
+    u.filter_absorption = s.brew.filter_absorption_rate_s;
+    const CsGeometry& g = s.geom;
+    u.geom_flags = g.flags;
+    u.cone_bot_y = g.cone_bot_y;
+    u.cone_top_y = g.cone_top_y;
+    u.filter_center_y = g.filter_center_y;
+    u.filter_top_rel = g.filter_top_rel;
+    u.filter_bot_rel = g.filter_bot_rel;
+    u.filter_top_radius = g.filter_top_radius;
+    u.filter_thickness = g.filter_thickness;
+    u.cup_top_y = g.cup_top_y;
+    u.cup_radius = g.cup_radius;
+    u.cup_floor_y = g.cup_floor_y;
+    u.wall_thickness = g.wall_thickness;
+    u.bed_surface_ref_y = g.bed_surface_ref_y;
+    u.bed_surface_span = g.bed_surface_span;
+    u.fixed_point = s.pressure_storage == CS_PRESSURE_FIXED_POINT ? 1u : 0u;
+    u.int64_grid = s.p2g_mode == CS_P2G_INT64 ? 1u : 0u;
+    u.warm = (s.warm_start != CS_WARM_NONE && !u.fixed_point && have_prev_p) ? 1u : 0u;
+}
+
+int Engine::upload_ctx() {
+    return check(cudaMemcpyAsync(d_ctx_.ptr, &ctx_, sizeof(Ctx), cudaMemcpyHostToDevice, stream_), "ctx upload");
+}
+
+// inflow.rs:122-242: plan on the host, build the samples, append them.
+int Engine::emit(float dt) {
+    uint32_t dropped = 0;
+    uint32_t live = num_water + num_bed;
+    uint32_t count = inflow.plan(settings, dt, live, &dropped);
+    frame_dropped += dropped;
+    total_dropped += dropped;
+    if (count == 0) return CS_OK;
+    host::JetFrame jf = host::jet_frame(settings, inflow, dt, count, live);
+    std::vector<float> parts((size_t)count * 8), affs((size_t)count * 12);
+    host::emit_host(jf, parts.data(), affs.data());
+    inflow.sequence += count;
+    int rc;
+    if ((rc = write_particles(0, live, count, parts.data()))) return rc;
+    if ((rc = write_particles(1, live, count, affs.data()))) return rc;
+    float pm = jf.particle_mass;
+    frame_emitted_mass += (float)count * pm;
+    total_emitted_mass += (float)count * pm;
+    num_water += count;
+    return CS_OK;
+}
+
+double Engine::residual() {
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    cudaMemsetAsync(resid_.ptr, 0, 2 * sizeof(double), stream_);
+    k_residual<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc);
+    double h[2] = {0.0, 0.0};
+    cudaMemcpyAsync(h, resid_.ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+    if (h[1] <= 0.0) return 0.0;
+    return std::sqrt(h[0]) / std::sqrt(h[1]);
+}
+
+int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    const CsSettings& s = settings;
+    const uint32_t half = (s.grid_dims[0] + 1) / 2;
+    const size_t ncol = (size_t)half * s.grid_dims[1] * s.grid_dims[2];
+    const int blocks = (int)std::min<size_t>((ncol + kThreads - 1) / kThreads, (size_t)sms_ * 16);
+    auto pair = [&]() {
+        k_rbgs_colour<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 0u);
+        k_rbgs_colour<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 1u);
+    };
+    sweeps = 0;
+    r0 = r1 = -1.0;
+    if (s.solve_mode == CS_SOLVE_RESIDUAL) {
+        uint32_t ce = s.check_every ? s.check_every : 1;
+        r0 = residual();
+        r1 = r0;
+        if (!(r0 <= (double)s.residual_tol)) {
+            while (sweeps < s.max_sweeps) {
+                pair();
+                ++sweeps;
+                if (sweeps % ce == 0 || sweeps == s.max_sweeps) {
+                    r1 = residual();
+                    if (r1 <= (double)s.residual_tol) break;
+                }
+            }
+        }
+    } else {
+        for (uint32_t k = 0; k < s.pressure_rbgs_pairs; ++k) pair();
+        sweeps = s.pressure_rbgs_pairs;
+        if (s.check_every) r1 = residual();
+    }
+    return check(cudaGetLastError(), "rbgs");
+}
+
+// mod.rs:271-419, one substep.  `passes` limits how many reference dispatches run
+// (numbered in the order of mod.rs:317-414, each number fixed).
+int Engine::substep(float sub_dt, uint32_t P) {
+    int rc;
+    if ((rc = emit(sub_dt))) return rc;
+    fill_params(ctx_.u, sub_dt);
+    if ((rc = upload_ctx())) return rc;
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    const uint32_t np = num_water + num_bed;
+    const int cb = launch_cells_blocks();
+    const int pb = launch_particle_blocks(np);
+    const int bb = launch_particle_blocks(num_bed);
+    const dim3 T(kThreads);
+    // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309)
+    cudaMemsetAsync(lanes_.ptr, 0, lanes_.bytes, stream_);
+    cudaMemsetAsync(gvel_.ptr, 0, gvel_.bytes, stream_);
+    if (P > 0) cudaMemsetAsync(metrics_.ptr, 0, metrics_.bytes, stream_);
+    if (P > 1) cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_);
+    if (P > 2 && num_bed) k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc);
+    if (P > 3 && np) k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc);
+    if (P > 4) k_grid_update<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 5 ? 1 : 0);
+    if (P > 6) k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc);
+    uint32_t sweeps = 0;
+    double r0 = -1.0, r1 = -1.0;
+    if (P > 7) {
+        if ((rc = solve_pressure(sweeps, r0, r1))) return rc;
+        have_prev_p = true;
+    }
+    if (P > 8) k_project<<<dim3(cb, 1), T, 0, stream_>>>(dc, 1 | (P > 9 ? 2 : 0) | (P > 10 ? 4 : 0));
+    if (P > 11) k_packing_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 12 ? 1 : 0);
+    if (P > 13) k_viscosity_prepare<<<dim3(cb, 1), T, 0, stream_>>>(dc);
+    if (P > 14) k_viscosity_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 15 ? 1 : 0);
+    if (P > 16 && np) k_g2p<<<dim3(pb, 1), T, 0, stream_>>>(dc);
+    if (P > 17 && np) k_bed_coupling<<<dim3(pb, 1), T, 0, stream_>>>(dc);
+    if (P > 18 && num_bed) k_extraction_advect<<<dim3(bb, 1), T, 0, stream_>>>(dc);
+    if (P > 19 && num_bed) k_bed_dynamics<<<dim3(bb, 1), T, 0, stream_>>>(dc);
+    if (P > 20 && np) k_prepare_render<<<dim3(pb, 1), T, 0, stream_>>>(dc);
+    if ((rc = check(cudaGetLastError(), "substep launch"))) return rc;
+    total_time += sub_dt;
+    last.last_sweeps = sweeps;
+    last.last_residual = r1;
+    last.initial_residual = r0;
+    return CS_OK;
+}
+
+// mod.rs:264-270
+int Engine::step_frame(float dt) {
+    float fdt = std::fmin(dt, settings.max_frame_dt);
+    uint32_t n = settings.substeps > 1 ? settings.substeps : 1;
+    float sdt = fdt / (float)n;
+    frame_emitted_mass = 0.0f;
+    frame_dropped = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        int rc = substep(sdt, 0xffffffffu);
+        if (rc) return rc;
+    }
+    return CS_OK;
+}
+
+int Engine::metrics(CsMetrics* out) {
+    uint32_t m[8];
+    int rc = check(cudaMemcpyAsync(m, metrics_.ptr, sizeof(m), cudaMemcpyDeviceToHost, stream_), "metrics");
+    if (rc) return rc;
+    if ((rc = sync())) return rc;
+    *out = last;
+    out->max_abs_div = (float)m[M_MAX_DIV] * (1.0f / METRICS_DIV_FP_SCALE);
+    out->fluid_cells = m[M_FLUID];
+    out->div_clamp_fires = m[M_DIV_CLAMP];
+    out->pressure_clamp_fires = m[M_P_CLAMP];
+    out->mass_overflow_fires = m[M_OVERFLOW];
+    out->nan_flag = m[M_NAN];
+    out->timeout_flag = m[M_TIMEOUT];
+    return CS_OK;
+}
+
+// what: 0 particles (8 f32), 1 affine (12 f32), 2 bed_extract (8 f32), 3 render (8 f32)
+int Engine::read_particles(int what, uint32_t first, uint32_t count, float* out) {
+    if ((uint64_t)first + count > settings.max_particles) {
+        set_error("readback range beyond max_particles");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (count == 0) return CS_OK;
+    size_t width = what == 1 ? 12 : 8;
+    k_pack_particles<<<dim3(launch_particle_blocks(count), 1), kThreads, 0, stream_>>>(
+        (const Ctx*)d_ctx_.ptr, first, count, (float*)staging_.ptr, what);
+    int rc = check(cudaMemcpyAsync(out, staging_.ptr, (size_t)count * width * sizeof(float), cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "readback");
+    if (rc) return rc;
+    return sync();
+}
+
+int Engine::write_particles(int what, uint32_t first, uint32_t count, const float* in) {
+    if ((uint64_t)first + count > settings.max_particles) {
+        set_error("upload range beyond max_particles");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (count == 0) return CS_OK;
+    size_t width = what == 1 ? 12 : 8;
+    int rc = upload_ctx();
+    if (rc) return rc;
+    if ((rc = check(cudaMemcpyAsync(staging_.ptr, in, (size_t)count * width * sizeof(float), cudaMemcpyHostToDevice,
+                                    stream_),
+                    "upload")))
+        return rc;
+    k_unpack_particles<<<dim3(launch_particle_blocks(count), 1), kThreads, 0, stream_>>>(
+        (const Ctx*)d_ctx_.ptr, first, count, (const float*)staging_.ptr, what);
+    // the staging buffer is reused by the next upload: wait for this one
+    return sync();
+}
+
+int Engine::read_lanes(int32_t* out) {
+    int rc = check(cudaMemcpyAsync(out, lanes_.ptr, cells_ * 6 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
+                   "lanes");
+    if (rc) return rc;
+    if (settings.pressure_storage != CS_PRESSURE_FIXED_POINT) {
+        k_lane0_encode<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>((const Ctx*)d_ctx_.ptr,
+                                                                                (int32_t*)staging_.ptr);
+        if ((rc = check(cudaMemcpyAsync(out, staging_.ptr, cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
+                        "lane0")))
+            return rc;
+    }
+    return sync();
+}
+int Engine::read_gvel(float* out) {
+    int rc = check(cudaMemcpyAsync(out, gvel_.ptr, cells_ * 16, cudaMemcpyDeviceToHost, stream_), "grid_vel");
+    return rc ? rc : sync();
+}
+int Engine::read_pressure(float* out) {
+    k_pressure_out<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>((const Ctx*)d_ctx_.ptr,
+                                                                           (float*)staging_.ptr);
+    int rc = check(cudaMemcpyAsync(out, staging_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "pressure");
+    return rc ? rc : sync();
+}
+int Engine::read_kind(int32_t* out) {
+    int rc = check(cudaMemcpyAsync(out, (int32_t*)lanes_.ptr + 3 * cells_, cells_ * 4, cudaMemcpyDeviceToHost, stream_),
+                   "kind");
+    return rc ? rc : sync();
+}
+int Engine::read_lookup(int32_t* out) {
+    int rc = check(cudaMemcpyAsync(out, lookup_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "lookup");
+    return rc ? rc : sync();
+}
+int Engine::read_delta(int32_t* out) {
+    int rc = check(cudaMemcpyAsync(out, delta_.ptr, delta_.bytes, cudaMemcpyDeviceToHost, stream_), "delta");
+    return rc ? rc : sync();
+}
+int Engine::read_sdf(float* out) {
+    int rc = check(cudaMemcpyAsync(out, sdf_.ptr, sdf_.bytes, cudaMemcpyDeviceToHost, stream_), "sdf");
+    return rc ? rc : sync();
+}
+int Engine::read_class(uint8_t* out) {
+    int rc = check(cudaMemcpyAsync(out, cls_.ptr, cells_, cudaMemcpyDeviceToHost, stream_), "class");
+    return rc ? rc : sync();
+}
+
+// Shader-style trilinear SDF sample on the host copy (shader.rs:678-699), used by
+// the water-block generator's open-space filter.
+static float host_sample_sdf(const std::vector<float>& sdf, const CsSettings& s, float px, float py, float pz) {
+    float b[3] = {s.bounds_size[0] * 0.5f, s.bounds_size[1] * 0.5f, s.bounds_size[2] * 0.5f};
+    float p[3] = {px, py, pz};
+    int base[3];
+    float f[3];
+    for (int a = 0; a < 3; ++a) {
+        float bs = b[a] * 2.0f;
+        float uv = (p[a] + b[a]) / bs * (float)SDF_RES - 0.5f;
+        float fl = std::floor(uv);
+        base[a] = (int)fl;
+        f[a] = uv - fl;
+    }
+    auto tex = [&](int x, int y, int z) {
+        x = std::min(std::max(x, 0), SDF_RES - 1);
+        y = std::min(std::max(y, 0), SDF_RES - 1);
+        z = std::min(std::max(z, 0), SDF_RES - 1);
+        return sdf[((size_t)z * SDF_RES + y) * SDF_RES + x];
+    };
+    auto mixh = [](float a, float bb, float t) { return a * (1.0f - t) + bb * t; };
+    float c00 = mixh(tex(base[0], base[1], base[2]), tex(base[0] + 1, base[1], base[2]), f[0]);
+    float c10 = mixh(tex(base[0], base[1] + 1, base[2]), tex(base[0] + 1, base[1] + 1, base[2]), f[0]);
+    float c01 = mixh(tex(base[0], base[1], base[2] + 1), tex(base[0] + 1, base[1], base[2] + 1), f[0]);
+    float c11 = mixh(tex(base[0], base[1] + 1, base[2] + 1), tex(base[0] + 1, base[1] + 1, base[2] + 1), f[0]);
+    return mixh(mixh(c00, c10, f[1]), mixh(c01, c11, f[1]), f[2]);
+}
+
+int Engine::add_water_block(const float lo[3], const float hi[3], uint32_t per_axis, float jitter, uint32_t seed,
+                            uint32_t require_open_sdf, uint32_t* added) {
+    host::WaterBlock wb = host::water_block(settings, lo, hi, per_axis, jitter, seed);
+    std::vector<float> parts;
+    size_t n_all = wb.xyz.size() / 3;
+    const float pm = settings.brew.water_mass_units_per_ml / settings.brew.water_particles_per_ml;
+    for (size_t k = 0; k < n_all; ++k) {
+        float x = wb.xyz[3 * k], y = wb.xyz[3 * k + 1], z = wb.xyz[3 * k + 2];
+        if (require_open_sdf && !(host_sample_sdf(sdf_host_, settings, x, y, z) > settings.geom.contact_offset)) continue;
+        float row[8] = {x, y, z, 1.0f, 0.0f, 0.0f, 0.0f, pm};
+        parts.insert(parts.end(), row, row + 8);
+    }
+    uint32_t cnt = (uint32_t)(parts.size() / 8);
+    uint32_t live = num_water + num_bed;
+    if ((uint64_t)live + cnt > settings.max_particles) {
+        set_error("water block exceeds max_particles");
+        return CS_ERR_CAPACITY;
+    }
+    std::vector<float> affs((size_t)cnt * 12, 0.0f);
+    int rc;
+    if ((rc = write_particles(0, live, cnt, parts.data()))) return rc;
+    if ((rc = write_particles(1, live, cnt, affs.data()))) return rc;
+    num_water += cnt;
+    if (added) *added = cnt;
+    return CS_OK;
+}
+
+// ---- checkpoint: host state + particle streams + warm-start pressure ----
+struct SnapHeader {
+    uint64_t magic;
+    uint32_t version, max_p;
+    uint64_t cells;
+    uint32_t num_water, num_bed;
+    float total_time, total_emitted_mass;
+    uint32_t total_dropped, have_prev_p;
+    host::Inflow inflow;
+};
+static const uint64_t kSnapMagic = 0x43534e4150423230ull;  // "CSNAPB20"
+
+int Engine::snapshot_size(uint64_t* bytes) {
+    const uint64_t mp = settings.max_particles;
+    *bytes = sizeof(SnapHeader) + mp * sizeof(float4) * 7 + mp * 4 * sizeof(int32_t) + cells_ * sizeof(float);
+    return CS_OK;
+}
+
+int Engine::snapshot_save(void* buf, uint64_t bytes) {
+    uint64_t need;
+    snapshot_size(&need);
+    if (bytes < need) {
+        set_error("snapshot buffer too small");
+        return CS_ERR_INVALID_ARG;
+    }
+    SnapHeader h;
+    std::memset(&h, 0, sizeof(h));
+    h.magic = kSnapMagic;
+    h.version = 1;
+    h.max_p = settings.max_particles;
+    h.cells = cells_;
+    h.num_water = num_water;
+    h.num_bed = num_bed;
+    h.total_time = total_time;
+    h.total_emitted_mass = total_emitted_mass;
+    h.total_dropped = total_dropped;
+    h.have_prev_p = have_prev_p ? 1 : 0;
+    h.inflow = inflow;
+    char* p = (char*)buf;
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    const size_t mpb = (size_t)settings.max_particles * sizeof(float4);
+    DeviceBuffer* streams[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_};
+    int rc;
+    for (DeviceBuffer* b : streams) {
+        if ((rc = check(cudaMemcpyAsync(p, b->ptr, mpb, cudaMemcpyDeviceToHost, stream_), "snapshot"))) return rc;
+        p += mpb;
+    }
+    if ((rc = check(cudaMemcpyAsync(p, delta_.ptr, delta_.bytes, cudaMemcpyDeviceToHost, stream_), "snapshot")))
+        return rc;
+    p += delta_.bytes;
+    if ((rc = check(cudaMemcpyAsync(p, pf_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "snapshot"))) return rc;
+    return sync();
+}
+
+int Engine::snapshot_load(const void* buf, uint64_t bytes) {
+    uint64_t need;
+    snapshot_size(&need);
+    SnapHeader h;
+    if (bytes < sizeof(h)) {
+        set_error("snapshot too small");
+        return CS_ERR_INVALID_ARG;
+    }
+    std::memcpy(&h, buf, sizeof(h));
+    if (h.magic != kSnapMagic || h.version != 1 || h.max_p != settings.max_particles || h.cells != cells_ ||
+        bytes < need) {
+        set_error("snapshot does not match this simulation's sizes");
+        return CS_ERR_INVALID_ARG;
+    }
+    const char* p = (const char*)buf + sizeof(h);
+    const size_t mpb = (size_t)settings.max_particles * sizeof(float4);
+    DeviceBuffer* streams[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_};
+    int rc;
+    for (DeviceBuffer* b : streams) {
+        if ((rc = check(cudaMemcpyAsync(b->ptr, p, mpb, cudaMemcpyHostToDevice, stream_), "restore"))) return rc;
+        p += mpb;
+    }
+    if ((rc = check(cudaMemcpyAsync(delta_.ptr, p, delta_.bytes, cudaMemcpyHostToDevice, stream_), "restore")))
+        return rc;
+    p += delta_.bytes;
+    if ((rc = check(cudaMemcpyAsync(pf_.ptr, p, cells_ * 4, cudaMemcpyHostToDevice, stream_), "restore"))) return rc;
+    num_water = h.num_water;
+    num_bed = h.num_bed;
+    total_time = h.total_time;
+    total_emitted_mass = h.total_emitted_mass;
+    total_dropped = h.total_dropped;
+    have_prev_p = h.have_prev_p != 0;
+    inflow = h.inflow;
+    return sync();
+}
+
+}  // namespace cs
+
+// ============================ C ABI ============================
+using cs::Engine;
+using cs::set_error;
+
+struct CsSim {
+    std::unique_ptr<Engine> e;
+};
+
+static int validate(const CsSettings* s) {
+    if (!s) {
+        set_error("settings is null");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (s->abi_version != CS_ABI_VERSION) {
+        set_error("settings.abi_version does not match CS_ABI_VERSION");
+        return CS_ERR_INVALID_ARG;
+    }
+    for (int a = 0; a < 3; ++a)
+        if (s->grid_dims[a] < 1 || s->grid_dims[a] > 1024 || !(s->bounds_size[a] > 0.0f)) {
+            set_error("grid_dims / bounds_size out of range");
+            return CS_ERR_INVALID_ARG;
+        }
+    if ((uint64_t)s->grid_dims[0] * s->grid_dims[1] * s->grid_dims[2] > (1ull << 30)) {
+        set_error("grid too large");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (s->max_particles == 0 || s->max_particles > (1u << 28)) {
+        set_error("max_particles out of range");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (s->num_obstacles > CS_MAX_OBSTACLES) {
+        set_error("too many obstacles");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (s->warm_start != CS_WARM_NONE && s->pressure_storage == CS_PRESSURE_FIXED_POINT) {
+        set_error("warm start needs CS_PRESSURE_FP32 storage");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (!(s->brew.water_particles_per_ml > 0.0f)) {
+        set_error("brew.water_particles_per_ml must be > 0");
+        return CS_ERR_INVALID_ARG;
+    }
+    return CS_OK;
+}
+
+#define CS_SIM(sim)                          \
+    if (!(sim) || !(sim)->e) {               \
+        set_error("null simulation handle"); \
+        return CS_ERR_INVALID_ARG;           \
+    }
+#define CS_PTR(p)                            \
+    if (!(p)) {                              \
+        set_error("null output pointer");    \
+        return CS_ERR_INVALID_ARG;           \
+    }
+
+extern "C" {
+
+const char* cs_last_error_string(void) { return cs::g_error.c_str(); }
+uint32_t cs_abi_version(void) { return CS_ABI_VERSION; }
+int32_t cs_is_gpu_engine(void) { return 1; }
+
+int32_t cs_settings_default_v60(CsSettings* out) {
+    CS_PTR(out);
+    cs::host::preset_default_v60(out);
+    return CS_OK;
+}
+int32_t cs_settings_benchmark_free_stream(CsSettings* out) {
+    CS_PTR(out);
+    cs::host::preset_free_stream(out);
+    return CS_OK;
+}
+int32_t cs_settings_benchmark_center_pour(CsSettings* out) {
+    CS_PTR(out);
+    cs::host::preset_center_pour(out);
+    return CS_OK;
+}
+int32_t cs_settings_aim_spout(CsSettings* s, float x, float y, float z) {
+    CS_PTR(s);
+    cs::host::spout_aim_at(s->spout, x, y, z);
+    return CS_OK;
+}
+
+int32_t cs_create(const CsSettings* settings, CsSim** out) {
+    int rc = validate(settings);
+    if (rc) return rc;
+    CS_PTR(out);
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        set_error("no CUDA device visible");
+        return CS_ERR_NO_DEVICE;
+    }
+    if (settings->device < 0 || settings->device >= n) {
+        set_error("settings.device is not a visible CUDA device");
+        return CS_ERR_INVALID_ARG;
+    }
+    std::unique_ptr<CsSim> sim(new CsSim());
+    sim->e.reset(new Engine(*settings));
+    if ((rc = sim->e->init())) return rc;
+    *out = sim.release();
+    return CS_OK;
+}
+int32_t cs_destroy(CsSim* sim) {
+    delete sim;
+    return CS_OK;
+}
+int32_t cs_reset(CsSim* sim) {
+    CS_SIM(sim);
+    return sim->e->reset();
+}
+int32_t cs_step_frame(CsSim* sim, float dt) {
+    CS_SIM(sim);
+    return sim->e->step_frame(dt);
+}
+int32_t cs_step_substep(CsSim* sim, float sub_dt) {
+    CS_SIM(sim);
+    sim->e->frame_emitted_mass = 0.0f;
+    sim->e->frame_dropped = 0;
+    return sim->e->substep(sub_dt, 0xffffffffu);
+}
+int32_t cs_step_substep_partial(CsSim* sim, float sub_dt, uint32_t passes) {
+    CS_SIM(sim);
+    sim->e->frame_emitted_mass = 0.0f;
+    sim->e->frame_dropped = 0;
+    return sim->e->substep(sub_dt, passes);
+}
+int32_t cs_set_kettle_angle(CsSim* sim, float a) {
+    CS_SIM(sim);
+    sim->e->inflow.angle = a;
+    return CS_OK;
+}
+int32_t cs_set_spout_position(CsSim* sim, float x, float y, float z) {
+    CS_SIM(sim);
+    cs::host::spout_translate_origin_to(sim->e->settings.spout, x, y, z);
+    return CS_OK;
+}
+int32_t cs_set_spout_target(CsSim* sim, float x, float y, float z) {
+    CS_SIM(sim);
+    cs::host::spout_aim_at(sim->e->settings.spout, x, y, z);
+    return CS_OK;
+}
+int32_t cs_set_flow_override(CsSim* sim, float flow, float speed) {
+    CS_SIM(sim);
+    sim->e->inflow.flow_override = flow > 0.0f ? flow : 0.0f;
+    sim->e->inflow.speed_override = flow > 0.0f ? speed : 0.0f;
+    return CS_OK;
+}
+int32_t cs_get_counts(const CsSim* sim, uint32_t* nw, uint32_t* nb, uint32_t* mp) {
+    CS_SIM(sim);
+    if (nw) *nw = sim->e->num_water;
+    if (nb) *nb = sim->e->num_bed;
+    if (mp) *mp = sim->e->settings.max_particles;
+    return CS_OK;
+}
+int32_t cs_get_kettle_angle(const CsSim* sim, float* out) {
+    CS_SIM(sim);
+    CS_PTR(out);
+    *out = sim->e->inflow.angle;
+    return CS_OK;
+}
+int32_t cs_get_spout_position(const CsSim* sim, float out[3]) {
+    CS_SIM(sim);
+    CS_PTR(out);
+    for (int k = 0; k < 3; ++k) out[k] = sim->e->settings.spout.origin[k];
+    return CS_OK;
+}
+int32_t cs_get_flow(const CsSim* sim, float* fr, float* es, float* esm) {
+    CS_SIM(sim);
+    if (fr) *fr = sim->e->inflow.flow_rate;
+    if (es) *es = sim->e->inflow.exit_speed;
+    if (esm) *esm = sim->e->inflow.exit_speed * (1.0f / sim->e->settings.sim_units_per_meter);
+    return CS_OK;
+}
+int32_t cs_get_time(const CsSim* sim, float* t) {
+    CS_SIM(sim);
+    CS_PTR(t);
+    *t = sim->e->total_time;
+    return CS_OK;
+}
+int32_t cs_get_emission(const CsSim* sim, float* fem, float* tem, uint32_t* fd, uint32_t* td) {
+    CS_SIM(sim);
+    if (fem) *fem = sim->e->frame_emitted_mass;
+    if (tem) *tem = sim->e->total_emitted_mass;
+    if (fd) *fd = sim->e->frame_dropped;
+    if (td) *td = sim->e->total_dropped;
+    return CS_OK;
+}
+int32_t cs_get_mass_units_per_ml(const CsSim* sim, float* out) {
+    CS_SIM(sim);
+    CS_PTR(out);
+    *out = sim->e->settings.brew.water_mass_units_per_ml;
+    return CS_OK;
+}
+int32_t cs_get_metrics(CsSim* sim, CsMetrics* out) {
+    CS_SIM(sim);
+    CS_PTR(out);
+    return sim->e->metrics(out);
+}
+int32_t cs_get_settings(const CsSim* sim, CsSettings* out) {
+    CS_SIM(sim);
+    CS_PTR(out);
+    *out = sim->e->settings;
+    return CS_OK;
+}
+int32_t cs_read_particles(CsSim* s, uint32_t f, uint32_t c, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_particles(0, f, c, o);
+}
+int32_t cs_read_affine(CsSim* s, uint32_t f, uint32_t c, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_particles(1, f, c, o);
+}
+int32_t cs_read_bed_extract(CsSim* s, uint32_t f, uint32_t c, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_particles(2, f, c, o);
+}
+int32_t cs_read_render(CsSim* s, uint32_t f, uint32_t c, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_particles(3, f, c, o);
+}
+int32_t cs_read_grid_lanes(CsSim* s, int32_t* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_lanes(o);
+}
+int32_t cs_read_grid_vel(CsSim* s, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_gvel(o);
+}
+int32_t cs_read_pressure(CsSim* s, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_pressure(o);
+}
+int32_t cs_read_cell_kind(CsSim* s, int32_t* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_kind(o);
+}
+int32_t cs_read_bed_lookup(CsSim* s, int32_t* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_lookup(o);
+}
+int32_t cs_read_bed_delta(CsSim* s, int32_t* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_delta(o);
+}
+int32_t cs_read_sdf(CsSim* s, float* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_sdf(o);
+}
+int32_t cs_read_sdf_class(CsSim* s, uint8_t* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    return s->e->read_class(o);
+}
+int32_t cs_write_particles(CsSim* s, uint32_t f, uint32_t c, const float* i) {
+    CS_SIM(s);
+    CS_PTR(i);
+    return s->e->write_particles(0, f, c, i);
+}
+int32_t cs_write_affine(CsSim* s, uint32_t f, uint32_t c, const float* i) {
+    CS_SIM(s);
+    CS_PTR(i);
+    return s->e->write_particles(1, f, c, i);
+}
+int32_t cs_write_bed_extract(CsSim* s, uint32_t f, uint32_t c, const float* i) {
+    CS_SIM(s);
+    CS_PTR(i);
+    return s->e->write_particles(2, f, c, i);
+}
+int32_t cs_set_counts(CsSim* s, uint32_t nw, uint32_t nb) {
+    CS_SIM(s);
+    if ((uint64_t)nw + nb > s->e->settings.max_particles) {
+        set_error("counts exceed max_particles");
+        return CS_ERR_CAPACITY;
+    }
+    s->e->num_water = nw;
+    s->e->num_bed = nb;
+    return CS_OK;
+}
+int32_t cs_add_water_block(CsSim* s, const float lo[3], const float hi[3], uint32_t per_axis, float jitter,
+                           uint32_t seed, uint32_t require_open_sdf, uint32_t* added) {
+    CS_SIM(s);
+    if (!lo || !hi || per_axis == 0) {
+        set_error("bad water block arguments");
+        return CS_ERR_INVALID_ARG;
+    }
+    return s->e->add_water_block(lo, hi, per_axis, jitter, seed, require_open_sdf, added);
+}
+int32_t cs_snapshot_size(CsSim* s, uint64_t* b) {
+    CS_SIM(s);
+    CS_PTR(b);
+    return s->e->snapshot_size(b);
+}
+int32_t cs_snapshot_save(CsSim* s, void* buf, uint64_t b) {
+    CS_SIM(s);
+    CS_PTR(buf);
+    return s->e->snapshot_save(buf, b);
+}
+int32_t cs_snapshot_load(CsSim* s, const void* buf, uint64_t b) {
+    CS_SIM(s);
+    CS_PTR(buf);
+    return s->e->snapshot_load(buf, b);
+}
+
+}  // extern "C"

@@ -1,0 +1,80 @@
+// engine.h — one simulation on one GPU: device buffers, the substep schedule, and
+// host-side state (the fields of MpmSim3D, mod.rs:179-193).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "cs_device.cuh"
+#include "host_scene.h"
+
+namespace cs {
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+class Engine {
+public:
+    explicit Engine(const CsSettings& s);
+    ~Engine();
+    int init();           // allocate, generate SDF/mask, seed the bed
+    int reset();          // mod.rs:432-446
+    int step_frame(float dt);
+    int substep(float sub_dt, uint32_t passes);
+    int sync();
+
+    // readback / upload (reference layouts)
+    int read_particles(int what, uint32_t first, uint32_t count, float* out);
+    int write_particles(int what, uint32_t first, uint32_t count, const float* in);
+    int read_lanes(int32_t* out);
+    int read_gvel(float* out);
+    int read_pressure(float* out);
+    int read_kind(int32_t* out);
+    int read_lookup(int32_t* out);
+    int read_delta(int32_t* out);
+    int read_sdf(float* out);
+    int read_class(uint8_t* out);
+    int metrics(CsMetrics* out);
+    int add_water_block(const float lo[3], const float hi[3], uint32_t per_axis, float jitter, uint32_t seed,
+                        uint32_t require_open_sdf, uint32_t* added);
+    int snapshot_size(uint64_t* bytes);
+    int snapshot_save(void* buf, uint64_t bytes);
+    int snapshot_load(const void* buf, uint64_t bytes);
+
+    CsSettings settings;
+    host::Inflow inflow;
+    uint32_t num_water = 0, num_bed = 0;
+    float total_time = 0.0f, frame_emitted_mass = 0.0f, total_emitted_mass = 0.0f;
+    uint32_t frame_dropped = 0, total_dropped = 0;
+    bool have_prev_p = false;
+    CsMetrics last{};
+
+private:
+    int alloc(DeviceBuffer& b, size_t bytes);
+    void free_all();
+    void fill_params(Params& u, float dt) const;
+    int upload_ctx();
+    int emit(float dt);
+    int solve_pressure(uint32_t& sweeps, double& r0, double& r1);
+    double residual();
+    int launch_cells_blocks() const;
+    int launch_particle_blocks(uint32_t n) const;
+    int check(cudaError_t e, const char* what);
+
+    cudaStream_t stream_ = nullptr;
+    size_t cells_ = 0;
+    int sms_ = 148;
+    std::vector<DeviceBuffer*> owned_;
+    DeviceBuffer d_ctx_, pos_, vel_, c0_, c1_, c2_, bedA_, bedB_, render_, snap_, delta_;
+    DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, lookup_, sdf_, cls_, metrics_, resid_;
+    DeviceBuffer staging_;  // AoS upload/readback staging
+    Ctx ctx_{};             // host copy of the device context
+    std::vector<float> sdf_host_;
+};
+
+void set_error(const std::string& msg);
+
+}  // namespace cs

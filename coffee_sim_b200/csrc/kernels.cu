@@ -1,0 +1,1159 @@
+// kernels.cu — sm_100a kernels of one MLS-MPM substep.
+//
+// One kernel (or one fused kernel) per reference compute entry point of
+// crates/sim-wasm/src/mpm_3d/shader.rs, in the dispatch order of mod.rs:317-414.
+// Kernels take an array of Ctx (one per simulation) and use blockIdx.y as the
+// instance, so a batched ensemble runs every member in the same launch.  Element
+// loops are grid-stride so launch shapes do not depend on the particle count (a
+// captured CUDA graph stays valid while particles are emitted).
+#include "kernels.cuh"
+#include "kernels_api.h"
+
+namespace cs {
+
+#define CS_FOR(i, n) for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+// ---------------- set-up: SDF and solid mask (state.rs:206-344) ----------------
+__device__ float sdf_interior(const CsObstacle& o, float px, float py, float pz) {
+    const float NO = 999.0f;
+    if (o.kind == CS_OBSTACLE_TRUNCATED_CONE) {
+        float ly = py - o.center[1];
+        if (ly > o.top_y || ly < o.bot_y) return NO;
+        float h = o.top_y - o.bot_y;
+        if (h < 1e-10f) return NO;
+        float t = (ly - o.bot_y) / h;
+        float cr = o.bot_radius + (o.top_radius - o.bot_radius) * t;
+        float ddx = px - o.center[0], ddz = pz - o.center[2];
+        return cr - sqrtf(ddx * ddx + ddz * ddz);
+    }
+    float ly = py - o.center[1];
+    if (ly > o.top_y) return NO;
+    float ddx = px - o.center[0], ddz = pz - o.center[2];
+    float radial = o.radius - sqrtf(ddx * ddx + ddz * ddz);
+    return fminf(radial, ly - o.bot_y);
+}
+
+__global__ void k_gen_sdf(float* sdf, SdfSpec spec) {
+    const uint32_t n = SDF_RES;
+    CS_FOR(i, n * n * n) {
+        uint32_t ix = i % n, iy = (i / n) % n, iz = i / (n * n);
+        float px = -spec.bounds[0] * 0.5f + ((float)ix + 0.5f) * spec.bounds[0] / (float)n;
+        float py = -spec.bounds[1] * 0.5f + ((float)iy + 0.5f) * spec.bounds[1] / (float)n;
+        float pz = -spec.bounds[2] * 0.5f + ((float)iz + 0.5f) * spec.bounds[2] / (float)n;
+        float v = 999.0f;
+        for (uint32_t k = 0; k < spec.count; ++k) {
+            float sd = sdf_interior(spec.obs[k], px, py, pz) - spec.wall_thickness * 0.5f;
+            if (v >= 999.0f - 1.0f) v = sd;
+            else v = fmaxf(v, sd);
+        }
+        sdf[i] = v;
+    }
+}
+
+// Solid mask from the host-side trilinear sample (state.rs:287-344): f32::fract is
+// x - trunc(x) and the lerp is a + (b - a) * t.
+__global__ void k_gen_class(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        float px = u.ox + ((float)ix + 0.5f) * u.dx;
+        float py = u.oy + ((float)iy + 0.5f) * u.dx;
+        float pz = u.oz + ((float)iz + 0.5f) * u.dx;
+        float bsx = u.bx * 2.0f, bsy = u.by * 2.0f, bsz = u.bz * 2.0f;
+        const float res = (float)SDF_RES;
+        float ux = (px + bsx * 0.5f) / bsx * res - 0.5f;
+        float uy = (py + bsy * 0.5f) / bsy * res - 0.5f;
+        float uz = (pz + bsz * 0.5f) / bsz * res - 0.5f;
+        int x = (int)floorf(ux), y = (int)floorf(uy), z = (int)floorf(uz);
+        float fx = ux - truncf(ux), fy = uy - truncf(uy), fz = uz - truncf(uz);
+        float c000 = sdf_texel(c, x, y, z), c100 = sdf_texel(c, x + 1, y, z);
+        float c010 = sdf_texel(c, x, y + 1, z), c110 = sdf_texel(c, x + 1, y + 1, z);
+        float c001 = sdf_texel(c, x, y, z + 1), c101 = sdf_texel(c, x + 1, y, z + 1);
+        float c011 = sdf_texel(c, x, y + 1, z + 1), c111 = sdf_texel(c, x + 1, y + 1, z + 1);
+        float c00 = c000 + (c100 - c000) * fx, c10 = c010 + (c110 - c010) * fx;
+        float c01 = c001 + (c101 - c001) * fx, c11 = c011 + (c111 - c011) * fx;
+        float c0 = c00 + (c10 - c00) * fy, c1 = c01 + (c11 - c01) * fy;
+        float v = c0 + (c1 - c0) * fz;
+        ((uint8_t*)c.cls)[i] = v < 0.0f ? 1 : 0;
+    }
+}
+
+// ---------------- bed_lookup_scatter (shader.rs:2305-2335) ----------------
+__global__ void k_bed_lookup_scatter(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(b, u.num_bed) {
+        if (is_water_phase(c.c0[b].w)) continue;
+        int cx, cy, cz;
+        world_to_cell(u, xyz(c.pos[b]), cx, cy, cz);
+        for (int di = -1; di <= 1; ++di)
+            for (int dj = -1; dj <= 1; ++dj)
+                for (int dk = -1; dk <= 1; ++dk) {
+                    int x = cx + di, y = cy + dj, z = cz + dk;
+                    if (!in_grid(u, x, y, z)) continue;
+                    atomicMax(&c.lookup[cidx(u, x, y, z)], (int32_t)b);
+                }
+    }
+}
+
+// ---------------- p2g (shader.rs:955-1052), one global atomic per node and lane ----
+__device__ __forceinline__ void p2g_particle(const Ctx& c, uint32_t pid) {
+    const Params& u = c.u;
+    float4 P = c.pos[pid], Vv = c.vel[pid], A0 = c.c0[pid];
+    float mp = Vv.w;
+    if (!is_water_phase(A0.w) || mp <= inactive_mass(u)) return;
+    float4 A1 = c.c1[pid], A2 = c.c2[pid];
+    float gx = (P.x - u.ox) * u.inv_dx, gy = (P.y - u.oy) * u.inv_dx, gz = (P.z - u.oz) * u.inv_dx;
+    int bx = (int)floorf(gx - 0.5f), by = (int)floorf(gy - 0.5f), bz = (int)floorf(gz - 0.5f);
+    float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+    float wx[3], wy[3], wz[3];
+    bspline(fx, wx);
+    bspline(fy, wy);
+    bspline(fz, wz);
+    f3 a0 = mk(mp * A0.x, mp * A0.y, mp * A0.z);
+    f3 a1 = mk(mp * A1.x, mp * A1.y, mp * A1.z);
+    f3 a2 = mk(mp * A2.x, mp * A2.y, mp * A2.z);
+    f3 mv = mk(mp * Vv.x, mp * Vv.y, mp * Vv.z);
+    float rpv = u.p_vol * mp / wmax(u.nominal_mass, 1e-6f);
+    float cpv = rpv * clamp_j(P.w);
+    const float lim = 1.0e9f;
+    bool overflow = false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                int cx = bx + i, cy = by + j, cz = bz + k;
+                if (!in_grid(u, cx, cy, cz)) continue;
+                float w = wx[i] * wy[j] * wz[k];
+                f3 dpos = mk(((float)i - fx) * u.dx, ((float)j - fy) * u.dx, ((float)k - fz) * u.dx);
+                float mfp = (w * mp) * FP_SCALE;
+                float rfp = (w * rpv) * FP_SCALE;
+                float cfp = (w * cpv) * FP_SCALE;
+                float mx = (w * (mv.x + dot3(a0, dpos))) * FP_SCALE;
+                float my = (w * (mv.y + dot3(a1, dpos))) * FP_SCALE;
+                float mz = (w * (mv.z + dot3(a2, dpos))) * FP_SCALE;
+                overflow |= fabsf(mfp) > lim || fabsf(mx) > lim || fabsf(my) > lim || fabsf(mz) > lim ||
+                            fabsf(rfp) > lim || fabsf(cfp) > lim;
+                uint32_t ci = cidx(u, cx, cy, cz);
+                atomicAdd(&c.lanes[ci], to_i32(mfp));
+                atomicAdd(&c.lanes[(size_t)u.cells + ci], to_i32(mx));
+                atomicAdd(&c.lanes[2 * (size_t)u.cells + ci], to_i32(my));
+                atomicAdd(&c.lanes[3 * (size_t)u.cells + ci], to_i32(mz));
+                atomicAdd(&c.lanes[4 * (size_t)u.cells + ci], to_i32(rfp));
+                atomicAdd(&c.lanes[5 * (size_t)u.cells + ci], to_i32(cfp));
+                if (overflow) {
+                    atomicAdd(&c.metrics[M_OVERFLOW], 1u);
+                    overflow = false;
+                }
+            }
+}
+
+__global__ void k_p2g_atomic(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    uint32_t n = c.u.num_water + c.u.num_bed;
+    CS_FOR(pid, n) p2g_particle(c, pid);
+}
+
+// ---------------- grid_update (shader.rs:1056-1082) [+ boundary_project] ----------------
+__global__ void k_grid_update(const Ctx* __restrict__ cp, int with_boundary) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        float mass = (float)c.lanes[i] * INV_FP_SCALE;
+        if (mass < 1e-6f) continue;
+        f3 v = mk((float)c.lanes[(size_t)u.cells + i] * INV_FP_SCALE / mass,
+                  (float)c.lanes[2 * (size_t)u.cells + i] * INV_FP_SCALE / mass,
+                  (float)c.lanes[3 * (size_t)u.cells + i] * INV_FP_SCALE / mass);
+        v.y += u.gravity * u.dt;
+        float sp = len3(v);
+        if (sp > u.vel_cap) v = v * (u.vel_cap / sp);
+        if (with_boundary) {
+            uint32_t ix, iy, iz;
+            decompose(u, i, ix, iy, iz);
+            v = boundary_velocity(c, ix, iy, iz, v);
+        }
+        c.gvel[i] = make_float4(v.x, v.y, v.z, mass);
+    }
+}
+
+// ---------------- boundary_project alone (shader.rs:1630-1679) ----------------
+__global__ void k_boundary(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        float4 g = c.gvel[i];
+        if (g.w < 1e-6f) continue;
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        f3 v = boundary_velocity(c, ix, iy, iz, xyz(g));
+        c.gvel[i] = make_float4(v.x, v.y, v.z, g.w);
+    }
+}
+
+// ---------------- classify_cells (shader.rs:1181-1367) ----------------
+__device__ float volume_target(const Params& u, float rest, float cur) {
+    float cv = u.dx * u.dx * u.dx;
+    float eps = wmax(cv * 1e-5f, u.p_vol * 1e-3f);
+    if (rest <= eps) return 0.0f;
+    float j = cur / rest;
+    float ce = wclamp(1.0f - j, 0.0f, 0.75f);
+    float ee = wclamp(j - 1.0f, 0.0f, 0.75f);
+    float t = ce * u.j_alpha - ee * u.j_expand_alpha;
+    float packed = wmax(rest, cur) / wmax(cv, 1e-8f);
+    float over = wmax(packed - u.max_rest_frac, 0.0f);
+    return wmax(t, over * u.j_alpha);
+}
+__device__ float bed_pore_target(const Ctx& c, uint32_t b, f3 cc, float rest, float cur) {
+    const Params& u = c.u;
+    float t = volume_target(u, rest, cur);
+    float cv = u.dx * u.dx * u.dx;
+    float poro = compacted_porosity(c, b);
+    float sat = wclamp(c.bedB[b].w, 0.0f, 1.0f);
+    float comp = wclamp(c.bedA[b].w, 0.0f, 2.25f);
+    float bcy = c.pos[b].y;
+    float st = smoothstepf(-0.25f, 0.75f, (cc.y - bcy) * u.inv_dx);
+    float open = wclamp((1.0f - 0.65f * sat) * (1.0f - 0.12f * comp), 0.20f, 1.0f);
+    float sopen = st * wclamp(u.surface_void_scale, 0.0f, 1.0f) * open;
+    float sporo = wmin(poro + 0.35f, 0.82f);
+    float eff = mixf(poro, sporo, sopen);
+    float occ = mixf(1.0f, 0.35f, sopen);
+    float satcap = mixf(1.0f, 0.32f, sat);
+    float compcap = mixf(1.0f, 0.58f, wclamp(comp / 1.5f, 0.0f, 1.0f));
+    float cap = eff * cv * wmax(u.pore_capacity_scale, 0.0f) * satcap * compcap;
+    float over = wmax(cur - cap, 0.0f) / wmax(cv, 1e-8f);
+    float resp = u.pore_overfill_alpha * occ * mixf(1.0f, 1.45f, sat);
+    return wmax(t, over * resp);
+}
+__device__ __forceinline__ bool open_nb(const Ctx& c, f3 cc, uint32_t x, uint32_t y, uint32_t z, float ox, float oy,
+                                        float oz) {
+    if (c.u.use_sdf_cache) return c.cls[cidx(c.u, x, y, z)] == 0;
+    return sample_sdf(c, cc + mk(ox, oy, oz)) >= 0.0f;
+}
+
+__global__ void k_classify(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        float mass = c.gvel[i].w;
+        float keep = (!u.fixed_point && u.warm) ? c.pf[i] : 0.0f;
+        pressure_store(c, i, 0.0f);
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        f3 cc = cell_center(u, ix, iy, iz);
+        bool solid = u.use_sdf_cache ? (c.cls[i] != 0) : (sample_sdf(c, cc) < 0.0f);
+        int32_t* kl = lane(c, 3);
+        if (solid) {
+            kl[i] = CELL_SOLID;
+            div_store(c, i, 0.0f);
+            c.fill[i] = 0.0f;
+            continue;
+        }
+        if (mass <= occupancy_mass(u)) {
+            kl[i] = CELL_AIR;
+            div_store(c, i, 0.0f);
+            c.fill[i] = 0.0f;
+            continue;
+        }
+        int32_t kind;
+        if (c.lookup[i] >= 0) {
+            kind = CELL_BED;
+        } else {
+            bool air = (ix == 0) || (ix + 1 >= u.gx) || (iy == 0) || (iy + 1 >= u.gy) || (iz == 0) || (iz + 1 >= u.gz);
+            if (!air) {
+                const float occ = occupancy_mass(u);
+                air = c.gvel[i - 1].w <= occ || c.gvel[i + 1].w <= occ || c.gvel[i - u.gx].w <= occ ||
+                      c.gvel[i + u.gx].w <= occ || c.gvel[i - u.gx * u.gy].w <= occ ||
+                      c.gvel[i + u.gx * u.gy].w <= occ;
+            }
+            kind = air ? CELL_SURFACE : CELL_INTERIOR;
+        }
+        kl[i] = kind;
+        c.fill[i] = liquid_fill(c, i, kind);
+        if (u.warm && !u.fixed_point) c.pf[i] = keep;
+        float4 sv = c.gvel[i];
+        const float d = u.dx;
+        float vxm = -sv.x, vxp = -sv.x, vym = -sv.y, vyp = -sv.y, vzm = -sv.z, vzp = -sv.z;
+        if (ix > 0 && open_nb(c, cc, ix - 1, iy, iz, -d, 0.0f, 0.0f)) vxm = c.gvel[i - 1].x;
+        if (ix + 1 < u.gx && open_nb(c, cc, ix + 1, iy, iz, d, 0.0f, 0.0f)) vxp = c.gvel[i + 1].x;
+        if (iy > 0 && open_nb(c, cc, ix, iy - 1, iz, 0.0f, -d, 0.0f)) vym = c.gvel[i - u.gx].y;
+        if (iy + 1 < u.gy && open_nb(c, cc, ix, iy + 1, iz, 0.0f, d, 0.0f)) vyp = c.gvel[i + u.gx].y;
+        if (iz > 0 && open_nb(c, cc, ix, iy, iz - 1, 0.0f, 0.0f, -d)) vzm = c.gvel[i - u.gx * u.gy].z;
+        if (iz + 1 < u.gz && open_nb(c, cc, ix, iy, iz + 1, 0.0f, 0.0f, d)) vzp = c.gvel[i + u.gx * u.gy].z;
+        float div = 0.5f * u.inv_dx * (((vxp - vxm) + (vyp - vym)) + (vzp - vzm));
+        float rest = rest_vol(c, i), cur = cur_vol(c, i);
+        float target = volume_target(u, rest, cur);
+        if (kind == CELL_BED) {
+            int32_t b = c.lookup[i];
+            if (b >= 0 && (uint32_t)b < u.num_bed) {
+                float pt = bed_pore_target(c, (uint32_t)b, cc, rest, cur);
+                float poro = wclamp(compacted_porosity(c, (uint32_t)b), 0.08f, 1.0f);
+                float sfrac = 1.0f - poro;
+                int x = ix, y = iy, z = iz;
+                float bxm = bed_velocity_cell(c, x - 1, y, z).x, bxp = bed_velocity_cell(c, x + 1, y, z).x;
+                float bym = bed_velocity_cell(c, x, y - 1, z).y, byp = bed_velocity_cell(c, x, y + 1, z).y;
+                float bzm = bed_velocity_cell(c, x, y, z - 1).z, bzp = bed_velocity_cell(c, x, y, z + 1).z;
+                float sdiv = 0.5f * u.inv_dx * (((bxp - bxm) + (byp - bym)) + (bzp - bzm));
+                target = (pt - sfrac * sdiv) / poro;
+            }
+        }
+        div_store(c, i, div - target);
+        uint32_t fd = to_u32(wclamp(fabsf(div) * METRICS_DIV_FP_SCALE, 0.0f, 2147483648.0f));
+        atomicMax(&c.metrics[M_MAX_DIV], fd);
+        atomicAdd(&c.metrics[M_FLUID], 1u);
+    }
+}
+
+// ---------------- pressure_rbgs_red / _black (shader.rs:1371-1453) ----------------
+// Thread t of a colour handles the t-th cell of that colour: rows of (y,z) hold
+// ceil(gx/2) slots, x = 2*slot + ((y+z+parity)&1).
+__device__ __forceinline__ void pressure_update(const Ctx& c, uint32_t i, uint32_t ix, uint32_t iy, uint32_t iz) {
+    const Params& u = c.u;
+    const int32_t* kl = lane(c, 3);
+    int32_t kind = kl[i];
+    if (!is_fluid(kind)) {
+        pressure_store(c, i, 0.0f);
+        return;
+    }
+    float sf = c.fill[i];
+    float nc = 0.0f, ps = 0.0f;
+    const uint32_t sy = u.gx, sz = u.gx * u.gy;
+#define CS_FACE(cond, off)                                               \
+    if (cond) {                                                          \
+        uint32_t ni = i + (off);                                         \
+        int32_t nk = kl[ni];                                             \
+        if (!is_solid(nk)) {                                             \
+            float w = face_weight(kind, sf, nk, c.fill[ni]);             \
+            if (w > 0.0f) {                                              \
+                nc += w;                                                 \
+                if (is_fluid(nk)) ps += w * pressure_load(c, ni);        \
+            }                                                            \
+        }                                                                \
+    }
+    CS_FACE(ix > 0, (uint32_t)-1)
+    CS_FACE(ix + 1 < u.gx, 1u)
+    CS_FACE(iy > 0, (uint32_t)0 - sy)
+    CS_FACE(iy + 1 < u.gy, sy)
+    CS_FACE(iz > 0, (uint32_t)0 - sz)
+    CS_FACE(iz + 1 < u.gz, sz)
+#undef CS_FACE
+    if (nc <= 0.0f) {
+        pressure_store(c, i, 0.0f);
+        return;
+    }
+    float rhs = div_load(c, i) * sf / wmax(u.dt, 1e-6f);
+    pressure_store(c, i, (ps - u.dx * u.dx * rhs) / nc);
+}
+
+__global__ void k_rbgs_colour(const Ctx* __restrict__ cp, uint32_t parity) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const uint32_t half = (u.gx + 1) / 2;
+    const uint32_t n = half * u.gy * u.gz;
+    CS_FOR(t, n) {
+        uint32_t row = t / half, slot = t - row * half;
+        uint32_t iy = row % u.gy, iz = row / u.gy;
+        uint32_t ix = 2 * slot + ((iy + iz + parity) & 1u);
+        if (ix >= u.gx) continue;
+        pressure_update(c, cidx(u, ix, iy, iz), ix, iy, iz);
+    }
+}
+
+// Residual of the pressure system in FP64 (definition: for each fluid cell
+// r = (sum_f w_f p_f - dx^2 rhs) - W p with the face weights of pressure_update).
+__global__ void k_residual(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const int32_t* kl = lane(c, 3);
+    double r2 = 0.0, b2 = 0.0;
+    CS_FOR(i, u.cells) {
+        int32_t kind = kl[i];
+        if (!is_fluid(kind)) continue;
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        float sf = c.fill[i];
+        double wsum = 0.0, psum = 0.0;
+        const uint32_t sy = u.gx, sz = u.gx * u.gy;
+#define CS_RFACE(cond, off)                                                        \
+    if (cond) {                                                                    \
+        uint32_t ni = i + (off);                                                   \
+        int32_t nk = kl[ni];                                                       \
+        if (!is_solid(nk)) {                                                       \
+            float w = face_weight(kind, sf, nk, c.fill[ni]);                       \
+            if (w > 0.0f) {                                                        \
+                wsum += (double)w;                                                 \
+                if (is_fluid(nk)) psum += (double)w * (double)pressure_load(c, ni); \
+            }                                                                      \
+        }                                                                          \
+    }
+        CS_RFACE(ix > 0, (uint32_t)-1)
+        CS_RFACE(ix + 1 < u.gx, 1u)
+        CS_RFACE(iy > 0, (uint32_t)0 - sy)
+        CS_RFACE(iy + 1 < u.gy, sy)
+        CS_RFACE(iz > 0, (uint32_t)0 - sz)
+        CS_RFACE(iz + 1 < u.gz, sz)
+#undef CS_RFACE
+        if (wsum <= 0.0) continue;
+        float rhs = div_load(c, i) * sf / wmax(u.dt, 1e-6f);
+        double b = (double)(u.dx * u.dx * rhs);
+        double r = (psum - b) - wsum * (double)pressure_load(c, i);
+        r2 += r * r;
+        b2 += b * b;
+    }
+    // warp then block reduction, one double atomic pair per block
+    for (int o = 16; o > 0; o >>= 1) {
+        r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        b2 += __shfl_down_sync(0xffffffffu, b2, o);
+    }
+    __shared__ double sr[32], sb[32];
+    int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane_id == 0) {
+        sr[warp] = r2;
+        sb[warp] = b2;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        r2 = lane_id < nw ? sr[lane_id] : 0.0;
+        b2 = lane_id < nw ? sb[lane_id] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            r2 += __shfl_down_sync(0xffffffffu, r2, o);
+            b2 += __shfl_down_sync(0xffffffffu, b2, o);
+        }
+        if (lane_id == 0) {
+            atomicAdd(&c.resid[0], r2);
+            atomicAdd(&c.resid[1], b2);
+        }
+    }
+}
+
+// ---------------- project_pressure (shader.rs:1457-1543) [+ boundary + packing_prepare] ----
+__device__ __forceinline__ float weighted_or_mirror(const Ctx& c, bool in, uint32_t ni, float mirror, int32_t sk,
+                                                    float sf) {
+    if (!in) return mirror;
+    int32_t k = lane(c, 3)[ni];
+    if (is_solid(k)) return mirror;
+    float np = 0.0f;
+    if (is_fluid(k)) np = pressure_load(c, ni);
+    return mixf(mirror, np, face_weight(sk, sf, k, c.fill[ni]));
+}
+
+// stages: bit0 project, bit1 boundary, bit2 packing_prepare
+__global__ void k_project(const Ctx* __restrict__ cp, int stages) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        int32_t kind = lane(c, 3)[i];
+        if (stages & 4) {
+            // packing_prepare (shader.rs:1566-1583): reads kind and volumes only
+            if (!is_fluid(kind) || kind == CELL_BED) {
+                packing_store(c, i, 0.0f);
+            } else {
+                float cv = u.dx * u.dx * u.dx;
+                float packed = wmax(rest_vol(c, i), cur_vol(c, i)) / wmax(cv, 1e-8f);
+                float over = wmax(packed - wmin(u.max_rest_frac, 1.0f), 0.0f);
+                packing_store(c, i, u.bulk_K * over);
+            }
+        }
+        float4 g = c.gvel[i];
+        if (g.w < 1e-6f) continue;
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        f3 v = xyz(g);
+        bool changed = false;
+        if ((stages & 1) && is_fluid(kind)) {
+            float ph = pressure_load(c, i);
+            float sf = c.fill[i];
+            const uint32_t sy = u.gx, sz = u.gx * u.gy;
+            float pxm = weighted_or_mirror(c, ix > 0, i - 1, ph, kind, sf);
+            float pxp = weighted_or_mirror(c, ix + 1 < u.gx, i + 1, ph, kind, sf);
+            float pym = weighted_or_mirror(c, iy > 0, i - sy, ph, kind, sf);
+            float pyp = weighted_or_mirror(c, iy + 1 < u.gy, i + sy, ph, kind, sf);
+            float pzm = weighted_or_mirror(c, iz > 0, i - sz, ph, kind, sf);
+            float pzp = weighted_or_mirror(c, iz + 1 < u.gz, i + sz, ph, kind, sf);
+            float h = 0.5f * u.inv_dx;
+            f3 grad = mk(h * (pxp - pxm), h * (pyp - pym), h * (pzp - pzm));
+            v = v - u.dt * grad;
+            if (kind == CELL_BED) {
+                int32_t b = c.lookup[i];
+                if (b >= 0 && (uint32_t)b < u.num_bed) {
+                    float perm = compacted_permeability(c, (uint32_t)b);
+                    float rate = u.nu_m2s / perm;
+                    float damp = 1.0f / (1.0f + wmax(rate * u.dt, 0.0f));
+                    f3 bv = bed_matrix_velocity(c, ix, iy, iz);
+                    f3 before = v;
+                    v = bv + (v - bv) * damp;
+                    f3 wi = g.w * (v - before);
+                    bed_impulse_neighborhood(c, ix, iy, iz, (-wi) * BED_REACTION_ALPHA);
+                }
+            }
+            float sp = len3(v);
+            if (sp > u.vel_cap) v = v * (u.vel_cap / sp);
+            changed = true;
+        }
+        if (stages & 2) {
+            v = boundary_velocity(c, ix, iy, iz, v);
+            changed = true;
+        }
+        if (changed) c.gvel[i] = make_float4(v.x, v.y, v.z, g.w);
+    }
+}
+
+// ---------------- packing_apply (shader.rs:1586-1626) [+ boundary] ----------------
+__device__ __forceinline__ float packing_or_mirror(const Ctx& c, bool in, uint32_t ni, float mirror) {
+    if (!in) return mirror;
+    int32_t k = lane(c, 3)[ni];
+    if (is_solid(k)) return mirror;
+    if (!is_fluid(k)) return 0.0f;
+    return packing_load(c, ni);
+}
+
+__global__ void k_packing_apply(const Ctx* __restrict__ cp, int with_boundary) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        float4 g = c.gvel[i];
+        if (g.w < 1e-6f) continue;
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        f3 v = xyz(g);
+        int32_t kind = lane(c, 3)[i];
+        if (g.w > occupancy_mass(u) && is_fluid(kind)) {
+            const uint32_t sy = u.gx, sz = u.gx * u.gy;
+            float ph = packing_load(c, i);
+            float pxm = packing_or_mirror(c, ix > 0, i - 1, ph), pxp = packing_or_mirror(c, ix + 1 < u.gx, i + 1, ph);
+            float pym = packing_or_mirror(c, iy > 0, i - sy, ph), pyp = packing_or_mirror(c, iy + 1 < u.gy, i + sy, ph);
+            float pzm = packing_or_mirror(c, iz > 0, i - sz, ph), pzp = packing_or_mirror(c, iz + 1 < u.gz, i + sz, ph);
+            float h = 0.5f * u.inv_dx;
+            f3 grad = mk(h * (pxp - pxm), h * (pyp - pym), h * (pzp - pzm));
+            v = v - u.dt * grad;
+            float sp = len3(v);
+            if (sp > u.vel_cap) v = v * (u.vel_cap / sp);
+        }
+        if (with_boundary) v = boundary_velocity(c, ix, iy, iz, v);
+        c.gvel[i] = make_float4(v.x, v.y, v.z, g.w);
+    }
+}
+
+// ---------------- viscosity_prepare (shader.rs:1086-1163) ----------------
+__global__ void k_viscosity_prepare(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        float4 g = c.gvel[i];
+        f3 vh = xyz(g);
+        if (g.w <= occupancy_mass(u) || u.viscosity <= 0.0f || g.w <= u.nominal_mass * 2.0f) {
+            vscratch_store(c, i, vh);
+            continue;
+        }
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        float alpha = wclamp(u.viscosity * u.dt / wmax(u.dx * u.dx, 1e-6f), 0.0f, 0.14f);
+        f3 sum = mk(0.0f, 0.0f, 0.0f);
+        float ws = 0.0f;
+        uint32_t nf = 0;
+        const float denom = wmax(wmax(g.w, u.nominal_mass), 1e-6f);
+        const uint32_t sy = u.gx, sz = u.gx * u.gy;
+#define CS_VFACE(cond, off)                                          \
+    if (!(cond) || c.cls[i + (off)] != 0) {                          \
+        ws += 1.0f;                                                  \
+    } else {                                                         \
+        float4 ng = c.gvel[i + (off)];                               \
+        if (ng.w > occupancy_mass(u)) {                              \
+            float nw = wclamp(ng.w / denom, 0.0f, 1.0f);             \
+            sum += xyz(ng) * nw;                                     \
+            ws += nw;                                                \
+            nf += 1;                                                 \
+        }                                                            \
+    }
+        CS_VFACE(ix > 0, (uint32_t)-1)
+        CS_VFACE(ix + 1 < u.gx, 1u)
+        CS_VFACE(iy > 0, (uint32_t)0 - sy)
+        CS_VFACE(iy + 1 < u.gy, sy)
+        CS_VFACE(iz > 0, (uint32_t)0 - sz)
+        CS_VFACE(iz + 1 < u.gz, sz)
+#undef CS_VFACE
+        if (nf < 3 || ws <= 1e-6f) {
+            vscratch_store(c, i, vh);
+            continue;
+        }
+        f3 avg = sum / ws;
+        float blend = wclamp(alpha * ws, 0.0f, 0.65f);
+        vscratch_store(c, i, mix3(vh, avg, blend));
+    }
+}
+
+// ---------------- viscosity_apply (shader.rs:1166-1177) [+ boundary] ----------------
+__global__ void k_viscosity_apply(const Ctx* __restrict__ cp, int with_boundary) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+        float mass = c.gvel[i].w;
+        if (mass <= occupancy_mass(u)) {
+            c.gvel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        f3 v = vscratch_load(c, i);
+        if (with_boundary && mass >= 1e-6f) {
+            uint32_t ix, iy, iz;
+            decompose(u, i, ix, iy, iz);
+            v = boundary_velocity(c, ix, iy, iz, v);
+        }
+        c.gvel[i] = make_float4(v.x, v.y, v.z, mass);
+    }
+}
+
+// ---------------- g2p (shader.rs:1683-1881) ----------------
+__device__ __forceinline__ void g2p_particle(const Ctx& c, uint32_t pid) {
+    const Params& u = c.u;
+    float4 A0 = c.c0[pid];
+    float phase = A0.w;
+    if (!is_water_phase(phase)) return;
+    float4 P = c.pos[pid], Vv = c.vel[pid];
+    float mp = Vv.w;
+    if (mp <= inactive_mass(u)) {
+        c.vel[pid].w = 0.0f;
+        return;
+    }
+    f3 xp = xyz(P);
+    float gx = (xp.x - u.ox) * u.inv_dx, gy = (xp.y - u.oy) * u.inv_dx, gz = (xp.z - u.oz) * u.inv_dx;
+    int bx = (int)floorf(gx - 0.5f), by = (int)floorf(gy - 0.5f), bz = (int)floorf(gz - 0.5f);
+    float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+    float wx[3], wy[3], wz[3];
+    bspline(fx, wx);
+    bspline(fy, wy);
+    bspline(fz, wz);
+    f3 nv = mk(0.0f, 0.0f, 0.0f), n0 = nv, n1 = nv, n2 = nv, bvs = nv;
+    float supp = 0.0f, lmass = 0.0f, bow = 0.0f, bperm = 0.0f;
+    const float B = 4.0f * u.inv_dx * u.inv_dx;
+    const bool has_bed = u.num_bed > 0u;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                int cx = bx + i, cy = by + j, cz = bz + k;
+                if (!in_grid(u, cx, cy, cz)) continue;
+                float w = wx[i] * wy[j] * wz[k];
+                uint32_t ci = cidx(u, cx, cy, cz);
+                float4 g = c.gvel[ci];
+                if (g.w > 1e-6f) {
+                    f3 gv = xyz(g);
+                    f3 dpos = mk(((float)i - fx) * u.dx, ((float)j - fy) * u.dx, ((float)k - fz) * u.dx);
+                    nv += w * gv;
+                    float wb = w * B;
+                    n0 += (wb * gv) * dpos.x;
+                    n1 += (wb * gv) * dpos.y;
+                    n2 += (wb * gv) * dpos.z;
+                    supp += w;
+                    lmass += w * g.w;
+                }
+                if (has_bed) {
+                    int32_t b = c.lookup[ci];
+                    if (valid_bed_solid(c, b)) {
+                        bow += w;
+                        bvs += w * xyz(c.vel[b]);
+                        bperm += w * compacted_permeability(c, (uint32_t)b);
+                    }
+                }
+            }
+    float sr = wclamp(supp, 0.0f, 1.0f);
+    float jsup = sr;
+    if (supp > 1e-6f) {
+        float inv = 1.0f / supp;
+        nv *= inv;
+        n0 *= inv;
+        n1 *= inv;
+        n2 *= inv;
+    }
+    float cr = u.cup_radius + u.contact_offset;
+    bool in_cup = (u.geom_flags & CS_GEOM_CUP) && xp.y < u.cup_top_y && (xp.x * xp.x + xp.z * xp.z) < cr * cr;
+    float dsr = wclamp(lmass / wmax(u.nominal_mass * 4.0f, 1e-6f), 0.0f, 1.0f);
+    float po = wclamp(bow, 0.0f, 1.0f);
+    f3 pbv = mk(0.0f, 0.0f, 0.0f);
+    float pbk = u.min_perm;
+    if (bow > 1e-6f) {
+        float inv = 1.0f / bow;
+        pbv = bvs * inv;
+        pbk = wmax(bperm * inv, u.min_perm);
+    }
+    if (sr < 0.999f) {
+        f3 bal = mk(Vv.x, Vv.y + u.gravity * u.dt, Vv.z);
+        float pg = mixf(in_cup ? 1.15f : 1.35f, 0.18f, po);
+        float pc = mixf(in_cup ? 0.95f : 0.995f, 0.16f, po);
+        float dpd = mixf(1.0f, 0.12f, dsr);
+        float pres = wclamp((1.0f - sr) * pg * dpd, 0.0f, pc);
+        nv = mix3(nv, bal, pres);
+        float ad = 1.0f - pres * 0.75f;
+        n0 *= ad;
+        n1 *= ad;
+        n2 *= ad;
+    }
+    bool airborne = po <= 0.05f && sample_sdf(c, xp) > u.contact_offset * 2.0f;
+    if (airborne) {
+        float dr = wclamp(lmass / wmax(u.nominal_mass * 4.0f, 1e-6f), 0.0f, 1.0f);
+        jsup = wmin(jsup, dr);
+        f3 bal = mk(Vv.x, Vv.y + u.gravity * u.dt, Vv.z);
+        float pg = in_cup ? 0.72f : 0.98f;
+        float pc = in_cup ? 0.88f : 0.98f;
+        float pres = wclamp((1.0f - dr) * pg, 0.0f, pc);
+        nv = mix3(nv, bal, pres);
+        float ad = 1.0f - pres * 0.65f;
+        n0 *= ad;
+        n1 *= ad;
+        n2 *= ad;
+    }
+    if (po > 1e-4f) {
+        f3 rel = nv - pbv;
+        float rate = u.nu_m2s / pbk;
+        float dd = 1.0f / (1.0f + wmax(rate * u.dt * po, 0.0f));
+        float rs = len3(rel);
+        float idmp = 1.0f / (1.0f + wmax(rs * u.dt * u.inv_dx * po * 0.35f, 0.0f));
+        f3 before = nv;
+        nv = pbv + rel * dd * idmp;
+        f3 wi = mp * (nv - before);
+        int wx_, wy_, wz_;
+        world_to_cell(u, xp, wx_, wy_, wz_);
+        bed_impulse_neighborhood(c, wx_, wy_, wz_, (-wi) * BED_REACTION_ALPHA);
+        float ad = mixf(1.0f, dd * idmp, po);
+        n0 *= ad;
+        n1 *= ad;
+        n2 *= ad;
+        jsup = wmax(jsup, po);
+    }
+    float tr = n0.x + n1.y + n2.z;
+    float jo = clamp_j(P.w > 0.0f ? P.w : 1.0f);
+    float ja = clamp_j(jo * exp_small(wclamp(u.dt * tr, -0.35f, 0.35f)));
+    float jb = smoothstepf(0.35f, 0.85f, wclamp(jsup, 0.0f, 1.0f));
+    float jn = clamp_j(mixf(jo, ja, jb));
+    f3 np = xp + nv * u.dt;
+    f3 cpos = mix3(xp, np, 0.5f);
+    f3 cvel = nv;
+    sdf_contact(c, cpos, cvel, false);
+    cpos = np;
+    sdf_contact(c, cpos, cvel, false);
+    np = cpos;
+    nv = cvel;
+    float m = u.dx * 0.5f;
+    np.x = wclamp(np.x, u.ox + m, u.bx - m);
+    np.y = wclamp(np.y, u.oy + m, u.by - m);
+    np.z = wclamp(np.z, u.oz + m, u.bz - m);
+    c.pos[pid] = make_float4(np.x, np.y, np.z, jn);
+    c.vel[pid] = make_float4(nv.x, nv.y, nv.z, mp);
+    c.c0[pid] = make_float4(n0.x, n0.y, n0.z, phase);
+    c.c1[pid] = make_float4(n1.x, n1.y, n1.z, 0.0f);
+    c.c2[pid] = make_float4(n2.x, n2.y, n2.z, 0.0f);
+}
+
+__global__ void k_g2p(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    uint32_t n = c.u.num_water + c.u.num_bed;
+    CS_FOR(pid, n) g2p_particle(c, pid);
+}
+
+// ---------------- bed_coupling (shader.rs:1885-1957) ----------------
+__device__ float filter_paper_weight(const Params& u, f3 p) {
+    float ftop = filter_top_y(u), fbot = filter_bot_y(u);
+    float pr = wmax(water_particle_radius(u), u.dx * 0.35f);
+    if (p.y < fbot - pr || p.y > ftop + pr) return 0.0f;
+    float ft = wclamp((p.y - fbot) / (ftop - fbot), 0.0f, 1.0f);
+    float outer = mixf(0.0f, u.filter_top_radius, ft);
+    float inner = wmax(outer - u.filter_thickness, 0.0f);
+    float r = len2(p.x, p.z);
+    float side = 1.0f - smoothstepf(pr, pr * 3.0f, fabsf(r - inner));
+    float lv = 1.0f - smoothstepf(0.0f, pr * 5.0f, wmax(p.y - fbot, 0.0f));
+    float lr = 1.0f - smoothstepf(inner, inner + pr * 3.0f, r);
+    return wclamp(wmax(side, lv * lr), 0.0f, 1.0f);
+}
+
+__global__ void k_bed_coupling(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    uint32_t n = u.num_water + u.num_bed;
+    CS_FOR(pid, n) {
+        if (!is_water_phase(c.c0[pid].w)) continue;
+        float4 P = c.pos[pid];
+        f3 pos = xyz(P);
+        int cx, cy, cz;
+        world_to_cell(u, pos, cx, cy, cz);
+        if (!in_grid(u, cx, cy, cz)) continue;
+        float4 Vv = c.vel[pid];
+        float mp = Vv.w;
+        float pw = filter_paper_weight(u, pos);
+        if (pw > 1e-4f && u.filter_absorption > 0.0f) {
+            float frac = wclamp(u.filter_absorption * pw * u.dt, 0.0f, 0.04f);
+            float ab = wmin(mp * frac, mp * 0.12f);
+            mp = wmax(mp - ab, inactive_mass(u) * 1.25f);
+            Vv.w = mp;
+            c.vel[pid] = Vv;
+        }
+        int32_t b = c.lookup[cidx(u, cx, cy, cz)];
+        if (b < 0 || (uint32_t)b >= u.num_bed) continue;
+        float4 BA = c.bedA[b];
+        float sat = c.bedB[b].w;
+        float cap = wmax(u.max_saturation - BA.x, 0.0f);
+        if (cap <= 1e-6f) continue;
+        float ar = u.absorption_rate * (1.0f - sat) * u.dt;
+        float speed = len3(xyz(Vv));
+        float absorbed = wmin(wmin(mp * wclamp(ar, 0.0f, 0.25f), mp * 0.5f), cap);
+        float rem_partial = mp - absorbed;
+        if (rem_partial > 0.0f && rem_partial <= u.nominal_mass * 0.22f) {
+            absorbed = wmin(mp, cap);
+        } else if (sat > 0.55f && speed < 1.35f) {
+            float almost = wmin(mp, cap);
+            if (mp - almost <= u.nominal_mass * 0.35f) absorbed = almost;
+        }
+        if (mp - absorbed <= inactive_mass(u) && absorbed < mp) absorbed = wmax(mp - inactive_mass(u) * 1.05f, 0.0f);
+        if (absorbed <= 1e-6f) continue;
+        float remaining = mp - absorbed;
+        if (remaining <= inactive_mass(u)) c.vel[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        else c.vel[pid] = make_float4(Vv.x, Vv.y, Vv.z, remaining);
+        // deposit_absorbed_bed_water (shader.rs:524-576)
+        float ns = absorbed * 0.35f;
+        float hs = absorbed - ns;
+        bed_water_add(c, (uint32_t)b, hs);
+        int32_t ids[6];
+        uint32_t cnt = 0;
+        const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            int x = cx + off[q][0], y = cy + off[q][1], z = cz + off[q][2];
+            if (!in_grid(u, x, y, z)) continue;
+            int32_t nid = c.lookup[cidx(u, x, y, z)];
+            if (nid < 0 || nid == b || (uint32_t)nid >= u.num_bed) continue;
+            bool dup = false;
+            for (uint32_t k = 0; k < cnt; ++k) dup |= ids[k] == nid;
+            if (!dup) ids[cnt++] = nid;
+        }
+        if (cnt == 0) {
+            bed_water_add(c, (uint32_t)b, ns);
+        } else {
+            float each = ns / (float)cnt;
+            for (uint32_t k = 0; k < cnt; ++k) bed_water_add(c, (uint32_t)ids[k], each);
+        }
+    }
+}
+
+// ---------------- extraction_advect (shader.rs:1961-1987) + Jacobi snapshot ----------------
+__global__ void k_extraction_advect(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(b, u.num_bed) {
+        float4 A = c.bedA[b], Bb = c.bedB[b];
+        int32_t raw = atomicExch(&delta_lane(c, 0)[b], 0);
+        float absorbed = (float)raw * INV_FP_SCALE;
+        if (absorbed > 0.0f) {
+            A.x += absorbed;
+            Bb.w = wclamp(A.x / wmax(u.max_saturation, 1e-6f), 0.0f, 1.0f);
+        }
+        if (Bb.w > 0.01f) {
+            float flux = u.extraction_rate * Bb.x * Bb.w * u.dt;
+            Bb.x = wmax(Bb.x - flux, 0.0f);
+            Bb.y += flux;
+        }
+        c.bedA[b] = A;
+        c.bedB[b] = Bb;
+        c.snap[b] = c.pos[b];
+    }
+}
+
+// ---------------- bed_dynamics (shader.rs:1991-2238) ----------------
+__device__ __forceinline__ float pressure_or_mirror_aliased(const Ctx& c, int x, int y, int z, float mirror) {
+    // shader.rs:224-236: the "kind" read here is lane 3, which viscosity_prepare has
+    // overwritten with FP velocity z by the time bed_dynamics runs; kept as is.
+    if (!in_grid(c.u, x, y, z)) return mirror;
+    uint32_t ci = cidx(c.u, x, y, z);
+    if (is_solid(lane(c, 3)[ci])) return mirror;
+    return pressure_load(c, ci);
+}
+
+__global__ void k_bed_dynamics(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(bid, u.num_bed) {
+        float4 P = c.pos[bid], Vv = c.vel[bid], A0 = c.c0[bid], A1 = c.c1[bid];
+        float4 BA = c.bedA[bid], BB = c.bedB[bid];
+        float phase = A0.w;
+        f3 rest = xyz(A1);
+        f3 pos = xyz(P);
+        float mp = Vv.w;
+        int32_t ex = atomicExch(&delta_lane(c, 1)[bid], 0);
+        int32_t ey = atomicExch(&delta_lane(c, 2)[bid], 0);
+        int32_t ez = atomicExch(&delta_lane(c, 3)[bid], 0);
+        f3 brv = mk((float)ex, (float)ey, (float)ez) * INV_FP_SCALE;
+        brv = brv / wmax(mp, u.nominal_mass * 0.25f);
+        float mrs = wmin(u.vel_cap * 0.012f, u.dx / wmax(u.dt, 1e-6f) * 0.02f);
+        float rsp = len3(brv);
+        if (rsp > mrs && rsp > 1e-6f) brv *= mrs / rsp;
+        float gx = (pos.x - u.ox) * u.inv_dx, gy = (pos.y - u.oy) * u.inv_dx, gz = (pos.z - u.oz) * u.inv_dx;
+        int bx = (int)floorf(gx - 0.5f), by = (int)floorf(gy - 0.5f), bz = (int)floorf(gz - 0.5f);
+        float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+        float wx[3], wy[3], wz[3];
+        bspline(fx, wx);
+        bspline(fy, wy);
+        bspline(fz, wz);
+        f3 wv = mk(0.0f, 0.0f, 0.0f);
+        float wm = 0.0f, asw = 0.0f, lasw = 0.0f;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) {
+                    int cx = bx + i, cy = by + j, cz = bz + k;
+                    if (!in_grid(u, cx, cy, cz)) continue;
+                    float w = wx[i] * wy[j] * wz[k];
+                    uint32_t ci = cidx(u, cx, cy, cz);
+                    float4 g = c.gvel[ci];
+                    wv += w * xyz(g);
+                    wm += w * g.w;
+                    int32_t sb = c.lookup[ci];
+                    if (sb >= 0 && (uint32_t)sb != bid) {
+                        asw += w;
+                        float ccy = u.oy + ((float)cy + 0.5f) * u.dx;
+                        if (ccy <= pos.y + u.dx * 0.25f) lasw += w;
+                    }
+                }
+        const float floor_y = coffee_floor_y(u);
+        if (is_suspended(phase)) {
+            float ws = wclamp(wm / wmax(u.nominal_mass * 2.0f, 1e-6f), 0.0f, 1.0f);
+            float drag = wclamp((8.0f + 18.0f * ws) * u.dt, 0.0f, 1.0f);
+            f3 unsup = xyz(Vv) + brv + mk(0.0f, u.gravity * u.dt * 0.85f, 0.0f);
+            float settle = mixf(1.10f, 0.32f, ws);
+            f3 carried = wv + mk(0.0f, -settle, 0.0f);
+            f3 sv = mix3(unsup, carried, drag);
+            float sp = len3(sv);
+            if (sp > u.vel_cap) sv = sv * (u.vel_cap / sp);
+            f3 sp_pos = pos + sv * u.dt;
+            sdf_contact(c, sp_pos, sv, true);
+            c.pos[bid] = make_float4(sp_pos.x, sp_pos.y, sp_pos.z, P.w);
+            c.vel[bid] = make_float4(sv.x, sv.y, sv.z, mp);
+            bool anch = lasw > 0.06f || asw > 0.20f;
+            bool dense = asw > 0.42f;
+            bool redep = (sp_pos.y <= floor_y + u.dx * 0.35f && ws < 0.35f) ||
+                         (anch && sv.y <= 0.20f && (ws < 0.55f || dense));
+            if (redep) phase = 1.0f;
+            c.c0[bid] = make_float4(A0.x, A0.y, A0.z, phase);
+            c.c1[bid] = make_float4(sp_pos.x, sp_pos.y, sp_pos.z, 0.0f);
+            BA.w *= 0.985f;
+            c.bedA[bid] = BA;
+            continue;
+        }
+        float sat = BB.w;
+        float wl = wclamp(wm / wmax(u.nominal_mass * 1.5f, 1e-6f), 0.0f, 1.0f);
+        float mob = wclamp((0.30f + wl * 0.62f) * (1.0f + sat * 0.40f), 0.0f, 1.0f);
+        float sfac = wclamp((rest.y + u.bed_surface_ref_y) / u.bed_surface_span, 0.12f, 1.0f);
+        float damping = wclamp(1.0f - u.bed_damping * u.dt, 0.0f, 1.0f);
+        f3 vel = xyz(Vv) + brv;
+        float srel = wclamp(1.0f - asw / 0.55f, 0.0f, 1.0f);
+        float ed = wclamp((2.0f + 5.0f * sat) * wl * srel * u.dt, 0.0f, 0.08f);
+        f3 gsv = mk(0.0f, -mixf(0.95f, 0.35f, wl), 0.0f);
+        vel = mix3(vel, wv + gsv, ed);
+        float ls = len2(wv.x, wv.z);
+        float ldx = 0.0f, ldz = 0.0f;
+        if (ls > 1e-6f) {
+            ldx = wv.x / ls;
+            ldz = wv.z / ls;
+        }
+        float lss = wmin(ls, fabsf(wmin(wv.y, 0.0f)) * 0.18f);
+        f3 iv = mk(ldx * lss * 0.08f, wmin(wv.y, 0.0f) * 0.62f, ldz * lss * 0.08f);
+        vel += iv * u.bed_impact * mob * sfac * u.dt;
+        int pcx, pcy, pcz;
+        world_to_cell(u, pos, pcx, pcy, pcz);
+        float pgx = 0.0f, pgz = 0.0f;
+        if (in_grid(u, pcx, pcy, pcz)) {
+            float ph = pressure_load(c, cidx(u, pcx, pcy, pcz));
+            float pxm = pressure_or_mirror_aliased(c, pcx - 1, pcy, pcz, ph);
+            float pxp = pressure_or_mirror_aliased(c, pcx + 1, pcy, pcz, ph);
+            float pzm = pressure_or_mirror_aliased(c, pcx, pcy, pcz - 1, ph);
+            float pzp = pressure_or_mirror_aliased(c, pcx, pcy, pcz + 1, ph);
+            float h = 0.5f * u.inv_dx;
+            pgx = h * (pxp - pxm);
+            pgz = h * (pzp - pzm);
+        }
+        float sfx = -pgx, sfz = -pgz;
+        float ssp = len2(sfx, sfz);
+        float sdx = 0.0f, sdz = 0.0f;
+        if (ssp > 1e-6f) {
+            sdx = sfx / ssp;
+            sdz = sfz / ssp;
+        }
+        float pdrive = wmin(ssp, u.vel_cap / wmax(u.dt, 1e-6f));
+        float pload = wclamp(wm * (0.25f + sat), 0.0f, 1.0f);
+        float slx = sdx * pdrive * pload * 0.08f, slz = sdz * pdrive * pload * 0.08f;
+        vel.x += slx * u.bed_impact * mob * sfac * u.dt;
+        vel.z += slz * u.bed_impact * mob * sfac * u.dt;
+        vel *= damping;
+        f3 npos = pos + vel * u.dt;
+        f3 off = npos - rest;
+        float ll = len2(off.x, off.z);
+        float lpt = u.dx * 0.22f;
+        if (ll > lpt && ll > 1e-6f) {
+            float lx = off.x / ll, lz = off.z / ll;
+            float lex = ll - lpt;
+            float lpl = wclamp((0.04f + sat * 0.35f + mob * 0.45f + pload * 0.25f) * sfac * u.compaction_rate * u.dt,
+                               0.0f, 0.18f);
+            rest.x += lx * lex * lpl;
+            rest.z += lz * lex * lpl;
+            off = npos - rest;
+        }
+        float cll = len2(off.x, off.z);
+        float mlat = u.dx * 0.9f * sfac;
+        if (cll > mlat && cll > 1e-6f) {
+            float lx = off.x / cll, lz = off.z / cll;
+            off.x = lx * mlat;
+            off.z = lz * mlat;
+            vel.x *= 0.4f;
+            vel.z *= 0.4f;
+        }
+        off.y = wclamp(off.y, -u.dx * (1.75f * sfac + 0.2f), u.dx * 0.04f);
+        npos = rest + off;
+        // resolve_coffee_particle_packing (shader.rs:825-877) against the snapshot
+        {
+            f3 cd = mk(0.0f, 0.0f, 0.0f);
+            float cdist = 1e9f;
+            bool found = false;
+            int qx, qy, qz;
+            world_to_cell(u, npos, qx, qy, qz);
+            for (int di = -1; di <= 1; ++di)
+                for (int dj = -1; dj <= 1; ++dj)
+                    for (int dk = -1; dk <= 1; ++dk) {
+                        int x = qx + di, y = qy + dj, z = qz + dk;
+                        if (!in_grid(u, x, y, z)) continue;
+                        int32_t o = c.lookup[cidx(u, x, y, z)];
+                        if (o < 0 || (uint32_t)o == bid || (uint32_t)o >= u.num_bed) continue;
+                        f3 d = npos - xyz(c.snap[o]);
+                        float dist = len3(d);
+                        if (dist < cdist) {
+                            cdist = dist;
+                            cd = d;
+                            found = true;
+                        }
+                    }
+            float min_sep = bed_particle_radius(u) * 1.78f;
+            if (found && cdist < min_sep) {
+                f3 n = mk(0.0f, 1.0f, 0.0f);
+                if (cdist > 1e-5f) n = cd / cdist;
+                npos += n * wmin((min_sep - cdist) * 0.65f, u.dx * 0.22f);
+                float vn = dot3(vel, n);
+                if (vn < 0.0f) vel -= n * vn;
+            }
+        }
+        float comp = wmax(rest.y - npos.y, 0.0f);
+        float pth = u.dx * 0.18f;
+        if (comp > pth) {
+            float pl = wclamp((0.05f + sat * 0.35f + mob * 0.55f) * sfac * u.compaction_rate * u.dt, 0.0f, 0.18f);
+            rest.y -= (comp - pth) * pl;
+        }
+        bool hd = sat > 0.82f && pload > 0.65f && wl > 0.65f && srel > 0.35f &&
+                  (comp > u.dx * 0.65f || cll > u.dx * 0.65f);
+        bool fe = sat > 0.58f && wl > 0.74f && srel > 0.55f && len3(wv) > 0.95f && npos.y > floor_y + u.dx * 0.70f;
+        bool iso = sat > 0.55f && wm < u.nominal_mass * 0.75f && asw < 0.04f && lasw < 0.03f &&
+                   npos.y > floor_y + u.dx * 0.50f;
+        if (hd || fe || iso) {
+            phase = 2.0f;
+            rest = npos;
+        }
+        sdf_contact(c, npos, vel, true);
+        c.pos[bid] = make_float4(npos.x, npos.y, npos.z, P.w);
+        c.vel[bid] = make_float4(vel.x, vel.y, vel.z, mp);
+        c.c0[bid] = make_float4(A0.x, A0.y, A0.z, phase);
+        c.c1[bid] = make_float4(rest.x, rest.y, rest.z, 0.0f);
+        float gc = wmax((rest.y - npos.y) / wmax(u.dx, 1e-6f), 0.0f);
+        BA.w = wmax(BA.w * 0.995f, gc);
+        c.bedA[bid] = BA;
+    }
+}
+
+// ---------------- prepare_render (shader.rs:2242-2276) ----------------
+__global__ void k_prepare_render(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    uint32_t n = u.num_water + u.num_bed;
+    CS_FOR(pid, n) {
+        float4 P = c.pos[pid], Vv = c.vel[pid];
+        float phase = c.c0[pid].w;
+        if (Vv.w <= inactive_mass(u)) {
+            c.render[2 * (size_t)pid] = make_float4(0.0f, -1e6f, 0.0f, -999.0f);
+            c.render[2 * (size_t)pid + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        float ct;
+        float rad = water_particle_radius(u);
+        if (is_water_phase(phase)) {
+            ct = wclamp(len3(xyz(Vv)) / 10.0f, 0.0f, 2.0f);
+        } else {
+            float sat = 0.0f;
+            if (pid < u.num_bed) {
+                sat = c.bedB[pid].w;
+                rad = bed_particle_radius(u);
+            }
+            ct = -1.0f - sat;
+        }
+        c.render[2 * (size_t)pid] = make_float4(P.x, P.y, P.z, ct);
+        c.render[2 * (size_t)pid + 1] = make_float4(rad, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// ---------------- readback helpers ----------------
+// Reference AoS layouts from the SoA streams.
+__global__ void k_pack_particles(const Ctx* __restrict__ cp, uint32_t first, uint32_t count, float* out, int what) {
+    const Ctx& c = cp[blockIdx.y];
+    CS_FOR(k, count) {
+        uint32_t p = first + k;
+        if (what == 0) {
+            float4 a = c.pos[p], b = c.vel[p];
+            float* o = out + (size_t)k * 8;
+            o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+            o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+        } else if (what == 1) {
+            float4 a = c.c0[p], b = c.c1[p], d = c.c2[p];
+            float* o = out + (size_t)k * 12;
+            o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+            o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+            o[8] = d.x; o[9] = d.y; o[10] = d.z; o[11] = d.w;
+        } else if (what == 2) {
+            float4 a = c.bedA[p], b = c.bedB[p];
+            float* o = out + (size_t)k * 8;
+            o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+            o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+        } else {
+            float4 a = c.render[2 * (size_t)p], b = c.render[2 * (size_t)p + 1];
+            float* o = out + (size_t)k * 8;
+            o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+            o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+        }
+    }
+}
+__global__ void k_unpack_particles(const Ctx* __restrict__ cp, uint32_t first, uint32_t count, const float* in, int what) {
+    const Ctx& c = cp[blockIdx.y];
+    CS_FOR(k, count) {
+        uint32_t p = first + k;
+        if (what == 0) {
+            const float* s = in + (size_t)k * 8;
+            c.pos[p] = make_float4(s[0], s[1], s[2], s[3]);
+            c.vel[p] = make_float4(s[4], s[5], s[6], s[7]);
+        } else if (what == 1) {
+            const float* s = in + (size_t)k * 12;
+            c.c0[p] = make_float4(s[0], s[1], s[2], s[3]);
+            c.c1[p] = make_float4(s[4], s[5], s[6], s[7]);
+            c.c2[p] = make_float4(s[8], s[9], s[10], s[11]);
+        } else {
+            const float* s = in + (size_t)k * 8;
+            c.bedA[p] = make_float4(s[0], s[1], s[2], s[3]);
+            c.bedB[p] = make_float4(s[4], s[5], s[6], s[7]);
+        }
+    }
+}
+// Pressure as float; lanes with lane 0 re-encoded in FP32 mode.
+__global__ void k_pressure_out(const Ctx* __restrict__ cp, float* out) {
+    const Ctx& c = cp[blockIdx.y];
+    CS_FOR(i, c.u.cells) out[i] = pressure_load(c, i);
+}
+__global__ void k_lane0_encode(const Ctx* __restrict__ cp, int32_t* out) {
+    const Ctx& c = cp[blockIdx.y];
+    CS_FOR(i, c.u.cells) out[i] = c.u.fixed_point ? c.lanes[i] : to_i32(c.pf[i] * FP_SCALE);
+}
+
+}  // namespace cs

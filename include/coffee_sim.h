@@ -1,0 +1,349 @@
+/*
+ * coffee_sim.h — C ABI of the B200 MLS-MPM pour-over engine.
+ *
+ * The reference (craigxchen/coffee-sim) has no FFI layer: the step sits behind
+ * `pub(crate) struct MpmSim3D` (crates/sim-wasm/src/mpm_3d/mod.rs:179-671) and is
+ * driven through wasm-bindgen by `WasmSim3D` (crates/sim-wasm/src/lib.rs:19-261).
+ * Every entry point below replaces one of those methods; each declaration cites the
+ * reference item it stands in for.  A Rust host binds these with `extern "C"`
+ * (see the rust/ crate), Python binds them with ctypes (coffee_sim_b200/__init__.py).
+ *
+ * Conventions
+ *  - Every call returns int32 status (CS_OK == 0).  cs_last_error_string() gives the
+ *    text of the last failure on the calling thread.  No call aborts the process.
+ *  - Plain C types only: pointers, sizes, fixed-width ints, float.
+ *  - The handle owns all device memory and one CUDA stream.  The caller owns host
+ *    buffers; readback and upload calls are synchronous and keep no pointer.
+ *  - One host thread per handle (the reference takes &mut self); separate handles may
+ *    live on separate threads or devices.
+ *  - Host-side array layouts are the reference's byte layouts (state.rs:90-153):
+ *      particle      8 x f32  pos.xyz, J, vel.xyz, mass          (shader.rs:24-27)
+ *      affine       12 x f32  col0.xyz, phase, col1.xyzw, col2.xyzw (shader.rs:29-33)
+ *      bed_extract   8 x f32  pore_water, porosity, permeability, compaction,
+ *                             extractable, dissolved, temperature, saturation
+ *                                                                 (shader.rs:35-38)
+ *      grid lanes    6 x cells i32, lane-major: mass, mom x/y/z, rest vol, cur vol
+ *                                                                 (shader.rs:152-164)
+ *      grid_vel      4 x f32 per cell: v.xyz, mass                (shader.rs:56)
+ *      render        8 x f32 per particle: pos.xyz, colour_t, radius, 0, 0, 0
+ *                                                                 (shader.rs:40-43)
+ */
+#ifndef COFFEE_SIM_H
+#define COFFEE_SIM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS_ABI_VERSION 3u
+
+typedef enum CsStatus {
+    CS_OK = 0,
+    CS_ERR_INVALID_ARG = 1,
+    CS_ERR_CAPACITY = 2,
+    CS_ERR_CUDA = 3,
+    CS_ERR_NAN = 4,
+    CS_ERR_OVERFLOW = 5,
+    CS_ERR_TIMEOUT = 6,
+    CS_ERR_UNSUPPORTED = 7,
+    CS_ERR_NO_DEVICE = 8
+} CsStatus;
+
+/* Obstacle kinds of the analytic SDF (mod.rs:71-85). */
+enum { CS_OBSTACLE_TRUNCATED_CONE = 0, CS_OBSTACLE_CYLINDER = 1 };
+#define CS_MAX_OBSTACLES 4
+
+typedef struct CsObstacle {
+    int32_t kind;
+    float center[3];
+    float top_radius; /* cone */
+    float bot_radius; /* cone */
+    float radius;     /* cylinder */
+    float top_y;
+    float bot_y;
+} CsObstacle;
+
+/* SpoutSettings (inflow.rs:8-25). */
+typedef struct CsSpout {
+    float origin[3];
+    float direction[3];
+    float target[3];
+    float nozzle_radius;
+    float stem_radius;
+    float activation_angle_deg;
+    float full_flow_angle_deg;
+    float head_at_activation;
+    float head_at_full_angle;
+    float discharge_coeff;
+    float volume_to_ml;
+    float max_flow_rate_ml_s;
+    float gentle_exit_speed;
+    float max_exit_speed;
+    float stem_length;
+} CsSpout;
+
+/* FilterConfig (filter.rs:3-26). */
+typedef struct CsFilter {
+    float center[3];
+    float top_y;
+    float bot_y;
+    float top_radius;
+    float bot_radius;
+    float thickness;
+    float hole_radius;
+} CsFilter;
+
+/* BedConfig (bed.rs:7-38) plus an optional log-normal permeability field. */
+typedef struct CsBed {
+    float center[3];
+    float top_y;
+    float bot_y;
+    float top_radius;
+    float bot_radius;
+    uint32_t num_particles;
+    float initial_porosity;
+    float initial_permeability;
+    float extractable_mass;
+    /* Extension: per-sample permeability = exp(ln(initial_permeability) + sigma*N(0,1))
+     * when log_perm_sigma > 0 (SplitMix64 + Box-Muller, seeded by perm_seed).
+     * Two-layer beds: samples with y below layer_split_y use porosity/permeability
+     * multiplied by lower_porosity_scale / lower_permeability_scale. */
+    float log_perm_sigma;
+    uint32_t perm_seed;
+    float layer_split_y;
+    float lower_porosity_scale;
+    float lower_permeability_scale;
+} CsBed;
+
+/* Run-time members of DEFAULT_BREW (brew_config.rs:38-71). */
+typedef struct CsBrew {
+    float water_particles_per_ml;
+    float water_mass_units_per_ml;
+    float water_sample_radius_dx;
+    float bed_sample_radius_dx;
+    float water_kinematic_viscosity_m2_s;
+    float min_bed_permeability_m2;
+    float bed_absorption_rate;
+    float target_bed_retention_ml;
+    float bed_pore_capacity_scale;
+    float bed_pore_overfill_alpha;
+    float bed_surface_void_scale;
+    float dripper_outlet_radius;
+    float filter_absorption_rate_s;
+    float bed_compaction_rate;
+    float bed_impact_rate;
+} CsBrew;
+
+/* Constants the reference hard-codes inside the WGSL (shader.rs:101-146, 744-823,
+ * 1778-1779, 2109).  The default-V60 presets reproduce them exactly; other scenes
+ * (SI-unit cones) set their own.  flags: bit0 cone radial barrier, bit1 paper-filter
+ * barrier for coffee, bit2 carafe barrier + floor. */
+enum { CS_GEOM_CONE = 1u, CS_GEOM_FILTER = 2u, CS_GEOM_CUP = 4u };
+typedef struct CsGeometry {
+    uint32_t flags;
+    float cone_bot_y;          /* -3.0 */
+    float cone_top_y;          /*  3.0 */
+    float cone_radius_span;    /*  4.2634315: top radius - outlet radius */
+    float filter_center_y;     /* -0.35 */
+    float filter_top_rel;      /*  2.75 */
+    float filter_bot_rel;      /*  3.02 (subtracted) */
+    float filter_top_radius;   /*  4.10 */
+    float filter_thickness;    /*  0.08 */
+    float cup_top_y;           /* -3.5 */
+    float cup_radius;          /*  3.0 */
+    float cup_floor_y;         /* -8.0 */
+    float wall_thickness;      /*  0.4 */
+    float bed_surface_ref_y;   /*  3.0 (surface_factor offset) */
+    float bed_surface_span;    /*  3.5 */
+    float sdf_friction;        /*  0.3 */
+    float sdf_restitution;     /*  0.0 */
+    float contact_offset;      /*  0.05 */
+} CsGeometry;
+
+/* Pressure storage / solve modes. */
+enum {
+    CS_PRESSURE_FIXED_POINT = 0, /* i32 * 2^18, as the reference (shader.rs:198-209) */
+    CS_PRESSURE_FP32 = 1
+};
+enum {
+    CS_SOLVE_FIXED_PAIRS = 0,    /* pressure_rbgs_pairs red+black pairs (mod.rs:352-357) */
+    CS_SOLVE_RESIDUAL = 1        /* sweep until relative residual <= residual_tol */
+};
+enum {
+    CS_P2G_ATOMIC32 = 0,         /* one global i32 atomic per node and lane (shader.rs:1043-1048) */
+    CS_P2G_SORTED_SHARED = 1,    /* cell-sorted particles, shared-memory tile accumulation */
+    CS_P2G_INT64 = 2             /* sorted + i64 fixed point (scale 2^32) */
+};
+enum {
+    CS_WARM_NONE = 0,            /* cold start, p = 0 (shader.rs:1187) */
+    CS_WARM_PREVIOUS = 1,        /* previous substep's pressure */
+    CS_WARM_LEARNED = 2          /* 3D U-Net guess, kept only if its residual is lower */
+};
+
+/* MpmSettings (mod.rs:87-104) + engine extensions. */
+typedef struct CsSettings {
+    uint32_t abi_version;         /* must be CS_ABI_VERSION */
+    float bounds_size[3];
+    uint32_t grid_dims[3];
+    uint32_t max_particles;
+    uint32_t substeps;
+    float gravity;
+    float bulk_modulus;
+    float viscosity;
+    float render_radius;
+    uint32_t pressure_rbgs_pairs;
+    uint32_t use_sdf_cache;
+    uint32_t num_obstacles;
+    CsObstacle obstacles[CS_MAX_OBSTACLES];
+    CsSpout spout;
+    float initial_kettle_angle_deg;
+    uint32_t has_filter;
+    CsFilter filter;
+    uint32_t has_bed;
+    CsBed bed;
+    CsBrew brew;
+    CsGeometry geom;
+    /* Unit map (units.rs:9-37). */
+    float sim_units_per_meter;    /* 57.7 for the V60 scene; 1.0 for SI scenes */
+    float standard_gravity_m_s2;  /* 9.80665 */
+    float max_velocity;           /* velocity cap, MAX_WATER_SPEED_SIM_UNITS */
+    float particle_volume_cells;  /* particle rest volume / dx^3; 0.25 (mod.rs:576) */
+    float max_frame_dt;           /* 1/30 (mod.rs:265) */
+    /* Engine extensions. */
+    uint32_t pressure_storage;    /* CS_PRESSURE_* */
+    uint32_t solve_mode;          /* CS_SOLVE_* */
+    float residual_tol;           /* relative residual target (FP64 norm) */
+    uint32_t max_sweeps;          /* cap on red+black pairs in residual mode */
+    uint32_t check_every;         /* pairs between residual evaluations */
+    uint32_t warm_start;          /* CS_WARM_* */
+    uint32_t p2g_mode;            /* CS_P2G_* */
+    uint32_t sort_every;          /* substeps between cell-key sorts (sorted modes) */
+    uint32_t device_emission;     /* 1: emit jet particles with a kernel (graph-capturable) */
+    uint32_t use_graph;           /* 1: capture the substep in a CUDA graph */
+    int32_t device;               /* CUDA device ordinal */
+    uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 persistent tiled */
+    float flow_override_ml_s;     /* >0: constant flow instead of the kettle-angle model */
+    float exit_speed_override;    /* >0 with flow override: jet speed */
+} CsSettings;
+
+/* Observability counters (mod.rs:50-68 / state.rs:22-28) + solver telemetry. */
+typedef struct CsMetrics {
+    float max_abs_div;
+    uint32_t fluid_cells;
+    uint32_t div_clamp_fires;
+    uint32_t pressure_clamp_fires;
+    uint32_t mass_overflow_fires;
+    uint32_t last_sweeps;          /* red+black pairs in the last substep's solve */
+    double last_residual;          /* relative residual after the solve (FP64), -1 if unmeasured */
+    double initial_residual;       /* relative residual of the warm start (FP64), -1 if unmeasured */
+    uint32_t nan_flag;             /* a non-finite particle or grid value was seen */
+    uint32_t timeout_flag;         /* a bounded device wait gave up */
+    uint32_t learned_used;         /* 1 if the learned guess was kept in the last solve */
+    uint32_t reserved;
+    double solve_ms;               /* device time of the last pressure solve, if timed */
+} CsMetrics;
+
+typedef struct CsSim CsSim;
+typedef struct CsEnsemble CsEnsemble;
+
+/* ---- library ---- */
+const char* cs_last_error_string(void);
+uint32_t cs_abi_version(void);
+/* 1 when the library runs the step on a GPU; 0 for the CPU oracle. */
+int32_t cs_is_gpu_engine(void);
+
+/* ---- settings presets (mod.rs:106-161) ---- */
+int32_t cs_settings_default_v60(CsSettings* out);           /* MpmSettings::default_v60 */
+int32_t cs_settings_benchmark_free_stream(CsSettings* out); /* MpmSettings::benchmark_free_stream */
+int32_t cs_settings_benchmark_center_pour(CsSettings* out); /* MpmSettings::benchmark_center_pour */
+/* SpoutSettings::aim_at / translate_origin_to on a settings value (inflow.rs:49-67). */
+int32_t cs_settings_aim_spout(CsSettings* s, float x, float y, float z);
+
+/* ---- lifetime (mod.rs:196-262, 432-446) ---- */
+int32_t cs_create(const CsSettings* settings, CsSim** out);   /* MpmSim3D::new */
+int32_t cs_destroy(CsSim* sim);
+int32_t cs_reset(CsSim* sim);                                  /* MpmSim3D::reset */
+
+/* ---- stepping (mod.rs:264-430) ---- */
+int32_t cs_step_frame(CsSim* sim, float dt);                   /* MpmSim3D::step_frame */
+/* One substep of length sub_dt: emission, uniforms, every kernel (mod.rs:271-419). */
+int32_t cs_step_substep(CsSim* sim, float sub_dt);
+/* Run the first `passes` kernels of one substep (debugging / parity localisation).
+ * Pass numbering follows the dispatch order of mod.rs:317-414. */
+int32_t cs_step_substep_partial(CsSim* sim, float sub_dt, uint32_t passes);
+
+/* ---- controls (mod.rs:448-458, lib.rs:72-86) ---- */
+int32_t cs_set_kettle_angle(CsSim* sim, float angle_deg);
+int32_t cs_set_spout_position(CsSim* sim, float x, float y, float z);
+int32_t cs_set_spout_target(CsSim* sim, float x, float y, float z);
+/* Constant jet (ml/s, scene units/s) instead of the kettle-angle model; flow <= 0 clears it. */
+int32_t cs_set_flow_override(CsSim* sim, float flow_ml_s, float exit_speed);
+
+/* ---- getters (mod.rs:460-544, lib.rs:87-252) ---- */
+int32_t cs_get_counts(const CsSim* sim, uint32_t* num_water, uint32_t* num_bed, uint32_t* max_particles);
+int32_t cs_get_kettle_angle(const CsSim* sim, float* out);
+int32_t cs_get_spout_position(const CsSim* sim, float out[3]);
+int32_t cs_get_flow(const CsSim* sim, float* flow_rate_ml_s, float* exit_speed, float* exit_speed_m_s);
+int32_t cs_get_time(const CsSim* sim, float* total_time);
+int32_t cs_get_emission(const CsSim* sim, float* frame_emitted_mass, float* total_emitted_mass,
+                        uint32_t* frame_dropped, uint32_t* total_dropped);
+int32_t cs_get_mass_units_per_ml(const CsSim* sim, float* out);
+/* refresh_metrics + metric getters (mod.rs:546-567, lib.rs:219-252); synchronises. */
+int32_t cs_get_metrics(CsSim* sim, CsMetrics* out);
+int32_t cs_get_settings(const CsSim* sim, CsSettings* out);
+
+/* ---- readback into caller buffers (physics_tests.rs:61-1083 read the same layouts) ---- */
+int32_t cs_read_particles(CsSim* sim, uint32_t first, uint32_t count, float* out);     /* 8 f32 each */
+int32_t cs_read_affine(CsSim* sim, uint32_t first, uint32_t count, float* out);        /* 12 f32 each */
+int32_t cs_read_bed_extract(CsSim* sim, uint32_t first, uint32_t count, float* out);   /* 8 f32 each */
+int32_t cs_read_grid_lanes(CsSim* sim, int32_t* out);       /* 6 x cells, reference lane aliasing */
+int32_t cs_read_grid_vel(CsSim* sim, float* out);           /* 4 x cells */
+int32_t cs_read_pressure(CsSim* sim, float* out);           /* cells, decoded to f32 */
+int32_t cs_read_cell_kind(CsSim* sim, int32_t* out);        /* cells, kind after classify */
+int32_t cs_read_bed_lookup(CsSim* sim, int32_t* out);       /* cells */
+int32_t cs_read_bed_delta(CsSim* sim, int32_t* out);        /* 4 x max_particles, lane-major */
+int32_t cs_read_render(CsSim* sim, uint32_t first, uint32_t count, float* out);        /* 8 f32 each */
+int32_t cs_read_sdf(CsSim* sim, float* out);                /* 128^3 R32F texels */
+int32_t cs_read_sdf_class(CsSim* sim, uint8_t* out);        /* cells */
+
+/* ---- upload from caller buffers ---- */
+int32_t cs_write_particles(CsSim* sim, uint32_t first, uint32_t count, const float* in);
+int32_t cs_write_affine(CsSim* sim, uint32_t first, uint32_t count, const float* in);
+int32_t cs_write_bed_extract(CsSim* sim, uint32_t first, uint32_t count, const float* in);
+/* Declare how many slots are live: bed first, then water (mod.rs:241-242). */
+int32_t cs_set_counts(CsSim* sim, uint32_t num_water, uint32_t num_bed);
+/* Append a block of water: per_axis^3 samples per cell inside [lo, hi], each jittered
+ * uniformly by +/- jitter*dx per axis (SplitMix64, seed), nominal mass, J = 1.
+ * When require_open_sdf != 0 a sample is kept only where the scene SDF exceeds the
+ * contact offset.  Returns the number appended in *added. */
+int32_t cs_add_water_block(CsSim* sim, const float lo[3], const float hi[3], uint32_t per_axis,
+                           float jitter, uint32_t seed, uint32_t require_open_sdf, uint32_t* added);
+
+/* ---- checkpoint / resume (no counterpart: the reference only has reset, mod.rs:432) ---- */
+int32_t cs_snapshot_size(CsSim* sim, uint64_t* bytes);
+int32_t cs_snapshot_save(CsSim* sim, void* buffer, uint64_t bytes);
+int32_t cs_snapshot_load(CsSim* sim, const void* buffer, uint64_t bytes);
+
+/* ---- batched ensemble of independent pours (no counterpart in the reference) ----
+ * n instances with their own settings (same grid dims) stepped together: one launch
+ * per pass covers every instance through per-instance offset tables. */
+int32_t cs_ensemble_create(const CsSettings* settings, uint32_t n, CsEnsemble** out);
+int32_t cs_ensemble_destroy(CsEnsemble* ens);
+int32_t cs_ensemble_step_substep(CsEnsemble* ens, float sub_dt);
+int32_t cs_ensemble_step_frame(CsEnsemble* ens, float dt);
+int32_t cs_ensemble_add_water_block(CsEnsemble* ens, uint32_t i, const float lo[3], const float hi[3],
+                                    uint32_t per_axis, float jitter, uint32_t seed,
+                                    uint32_t require_open_sdf, uint32_t* added);
+int32_t cs_ensemble_set_kettle_angle(CsEnsemble* ens, uint32_t i, float angle_deg);
+int32_t cs_ensemble_set_flow_override(CsEnsemble* ens, uint32_t i, float flow_ml_s, float exit_speed);
+int32_t cs_ensemble_get_counts(CsEnsemble* ens, uint32_t i, uint32_t* num_water, uint32_t* num_bed);
+int32_t cs_ensemble_read_particles(CsEnsemble* ens, uint32_t i, uint32_t first, uint32_t count, float* out);
+int32_t cs_ensemble_get_metrics(CsEnsemble* ens, uint32_t i, CsMetrics* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COFFEE_SIM_H */

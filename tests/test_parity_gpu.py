@@ -1,0 +1,158 @@
+"""CUDA engine vs the CPU oracle, through the C ABI.
+
+The engine is built with -fmad=false and restates every WGSL expression in the same
+order as the oracle, so in the reference configuration (fixed-point pressure, fixed
+40 red+black pairs, i32 atomics) results are expected to agree bit for bit; each
+comparison asserts exact equality and prints the first mismatching pass otherwise.
+"""
+import numpy as np
+import pytest
+
+from coffee_sim_b200 import scenes
+from coffee_sim_b200.sim import MpmSettings, MpmSim3D
+from helpers import copy_state, mismatch, pair, relerr
+
+pytestmark = pytest.mark.gpu
+
+FRAME = 1.0 / 60.0
+
+# Reference dispatch numbering (mod.rs:317-414); a partial substep runs passes [0, n).
+AFTER_P2G = 4
+AFTER_GRID_UPDATE = 6
+AFTER_CLASSIFY = 7
+AFTER_RBGS = 8
+AFTER_PROJECT = 11
+AFTER_PACKING = 13
+AFTER_VISCOSITY = 16
+AFTER_G2P = 17
+AFTER_COUPLING = 18
+AFTER_BED = 20
+ALL = 0xFFFFFFFF
+
+
+def _state(sim, cells=True):
+    n = sim.particle_count()
+    d = {"particles": sim.read_particles(0, n), "affine": sim.read_affine(0, n)}
+    if sim.num_bed:
+        d["bed_extract"] = sim.read_bed_extract(0, sim.num_bed)
+    if cells:
+        d["lanes"] = sim.read_grid_lanes()
+        d["grid_vel"] = sim.read_grid_vel()
+        d["lookup"] = sim.read_bed_lookup()
+        d["kind"] = sim.read_cell_kind()
+        d["pressure"] = sim.read_pressure()
+    return d
+
+
+def _assert_same(a, b, what, keys=None):
+    bad = {}
+    for k in keys or a:
+        if k not in b:
+            continue
+        m = mismatch(a[k], b[k])
+        if m:
+            bad[k] = (m, relerr(a[k], b[k]))
+    assert not bad, f"{what}: mismatching arrays (count, norm-rel err) {bad}"
+
+
+def _prepared(settings, oracle, frames, angle):
+    """Run the oracle to an interesting state and return it."""
+    src = MpmSim3D(settings, oracle)
+    src.set_kettle_angle(angle)
+    for _ in range(frames):
+        src.step_frame(FRAME)
+    return src
+
+
+@pytest.fixture(scope="module")
+def free_stream_state(oracle):
+    s = MpmSettings.benchmark_free_stream(oracle)
+    return s, _prepared(s, oracle, 18, 36.0)
+
+
+@pytest.fixture(scope="module")
+def center_pour_state(oracle):
+    s = MpmSettings.benchmark_center_pour(oracle)
+    return s, _prepared(s, oracle, 20, 36.0)
+
+
+def test_setup_matches_oracle(engine, oracle):
+    """SDF texture, solid mask and the seeded bed (state.rs:206-344, bed.rs:107-314)."""
+    s = MpmSettings.benchmark_center_pour(engine)
+    e, o = pair(s, engine, oracle)
+    assert e.num_bed == o.num_bed == 12000
+    assert mismatch(e.read_sdf(), o.read_sdf()) == 0
+    assert mismatch(e.read_sdf_class(), o.read_sdf_class()) == 0
+    _assert_same(_state(e), _state(o), "initial state", ["particles", "affine", "bed_extract", "lookup"])
+
+
+@pytest.mark.parametrize("passes", [AFTER_P2G, AFTER_GRID_UPDATE, AFTER_CLASSIFY, AFTER_RBGS, AFTER_PROJECT,
+                                    AFTER_PACKING, AFTER_VISCOSITY, AFTER_G2P, ALL])
+def test_free_stream_pass_by_pass(engine, oracle, free_stream_state, passes):
+    settings, src = free_stream_state
+    e, o = pair(settings, engine, oracle)
+    copy_state(src, e)
+    copy_state(src, o)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+        sim.step_substep_partial(FRAME / 10, passes)
+    a, b = _state(e), _state(o)
+    keys = ["particles", "affine", "grid_vel", "lookup"]
+    if passes in (AFTER_P2G,):
+        keys.append("lanes")
+    if passes >= AFTER_CLASSIFY:
+        keys += ["kind", "pressure"]
+    if passes == ALL:
+        keys.append("lanes")
+    _assert_same(a, b, f"free stream after {passes} passes", keys)
+
+
+@pytest.mark.parametrize("passes", [AFTER_P2G, AFTER_CLASSIFY, AFTER_RBGS, AFTER_PROJECT, AFTER_G2P,
+                                    AFTER_COUPLING, AFTER_BED, ALL])
+def test_center_pour_pass_by_pass(engine, oracle, center_pour_state, passes):
+    settings, src = center_pour_state
+    e, o = pair(settings, engine, oracle)
+    copy_state(src, e)
+    copy_state(src, o)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+        sim.step_substep_partial(FRAME / 10, passes)
+    a, b = _state(e), _state(o)
+    keys = ["particles", "affine", "bed_extract", "grid_vel", "lookup"]
+    if passes >= AFTER_CLASSIFY:
+        keys += ["kind", "pressure"]
+    if passes in (AFTER_P2G, ALL):
+        keys.append("lanes")
+    _assert_same(a, b, f"center pour after {passes} passes", keys)
+    if passes == ALL:
+        assert mismatch(e.read_bed_delta(), o.read_bed_delta()) == 0
+
+
+def test_center_pour_frames_bit_exact(engine, oracle):
+    """Ten frames of pouring onto the bed from the initial state, compared every frame."""
+    s = MpmSettings.benchmark_center_pour(engine)
+    e, o = pair(s, engine, oracle)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+    for f in range(10):
+        e.step_frame(FRAME)
+        o.step_frame(FRAME)
+        assert e.particle_count() == o.particle_count()
+        _assert_same(_state(e, cells=False), _state(o, cells=False), f"frame {f}")
+    me, mo = e.latest_metrics(), o.latest_metrics()
+    assert (me.fluid_cells, me.div_clamp_fires, me.pressure_clamp_fires) == (
+        mo.fluid_cells, mo.div_clamp_fires, mo.pressure_clamp_fires)
+    assert me.max_abs_div == mo.max_abs_div
+    assert e.total_emitted_mass() == o.total_emitted_mass()
+
+
+def test_c1_water_block_200_steps(engine, oracle):
+    """the 32^3 water block, 200 substeps, compared every 50."""
+    se = scenes.c1_water_block(engine)
+    e, o = MpmSim3D(se, engine), MpmSim3D(se, oracle)
+    assert scenes.populate_c1(e) == scenes.populate_c1(o)
+    for k in range(200):
+        e.step_substep(scenes.C1_DT)
+        o.step_substep(scenes.C1_DT)
+        if k % 50 == 49:
+            _assert_same(_state(e), _state(o), f"C1 step {k}", ["particles", "affine", "grid_vel", "pressure"])
