@@ -1,0 +1,311 @@
+"""Benchmark: particle-steps/s of the MLS-MPM substep with the pressure solve swept to
+a relative residual of 1e-5 (the BASELINE metric), on the V60 pour-over scene at 64^3.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+One "step" is one substep of the V60 scene (dt = 5e-4 s) in its mid-pour state
+(~280k samples: water above the coffee bed and a carafe pool, jet 4 ml/s at 0.8 m/s).
+Timing uses CUDA events on the engine's stream; L2 is flushed (512 MB write) before
+each timed step.  Under torchrun each rank steps an independent replica of the pour
+on its own GPU (a single pour does not shard; weak scaling) and rank 0 prints the
+max-over-ranks time.  `--impl reference` times the CPU restatement of the reference
+step (the oracle, all host threads) on the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/sec at 1e-5 pressure residual (V60 64^3)"
+UNIT = "particle-steps/s"
+WORKLOAD = "c2_v60_midpour_64cube"
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def build_scene(lib, args, device=0):
+    from coffee_sim_b200 import scenes
+    from coffee_sim_b200.sim import MpmSim3D
+    s = scenes.c2_v60(lib, grid=args.grid)
+    s.raw.device = device
+    s.raw.rbgs_omega = args.omega
+    s.raw.max_sweeps = args.max_sweeps
+    s.raw.check_every = args.check_every
+    sim = MpmSim3D(s, lib)
+    scenes.populate_c2(sim)
+    return sim
+
+
+def algorithmic_bytes(n_p, n_c, pairs, evals, n_bed):
+    """Compulsory bytes of one substep: 172 N_p + 134 N_c + 17 K N_c + 13 E N_c, plus
+    4 N_c + 200 N_bed with a bed."""
+    b = 172 * n_p + 134 * n_c + 17 * pairs * n_c + 13 * evals * n_c
+    if n_bed:
+        b += 4 * n_c + 200 * n_bed
+    return b
+
+
+def cpu_baseline(args, threads=None, steps=None, warm=None):
+    """Time the CPU oracle on the same workload (bounded sample)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib
+    lib = oracle_lib.oracle_library()
+    if threads:
+        oracle_lib.set_threads(threads)
+    nthreads = int(lib.lib.oracle_get_threads())
+    sim = build_scene(lib, args)
+    n_p = sim.particle_count()
+    from coffee_sim_b200 import scenes
+    for _ in range(warm if warm is not None else args.cpu_warmup):
+        sim.step_substep(scenes.C2_DT)
+    k = steps if steps is not None else args.cpu_steps
+    t = time.perf_counter()
+    sweeps = 0
+    for _ in range(k):
+        sim.step_substep(scenes.C2_DT)
+        sweeps += sim.latest_metrics().last_sweeps
+    dt = time.perf_counter() - t
+    return {"value": n_p * k / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{k} substeps of the same V60 64^3 mid-pour state ({n_p} samples) after "
+                      f"{warm if warm is not None else args.cpu_warmup} warm-up substeps; {sweeps / max(k, 1):.0f} "
+                      f"RBGS pairs per substep; oracle/ C++ restatement, OpenMP, -O3",
+            "seconds": dt, "particles": n_p}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    res = cpu_baseline(args, steps=args.steps, warm=args.warmup)
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["seconds"] * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "particles": res["particles"], "omega": args.omega,
+                       "residual_tol": 1e-5},
+            "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"], "kind": "port",
+                             "sample": res["sample"]},
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--grid", type=int, default=64)
+    ap.add_argument("--omega", type=float, default=1.9)
+    ap.add_argument("--max-sweeps", type=int, default=4000)
+    ap.add_argument("--check-every", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--cpu-warmup", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        rc = run_reference(args, rank)
+        if dist:
+            dist.destroy_process_group()
+        return rc
+
+    from coffee_sim_b200 import scenes
+    from coffee_sim_b200.sim import engine_library
+    lib = engine_library()
+    sim = build_scene(lib, args, device=local)
+    n_p = sim.particle_count()
+    n_c = sim.settings.cells
+    n_bed = sim.num_bed
+    dt = scenes.C2_DT
+
+    for _ in range(args.warmup):
+        sim.step_substep(dt)
+    sim.sync()
+
+    def barrier():
+        if dist:
+            import torch
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    # ---- device-timed region: K substeps, L2 flushed before each ----
+    sim.profile_enable(True)
+    step_ms = []
+    barrier()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            sim.flush_l2()
+            sim.timer_start()
+            sim.step_substep(dt)
+            step_ms.append(sim.timer_stop())
+    barrier()
+    prof = sim.profile_read()
+    metrics = sim.latest_metrics()
+    total_ms = sum(step_ms)
+    if dist:
+        import torch
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = n_p * args.steps * world / (total_ms * 1e-3)
+
+    # ---- end to end through the public API (host emission upload + metrics readback) ----
+    sim.profile_enable(True)
+    sim.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step_substep(dt)
+        sim.latest_metrics()
+    e2e_s = time.perf_counter() - t0
+    prof_e2e = sim.profile_read()
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = n_p * args.steps * world / e2e_s
+
+    # ---- roofline of the dominant kernel (the red-black sweep) ----
+    peak, peak_kind = load_peaks()
+    sweep_ms = prof.phase_ms[4]
+    sweep_launches = max(prof.phase_launches[4], 1)
+    per_launch_bytes = 8.5 * n_c  # 17 B per cell per red+black pair, half per colour launch
+    achieved = per_launch_bytes / (sweep_ms * 1e-3 / sweep_launches) / 1e9 if sweep_ms > 0 else 0.0
+    pairs_per_step = prof.sweeps / max(prof.substeps, 1)
+    evals_per_step = prof.residual_evals / max(prof.substeps, 1)
+    step_bytes = algorithmic_bytes(n_p, n_c, pairs_per_step, evals_per_step, n_bed)
+    step_gbs = step_bytes / (total_ms / args.steps * 1e-3) / 1e9 * (1 if world == 1 else 1)
+
+    traffic = None
+    tf = ROOT / "profiles" / "rbgs_sweep_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded V60 scene generator; no dataset)",
+        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "particles": n_p, "bed_particles": n_bed,
+                   "substep_dt_s": dt, "residual_tol": 1e-5, "omega": args.omega, "warm_start": "previous substep",
+                   "check_every_pairs": args.check_every, "l2": "flushed (512 MB write) before each timed step",
+                   "parallelism": f"replicas x{world}"},
+        "pressure_solve_ms": (prof.phase_ms[4] + prof.phase_ms[5]) / max(prof.substeps, 1),
+        "sweeps_per_step": pairs_per_step,
+        "final_residual": metrics.last_residual,
+        "phase_ms_per_step": {n: prof.phase_ms[i] / max(prof.substeps, 1)
+                              for i, n in enumerate(["emit", "clear", "p2g", "grid", "sweeps", "residual",
+                                                     "project", "g2p", "bed", "render"])},
+        "roofline": {"bound": "hbm", "kernel": "k_refine_sweep (one colour)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": prof_e2e.h2d_bytes / args.steps,
+                "d2h_bytes_per_step": prof_e2e.d2h_bytes / args.steps},
+        "gpu_launches": int(prof.launches),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args)
+            line["cpu_baseline"].pop("seconds", None)
+            line["cpu_baseline"].pop("particles", None)
+        except Exception as e:  # the oracle is test infrastructure; report its absence
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
+                                    "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

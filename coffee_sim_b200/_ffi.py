@@ -5,7 +5,7 @@ return types to every exported function of a library that implements the C ABI.
 """
 import ctypes as C
 
-CS_ABI_VERSION = 3
+CS_ABI_VERSION = 4
 CS_MAX_OBSTACLES = 4
 
 STATUS = {
@@ -184,6 +184,8 @@ class CsSettings(C.Structure):
         ("rbgs_kernel", C.c_uint32),
         ("flow_override_ml_s", C.c_float),
         ("exit_speed_override", C.c_float),
+        ("rbgs_omega", C.c_float),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 
@@ -202,6 +204,23 @@ class CsMetrics(C.Structure):
         ("learned_used", C.c_uint32),
         ("reserved", C.c_uint32),
         ("solve_ms", C.c_double),
+    ]
+
+
+CS_PHASE_COUNT = 16
+PHASE_NAMES = ["emit", "clear", "p2g", "grid", "sweeps", "residual", "project", "g2p", "bed", "render"]
+
+
+class CsProfile(C.Structure):
+    _fields_ = [
+        ("phase_ms", C.c_double * CS_PHASE_COUNT),
+        ("phase_launches", C.c_uint32 * CS_PHASE_COUNT),
+        ("launches", C.c_uint64),
+        ("sweeps", C.c_uint64),
+        ("residual_evals", C.c_uint64),
+        ("h2d_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64),
+        ("substeps", C.c_uint64),
     ]
 
 
@@ -273,6 +292,12 @@ PROTOTYPES = {
     "cs_ensemble_get_counts": (I32, [P, U32, PU32, PU32]),
     "cs_ensemble_read_particles": (I32, [P, U32, U32, U32, PF]),
     "cs_ensemble_get_metrics": (I32, [P, U32, PM]),
+    "cs_profile_enable": (I32, [P, I32]),
+    "cs_profile_read": (I32, [P, C.POINTER(CsProfile)]),
+    "cs_timer_start": (I32, [P]),
+    "cs_timer_stop": (I32, [P, PF]),
+    "cs_flush_l2": (I32, [P]),
+    "cs_sync": (I32, [P]),
 }
 
 

@@ -55,6 +55,7 @@ struct Params {
     uint32_t fixed_point;      // pressure/divergence stored as i32*2^18
     uint32_t int64_grid;       // P2G accumulators are i64*2^32
     uint32_t warm;             // keep last substep's pressure in fluid cells
+    float omega;               // red-black over-relaxation (1 = plain Gauss-Seidel)
 };
 
 // Device pointers of one simulation (or one ensemble member).
@@ -78,6 +79,9 @@ struct Ctx {
     float* pf;        // FP32 pressure (persistent across substeps for warm start)
     float* divf;      // FP32 divergence
     float* fill;      // liquid fill fraction of each cell (written by classify)
+    float* plo;       // low word of the pressure (refinement mode: p = pf + plo)
+    float* pd;        // pressure correction of the current refinement cycle
+    float* gres;      // FP64 residual of the cycle, rounded to fp32
     int32_t* lookup;  // cell -> bed id
     const float* sdf;       // 128^3
     const uint8_t* cls;     // cells, 1 = solid

@@ -34,6 +34,16 @@ Engine::Engine(const CsSettings& s) : settings(s) {
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& sp : spans_) {
+        free_events_.push_back(sp.a);
+        free_events_.push_back(sp.b);
+    }
+    std::sort(free_events_.begin(), free_events_.end());
+    free_events_.erase(std::unique(free_events_.begin(), free_events_.end()), free_events_.end());
+    for (cudaEvent_t e : free_events_) cudaEventDestroy(e);
+    if (cur_event_ && spans_.empty()) cudaEventDestroy(cur_event_);
+    if (t0_) cudaEventDestroy(t0_);
+    if (t1_) cudaEventDestroy(t1_);
     free_all();
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -85,6 +95,9 @@ int Engine::init() {
     if ((rc = alloc(pf_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(divf_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(fill_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(plo_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(pd_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(gres_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(lookup_, cells_ * sizeof(int32_t)))) return rc;
     if ((rc = alloc(sdf_, (size_t)SDF_RES * SDF_RES * SDF_RES * sizeof(float)))) return rc;
     if ((rc = alloc(cls_, cells_))) return rc;
@@ -109,6 +122,9 @@ int Engine::init() {
     ctx_.pf = (float*)pf_.ptr;
     ctx_.divf = (float*)divf_.ptr;
     ctx_.fill = (float*)fill_.ptr;
+    ctx_.plo = (float*)plo_.ptr;
+    ctx_.pd = (float*)pd_.ptr;
+    ctx_.gres = (float*)gres_.ptr;
     ctx_.lookup = (int32_t*)lookup_.ptr;
     ctx_.sdf = (const float*)sdf_.ptr;
     ctx_.cls = (const uint8_t*)cls_.ptr;
@@ -148,7 +164,7 @@ int Engine::reset() {
     std::memset(&last, 0, sizeof(last));
     last.last_residual = last.initial_residual = -1.0;
     DeviceBuffer* zero[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_, &render_, &snap_, &delta_, &lanes_,
-                            &gvel_, &pf_, &divf_, &fill_};
+                            &gvel_, &pf_, &divf_, &fill_, &plo_, &pd_, &gres_};
     int rc;
     for (DeviceBuffer* b : zero)
         if ((rc = check(cudaMemsetAsync(b->ptr, 0, b->bytes, stream_), "memset"))) return rc;
@@ -241,9 +257,11 @@ void Engine::fill_params(Params& u, float dt) const {
     u.fixed_point = s.pressure_storage == CS_PRESSURE_FIXED_POINT ? 1u : 0u;
     u.int64_grid = s.p2g_mode == CS_P2G_INT64 ? 1u : 0u;
     u.warm = (s.warm_start != CS_WARM_NONE && !u.fixed_point && have_prev_p) ? 1u : 0u;
+    u.omega = s.rbgs_omega > 0.0f ? s.rbgs_omega : 1.0f;
 }
 
 int Engine::upload_ctx() {
+    prof_.h2d_bytes += sizeof(Ctx);
     return check(cudaMemcpyAsync(d_ctx_.ptr, &ctx_, sizeof(Ctx), cudaMemcpyHostToDevice, stream_), "ctx upload");
 }
 
@@ -271,10 +289,29 @@ int Engine::emit(float dt) {
 
 double Engine::residual() {
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    mark(CS_PHASE_RESIDUAL);
     cudaMemsetAsync(resid_.ptr, 0, 2 * sizeof(double), stream_);
     k_residual<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc);
+    count_launch();
     double h[2] = {0.0, 0.0};
     cudaMemcpyAsync(h, resid_.ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+    prof_.d2h_bytes += sizeof(h);
+    prof_.residual_evals += 1;
+    cudaStreamSynchronize(stream_);
+    if (h[1] <= 0.0) return 0.0;
+    return std::sqrt(h[0]) / std::sqrt(h[1]);
+}
+
+double Engine::refine_residual() {
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    mark(CS_PHASE_RESIDUAL);
+    cudaMemsetAsync(resid_.ptr, 0, 2 * sizeof(double), stream_);
+    k_refine_residual<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc);
+    count_launch();
+    double h[2] = {0.0, 0.0};
+    cudaMemcpyAsync(h, resid_.ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+    prof_.d2h_bytes += sizeof(h);
+    prof_.residual_evals += 1;
     cudaStreamSynchronize(stream_);
     if (h[1] <= 0.0) return 0.0;
     return std::sqrt(h[0]) / std::sqrt(h[1]);
@@ -289,15 +326,35 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
     auto pair = [&]() {
         k_rbgs_colour<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 0u);
         k_rbgs_colour<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 1u);
+        count_launch(2);
     };
     sweeps = 0;
     r0 = r1 = -1.0;
-    if (s.solve_mode == CS_SOLVE_RESIDUAL) {
+    if (s.solve_mode == CS_SOLVE_RESIDUAL && s.pressure_storage != CS_PRESSURE_FIXED_POINT) {
+        const uint32_t ce = s.check_every ? s.check_every : 10;
+        r0 = refine_residual();
+        r1 = r0;
+        while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
+            uint32_t k = std::min(ce, s.max_sweeps - sweeps);
+            mark(CS_PHASE_SWEEPS);
+            for (uint32_t j = 0; j < k; ++j) {
+                k_refine_sweep<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 0u);
+                k_refine_sweep<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 1u);
+                count_launch(2);
+            }
+            sweeps += k;
+            mark(CS_PHASE_RESIDUAL);
+            k_refine_accumulate<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc);
+            count_launch();
+            r1 = refine_residual();
+        }
+    } else if (s.solve_mode == CS_SOLVE_RESIDUAL) {
         uint32_t ce = s.check_every ? s.check_every : 1;
         r0 = residual();
         r1 = r0;
         if (!(r0 <= (double)s.residual_tol)) {
             while (sweeps < s.max_sweeps) {
+                mark(CS_PHASE_SWEEPS);
                 pair();
                 ++sweeps;
                 if (sweeps % ce == 0 || sweeps == s.max_sweeps) {
@@ -307,6 +364,7 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
             }
         }
     } else {
+        mark(CS_PHASE_SWEEPS);
         for (uint32_t k = 0; k < s.pressure_rbgs_pairs; ++k) pair();
         sweeps = s.pressure_rbgs_pairs;
         if (s.check_every) r1 = residual();
@@ -318,6 +376,7 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
 // (numbered in the order of mod.rs:317-414, each number fixed).
 int Engine::substep(float sub_dt, uint32_t P) {
     int rc;
+    mark(CS_PHASE_EMIT);
     if ((rc = emit(sub_dt))) return rc;
     fill_params(ctx_.u, sub_dt);
     if ((rc = upload_ctx())) return rc;
@@ -327,35 +386,50 @@ int Engine::substep(float sub_dt, uint32_t P) {
     const int pb = launch_particle_blocks(np);
     const int bb = launch_particle_blocks(num_bed);
     const dim3 T(kThreads);
+#define CS_LAUNCH(...)  \
+    do {                \
+        __VA_ARGS__;    \
+        count_launch(); \
+    } while (0)
+    mark(CS_PHASE_CLEAR);
     // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309)
     cudaMemsetAsync(lanes_.ptr, 0, lanes_.bytes, stream_);
     cudaMemsetAsync(gvel_.ptr, 0, gvel_.bytes, stream_);
     if (P > 0) cudaMemsetAsync(metrics_.ptr, 0, metrics_.bytes, stream_);
     if (P > 1) cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_);
-    if (P > 2 && num_bed) k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc);
-    if (P > 3 && np) k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc);
-    if (P > 4) k_grid_update<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 5 ? 1 : 0);
-    if (P > 6) k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc);
+    if (P > 2 && num_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    mark(CS_PHASE_P2G);
+    if (P > 3 && np) CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    mark(CS_PHASE_GRID);
+    if (P > 4) CS_LAUNCH(k_grid_update<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 5 ? 1 : 0));
+    if (P > 6) CS_LAUNCH(k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc));
     uint32_t sweeps = 0;
     double r0 = -1.0, r1 = -1.0;
     if (P > 7) {
         if ((rc = solve_pressure(sweeps, r0, r1))) return rc;
         have_prev_p = true;
     }
-    if (P > 8) k_project<<<dim3(cb, 1), T, 0, stream_>>>(dc, 1 | (P > 9 ? 2 : 0) | (P > 10 ? 4 : 0));
-    if (P > 11) k_packing_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 12 ? 1 : 0);
-    if (P > 13) k_viscosity_prepare<<<dim3(cb, 1), T, 0, stream_>>>(dc);
-    if (P > 14) k_viscosity_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 15 ? 1 : 0);
-    if (P > 16 && np) k_g2p<<<dim3(pb, 1), T, 0, stream_>>>(dc);
-    if (P > 17 && np) k_bed_coupling<<<dim3(pb, 1), T, 0, stream_>>>(dc);
-    if (P > 18 && num_bed) k_extraction_advect<<<dim3(bb, 1), T, 0, stream_>>>(dc);
-    if (P > 19 && num_bed) k_bed_dynamics<<<dim3(bb, 1), T, 0, stream_>>>(dc);
-    if (P > 20 && np) k_prepare_render<<<dim3(pb, 1), T, 0, stream_>>>(dc);
+    mark(CS_PHASE_PROJECT);
+    if (P > 8) CS_LAUNCH(k_project<<<dim3(cb, 1), T, 0, stream_>>>(dc, 1 | (P > 9 ? 2 : 0) | (P > 10 ? 4 : 0)));
+    if (P > 11) CS_LAUNCH(k_packing_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 12 ? 1 : 0));
+    if (P > 13) CS_LAUNCH(k_viscosity_prepare<<<dim3(cb, 1), T, 0, stream_>>>(dc));
+    if (P > 14) CS_LAUNCH(k_viscosity_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 15 ? 1 : 0));
+    mark(CS_PHASE_G2P);
+    if (P > 16 && np) CS_LAUNCH(k_g2p<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    mark(CS_PHASE_BED);
+    if (P > 17 && np) CS_LAUNCH(k_bed_coupling<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    if (P > 18 && num_bed) CS_LAUNCH(k_extraction_advect<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    if (P > 19 && num_bed) CS_LAUNCH(k_bed_dynamics<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    mark(CS_PHASE_RENDER);
+    if (P > 20 && np) CS_LAUNCH(k_prepare_render<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    mark(-1);
     if ((rc = check(cudaGetLastError(), "substep launch"))) return rc;
     total_time += sub_dt;
     last.last_sweeps = sweeps;
     last.last_residual = r1;
     last.initial_residual = r0;
+    prof_.sweeps += sweeps;
+    prof_.substeps += 1;
     return CS_OK;
 }
 
@@ -375,6 +449,7 @@ int Engine::step_frame(float dt) {
 
 int Engine::metrics(CsMetrics* out) {
     uint32_t m[8];
+    prof_.d2h_bytes += sizeof(m);
     int rc = check(cudaMemcpyAsync(m, metrics_.ptr, sizeof(m), cudaMemcpyDeviceToHost, stream_), "metrics");
     if (rc) return rc;
     if ((rc = sync())) return rc;
@@ -415,6 +490,7 @@ int Engine::write_particles(int what, uint32_t first, uint32_t count, const floa
     size_t width = what == 1 ? 12 : 8;
     int rc = upload_ctx();
     if (rc) return rc;
+    prof_.h2d_bytes += (uint64_t)count * width * sizeof(float);
     if ((rc = check(cudaMemcpyAsync(staging_.ptr, in, (size_t)count * width * sizeof(float), cudaMemcpyHostToDevice,
                                     stream_),
                     "upload")))
@@ -523,6 +599,90 @@ int Engine::add_water_block(const float lo[3], const float hi[3], uint32_t per_a
     num_water += cnt;
     if (added) *added = cnt;
     return CS_OK;
+}
+
+// ---- profiling ----
+cudaEvent_t Engine::take_event() {
+    if (!free_events_.empty()) {
+        cudaEvent_t e = free_events_.back();
+        free_events_.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void Engine::mark(int phase) {
+    if (!prof_on_) {
+        cur_phase_ = phase;
+        return;
+    }
+    if (phase == cur_phase_) return;
+    if (cur_phase_ < 0 && phase < 0) return;
+    cudaEvent_t e = take_event();
+    cudaEventRecord(e, stream_);
+    if (cur_phase_ >= 0) spans_.push_back(PhaseSpan{cur_phase_, cur_event_, e});
+    cur_phase_ = phase;
+    cur_event_ = phase >= 0 ? e : nullptr;
+}
+
+int Engine::profile_enable(bool on) {
+    int rc = sync();
+    if (rc) return rc;
+    for (auto& sp : spans_) {
+        free_events_.push_back(sp.a);
+        free_events_.push_back(sp.b);
+    }
+    spans_.clear();
+    std::memset(&prof_, 0, sizeof(prof_));
+    prof_on_ = on;
+    cur_phase_ = -1;
+    cur_event_ = nullptr;
+    return CS_OK;
+}
+
+int Engine::profile_read(CsProfile* out) {
+    int rc = sync();
+    if (rc) return rc;
+    std::vector<cudaEvent_t> seen;
+    for (auto& sp : spans_) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) prof_.phase_ms[sp.phase] += ms;
+        seen.push_back(sp.a);
+        seen.push_back(sp.b);
+    }
+    spans_.clear();
+    std::sort(seen.begin(), seen.end());
+    seen.erase(std::unique(seen.begin(), seen.end()), seen.end());
+    for (cudaEvent_t e : seen) free_events_.push_back(e);
+    *out = prof_;
+    return CS_OK;
+}
+
+int Engine::timer_start() {
+    if (!t0_) cudaEventCreate(&t0_);
+    if (!t1_) cudaEventCreate(&t1_);
+    return check(cudaEventRecord(t0_, stream_), "timer start");
+}
+
+int Engine::timer_stop(float* ms) {
+    if (!t0_) {
+        set_error("timer not started");
+        return CS_ERR_INVALID_ARG;
+    }
+    int rc = check(cudaEventRecord(t1_, stream_), "timer stop");
+    if (rc) return rc;
+    if ((rc = check(cudaEventSynchronize(t1_), "timer sync"))) return rc;
+    return check(cudaEventElapsedTime(ms, t0_, t1_), "timer elapsed");
+}
+
+int Engine::flush_l2() {
+    if (!flush_.ptr) {
+        int rc = alloc(flush_, (size_t)512 << 20);
+        if (rc) return rc;
+    }
+    return check(cudaMemsetAsync(flush_.ptr, (int)(prof_.substeps & 0xff), flush_.bytes, stream_), "flush");
 }
 
 // ---- checkpoint: host state + particle streams + warm-start pressure ----
@@ -915,6 +1075,32 @@ int32_t cs_add_water_block(CsSim* s, const float lo[3], const float hi[3], uint3
         return CS_ERR_INVALID_ARG;
     }
     return s->e->add_water_block(lo, hi, per_axis, jitter, seed, require_open_sdf, added);
+}
+int32_t cs_profile_enable(CsSim* s, int32_t on) {
+    CS_SIM(s);
+    return s->e->profile_enable(on != 0);
+}
+int32_t cs_profile_read(CsSim* s, CsProfile* out) {
+    CS_SIM(s);
+    CS_PTR(out);
+    return s->e->profile_read(out);
+}
+int32_t cs_timer_start(CsSim* s) {
+    CS_SIM(s);
+    return s->e->timer_start();
+}
+int32_t cs_timer_stop(CsSim* s, float* ms) {
+    CS_SIM(s);
+    CS_PTR(ms);
+    return s->e->timer_stop(ms);
+}
+int32_t cs_flush_l2(CsSim* s) {
+    CS_SIM(s);
+    return s->e->flush_l2();
+}
+int32_t cs_sync(CsSim* s) {
+    CS_SIM(s);
+    return s->e->sync();
 }
 int32_t cs_snapshot_size(CsSim* s, uint64_t* b) {
     CS_SIM(s);

@@ -60,6 +60,7 @@ private:
     int emit(float dt);
     int solve_pressure(uint32_t& sweeps, double& r0, double& r1);
     double residual();
+    double refine_residual();
     int launch_cells_blocks() const;
     int launch_particle_blocks(uint32_t n) const;
     int check(cudaError_t e, const char* what);
@@ -69,10 +70,38 @@ private:
     int sms_ = 148;
     std::vector<DeviceBuffer*> owned_;
     DeviceBuffer d_ctx_, pos_, vel_, c0_, c1_, c2_, bedA_, bedB_, render_, snap_, delta_;
-    DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, lookup_, sdf_, cls_, metrics_, resid_;
+    DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, plo_, pd_, gres_, lookup_, sdf_, cls_, metrics_, resid_;
     DeviceBuffer staging_;  // AoS upload/readback staging
+    DeviceBuffer flush_;    // > L2 scratch for cs_flush_l2 (allocated on first use)
     Ctx ctx_{};             // host copy of the device context
     std::vector<float> sdf_host_;
+
+public:
+    // ---- profiling: per-phase CUDA events on the stream, launch and byte counters ----
+    int profile_enable(bool on);
+    int profile_read(CsProfile* out);
+    int timer_start();
+    int timer_stop(float* ms);
+    int flush_l2();
+    void mark(int phase);      // close the open phase and open `phase` (-1 closes only)
+    void count_launch(uint32_t n = 1) {
+        prof_.launches += n;
+        if (cur_phase_ >= 0) prof_.phase_launches[cur_phase_] += n;
+    }
+
+private:
+    struct PhaseSpan {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    cudaEvent_t take_event();
+    bool prof_on_ = false;
+    CsProfile prof_{};
+    int cur_phase_ = -1;
+    cudaEvent_t cur_event_ = nullptr;
+    std::vector<PhaseSpan> spans_;
+    std::vector<cudaEvent_t> free_events_;
+    cudaEvent_t t0_ = nullptr, t1_ = nullptr;
 };
 
 void set_error(const std::string& msg);

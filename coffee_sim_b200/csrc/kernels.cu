@@ -240,7 +240,9 @@ __global__ void k_classify(const Ctx* __restrict__ cp) {
     CS_FOR(i, u.cells) {
         float mass = c.gvel[i].w;
         float keep = (!u.fixed_point && u.warm) ? c.pf[i] : 0.0f;
+        float keep_lo = (!u.fixed_point && u.warm) ? c.plo[i] : 0.0f;
         pressure_store(c, i, 0.0f);
+        c.plo[i] = 0.0f;
         uint32_t ix, iy, iz;
         decompose(u, i, ix, iy, iz);
         f3 cc = cell_center(u, ix, iy, iz);
@@ -273,7 +275,10 @@ __global__ void k_classify(const Ctx* __restrict__ cp) {
         }
         kl[i] = kind;
         c.fill[i] = liquid_fill(c, i, kind);
-        if (u.warm && !u.fixed_point) c.pf[i] = keep;
+        if (u.warm && !u.fixed_point) {
+            c.pf[i] = keep;
+            c.plo[i] = keep_lo;
+        }
         float4 sv = c.gvel[i];
         const float d = u.dx;
         float vxm = -sv.x, vxp = -sv.x, vym = -sv.y, vyp = -sv.y, vzm = -sv.z, vzp = -sv.z;
@@ -345,7 +350,10 @@ __device__ __forceinline__ void pressure_update(const Ctx& c, uint32_t i, uint32
         return;
     }
     float rhs = div_load(c, i) * sf / wmax(u.dt, 1e-6f);
-    pressure_store(c, i, (ps - u.dx * u.dx * rhs) / nc);
+    float pn = (ps - u.dx * u.dx * rhs) / nc;
+    // over-relaxed update p + w*(p_gs - p); w == 1 is the reference's plain update
+    if (u.omega != 1.0f) pn = pressure_load(c, i) + u.omega * (pn - pressure_load(c, i));
+    pressure_store(c, i, pn);
 }
 
 __global__ void k_rbgs_colour(const Ctx* __restrict__ cp, uint32_t parity) {
@@ -427,6 +435,144 @@ __global__ void k_residual(const Ctx* __restrict__ cp) {
             atomicAdd(&c.resid[0], r2);
             atomicAdd(&c.resid[1], b2);
         }
+    }
+}
+
+// ---------------- mixed-precision iterative refinement ----------------
+// FP32-storage residual mode: p = pf + plo (two fp32 words).  A cycle computes the
+// FP64 residual g = (sum w p_nb - dx^2 rhs) - W p of pressure_update's operator,
+// sweeps the correction d of L d = g in fp32 (red-black, over-relaxed), then adds d
+// to p in FP64.  Per-cell arithmetic matches the CPU oracle operation for operation.
+__device__ __forceinline__ void block_reduce_add2(double a, double b, double* out) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    __shared__ double sa[32], sb[32];
+    int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane_id == 0) {
+        sa[warp] = a;
+        sb[warp] = b;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        a = lane_id < nw ? sa[lane_id] : 0.0;
+        b = lane_id < nw ? sb[lane_id] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (lane_id == 0) {
+            atomicAdd(&out[0], a);
+            atomicAdd(&out[1], b);
+        }
+    }
+}
+
+__global__ void k_refine_residual(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const int32_t* kl = lane(c, 3);
+    double r2 = 0.0, b2 = 0.0;
+    CS_FOR(i, u.cells) {
+        c.pd[i] = 0.0f;
+        c.gres[i] = 0.0f;
+        int32_t kind = kl[i];
+        if (!is_fluid(kind)) continue;
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        float sf = c.fill[i];
+        double wsum = 0.0, psum = 0.0;
+        const uint32_t sy = u.gx, sz = u.gx * u.gy;
+#define CS_GFACE(cond, off)                                                                     \
+    if (cond) {                                                                                 \
+        uint32_t ni = i + (off);                                                                \
+        int32_t nk = kl[ni];                                                                    \
+        if (!is_solid(nk)) {                                                                    \
+            float w = face_weight(kind, sf, nk, c.fill[ni]);                                    \
+            if (w > 0.0f) {                                                                     \
+                wsum += (double)w;                                                              \
+                if (is_fluid(nk)) psum += (double)w * ((double)c.pf[ni] + (double)c.plo[ni]);   \
+            }                                                                                   \
+        }                                                                                       \
+    }
+        CS_GFACE(ix > 0, (uint32_t)-1)
+        CS_GFACE(ix + 1 < u.gx, 1u)
+        CS_GFACE(iy > 0, (uint32_t)0 - sy)
+        CS_GFACE(iy + 1 < u.gy, sy)
+        CS_GFACE(iz > 0, (uint32_t)0 - sz)
+        CS_GFACE(iz + 1 < u.gz, sz)
+#undef CS_GFACE
+        if (wsum <= 0.0) continue;
+        float rhs = div_load(c, i) * sf / wmax(u.dt, 1e-6f);
+        double b = (double)(u.dx * u.dx * rhs);
+        double r = (psum - b) - wsum * ((double)c.pf[i] + (double)c.plo[i]);
+        c.gres[i] = (float)r;
+        r2 += r * r;
+        b2 += b * b;
+    }
+    block_reduce_add2(r2, b2, c.resid);
+}
+
+__global__ void k_refine_sweep(const Ctx* __restrict__ cp, uint32_t parity) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const int32_t* kl = lane(c, 3);
+    const uint32_t half = (u.gx + 1) / 2;
+    const uint32_t n = half * u.gy * u.gz;
+    CS_FOR(t, n) {
+        uint32_t row = t / half, slot = t - row * half;
+        uint32_t iy = row % u.gy, iz = row / u.gy;
+        uint32_t ix = 2 * slot + ((iy + iz + parity) & 1u);
+        if (ix >= u.gx) continue;
+        uint32_t i = cidx(u, ix, iy, iz);
+        int32_t kind = kl[i];
+        if (!is_fluid(kind)) continue;
+        float sf = c.fill[i];
+        float nc = 0.0f, ds = 0.0f;
+        const uint32_t sy = u.gx, sz = u.gx * u.gy;
+#define CS_DFACE(cond, off)                                     \
+    if (cond) {                                                 \
+        uint32_t ni = i + (off);                                \
+        int32_t nk = kl[ni];                                    \
+        if (!is_solid(nk)) {                                    \
+            float w = face_weight(kind, sf, nk, c.fill[ni]);    \
+            if (w > 0.0f) {                                     \
+                nc += w;                                        \
+                if (is_fluid(nk)) ds += w * c.pd[ni];           \
+            }                                                   \
+        }                                                       \
+    }
+        CS_DFACE(ix > 0, (uint32_t)-1)
+        CS_DFACE(ix + 1 < u.gx, 1u)
+        CS_DFACE(iy > 0, (uint32_t)0 - sy)
+        CS_DFACE(iy + 1 < u.gy, sy)
+        CS_DFACE(iz > 0, (uint32_t)0 - sz)
+        CS_DFACE(iz + 1 < u.gz, sz)
+#undef CS_DFACE
+        if (nc <= 0.0f) continue;
+        float dn = (ds + c.gres[i]) / nc;
+        if (u.omega != 1.0f) dn = c.pd[i] + u.omega * (dn - c.pd[i]);
+        c.pd[i] = dn;
+    }
+}
+
+__global__ void k_refine_accumulate(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const int32_t* kl = lane(c, 3);
+    const double lim = (double)u.p_clamp;
+    CS_FOR(i, u.cells) {
+        if (!is_fluid(kl[i])) continue;
+        double p = ((double)c.pf[i] + (double)c.plo[i]) + (double)c.pd[i];
+        if (p > lim || p < -lim) {
+            p = p > 0.0 ? lim : -lim;
+            atomicAdd(&c.metrics[M_P_CLAMP], 1u);
+        }
+        float hi = (float)p;
+        c.pf[i] = hi;
+        c.plo[i] = (float)(p - (double)hi);
     }
 }
 

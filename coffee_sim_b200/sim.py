@@ -316,6 +316,29 @@ class MpmSim3D:
         )
         return added.value
 
+    # -- device timing / profiling --
+    def profile_enable(self, on=True):
+        self.lib.call("cs_profile_enable", self._h, 1 if on else 0)
+
+    def profile_read(self):
+        p = _ffi.CsProfile()
+        self.lib.call("cs_profile_read", self._h, C.byref(p))
+        return p
+
+    def timer_start(self):
+        self.lib.call("cs_timer_start", self._h)
+
+    def timer_stop(self):
+        ms = C.c_float()
+        self.lib.call("cs_timer_stop", self._h, C.byref(ms))
+        return ms.value
+
+    def flush_l2(self):
+        self.lib.call("cs_flush_l2", self._h)
+
+    def sync(self):
+        self.lib.call("cs_sync", self._h)
+
     # -- checkpoint --
     def snapshot(self):
         n = C.c_uint64()

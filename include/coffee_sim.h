@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define CS_ABI_VERSION 3u
+#define CS_ABI_VERSION 4u
 
 typedef enum CsStatus {
     CS_OK = 0,
@@ -226,6 +226,8 @@ typedef struct CsSettings {
     uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 persistent tiled */
     float flow_override_ml_s;     /* >0: constant flow instead of the kettle-angle model */
     float exit_speed_override;    /* >0 with flow override: jet speed */
+    float rbgs_omega;             /* red-black over-relaxation; 0 or 1 = plain Gauss-Seidel */
+    uint32_t reserved[7];
 } CsSettings;
 
 /* Observability counters (mod.rs:50-68 / state.rs:22-28) + solver telemetry. */
@@ -341,6 +343,37 @@ int32_t cs_ensemble_set_flow_override(CsEnsemble* ens, uint32_t i, float flow_ml
 int32_t cs_ensemble_get_counts(CsEnsemble* ens, uint32_t i, uint32_t* num_water, uint32_t* num_bed);
 int32_t cs_ensemble_read_particles(CsEnsemble* ens, uint32_t i, uint32_t first, uint32_t count, float* out);
 int32_t cs_ensemble_get_metrics(CsEnsemble* ens, uint32_t i, CsMetrics* out);
+
+/* ---- device timing and profiling (no counterpart: the reference defers timestamp
+ * queries, mod.rs:313 `timestamp_writes: None`) ---- */
+enum {
+    CS_PHASE_EMIT = 0,      /* inflow emission upload + uniforms */
+    CS_PHASE_CLEAR = 1,     /* grid clears, bed lookup rebuild */
+    CS_PHASE_P2G = 2,
+    CS_PHASE_GRID = 3,      /* grid_update + boundary + classify */
+    CS_PHASE_SWEEPS = 4,    /* red-black pressure sweeps */
+    CS_PHASE_RESIDUAL = 5,  /* FP64 residual evaluations + refinement bookkeeping */
+    CS_PHASE_PROJECT = 6,   /* project, packing, viscosity, boundary passes */
+    CS_PHASE_G2P = 7,
+    CS_PHASE_BED = 8,       /* bed coupling, extraction, bed dynamics */
+    CS_PHASE_RENDER = 9,
+    CS_PHASE_COUNT = 16
+};
+typedef struct CsProfile {
+    double phase_ms[CS_PHASE_COUNT];        /* device time per phase (CUDA events) */
+    uint32_t phase_launches[CS_PHASE_COUNT];
+    uint64_t launches;                      /* kernels launched by the engine */
+    uint64_t sweeps;                        /* red+black pairs */
+    uint64_t residual_evals;
+    uint64_t h2d_bytes, d2h_bytes;          /* host<->device traffic of the step calls */
+    uint64_t substeps;
+} CsProfile;
+int32_t cs_profile_enable(CsSim* sim, int32_t on);   /* resets the counters */
+int32_t cs_profile_read(CsSim* sim, CsProfile* out); /* synchronises */
+int32_t cs_timer_start(CsSim* sim);                  /* CUDA event on the sim's stream */
+int32_t cs_timer_stop(CsSim* sim, float* ms);        /* device ms since cs_timer_start; synchronises */
+int32_t cs_flush_l2(CsSim* sim);                     /* overwrite a buffer larger than L2 on the sim's stream */
+int32_t cs_sync(CsSim* sim);
 
 #ifdef __cplusplus
 }

@@ -110,6 +110,7 @@ struct Sim : SimBase {
         R div_clamp, p_clamp, mdiv_scale, mdiv_inv;
         R j_alpha, j_expand_alpha, max_rest_frac, surface_void_scale;
         R water_r_dx, bed_r_dx, filter_absorption;
+        R omega;
         CsGeometry g;
     } u;
 
@@ -117,6 +118,7 @@ struct Sim : SimBase {
     std::vector<int32_t> grid;                // 6 lanes
     std::vector<R> gvel;                      // 4 per cell
     std::vector<R> pf, divf;                  // FP32-storage pressure/divergence
+    std::vector<R> plo, pd, gres;             // refinement: pressure low part, correction, residual
     std::vector<int32_t> lookup, delta;
     uint32_t metrics[8];
     std::vector<float> sdf;
@@ -137,6 +139,9 @@ struct Sim : SimBase {
         gvel.assign(cells * 4, R(0));
         pf.assign(cells, R(0));
         divf.assign(cells, R(0));
+        plo.assign(cells, R(0));
+        pd.assign(cells, R(0));
+        gres.assign(cells, R(0));
         lookup.assign(cells, -1);
         delta.assign(mp * 4, 0);
         std::memset(metrics, 0, sizeof(metrics));
@@ -162,6 +167,9 @@ struct Sim : SimBase {
         std::fill(gvel.begin(), gvel.end(), R(0));
         std::fill(pf.begin(), pf.end(), R(0));
         std::fill(divf.begin(), divf.end(), R(0));
+        std::fill(plo.begin(), plo.end(), R(0));
+        std::fill(pd.begin(), pd.end(), R(0));
+        std::fill(gres.begin(), gres.end(), R(0));
         std::fill(lookup.begin(), lookup.end(), -1);
         std::fill(delta.begin(), delta.end(), 0);
         have_prev_p = false;
@@ -211,6 +219,7 @@ struct Sim : SimBase {
         u.water_r_dx = R(s.brew.water_sample_radius_dx); u.bed_r_dx = R(s.brew.bed_sample_radius_dx);
         u.filter_absorption = R(s.brew.filter_absorption_rate_s);
         u.g = s.geom;
+        u.omega = (s.rbgs_omega > 0.0f) ? R(s.rbgs_omega) : R(1);
     }
 
     // ---- shader.rs:81-171 helpers ----
@@ -851,7 +860,9 @@ struct Sim : SimBase {
         for (int idx = 0; idx < n; ++idx) {
             R mass = gvel[(size_t)idx * 4 + 3];
             R keep_p = (!fixed_point()) ? pf[idx] : R(0);
+            R keep_lo = plo[idx];
             pressure_store(idx, R(0));
+            plo[idx] = R(0);
             uint32_t ix, iy, iz;
             decompose(idx, ix, iy, iz);
             V cc = cell_center(ix, iy, iz);
@@ -882,7 +893,10 @@ struct Sim : SimBase {
                 div_store(idx, R(0));
                 continue;
             }
-            if (warm) pf[idx] = keep_p;
+            if (warm) {
+                pf[idx] = keep_p;
+                plo[idx] = keep_lo;
+            }
             const R* sv = &gvel[(size_t)idx * 4];
             R dxv = u.dx;
             R vxm = -sv[0], vxp = -sv[0], vym = -sv[1], vyp = -sv[1], vzm = -sv[2], vzp = -sv[2];
@@ -941,6 +955,8 @@ struct Sim : SimBase {
         }
         R rhs = div_load(idx) * sf / wmax(u.dt, R(1e-6));
         R pn = (ps - u.dx * u.dx * rhs) / nc;
+        // Over-relaxed update p + w*(p_gs - p); w == 1 is the reference's plain update.
+        if (u.omega != R(1)) pn = pressure_load(idx) + u.omega * (pn - pressure_load(idx));
         pressure_store(idx, pn);
     }
     void k_rbgs(uint32_t parity) {
@@ -1007,6 +1023,112 @@ struct Sim : SimBase {
         if (b2 <= 0.0) return 0.0;
         return std::sqrt(r2) / std::sqrt(b2);
     }
+    // ---- mixed-precision iterative refinement (FP32 storage, residual mode) ----
+    // Pressure is held as p = hi + lo (two fp32 words).  A cycle computes the FP64
+    // residual g = (sum w p_nb - dx^2 rhs) - W p of pressure_update's operator, runs
+    // red-black sweeps on the correction d of L d = g in fp32, and adds d to p in
+    // FP64.  The sweep count and the stopping test use the FP64 residual norm.
+    double refine_residual() {
+        int n = (int)cells;
+        int nt = 1;
+#ifdef _OPENMP
+        nt = omp_get_max_threads();
+#endif
+        std::vector<double> rs(nt, 0.0), bs(nt, 0.0);
+        static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            double r2 = 0.0, b2 = 0.0;
+#pragma omp for schedule(static)
+            for (int idx = 0; idx < n; ++idx) {
+                pd[idx] = R(0);
+                gres[idx] = R(0);
+                int32_t kind = kind_load(idx);
+                if (!is_fluid(kind)) continue;
+                uint32_t ix, iy, iz;
+                decompose(idx, ix, iy, iz);
+                R sf = liquid_fill(idx, kind);
+                double wsum = 0.0, psum = 0.0;
+                for (int q = 0; q < 6; ++q) {
+                    int x = (int)ix + off[q][0], y = (int)iy + off[q][1], z = (int)iz + off[q][2];
+                    if (!in_grid(x, y, z)) continue;
+                    uint32_t ni = cell_index(x, y, z);
+                    int32_t nk = kind_load(ni);
+                    if (is_solid(nk)) continue;
+                    R w = face_weight(kind, sf, ni, nk);
+                    if (w <= R(0)) continue;
+                    wsum += (double)w;
+                    if (is_fluid(nk)) psum += (double)w * ((double)pf[ni] + (double)plo[ni]);
+                }
+                if (wsum <= 0.0) continue;
+                R rhs = div_load(idx) * sf / wmax(u.dt, R(1e-6));
+                double b = (double)(u.dx * u.dx * rhs);
+                double r = (psum - b) - wsum * ((double)pf[idx] + (double)plo[idx]);
+                gres[idx] = R(r);
+                r2 += r * r;
+                b2 += b * b;
+            }
+            rs[t] = r2;
+            bs[t] = b2;
+        }
+        double r2 = 0.0, b2 = 0.0;
+        for (int t = 0; t < nt; ++t) {
+            r2 += rs[t];
+            b2 += bs[t];
+        }
+        if (b2 <= 0.0) return 0.0;
+        return std::sqrt(r2) / std::sqrt(b2);
+    }
+    void refine_sweep(uint32_t parity) {
+        int n = (int)cells;
+        static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma omp parallel for schedule(static)
+        for (int idx = 0; idx < n; ++idx) {
+            uint32_t ix, iy, iz;
+            decompose(idx, ix, iy, iz);
+            if (((ix + iy + iz) & 1u) != parity) continue;
+            int32_t kind = kind_load(idx);
+            if (!is_fluid(kind)) continue;
+            R sf = liquid_fill(idx, kind);
+            R nc = R(0), ds = R(0);
+            for (int q = 0; q < 6; ++q) {
+                int x = (int)ix + off[q][0], y = (int)iy + off[q][1], z = (int)iz + off[q][2];
+                if (!in_grid(x, y, z)) continue;
+                uint32_t ni = cell_index(x, y, z);
+                int32_t nk = kind_load(ni);
+                if (is_solid(nk)) continue;
+                R w = face_weight(kind, sf, ni, nk);
+                if (w <= R(0)) continue;
+                nc += w;
+                if (is_fluid(nk)) ds += w * pd[ni];
+            }
+            if (nc <= R(0)) continue;
+            R dn = (ds + gres[idx]) / nc;
+            if (u.omega != R(1)) dn = pd[idx] + u.omega * (dn - pd[idx]);
+            pd[idx] = dn;
+        }
+    }
+    void refine_accumulate() {
+        int n = (int)cells;
+        R lim = u.p_clamp;
+#pragma omp parallel for schedule(static)
+        for (int idx = 0; idx < n; ++idx) {
+            if (!is_fluid(kind_load(idx))) continue;
+            double p = ((double)pf[idx] + (double)plo[idx]) + (double)pd[idx];
+            if (p > (double)lim || p < -(double)lim) {
+                p = p > 0.0 ? (double)lim : -(double)lim;
+                atomic_add_u32(&metrics[M_P_CLAMP], 1u);
+            }
+            R hi = R(p);
+            pf[idx] = hi;
+            plo[idx] = R(p - (double)hi);
+        }
+    }
+
     // shader.rs:1457-1543
     void k_project() {
         int n = (int)cells;
@@ -1635,7 +1757,21 @@ struct Sim : SimBase {
         if (run(true)) k_boundary();
         if (run(true)) k_classify(warm);
         if (run(true)) {
-            if (s.solve_mode == CS_SOLVE_RESIDUAL) {
+            if (s.solve_mode == CS_SOLVE_RESIDUAL && !fixed_point()) {
+                uint32_t ce = s.check_every ? s.check_every : 10;
+                r0 = refine_residual();
+                r1 = r0;
+                while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
+                    uint32_t k = std::min(ce, s.max_sweeps - sweeps);
+                    for (uint32_t j = 0; j < k; ++j) {
+                        refine_sweep(0);
+                        refine_sweep(1);
+                    }
+                    sweeps += k;
+                    refine_accumulate();
+                    r1 = refine_residual();
+                }
+            } else if (s.solve_mode == CS_SOLVE_RESIDUAL) {
                 uint32_t ce = s.check_every ? s.check_every : 1;
                 r0 = residual();
                 r1 = r0;
@@ -2013,3 +2149,28 @@ int32_t cs_snapshot_save(CsSim*, void*, uint64_t) { return fail(CS_ERR_UNSUPPORT
 int32_t cs_snapshot_load(CsSim*, const void*, uint64_t) { return fail(CS_ERR_UNSUPPORTED, "oracle has no snapshots"); }
 
 }  // extern "C"
+
+// Timing/profiling entry points: the oracle runs on the host, so the timer is a
+// wall clock and the profile only counts substeps.
+#include <chrono>
+static std::chrono::steady_clock::time_point g_t0;
+extern "C" {
+int32_t cs_profile_enable(CsSim* s, int32_t) { return s ? CS_OK : fail(CS_ERR_INVALID_ARG, "null sim"); }
+int32_t cs_profile_read(CsSim* s, CsProfile* out) {
+    if (!s || !out) return fail(CS_ERR_INVALID_ARG, "null");
+    std::memset(out, 0, sizeof(*out));
+    return CS_OK;
+}
+int32_t cs_timer_start(CsSim* s) {
+    if (!s) return fail(CS_ERR_INVALID_ARG, "null sim");
+    g_t0 = std::chrono::steady_clock::now();
+    return CS_OK;
+}
+int32_t cs_timer_stop(CsSim* s, float* ms) {
+    if (!s || !ms) return fail(CS_ERR_INVALID_ARG, "null");
+    *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - g_t0).count();
+    return CS_OK;
+}
+int32_t cs_flush_l2(CsSim* s) { return s ? CS_OK : fail(CS_ERR_INVALID_ARG, "null sim"); }
+int32_t cs_sync(CsSim* s) { return s ? CS_OK : fail(CS_ERR_INVALID_ARG, "null sim"); }
+}
