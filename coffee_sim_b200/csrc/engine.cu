@@ -9,8 +9,11 @@
 #include <memory>
 #include <string>
 
+#include <cub/device/device_scan.cuh>
+
 #include "engine.h"
 #include "kernels.cu"
+#include "solver_cluster.cuh"
 
 namespace cs {
 
@@ -105,6 +108,49 @@ int Engine::init() {
     if ((rc = alloc(resid_, 4 * sizeof(double)))) return rc;
     if ((rc = alloc(d_ctx_, sizeof(Ctx)))) return rc;
     if ((rc = alloc(staging_, std::max<size_t>(mp * 12 * sizeof(float), cells_ * 6 * sizeof(int32_t))))) return rc;
+    // cluster-resident solver: buffers and the largest launchable cluster size
+    {
+        uint32_t side = 1;
+        while (side < settings.grid_dims[0] || side < settings.grid_dims[1] || side < settings.grid_dims[2]) side <<= 1;
+        sc_codes_ = (size_t)side * side * side;
+    }
+    if ((rc = alloc(sc_flags_, sc_codes_ * sizeof(unsigned long long)))) return rc;
+    if ((rc = alloc(sc_scan_, sc_codes_ * sizeof(unsigned long long)))) return rc;
+    if ((rc = alloc(sc_ref_, cells_ * sizeof(uint16_t)))) return rc;
+    if ((rc = alloc(sc_cell_, (size_t)SC_MAX_RANKS * 4096 * sizeof(uint32_t)))) return rc;
+    if ((rc = alloc(sc_info_, sizeof(ScInfo)))) return rc;
+    if ((rc = alloc(sc_result_, sizeof(ScResult)))) return rc;
+    {
+        size_t temp = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, temp, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                      (int)sc_codes_, stream_);
+        if ((rc = alloc(sc_temp_, temp))) return rc;
+        sc_ranks_ = 0;
+        if (cudaFuncSetAttribute(k_sc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ScLayout::bytes) ==
+                cudaSuccess &&
+            cudaFuncSetAttribute(k_sc_solve, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            for (int r : {16, 8}) {
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(r, 1, 1);
+                cfg.blockDim = dim3(SC_THREADS, 1, 1);
+                cfg.dynamicSmemBytes = ScLayout::bytes;
+                cudaLaunchAttribute attr;
+                attr.id = cudaLaunchAttributeClusterDimension;
+                attr.val.clusterDim.x = r;
+                attr.val.clusterDim.y = 1;
+                attr.val.clusterDim.z = 1;
+                cfg.attrs = &attr;
+                cfg.numAttrs = 1;
+                int nclusters = 0;
+                if (cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_sc_solve, &cfg) == cudaSuccess &&
+                    nclusters > 0) {
+                    sc_ranks_ = r;
+                    break;
+                }
+            }
+        }
+        cudaGetLastError();  // clear a refused attribute or occupancy query
+    }
 
     ctx_.pos = (float4*)pos_.ptr;
     ctx_.vel = (float4*)vel_.ptr;
@@ -317,6 +363,60 @@ double Engine::refine_residual() {
     return std::sqrt(h[0]) / std::sqrt(h[1]);
 }
 
+// One-launch solve on a thread-block cluster (solver_cluster.cuh).  `done` is false
+// when the fluid cells exceed the cluster's shared-memory capacity.
+int Engine::solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done) {
+    done = false;
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    ScBuffers sb;
+    sb.flags = (unsigned long long*)sc_flags_.ptr;
+    sb.scan = (unsigned long long*)sc_scan_.ptr;
+    sb.ref_of_cell = (uint16_t*)sc_ref_.ptr;
+    sb.cell_of = (uint32_t*)sc_cell_.ptr;
+    sb.info = (ScInfo*)sc_info_.ptr;
+    sb.result = (ScResult*)sc_result_.ptr;
+    const uint32_t codes = (uint32_t)sc_codes_;
+    const int cb = (int)std::min<size_t>((sc_codes_ + kThreads - 1) / kThreads, (size_t)sms_ * 16);
+    mark(CS_PHASE_RESIDUAL);
+    k_sc_flags<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, sb, codes);
+    size_t temp = sc_temp_.bytes;
+    cub::DeviceScan::ExclusiveSum(sc_temp_.ptr, temp, sb.flags, sb.scan, (int)codes, stream_);
+    k_sc_totals<<<dim3(1, 1), 1, 0, stream_>>>(dc, sb, (uint32_t)sc_ranks_, codes);
+    k_sc_starts<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, sb, codes);
+    k_sc_map<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, sb, codes);
+    count_launch(4);
+    mark(CS_PHASE_SWEEPS);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sc_ranks_, 1, 1);
+    cfg.blockDim = dim3(SC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = ScLayout::bytes;
+    cfg.stream = stream_;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = sc_ranks_;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    const CsSettings& s = settings;
+    int rc = check(cudaLaunchKernelEx(&cfg, k_sc_solve, dc, sb, s.residual_tol, s.max_sweeps, s.check_every),
+                   "cluster solve launch");
+    if (rc) return rc;
+    count_launch();
+    ScResult res;
+    if ((rc = check(cudaMemcpyAsync(&res, sc_result_.ptr, sizeof(res), cudaMemcpyDeviceToHost, stream_), "solve result")))
+        return rc;
+    prof_.d2h_bytes += sizeof(res);
+    if ((rc = sync())) return rc;
+    if (res.status != 1) return CS_OK;
+    sweeps = res.sweeps;
+    r0 = res.r0;
+    r1 = res.r1;
+    prof_.residual_evals += res.evals;
+    done = true;
+    return CS_OK;
+}
+
 int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
     const CsSettings& s = settings;
@@ -330,7 +430,14 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
     };
     sweeps = 0;
     r0 = r1 = -1.0;
-    if (s.solve_mode == CS_SOLVE_RESIDUAL && s.pressure_storage != CS_PRESSURE_FIXED_POINT) {
+    const bool refine = s.solve_mode == CS_SOLVE_RESIDUAL && s.pressure_storage != CS_PRESSURE_FIXED_POINT;
+    if (refine && s.rbgs_kernel != 1 && sc_ranks_ > 0) {
+        bool done = false;
+        int rc = solve_cluster(sweeps, r0, r1, done);
+        if (rc) return rc;
+        if (done) return CS_OK;
+    }
+    if (refine) {
         const uint32_t ce = s.check_every ? s.check_every : 10;
         r0 = refine_residual();
         r1 = r0;

@@ -72,6 +72,11 @@ private:
     DeviceBuffer d_ctx_, pos_, vel_, c0_, c1_, c2_, bedA_, bedB_, render_, snap_, delta_;
     DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, plo_, pd_, gres_, lookup_, sdf_, cls_, metrics_, resid_;
     DeviceBuffer staging_;  // AoS upload/readback staging
+    // cluster-resident solver
+    DeviceBuffer sc_flags_, sc_scan_, sc_ref_, sc_cell_, sc_info_, sc_result_, sc_temp_;
+    int sc_ranks_ = 0;      // cluster size usable for the solve (0 = unavailable)
+    size_t sc_codes_ = 0;   // Morton codes covering the grid (power-of-two cube)
+    int solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done);
     DeviceBuffer flush_;    // > L2 scratch for cs_flush_l2 (allocated on first use)
     Ctx ctx_{};             // host copy of the device context
     std::vector<float> sdf_host_;

@@ -552,7 +552,7 @@ __global__ void k_refine_sweep(const Ctx* __restrict__ cp, uint32_t parity) {
         CS_DFACE(iz + 1 < u.gz, sz)
 #undef CS_DFACE
         if (nc <= 0.0f) continue;
-        float dn = (ds + c.gres[i]) / nc;
+        float dn = (ds + c.gres[i]) * (1.0f / nc);
         if (u.omega != 1.0f) dn = c.pd[i] + u.omega * (dn - c.pd[i]);
         c.pd[i] = dn;
     }

@@ -1107,7 +1107,7 @@ struct Sim : SimBase {
                 if (is_fluid(nk)) ds += w * pd[ni];
             }
             if (nc <= R(0)) continue;
-            R dn = (ds + gres[idx]) / nc;
+            R dn = (ds + gres[idx]) * (R(1) / nc);
             if (u.omega != R(1)) dn = pd[idx] + u.omega * (dn - pd[idx]);
             pd[idx] = dn;
         }

@@ -178,3 +178,24 @@ def test_v60_refinement_solve_matches_oracle(engine, oracle, grid, omega):
             assert me.last_residual <= 1e-5
         a, b = _state(e), _state(o)
         _assert_same(a, b, f"V60 {grid}^3 substep {k}", ["particles", "affine", "bed_extract", "grid_vel", "pressure"])
+
+
+def test_cluster_solver_matches_per_colour_launches(engine):
+    """The one-launch cluster-resident solve (solver_cluster.cuh) against the
+    per-colour launch path on the same state: identical sweep counts and pressures."""
+    sims = []
+    for kernel in (1, 2):
+        s = scenes.c2_v60(engine)
+        s.raw.rbgs_omega = 1.9
+        s.raw.rbgs_kernel = kernel
+        sim = MpmSim3D(s, engine)
+        scenes.populate_c2(sim)
+        sims.append(sim)
+    for k in range(3):
+        for sim in sims:
+            sim.step_substep(scenes.C2_DT)
+        ma, mb = sims[0].latest_metrics(), sims[1].latest_metrics()
+        assert ma.last_sweeps == mb.last_sweeps
+        assert mb.last_residual <= 1e-5
+        assert mismatch(sims[0].read_pressure(), sims[1].read_pressure()) == 0
+        assert mismatch(sims[0].read_particles(), sims[1].read_particles()) == 0
