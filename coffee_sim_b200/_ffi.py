@@ -298,6 +298,8 @@ PROTOTYPES = {
     "cs_timer_stop": (I32, [P, PF]),
     "cs_flush_l2": (I32, [P]),
     "cs_sync": (I32, [P]),
+    "cs_pressure_solve_noalloc": (I32, [U32, U32, U32, F32, F32, F32, F32, U32, U32, P, P, P, P, P, P, PU32,
+                                       C.POINTER(C.c_double)]),
 }
 
 

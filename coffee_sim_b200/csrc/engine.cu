@@ -883,6 +883,75 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
     return sync();
 }
 
+// ---- launch helpers for callers outside Engine (noalloc.cu) ----
+// Largest cluster size the solve kernel can be launched with on the current device
+// (16 with the non-portable opt-in, else 8), 0 when neither fits.
+int sc_max_cluster_ranks() {
+    if (cudaFuncSetAttribute(k_sc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ScLayout::bytes) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_sc_solve, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (int r : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(r, 1, 1);
+        cfg.blockDim = dim3(SC_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = ScLayout::bytes;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = r;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (void*)k_sc_solve, &cfg) == cudaSuccess && n > 0) return r;
+    }
+    cudaGetLastError();
+    return 0;
+}
+
+size_t sc_scan_temp_bytes(uint32_t codes) {
+    size_t temp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, temp, (unsigned long long*)nullptr, (unsigned long long*)nullptr, (int)codes,
+                                  (cudaStream_t)0);
+    return temp;
+}
+
+// The launch sequence of Engine::solve_cluster on caller-provided memory.
+int sc_launch_solve(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, float tol, uint32_t max_pairs,
+                    uint32_t check_every, void* cub_temp, size_t cub_bytes, cudaStream_t stream, int sms) {
+    const int cb = (int)std::min<size_t>((codes + kThreads - 1) / kThreads, (size_t)sms * 16);
+    k_sc_flags<<<dim3(cb, 1), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    size_t temp = cub_bytes;
+    if (cub::DeviceScan::ExclusiveSum(cub_temp, temp, sb.flags, sb.scan, (int)codes, stream) != cudaSuccess) {
+        set_error("scan launch failed");
+        return CS_ERR_CUDA;
+    }
+    k_sc_totals<<<dim3(1, 1), 1, 0, stream>>>(d_ctx, sb, (uint32_t)ranks, codes);
+    k_sc_starts<<<dim3(cb, 1), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    k_sc_map<<<dim3(cb, 1), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ranks, 1, 1);
+    cfg.blockDim = dim3(SC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = ScLayout::bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = ranks;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_sc_solve, d_ctx, sb, tol, max_pairs, check_every);
+    if (e != cudaSuccess) {
+        set_error(std::string("cluster solve launch: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+
 }  // namespace cs
 
 // ============================ C ABI ============================

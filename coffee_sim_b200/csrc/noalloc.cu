@@ -1,0 +1,188 @@
+// noalloc.cu — the pressure solve on caller-owned device arrays, without allocating.
+//
+// Who needs this: hosts that own every byte of device memory themselves and may not
+// call cudaMalloc once they are running — a renderer or game engine that reserves
+// its GPU budget at start-up, or a real-time frame loop where cudaMalloc's latency
+// and implicit synchronisation are not acceptable.  Such a caller cannot create a
+// CsSim (cs_create allocates), but can hand this entry point the fields it already
+// keeps on the device and get the solved pressure back in place.
+//
+// Every scratch buffer of the solve (Morton flags and their scan, neighbour
+// references, chunk tables, CUB scan storage, the solver context and result, the
+// clamp counters) lives in one file-scope __device__ array sized for grids of at
+// most 64 cells per side.  Every GPU that loads this library keeps that array
+// (about 4.9 MB) until the process exits.  Calls share it and it keeps the previous
+// call's contents: each call rewrites or clears everything it reads, and calls that
+// overlap on the GPU race with each other.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "cs_device.cuh"
+#include "solver_types.cuh"
+
+namespace cs {
+void set_error(const std::string& msg);
+int sc_max_cluster_ranks();
+size_t sc_scan_temp_bytes(uint32_t codes);
+int sc_launch_solve(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, float tol, uint32_t max_pairs,
+                    uint32_t check_every, void* cub_temp, size_t cub_bytes, cudaStream_t stream, int sms);
+}  // namespace cs
+
+namespace {
+
+constexpr uint32_t kMaxSide = 64;                       // cells per grid side
+constexpr size_t kMaxCodes = (size_t)kMaxSide * kMaxSide * kMaxSide;
+constexpr size_t kCubBytes = 256 * 1024;
+constexpr size_t al(size_t n) { return (n + 255) & ~size_t(255); }
+constexpr size_t kOffCtx = 0;
+constexpr size_t kOffInfo = kOffCtx + al(sizeof(cs::Ctx));
+constexpr size_t kOffResult = kOffInfo + al(sizeof(cs::ScInfo));
+constexpr size_t kOffMetrics = kOffResult + al(sizeof(cs::ScResult));
+constexpr size_t kOffFlags = kOffMetrics + 256;
+constexpr size_t kOffScan = kOffFlags + kMaxCodes * sizeof(unsigned long long);
+constexpr size_t kOffRef = kOffScan + kMaxCodes * sizeof(unsigned long long);
+constexpr size_t kOffCellOf = kOffRef + al(kMaxCodes * sizeof(uint16_t));
+constexpr size_t kOffCub = kOffCellOf + (size_t)cs::SC_MAX_RANKS * 4096 * sizeof(uint32_t);
+constexpr size_t kScratchBytes = kOffCub + kCubBytes;
+
+static __device__ __align__(256) unsigned char g_solve_scratch[kScratchBytes];
+
+struct DeviceSlot {
+    bool ready = false;
+    unsigned char* base = nullptr;  // device address of g_solve_scratch on this device
+    int ranks = 0;
+    int sms = 0;
+};
+constexpr int kMaxDevices = 64;
+DeviceSlot g_slots[kMaxDevices];
+std::mutex g_setup;
+
+// Once per device, with that device current: the array's device address (the host
+// symbol is only a stand-in), the cluster size and the SM count.
+int setup_device(int dev, DeviceSlot** out) {
+    if (dev < 0 || dev >= kMaxDevices) {
+        cs::set_error("device ordinal out of range for the allocation-free solve");
+        return CS_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_setup);
+    DeviceSlot& s = g_slots[dev];
+    if (!s.ready) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_solve_scratch);
+        if (e != cudaSuccess) {
+            cs::set_error(std::string("cudaGetSymbolAddress(g_solve_scratch): ") + cudaGetErrorString(e));
+            return CS_ERR_CUDA;
+        }
+        if (cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cs::set_error("cudaDeviceGetAttribute(multiProcessorCount) failed");
+            return CS_ERR_CUDA;
+        }
+        s.ranks = cs::sc_max_cluster_ranks();
+        if (s.ranks == 0) {
+            cs::set_error("this device cannot launch the solver's thread-block cluster");
+            return CS_ERR_UNSUPPORTED;
+        }
+        if (cs::sc_scan_temp_bytes((uint32_t)kMaxCodes) > kCubBytes) {
+            cs::set_error("scan storage does not fit the reserved scratch");
+            return CS_ERR_CAPACITY;
+        }
+        s.base = (unsigned char*)ptr;
+        s.ready = true;
+    }
+    *out = &s;
+    return CS_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t gz, float dx, float dt, float omega,
+                                             float residual_tol, uint32_t max_pairs, uint32_t check_every,
+                                             const int32_t* kind, const float* fill, const float* div, float* p_hi,
+                                             float* p_lo, void* stream, uint32_t* pairs_out, double* residual_out) {
+    if (gx == 0 || gy == 0 || gz == 0 || gx > kMaxSide || gy > kMaxSide || gz > kMaxSide) {
+        cs::set_error("grid exceeds the allocation-free solve's scratch: at most 64 cells per side");
+        return CS_ERR_CAPACITY;
+    }
+    if (!kind || !fill || !div || !p_hi || !p_lo || !(dx > 0.0f) || !(dt > 0.0f) || !(omega > 0.0f) ||
+        !(omega < 2.0f)) {
+        cs::set_error("invalid argument to cs_pressure_solve_noalloc");
+        return CS_ERR_INVALID_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cs::set_error("no CUDA device is current");
+        return CS_ERR_NO_DEVICE;
+    }
+    DeviceSlot* slot = nullptr;
+    int rc = setup_device(dev, &slot);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char* base = slot->base;
+
+    uint32_t side = 1;
+    while (side < gx || side < gy || side < gz) side <<= 1;
+    const uint32_t codes = side * side * side;
+    const uint32_t cells = gx * gy * gz;
+
+    cs::Ctx ctx;
+    std::memset(&ctx, 0, sizeof(ctx));
+    cs::Params& u = ctx.u;
+    u.gx = gx;
+    u.gy = gy;
+    u.gz = gz;
+    u.cells = cells;
+    u.dx = dx;
+    u.inv_dx = 1.0f / dx;
+    u.dt = dt;
+    u.omega = omega;
+    u.p_clamp = cs::FP_VALUE_LIMIT - 1.0f;
+    u.fixed_point = 0;
+    // the solver reads the cell kind as lane 3 of the grid lanes
+    ctx.lanes = reinterpret_cast<int32_t*>(reinterpret_cast<uintptr_t>(kind) - 3 * (uintptr_t)cells * sizeof(int32_t));
+    ctx.fill = const_cast<float*>(fill);
+    ctx.divf = const_cast<float*>(div);
+    ctx.pf = p_hi;
+    ctx.plo = p_lo;
+    ctx.metrics = reinterpret_cast<uint32_t*>(base + kOffMetrics);
+
+    cs::ScBuffers sb;
+    sb.flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);
+    sb.scan = reinterpret_cast<unsigned long long*>(base + kOffScan);
+    sb.ref_of_cell = reinterpret_cast<uint16_t*>(base + kOffRef);
+    sb.cell_of = reinterpret_cast<uint32_t*>(base + kOffCellOf);
+    sb.info = reinterpret_cast<cs::ScInfo*>(base + kOffInfo);
+    sb.result = reinterpret_cast<cs::ScResult*>(base + kOffResult);
+
+    cudaError_t e = cudaMemcpyAsync(base + kOffCtx, &ctx, sizeof(ctx), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + kOffMetrics, 0, 256, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + kOffResult, 0, sizeof(cs::ScResult), st);
+    if (e != cudaSuccess) {
+        cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    rc = cs::sc_launch_solve(reinterpret_cast<const cs::Ctx*>(base + kOffCtx), sb, codes, slot->ranks, residual_tol,
+                             max_pairs, check_every, base + kOffCub, kCubBytes, st, slot->sms);
+    if (rc) return rc;
+    cs::ScResult res;
+    e = cudaMemcpyAsync(&res, base + kOffResult, sizeof(res), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    if (res.status == 2) {
+        cs::set_error("more fluid cells than the solver's thread-block cluster holds (16 x 4095)");
+        return CS_ERR_CAPACITY;
+    }
+    if (res.status != 1) {
+        cs::set_error("the cluster solve did not complete");
+        return CS_ERR_CUDA;
+    }
+    if (pairs_out) *pairs_out = res.sweeps;
+    if (residual_out) *residual_out = res.r1;
+    return CS_OK;
+}

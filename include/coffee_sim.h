@@ -375,6 +375,25 @@ int32_t cs_timer_stop(CsSim* sim, float* ms);        /* device ms since cs_timer
 int32_t cs_flush_l2(CsSim* sim);                     /* overwrite a buffer larger than L2 on the sim's stream */
 int32_t cs_sync(CsSim* sim);
 
+/* ---- allocation-free pressure solve (no counterpart in the reference) ----
+ * For hosts that may not call cudaMalloc while they run (an engine that reserves its
+ * whole GPU budget up front, a real-time loop that cannot afford cudaMalloc's latency
+ * and implicit synchronisation): the mixed-precision red-black SOR solve of the
+ * FP32-storage residual mode, run on the caller's device arrays of gx*gy*gz cells:
+ * kind (CELL kinds 0..4 as classify writes them), fill (liquid fill fraction),
+ * div (classify's divergence minus target), p_hi/p_lo (pressure words: warm start
+ * in, solution out).  Scratch lives in a static device array reserved when the
+ * library is loaded (about 4.9 MB per GPU, held until exit), so grids are limited to
+ * 64 cells per side and 16 x 4095 fluid cells; larger inputs return CS_ERR_CAPACITY.
+ * The first call on a device looks up that array's device address; make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU race.
+ * `stream` is a cudaStream_t (NULL = default stream); the call synchronises it and
+ * writes the red+black pair count and the final relative residual to the host. */
+int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t gz, float dx, float dt, float omega,
+                                  float residual_tol, uint32_t max_pairs, uint32_t check_every,
+                                  const int32_t* kind, const float* fill, const float* div, float* p_hi,
+                                  float* p_lo, void* stream, uint32_t* pairs_out, double* residual_out);
+
 #ifdef __cplusplus
 }
 #endif
