@@ -2174,3 +2174,36 @@ int32_t cs_timer_stop(CsSim* s, float* ms) {
 int32_t cs_flush_l2(CsSim* s) { return s ? CS_OK : fail(CS_ERR_INVALID_ARG, "null sim"); }
 int32_t cs_sync(CsSim* s) { return s ? CS_OK : fail(CS_ERR_INVALID_ARG, "null sim"); }
 }
+
+// Host-function probes for the known-answer tests (inflow.rs:244-293, bed.rs:41-82,
+// brew_config.rs:92-96).  fn: 0 kozeny_carman(a0 grind um, a1 porosity);
+// 1 effective head, speed cap, exit speed, flow rate at angle a0 for settings s;
+// 2 exit_speed_from_head(a0 head, a1 cap, s gravity/units);
+// 3 flow_rate_from_speed(a0 speed, a1 nozzle, a2 cd, a3 vol_to_ml, a4 max).
+extern "C" int32_t oracle_eval(int32_t fn, const CsSettings* s, const float* a, float* out) {
+    if (!a || !out) return fail(CS_ERR_INVALID_ARG, "null");
+    switch (fn) {
+        case 0: out[0] = kozeny_carman(a[0], a[1]); return CS_OK;
+        case 1:
+            if (!s) return fail(CS_ERR_INVALID_ARG, "null settings");
+            out[0] = effective_head(a[0], s->spout);
+            out[1] = exit_speed_cap(a[0], s->spout);
+            out[2] = exit_speed_from_head(out[0], out[1], s->standard_gravity_m_s2, s->sim_units_per_meter);
+            out[3] = flow_rate_from_speed(out[2], s->spout.nozzle_radius, s->spout.discharge_coeff,
+                                          s->spout.volume_to_ml, s->spout.max_flow_rate_ml_s);
+            return CS_OK;
+        case 2:
+            out[0] = exit_speed_from_head(a[0], a[1], s ? s->standard_gravity_m_s2 : 9.80665f,
+                                          s ? s->sim_units_per_meter : Units::sim_units_per_meter());
+            return CS_OK;
+        case 3: out[0] = flow_rate_from_speed(a[0], a[1], a[2], a[3], a[4]); return CS_OK;
+    }
+    return fail(CS_ERR_INVALID_ARG, "unknown probe");
+}
+
+// BedConfig::seated_in_filter (bed.rs:41-82) for an arbitrary filter.
+extern "C" int32_t oracle_bed_seated(const CsFilter* f, CsBed* out) {
+    if (!f || !out) return fail(CS_ERR_INVALID_ARG, "null");
+    *out = bed_seated_in_filter(*f);
+    return CS_OK;
+}
