@@ -104,6 +104,19 @@ def build_scene(lib, args, device=0):
     return sim
 
 
+def ncu_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu summary
+    (a line `dram_bytes_per_launch = N` in profiles/<kernel>_*.md), or None."""
+    for f in sorted((ROOT / "profiles").glob(f"{kernel}_*.md")):
+        for ln in f.read_text().splitlines():
+            if ln.strip().startswith("dram_bytes_per_launch"):
+                try:
+                    return float(ln.split("=", 1)[1].strip().split()[0])
+                except (IndexError, ValueError):
+                    return None
+    return None
+
+
 def algorithmic_bytes(n_p, n_c, pairs, evals, n_bed):
     """Compulsory bytes of one substep: 172 N_p + 134 N_c + 17 K N_c + 13 E N_c, plus
     4 N_c + 200 N_bed with a bed."""
@@ -246,24 +259,29 @@ def main():
         e2e_s = float(t.item())
     e2e_value = n_p * args.steps * world / e2e_s
 
-    # ---- roofline of the dominant kernel (the red-black sweep) ----
+    # ---- roofline of the dominant kernel ----
+    # The cluster-resident solve (k_sc_solve) is one launch per substep and the only
+    # launch of the sweep phase; its algorithmic bytes are those of the sweeps and
+    # residual checks it performs: 17 B/cell/pair + 13 B/cell/evaluation on the dense
+    # grid.  If the per-colour path ran instead, the kernel is k_refine_sweep (one
+    # colour launch = half a pair, 8.5 B/cell).
     peak, peak_kind = load_peaks()
     sweep_ms = prof.phase_ms[4]
     sweep_launches = max(prof.phase_launches[4], 1)
-    per_launch_bytes = 8.5 * n_c  # 17 B per cell per red+black pair, half per colour launch
-    achieved = per_launch_bytes / (sweep_ms * 1e-3 / sweep_launches) / 1e9 if sweep_ms > 0 else 0.0
     pairs_per_step = prof.sweeps / max(prof.substeps, 1)
     evals_per_step = prof.residual_evals / max(prof.substeps, 1)
+    cluster = prof.phase_launches[4] == prof.substeps
+    if cluster:
+        kernel = "k_sc_solve"
+        per_launch_bytes = (17.0 * prof.sweeps + 13.0 * prof.residual_evals) * n_c / sweep_launches
+    else:
+        kernel = "k_refine_sweep"
+        per_launch_bytes = 8.5 * n_c
+    launch_ms = sweep_ms / sweep_launches
+    achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9 if sweep_ms > 0 else 0.0
     step_bytes = algorithmic_bytes(n_p, n_c, pairs_per_step, evals_per_step, n_bed)
-    step_gbs = step_bytes / (total_ms / args.steps * 1e-3) / 1e9 * (1 if world == 1 else 1)
-
-    traffic = None
-    tf = ROOT / "profiles" / "rbgs_sweep_traffic.json"
-    if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    step_gbs = step_bytes / (total_ms / args.steps * 1e-3) / 1e9
+    traffic = ncu_traffic(kernel)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -280,10 +298,13 @@ def main():
         "phase_ms_per_step": {n: prof.phase_ms[i] / max(prof.substeps, 1)
                               for i, n in enumerate(["emit", "clear", "p2g", "grid", "sweeps", "residual",
                                                      "project", "g2p", "bed", "render"])},
-        "roofline": {"bound": "hbm", "kernel": "k_refine_sweep (one colour)", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": launch_ms,
+                     "launches": int(prof.phase_launches[4]),
+                     "step_algorithmic_bytes": step_bytes,
                      "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": prof_e2e.h2d_bytes / args.steps,

@@ -114,42 +114,12 @@ int Engine::init() {
         while (side < settings.grid_dims[0] || side < settings.grid_dims[1] || side < settings.grid_dims[2]) side <<= 1;
         sc_codes_ = (size_t)side * side * side;
     }
-    if ((rc = alloc(sc_flags_, sc_codes_ * sizeof(unsigned long long)))) return rc;
-    if ((rc = alloc(sc_scan_, sc_codes_ * sizeof(unsigned long long)))) return rc;
-    if ((rc = alloc(sc_ref_, cells_ * sizeof(uint16_t)))) return rc;
-    if ((rc = alloc(sc_cell_, (size_t)SC_MAX_RANKS * 4096 * sizeof(uint32_t)))) return rc;
-    if ((rc = alloc(sc_info_, sizeof(ScInfo)))) return rc;
-    if ((rc = alloc(sc_result_, sizeof(ScResult)))) return rc;
     {
-        size_t temp = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, temp, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                      (int)sc_codes_, stream_);
-        if ((rc = alloc(sc_temp_, temp))) return rc;
-        sc_ranks_ = 0;
-        if (cudaFuncSetAttribute(k_sc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ScLayout::bytes) ==
-                cudaSuccess &&
-            cudaFuncSetAttribute(k_sc_solve, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
-            for (int r : {16, 8}) {
-                cudaLaunchConfig_t cfg = {};
-                cfg.gridDim = dim3(r, 1, 1);
-                cfg.blockDim = dim3(SC_THREADS, 1, 1);
-                cfg.dynamicSmemBytes = ScLayout::bytes;
-                cudaLaunchAttribute attr;
-                attr.id = cudaLaunchAttributeClusterDimension;
-                attr.val.clusterDim.x = r;
-                attr.val.clusterDim.y = 1;
-                attr.val.clusterDim.z = 1;
-                cfg.attrs = &attr;
-                cfg.numAttrs = 1;
-                int nclusters = 0;
-                if (cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_sc_solve, &cfg) == cudaSuccess &&
-                    nclusters > 0) {
-                    sc_ranks_ = r;
-                    break;
-                }
-            }
-        }
-        cudaGetLastError();  // clear a refused attribute or occupancy query
+        const size_t cub = sc_scan_temp_bytes((uint32_t)sc_codes_);
+        const ScScratch lay = sc_scratch_layout(cells_, sc_codes_, cub);
+        if ((rc = alloc(sc_scratch_, lay.total))) return rc;
+        sc_buf_ = sc_buffers_at((unsigned char*)sc_scratch_.ptr, lay, cub);
+        sc_ranks_ = sc_max_cluster_ranks();
     }
 
     ctx_.pos = (float4*)pos_.ptr;
@@ -368,43 +338,19 @@ double Engine::refine_residual() {
 int Engine::solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done) {
     done = false;
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
-    ScBuffers sb;
-    sb.flags = (unsigned long long*)sc_flags_.ptr;
-    sb.scan = (unsigned long long*)sc_scan_.ptr;
-    sb.ref_of_cell = (uint16_t*)sc_ref_.ptr;
-    sb.cell_of = (uint32_t*)sc_cell_.ptr;
-    sb.info = (ScInfo*)sc_info_.ptr;
-    sb.result = (ScResult*)sc_result_.ptr;
     const uint32_t codes = (uint32_t)sc_codes_;
-    const int cb = (int)std::min<size_t>((sc_codes_ + kThreads - 1) / kThreads, (size_t)sms_ * 16);
     mark(CS_PHASE_RESIDUAL);
-    k_sc_flags<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, sb, codes);
-    size_t temp = sc_temp_.bytes;
-    cub::DeviceScan::ExclusiveSum(sc_temp_.ptr, temp, sb.flags, sb.scan, (int)codes, stream_);
-    k_sc_totals<<<dim3(1, 1), 1, 0, stream_>>>(dc, sb, (uint32_t)sc_ranks_, codes);
-    k_sc_starts<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, sb, codes);
-    k_sc_map<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, sb, codes);
-    count_launch(4);
-    mark(CS_PHASE_SWEEPS);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(sc_ranks_, 1, 1);
-    cfg.blockDim = dim3(SC_THREADS, 1, 1);
-    cfg.dynamicSmemBytes = ScLayout::bytes;
-    cfg.stream = stream_;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeClusterDimension;
-    attr.val.clusterDim.x = sc_ranks_;
-    attr.val.clusterDim.y = 1;
-    attr.val.clusterDim.z = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    const CsSettings& s = settings;
-    int rc = check(cudaLaunchKernelEx(&cfg, k_sc_solve, dc, sb, s.residual_tol, s.max_sweeps, s.check_every),
-                   "cluster solve launch");
+    int rc = sc_launch_prep(dc, sc_buf_, codes, sc_ranks_, 1, stream_, sms_);
     if (rc) return rc;
+    count_launch(kScPrepLaunches);
+    mark(CS_PHASE_SWEEPS);
+    const CsSettings& s = settings;
+    if ((rc = sc_launch_cluster(dc, sc_buf_, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every, stream_)))
+        return rc;
     count_launch();
     ScResult res;
-    if ((rc = check(cudaMemcpyAsync(&res, sc_result_.ptr, sizeof(res), cudaMemcpyDeviceToHost, stream_), "solve result")))
+    if ((rc = check(cudaMemcpyAsync(&res, sc_buf_.result, sizeof(res), cudaMemcpyDeviceToHost, stream_),
+                    "solve result")))
         return rc;
     prof_.d2h_bytes += sizeof(res);
     if ((rc = sync())) return rc;
@@ -883,7 +829,7 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
     return sync();
 }
 
-// ---- launch helpers for callers outside Engine (noalloc.cu) ----
+// ---- launch helpers shared by Engine and noalloc.cu ----
 // Largest cluster size the solve kernel can be launched with on the current device
 // (16 with the non-portable opt-in, else 8), 0 when neither fits.
 int sc_max_cluster_ranks() {
@@ -919,21 +865,38 @@ size_t sc_scan_temp_bytes(uint32_t codes) {
     return temp;
 }
 
-// The launch sequence of Engine::solve_cluster on caller-provided memory.
-int sc_launch_solve(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, float tol, uint32_t max_pairs,
-                    uint32_t check_every, void* cub_temp, size_t cub_bytes, cudaStream_t stream, int sms) {
+// Morton scan, chunking, neighbour slots, halo/send lists and coefficients for
+// `instances` solves whose scratch blocks lie back to back (kScPrepLaunches launches
+// for one instance).
+int sc_launch_prep(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, uint32_t instances,
+                   cudaStream_t stream, int sms) {
     const int cb = (int)std::min<size_t>((codes + kThreads - 1) / kThreads, (size_t)sms * 16);
-    k_sc_flags<<<dim3(cb, 1), kThreads, 0, stream>>>(d_ctx, sb, codes);
-    size_t temp = cub_bytes;
-    if (cub::DeviceScan::ExclusiveSum(cub_temp, temp, sb.flags, sb.scan, (int)codes, stream) != cudaSuccess) {
-        set_error("scan launch failed");
+    k_sc_flags<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    for (uint32_t k = 0; k < instances; ++k) {
+        const ScBuffers b = sc_instance(sb, k);
+        size_t temp = b.cub_bytes;
+        if (cub::DeviceScan::ExclusiveSum(b.cub_temp, temp, b.flags, b.scan, (int)codes, stream) != cudaSuccess) {
+            set_error("scan launch failed");
+            return CS_ERR_CUDA;
+        }
+    }
+    k_sc_totals<<<dim3(1, instances), 1, 0, stream>>>(d_ctx, sb, (uint32_t)ranks, codes);
+    k_sc_starts<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    k_sc_map<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    k_sc_halo<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("solver prep launch: ") + cudaGetErrorString(e));
         return CS_ERR_CUDA;
     }
-    k_sc_totals<<<dim3(1, 1), 1, 0, stream>>>(d_ctx, sb, (uint32_t)ranks, codes);
-    k_sc_starts<<<dim3(cb, 1), kThreads, 0, stream>>>(d_ctx, sb, codes);
-    k_sc_map<<<dim3(cb, 1), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    return CS_OK;
+}
+
+// The cluster solve of `instances` independent systems: one cluster of `ranks` CTAs each.
+int sc_launch_cluster(const Ctx* d_ctx, const ScBuffers& sb, int ranks, uint32_t instances, float tol,
+                      uint32_t max_pairs, uint32_t check_every, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(ranks, 1, 1);
+    cfg.gridDim = dim3(ranks, instances, 1);
     cfg.blockDim = dim3(SC_THREADS, 1, 1);
     cfg.dynamicSmemBytes = ScLayout::bytes;
     cfg.stream = stream;

@@ -8,6 +8,7 @@
 
 #include "cs_device.cuh"
 #include "host_scene.h"
+#include "solver_launch.h"
 
 namespace cs {
 
@@ -73,7 +74,8 @@ private:
     DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, plo_, pd_, gres_, lookup_, sdf_, cls_, metrics_, resid_;
     DeviceBuffer staging_;  // AoS upload/readback staging
     // cluster-resident solver
-    DeviceBuffer sc_flags_, sc_scan_, sc_ref_, sc_cell_, sc_info_, sc_result_, sc_temp_;
+    DeviceBuffer sc_scratch_;  // every solver scratch buffer, laid out by sc_scratch_layout
+    ScBuffers sc_buf_{};
     int sc_ranks_ = 0;      // cluster size usable for the solve (0 = unavailable)
     size_t sc_codes_ = 0;   // Morton codes covering the grid (power-of-two cube)
     int solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done);

@@ -22,32 +22,18 @@
 #include <string>
 
 #include "cs_device.cuh"
-#include "solver_types.cuh"
-
-namespace cs {
-void set_error(const std::string& msg);
-int sc_max_cluster_ranks();
-size_t sc_scan_temp_bytes(uint32_t codes);
-int sc_launch_solve(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, float tol, uint32_t max_pairs,
-                    uint32_t check_every, void* cub_temp, size_t cub_bytes, cudaStream_t stream, int sms);
-}  // namespace cs
+#include "solver_launch.h"
 
 namespace {
 
 constexpr uint32_t kMaxSide = 64;                       // cells per grid side
 constexpr size_t kMaxCodes = (size_t)kMaxSide * kMaxSide * kMaxSide;
 constexpr size_t kCubBytes = 256 * 1024;
-constexpr size_t al(size_t n) { return (n + 255) & ~size_t(255); }
 constexpr size_t kOffCtx = 0;
-constexpr size_t kOffInfo = kOffCtx + al(sizeof(cs::Ctx));
-constexpr size_t kOffResult = kOffInfo + al(sizeof(cs::ScInfo));
-constexpr size_t kOffMetrics = kOffResult + al(sizeof(cs::ScResult));
-constexpr size_t kOffFlags = kOffMetrics + 256;
-constexpr size_t kOffScan = kOffFlags + kMaxCodes * sizeof(unsigned long long);
-constexpr size_t kOffRef = kOffScan + kMaxCodes * sizeof(unsigned long long);
-constexpr size_t kOffCellOf = kOffRef + al(kMaxCodes * sizeof(uint16_t));
-constexpr size_t kOffCub = kOffCellOf + (size_t)cs::SC_MAX_RANKS * 4096 * sizeof(uint32_t);
-constexpr size_t kScratchBytes = kOffCub + kCubBytes;
+constexpr size_t kOffMetrics = kOffCtx + cs::sc_align(sizeof(cs::Ctx));
+constexpr size_t kOffSolver = kOffMetrics + 256;
+constexpr cs::ScScratch kSolver = cs::sc_scratch_layout(kMaxCodes, kMaxCodes, kCubBytes);
+constexpr size_t kScratchBytes = kOffSolver + kSolver.total;
 
 static __device__ __align__(256) unsigned char g_solve_scratch[kScratchBytes];
 
@@ -149,33 +135,28 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
     ctx.plo = p_lo;
     ctx.metrics = reinterpret_cast<uint32_t*>(base + kOffMetrics);
 
-    cs::ScBuffers sb;
-    sb.flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);
-    sb.scan = reinterpret_cast<unsigned long long*>(base + kOffScan);
-    sb.ref_of_cell = reinterpret_cast<uint16_t*>(base + kOffRef);
-    sb.cell_of = reinterpret_cast<uint32_t*>(base + kOffCellOf);
-    sb.info = reinterpret_cast<cs::ScInfo*>(base + kOffInfo);
-    sb.result = reinterpret_cast<cs::ScResult*>(base + kOffResult);
+    const cs::ScBuffers sb = cs::sc_buffers_at(base + kOffSolver, kSolver, kCubBytes);
+    const cs::Ctx* dctx = reinterpret_cast<const cs::Ctx*>(base + kOffCtx);
 
     cudaError_t e = cudaMemcpyAsync(base + kOffCtx, &ctx, sizeof(ctx), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + kOffMetrics, 0, 256, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(base + kOffResult, 0, sizeof(cs::ScResult), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sb.result, 0, sizeof(cs::ScResult), st);
     if (e != cudaSuccess) {
         cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
         return CS_ERR_CUDA;
     }
-    rc = cs::sc_launch_solve(reinterpret_cast<const cs::Ctx*>(base + kOffCtx), sb, codes, slot->ranks, residual_tol,
-                             max_pairs, check_every, base + kOffCub, kCubBytes, st, slot->sms);
-    if (rc) return rc;
+    if ((rc = cs::sc_launch_prep(dctx, sb, codes, slot->ranks, 1, st, slot->sms))) return rc;
+    if ((rc = cs::sc_launch_cluster(dctx, sb, slot->ranks, 1, residual_tol, max_pairs, check_every, st))) return rc;
     cs::ScResult res;
-    e = cudaMemcpyAsync(&res, base + kOffResult, sizeof(res), cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(&res, sb.result, sizeof(res), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
         return CS_ERR_CUDA;
     }
     if (res.status == 2) {
-        cs::set_error("more fluid cells than the solver's thread-block cluster holds (16 x 4095)");
+        cs::set_error("the fluid cells exceed what the solver's thread-block cluster holds "
+                      "(16 x 4095 cells, 4095 halo cells per CTA)");
         return CS_ERR_CAPACITY;
     }
     if (res.status != 1) {

@@ -5,18 +5,25 @@
 //
 // Layout.  Fluid cells are numbered by an exclusive scan in Morton order and cut into
 // R contiguous chunks (R = cluster size, chunk <= SC_CAP cells); inside a chunk the
-// red cells (ix+iy+iz even) come first.  Every cell carries, in the shared memory of
-// the CTA that owns it: the correction d and its fill code (float2; fill code 2.0
-// marks a bed-coupled cell), the residual g, the fp32 face-weight sum W, the pressure
-// hi/lo words, dx^2*rhs, six 16-bit neighbour references (rank << 12 | local index,
-// 0xFFFF = no fluid neighbour) and the number of air faces.  Neighbours owned by
-// another CTA are read through distributed shared memory.
+// red cells (ix+iy+iz even) come first.  Each CTA keeps, for the cells it owns: the
+// correction d and the fill code (fill code 2.0 marks a bed-coupled cell), the
+// residual g, 1/W, the pressure hi/lo words, dx^2*rhs, the flags byte and the six
+// neighbour slots (13-bit slot indices packed two per word).  A neighbour owned by
+// another CTA is read from a halo slot of the same correction array; after sweeping a
+// colour, each CTA pushes the new values of its cells that other CTAs hold as halo
+// with posted DSMEM stores, and the cluster barrier that separates the colours
+// publishes them.  A face without a fluid
+// neighbour points at a slot that always holds zero, so the sweep has no per-face
+// branches and every load in it is a local shared-memory load.
+//
+// The prep kernels (k_sc_flags .. k_sc_halo) run on the whole GPU: Morton scan and
+// chunking, neighbour slots, halo and send lists, and the per-cell coefficients.
 //
 // Arithmetic is that of k_refine_residual / k_refine_sweep / k_refine_accumulate,
 // operation for operation (face order -x,+x,-y,+y,-z,+z; weights of fluid faces
-// recomputed from fill codes; the FP64 weight sum is exact because it adds at most
-// six floats in (0,1]), so the result equals the per-colour-launch solve bit for bit
-// except for the order of the FP64 norm reductions.
+// recomputed from fill codes; a missing face adds an exact zero; the FP64 weight sum
+// is exact because it adds at most six floats in (0,1]), so the result equals the
+// per-colour-launch solve except for the order of the FP64 norm reductions.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -27,22 +34,15 @@
 namespace cs {
 namespace cg = cooperative_groups;
 
-// Distributed shared memory through 32-bit cluster addresses.  The loads are volatile
-// so they stay between the cluster barriers that order them.
+// Distributed shared memory through 32-bit cluster addresses.  The accesses are
+// volatile so they stay between the cluster barriers that order them.
 __device__ __forceinline__ uint32_t sc_mapa(uint32_t addr, uint32_t rank) {
     uint32_t r;
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
     return r;
 }
-__device__ __forceinline__ float2 sc_ld2(uint32_t addr) {
-    float2 v;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
-    return v;
-}
-__device__ __forceinline__ float sc_ld(uint32_t addr) {
-    float v;
-    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
-    return v;
+__device__ __forceinline__ void sc_st(uint32_t addr, float v) {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
 }
 
 // Cells are numbered along a Morton (Z-order) curve over the grid padded to a power
@@ -64,7 +64,8 @@ __device__ __forceinline__ bool sc_cell_of_code(const Params& u, uint32_t m, uin
     return true;
 }
 
-__global__ void k_sc_flags(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t codes) {
+__global__ void k_sc_flags(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t codes) {
+    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const int32_t* kl = c.lanes + 3 * (size_t)u.cells;
@@ -77,7 +78,8 @@ __global__ void k_sc_flags(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t co
 }
 
 // Totals and chunking (one thread), then the red count before each chunk's first cell.
-__global__ void k_sc_totals(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t ranks, uint32_t codes) {
+__global__ void k_sc_totals(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t ranks, uint32_t codes) {
+    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
     unsigned long long last = sb.scan[codes - 1] + sb.flags[codes - 1];
     uint32_t nf = (uint32_t)(last & 0xffffffffull), nr = (uint32_t)(last >> 32);
     uint32_t chunk = (nf + ranks - 1) / ranks;
@@ -86,9 +88,11 @@ __global__ void k_sc_totals(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t r
     sb.info->chunk = chunk;
     sb.info->overflow = chunk > (uint32_t)SC_CAP ? 1u : 0u;
     for (uint32_t r = 0; r <= SC_MAX_RANKS; ++r) sb.info->red_before[r] = nr;
+    for (int k = 0; k < SC_COUNTS; ++k) sb.counts[k] = 0u;
 }
 
-__global__ void k_sc_starts(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t codes) {
+__global__ void k_sc_starts(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t codes) {
+    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
     const uint32_t chunk = sb.info->chunk;
     if (chunk == 0) return;
     CS_FOR(m, codes) {
@@ -98,7 +102,8 @@ __global__ void k_sc_starts(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t c
     }
 }
 
-__global__ void k_sc_map(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t codes) {
+__global__ void k_sc_map(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t codes) {
+    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const ScInfo& inf = *sb.info;
@@ -123,6 +128,101 @@ __global__ void k_sc_map(const Ctx* __restrict__ cp, ScBuffers sb, uint32_t code
     }
 }
 
+// Neighbour slots, halo and send lists, and coefficients of every fluid cell.  A face
+// toward a cell of the same CTA gets that cell's local slot, a face without a fluid
+// neighbour gets SC_DUMMY, and a face toward another CTA's cell gets the halo slot the
+// neighbour allocated for it: each cell takes one halo slot in every other CTA that
+// owns one of its neighbours, writes that slot into those neighbours' face entries
+// (face f of this cell is face f^1 of the neighbour) and adds itself to its own CTA's
+// send list for its colour.  Validity of a fluid face is symmetric (face_weight of
+// two fluid cells is 1 or min of the fills), so both sides agree on which faces exist.
+// Halo slot order comes from atomics and differs between runs; it only places copies.
+__global__ void k_sc_halo(const Ctx* __restrict__ cp, ScBuffers sb0) {
+    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const ScInfo& inf = *sb.info;
+    if (inf.overflow || inf.chunk == 0) return;
+    const int32_t* kl = c.lanes + 3 * (size_t)u.cells;
+    const uint32_t sy = u.gx, sz = u.gx * u.gy;
+    CS_FOR(ci, u.cells) {
+        const uint16_t rc = sb.ref_of_cell[ci];
+        if (rc == SC_NONE) continue;
+        const uint32_t r = rc >> 12, i = rc & 4095u;
+        uint32_t ix, iy, iz;
+        decompose(u, ci, ix, iy, iz);
+        const uint32_t par = (ix + iy + iz) & 1u;
+        const int32_t kind = kl[ci];
+        const float sf = c.fill[ci];
+        const float fci = kind == CELL_BED ? 2.0f : sf;
+        float W = 0.0f;
+        uint32_t na = 0;
+        bool unit = true;
+        const bool in[6] = {ix > 0, ix + 1 < u.gx, iy > 0, iy + 1 < u.gy, iz > 0, iz + 1 < u.gz};
+        const uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
+        uint32_t fq[6], fj[6];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            uint32_t e = SC_DUMMY;
+            fq[f] = 0xffu;
+            fj[f] = 0u;
+            if (in[f]) {
+                const uint32_t ni = ci + off[f];
+                const int32_t nk = kl[ni];
+                if (!is_solid(nk)) {
+                    const float w = face_weight(kind, sf, nk, c.fill[ni]);
+                    if (w > 0.0f) {
+                        W += w;
+                        if (is_fluid(nk)) {
+                            const uint16_t rn = sb.ref_of_cell[ni];
+                            unit = unit && (w == 1.0f);
+                            if ((uint32_t)(rn >> 12) == r) {
+                                e = rn & 4095u;
+                            } else {
+                                fq[f] = rn >> 12;
+                                fj[f] = rn & 4095u;
+                                e = 0xffffffffu;  // written by the neighbour
+                            }
+                        } else {
+                            ++na;
+                        }
+                    }
+                }
+            }
+            if (e != 0xffffffffu) sb.slot_ref[(((size_t)r * 3 + (f >> 1)) * 4096 + i) * 2 + (f & 1)] = (uint16_t)e;
+        }
+        // one halo slot per distinct foreign owner
+        uint32_t hs[6];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            hs[f] = 0xffffffffu;
+            if (fq[f] == 0xffu) continue;
+            for (int g = 0; g < f; ++g)
+                if (fq[g] == fq[f]) hs[f] = hs[g];
+            if (hs[f] == 0xffffffffu) {
+                const uint32_t q = fq[f];
+                const uint32_t h = atomicAdd(&sb.counts[q], 1u);
+                hs[f] = h;
+                if (h < (uint32_t)SC_HALO) {
+                    sb.halo_fill[(size_t)q * SC_HALO + h] = fci;
+                    const uint32_t e = atomicAdd(&sb.counts[SC_MAX_RANKS + r * 2 + par], 1u);
+                    if (e < (uint32_t)SC_SEND) sb.send[((size_t)r * 2 + par) * SC_SEND + e] = i | (q << 12) | (h << 16);
+                }
+            }
+            const uint32_t g = f ^ 1;  // the neighbour's face toward this cell
+            sb.slot_ref[(((size_t)fq[f] * 3 + (g >> 1)) * 4096 + fj[f]) * 2 + (g & 1)] =
+                (uint16_t)(hs[f] < (uint32_t)SC_HALO ? SC_HALO0 + hs[f] : SC_DUMMY);
+        }
+        const float rhs = div_load(c, ci) * sf / wmax(u.dt, 1e-6f);
+        bool sent = false;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) sent = sent || fq[f] != 0xffu;
+        const uint32_t fl = na | (sent ? SC_SENT : 0u) | (unit ? SC_UNIT : 0u) | (W > 0.0f ? 0u : SC_EMPTY);
+        sb.slot_coef[(size_t)r * 4096 + i] =
+            make_float4(W > 0.0f ? 1.0f / W : 0.0f, fci, u.dx * u.dx * rhs, __uint_as_float(fl));
+    }
+}
+
 template <class T>
 __device__ __forceinline__ T* sc_arr(unsigned char* base, size_t off) {
     return reinterpret_cast<T*>(base + off);
@@ -135,208 +235,218 @@ __device__ __forceinline__ float sc_weight(float fc_i, float fc_j) {
 
 // One cluster per instance (blockIdx.y); R = cluster size along x.
 __global__ void __launch_bounds__(SC_THREADS, 1)
-    k_sc_solve(const Ctx* __restrict__ cp, ScBuffers sb, float tol, uint32_t max_pairs, uint32_t check_every) {
+    k_sc_solve(const Ctx* __restrict__ cp, ScBuffers sb0, float tol, uint32_t max_pairs, uint32_t check_every) {
     extern __shared__ __align__(16) unsigned char smem[];
     cg::cluster_group cluster = cg::this_cluster();
+    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const uint32_t R = cluster.num_blocks();
     const uint32_t rank = cluster.block_rank();
     const ScInfo& inf = *sb.info;
-    if (inf.overflow) {
+    // capacity: every rank reads the same counters, so the exit is uniform
+    bool over = inf.overflow != 0u;
+    for (uint32_t q = 0; q < R; ++q)
+        over = over || sb.counts[q] > (uint32_t)SC_HALO || sb.counts[SC_MAX_RANKS + 2 * q] > (uint32_t)SC_SEND ||
+               sb.counts[SC_MAX_RANKS + 2 * q + 1] > (uint32_t)SC_SEND;
+    if (over) {
         if (rank == 0 && threadIdx.x == 0) sb.result->status = 2;
-        return;  // uniform across the cluster: every rank reads the same flag
+        return;
     }
     const uint32_t chunk = inf.chunk;
     const uint32_t start = rank * chunk;
     const uint32_t n_loc = (chunk == 0 || start >= inf.n_fluid) ? 0u : min(chunk, inf.n_fluid - start);
     const uint32_t n_red = inf.red_before[rank + 1] - inf.red_before[rank];
+    const uint32_t n_halo = sb.counts[rank];
+    const uint32_t n_send[2] = {sb.counts[SC_MAX_RANKS + 2 * rank], sb.counts[SC_MAX_RANKS + 2 * rank + 1]};
 
-    float2* dfill = sc_arr<float2>(smem, ScLayout::dfill);
+    float* dval = sc_arr<float>(smem, ScLayout::dval);
+    float* fcode = sc_arr<float>(smem, ScLayout::fcode);
     float* gg = sc_arr<float>(smem, ScLayout::g);
     float* invW = sc_arr<float>(smem, ScLayout::invW);
     float* ph = sc_arr<float>(smem, ScLayout::ph);
     float* pl = sc_arr<float>(smem, ScLayout::pl);
     float* bb = sc_arr<float>(smem, ScLayout::b);
-    uint16_t* ref = sc_arr<uint16_t>(smem, ScLayout::ref);
+    uint32_t* ref = sc_arr<uint32_t>(smem, ScLayout::ref);
+    uint32_t* snd = sc_arr<uint32_t>(smem, ScLayout::snd);
     uint8_t* flg = sc_arr<uint8_t>(smem, ScLayout::flags);
     double* part = sc_arr<double>(smem, ScLayout::part);
     double* red = sc_arr<double>(smem, ScLayout::red);
-    const uint32_t a_dfill = (uint32_t)__cvta_generic_to_shared(dfill);
-    const uint32_t a_ph = (uint32_t)__cvta_generic_to_shared(ph);
-    const uint32_t a_pl = (uint32_t)__cvta_generic_to_shared(pl);
-
-    const int32_t* kl = c.lanes + 3 * (size_t)u.cells;
+    const uint32_t a_dval = (uint32_t)__cvta_generic_to_shared(dval);
+    const uint32_t* cell_of = sb.cell_of + rank * 4096u;
     const uint32_t sy = u.gx, sz = u.gx * u.gy;
 
-    // ---- set-up: coefficients of the cells this CTA owns ----
-    for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x) {
-        uint32_t ci = sb.cell_of[rank * 4096u + i];
-        uint32_t ix, iy, iz;
-        decompose(u, ci, ix, iy, iz);
-        int32_t kind = kl[ci];
-        float sf = c.fill[ci];
-        float fci = kind == CELL_BED ? 2.0f : sf;
-        float W = 0.0f;
-        uint32_t na = 0;
-        bool unit = true;
-        bool in[6] = {ix > 0, ix + 1 < u.gx, iy > 0, iy + 1 < u.gy, iz > 0, iz + 1 < u.gz};
-        uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            uint16_t r = SC_NONE;
-            if (in[f]) {
-                uint32_t ni = ci + off[f];
-                int32_t nk = kl[ni];
-                if (!is_solid(nk)) {
-                    float w = face_weight(kind, sf, nk, c.fill[ni]);
-                    if (w > 0.0f) {
-                        W += w;
-                        if (is_fluid(nk)) {
-                            r = sb.ref_of_cell[ni];
-                            unit = unit && (w == 1.0f);
-                        } else {
-                            ++na;
-                        }
-                    }
-                }
-            }
-            ref[i * 6 + f] = r;
+    // ---- set-up: copy this CTA's slice of the prep tables into shared memory ----
+    {
+        const float4* coef = sb.slot_coef + rank * 4096u;
+        const uint32_t* sref = reinterpret_cast<const uint32_t*>(sb.slot_ref) + rank * 3u * 4096u;
+        for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x) {
+            const float4 k = coef[i];
+            const uint32_t fl = __float_as_uint(k.w);
+            invW[i] = k.x;
+            dval[i] = 0.0f;
+            fcode[i] = k.y;
+            bb[i] = k.z;
+            flg[i] = (uint8_t)fl;
+            ref[i] = sref[i] | ((fl & SC_UNIT) ? SC_REF_UNIT : 0u);
+            ref[4096 + i] = sref[4096 + i];
+            ref[8192 + i] = sref[8192 + i];
+            const uint32_t ci = cell_of[i];
+            ph[i] = c.pf[ci];
+            pl[i] = c.plo[ci];
         }
-        invW[i] = W > 0.0f ? 1.0f / W : 0.0f;
-        flg[i] = (uint8_t)(na | (unit ? SC_UNIT : 0) | (W > 0.0f ? 0 : SC_EMPTY));
-        dfill[i] = make_float2(0.0f, fci);
-        ph[i] = c.pf[ci];
-        pl[i] = c.plo[ci];
-        float rhs = div_load(c, ci) * sf / wmax(u.dt, 1e-6f);
-        bb[i] = u.dx * u.dx * rhs;
+        const float* hf = sb.halo_fill + (size_t)rank * SC_HALO;
+        for (uint32_t h = threadIdx.x; h < n_halo; h += blockDim.x) {
+            dval[SC_HALO0 + h] = 0.0f;
+            fcode[SC_HALO0 + h] = hf[h];
+        }
+        if (threadIdx.x == 0) {
+            dval[SC_DUMMY] = 0.0f;
+            fcode[SC_DUMMY] = 0.0f;
+        }
+        for (uint32_t col = 0; col < 2; ++col) {
+            const uint32_t* src = sb.send + ((size_t)rank * 2 + col) * SC_SEND;
+            for (uint32_t e = threadIdx.x; e < n_send[col]; e += blockDim.x) snd[col * SC_SEND + e] = src[e];
+        }
     }
     cluster.sync();
 
-    // FP64 residual of the current pressure; g <- residual, d <- 0.  Returns the
-    // relative norm, identical in every rank (partials summed in rank order).
+    // FP64 residual of the current pressure; g <- residual, d <- 0 (halo copies too).
+    // Neighbour pressures come from this CTA's shared memory or, for halo cells, from
+    // the global pressure arrays that accumulate() keeps current for every cell held
+    // as halo.  Each CTA pushes its partial sums into every rank's shared memory, so
+    // after the barrier all ranks add the same values in the same order and take the
+    // same stop decision.
     auto residual = [&](int slot) -> double {
         double r2 = 0.0, b2 = 0.0;
         for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x) {
-            dfill[i].x = 0.0f;
-            uint8_t fl = flg[i];
+            dval[i] = 0.0f;
+            const uint8_t fl = flg[i];
             if (fl & SC_EMPTY) {
                 gg[i] = 0.0f;
                 continue;
             }
-            float fci = dfill[i].y;
-            float sfi = fci > 1.5f ? 1.0f : fci;
+            const float fci = fcode[i];
+            const float sfi = fci > 1.5f ? 1.0f : fci;
             double wsum = (double)(fl & 7u) * (double)sfi;
             double psum = 0.0;
-            const uint32_t* rp = reinterpret_cast<const uint32_t*>(ref + i * 6);
-            uint32_t rw[3] = {rp[0], rp[1], rp[2]};
+            const uint32_t ci = cell_of[i];
+            const uint32_t rw[3] = {ref[i], ref[4096 + i], ref[8192 + i]};
+            const uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
 #pragma unroll
             for (int f = 0; f < 6; ++f) {
-                uint32_t r = (rw[f >> 1] >> ((f & 1) * 16)) & 0xffffu;
-                if (r == SC_NONE) continue;
-                uint32_t rr = r >> 12, j = r & 4095u;
-                float fcj = sc_ld2(sc_mapa(a_dfill + j * 8u, rr)).y;
-                float w = sc_weight(fci, fcj);
-                double pj = (double)sc_ld(sc_mapa(a_ph + j * 4u, rr)) + (double)sc_ld(sc_mapa(a_pl + j * 4u, rr));
+                const uint32_t r = (rw[f >> 1] >> ((f & 1) * 16)) & SC_SLOT_MASK;
+                if (r == SC_DUMMY) continue;
+                const float w = sc_weight(fci, fcode[r]);
+                double pj;
+                if (r < (uint32_t)SC_HALO0) {
+                    pj = (double)ph[r] + (double)pl[r];
+                } else {
+                    const uint32_t nj = ci + off[f];
+                    pj = (double)__ldcg(c.pf + nj) + (double)__ldcg(c.plo + nj);
+                }
                 wsum += (double)w;
                 psum += (double)w * pj;
             }
-            double b = (double)bb[i];
-            double r = (psum - b) - wsum * ((double)ph[i] + (double)pl[i]);
+            const double b = (double)bb[i];
+            const double r = (psum - b) - wsum * ((double)ph[i] + (double)pl[i]);
             gg[i] = (float)r;
             r2 += r * r;
             b2 += b * b;
         }
+        for (uint32_t h = threadIdx.x; h < n_halo; h += blockDim.x) dval[SC_HALO0 + h] = 0.0f;
         for (int o = 16; o > 0; o >>= 1) {
             r2 += __shfl_down_sync(0xffffffffu, r2, o);
             b2 += __shfl_down_sync(0xffffffffu, b2, o);
         }
-        int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
         if (lane_id == 0) {
             red[warp] = r2;
             red[32 + warp] = b2;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < R) {
             double a = 0.0, bsum = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
                 a += red[w];
                 bsum += red[32 + w];
             }
-            double* dst = cluster.map_shared_rank(part, 0);
+            double* dst = cluster.map_shared_rank(part, threadIdx.x);
             dst[slot * 2 * SC_MAX_RANKS + rank] = a;
             dst[slot * 2 * SC_MAX_RANKS + SC_MAX_RANKS + rank] = bsum;
         }
         cluster.sync();
-        const double* src = cluster.map_shared_rank(part, 0);
         double a = 0.0, bsum = 0.0;
         for (uint32_t q = 0; q < R; ++q) {
-            a += src[slot * 2 * SC_MAX_RANKS + q];
-            bsum += src[slot * 2 * SC_MAX_RANKS + SC_MAX_RANKS + q];
+            a += part[slot * 2 * SC_MAX_RANKS + q];
+            bsum += part[slot * 2 * SC_MAX_RANKS + SC_MAX_RANKS + q];
         }
         if (bsum <= 0.0) return 0.0;
         return sqrt(a) / sqrt(bsum);
     };
 
     const float omega = u.omega;
-    // Neighbour corrections of cell i, fetched before any arithmetic so a thread's
-    // loads for its two cells are in flight together.
-    struct Face6 {
-        float2 v[6];
-        uint32_t mask;
-    };
-    auto gather = [&](uint32_t i, Face6& fc) {
-        const uint32_t* rp = reinterpret_cast<const uint32_t*>(ref + i * 6);
-        uint32_t rw[3] = {rp[0], rp[1], rp[2]};
-        fc.mask = 0;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            uint32_t r = (rw[f >> 1] >> ((f & 1) * 16)) & 0xffffu;
-            if (r != SC_NONE) {
-                fc.v[f] = sc_ld2(sc_mapa(a_dfill + (r & 4095u) * 8u, r >> 12));
-                fc.mask |= 1u << f;
-            } else {
-                fc.v[f] = make_float2(0.0f, 0.0f);
-            }
-        }
-    };
-    auto relax = [&](uint32_t i, const Face6& fc) {
-        uint8_t fl = flg[i];
-        if (fl & SC_EMPTY) return;
-        float2 me = dfill[i];
+    // New correction of one cell from its six neighbour slots (local loads only).  A
+    // cell without faces has 1/W = 0, g = 0 and only zero neighbours, so its
+    // correction stays exactly zero without a branch.
+    auto relax = [&](uint32_t i) {
+        const uint32_t r0 = ref[i], r1 = ref[4096 + i], r2 = ref[8192 + i];
+        const uint32_t j0 = r0 & SC_SLOT_MASK, j1 = r0 >> 16, j2 = r1 & 0xffffu, j3 = r1 >> 16, j4 = r2 & 0xffffu,
+                       j5 = r2 >> 16;
+        const float v0 = dval[j0], v1 = dval[j1], v2 = dval[j2], v3 = dval[j3], v4 = dval[j4], v5 = dval[j5];
+        const float me = dval[i];
         float ds = 0.0f;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            if (!(fc.mask & (1u << f))) continue;
-            ds += (fl & SC_UNIT) ? fc.v[f].x : sc_weight(me.y, fc.v[f].y) * fc.v[f].x;
+        if (r0 & SC_REF_UNIT) {
+            ds += v0;
+            ds += v1;
+            ds += v2;
+            ds += v3;
+            ds += v4;
+            ds += v5;
+        } else {
+            const float fi = fcode[i];
+            ds += sc_weight(fi, fcode[j0]) * v0;
+            ds += sc_weight(fi, fcode[j1]) * v1;
+            ds += sc_weight(fi, fcode[j2]) * v2;
+            ds += sc_weight(fi, fcode[j3]) * v3;
+            ds += sc_weight(fi, fcode[j4]) * v4;
+            ds += sc_weight(fi, fcode[j5]) * v5;
         }
         float dn = (ds + gg[i]) * invW[i];
-        if (omega != 1.0f) dn = me.x + omega * (dn - me.x);
-        dfill[i].x = dn;
+        if (omega != 1.0f) dn = me + omega * (dn - me);
+        dval[i] = dn;
     };
-    auto sweep = [&](uint32_t lo, uint32_t hi) {
-        const uint32_t step = 2 * blockDim.x;
-        for (uint32_t i0 = lo + threadIdx.x; i0 < hi; i0 += step) {
-            const uint32_t i1 = i0 + blockDim.x;
-            Face6 a, b;
-            gather(i0, a);
-            if (i1 < hi) gather(i1, b);
-            relax(i0, a);
-            if (i1 < hi) relax(i1, b);
+    auto sweep = [&](uint32_t lo, uint32_t hi, uint32_t col) {
+        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) relax(i);
+        __syncthreads();
+        // push the new values of this colour to the CTAs that hold them as halo
+        const uint32_t* list = snd + col * SC_SEND;
+        for (uint32_t e = threadIdx.x; e < n_send[col]; e += blockDim.x) {
+            const uint32_t s = list[e];
+            const uint32_t src = s & 4095u, q = (s >> 12) & 15u, h = s >> 16;
+            sc_st(sc_mapa(a_dval + (uint32_t)(SC_HALO0 + h) * 4u, q), dval[src]);
         }
     };
 
+    // p <- p + d in FP64, split back into hi/lo.  Cells other CTAs hold as halo are
+    // published to the global arrays for the next residual (all cells at the end).
     auto accumulate = [&]() {
         const double lim = (double)u.p_clamp;
         for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x) {
-            double p = ((double)ph[i] + (double)pl[i]) + (double)dfill[i].x;
+            double p = ((double)ph[i] + (double)pl[i]) + (double)dval[i];
             if (p > lim || p < -lim) {
                 p = p > 0.0 ? lim : -lim;
                 atomicAdd(&c.metrics[M_P_CLAMP], 1u);
             }
-            float hi = (float)p;
+            const float hi = (float)p;
+            const float lo = (float)(p - (double)hi);
             ph[i] = hi;
-            pl[i] = (float)(p - (double)hi);
+            pl[i] = lo;
+            if (flg[i] & SC_SENT) {
+                const uint32_t ci = cell_of[i];
+                c.pf[ci] = hi;
+                c.plo[ci] = lo;
+            }
         }
     };
 
@@ -349,12 +459,11 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         uint32_t k = min(ce, max_pairs - pairs);
         for (uint32_t j = 0; j < k; ++j) {
             cluster.sync();
-            sweep(0, n_red);
+            sweep(0, n_red, 0);
             cluster.sync();
-            sweep(n_red, n_loc);
+            sweep(n_red, n_loc, 1);
         }
         pairs += k;
-        // the black sweep and accumulate map cells to threads differently
         __syncthreads();
         accumulate();
         cluster.sync();
@@ -362,12 +471,14 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         r1 = residual(slot);
         ++evals;
     }
-    // write the pressure back (non-fluid cells were zeroed by classify)
-    for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x) {
-        uint32_t ci = sb.cell_of[rank * 4096u + i];
-        c.pf[ci] = ph[i];
-        c.plo[ci] = pl[i];
-    }
+    // publish every owned cell (the loop above published only halo-held ones)
+    if (pairs > 0)
+        for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x)
+            if (!(flg[i] & SC_SENT)) {
+                const uint32_t ci = cell_of[i];
+                c.pf[ci] = ph[i];
+                c.plo[ci] = pl[i];
+            }
     if (rank == 0 && threadIdx.x == 0) {
         sb.result->sweeps = pairs;
         sb.result->evals = evals;
@@ -375,7 +486,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         sb.result->r0 = r0;
         sb.result->r1 = r1;
     }
-    cluster.sync();  // keep every CTA's shared memory alive until remote reads end
+    cluster.sync();  // keep every CTA's shared memory alive until remote accesses end
 }
 
 }  // namespace cs

@@ -1,0 +1,23 @@
+// solver_launch.h — host entry points of the cluster-resident pressure solve, shared
+// by the engine and the allocation-free entry point (definitions in engine.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cs_device.cuh"
+#include "solver_types.cuh"
+
+namespace cs {
+
+constexpr uint32_t kScPrepLaunches = 5;  // own kernels of sc_launch_prep per call (CUB's not counted)
+
+void set_error(const std::string& msg);
+int sc_max_cluster_ranks();
+size_t sc_scan_temp_bytes(uint32_t codes);
+int sc_launch_prep(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, uint32_t instances,
+                   cudaStream_t stream, int sms);
+int sc_launch_cluster(const Ctx* d_ctx, const ScBuffers& sb, int ranks, uint32_t instances, float tol,
+                      uint32_t max_pairs, uint32_t check_every, cudaStream_t stream);
+
+}  // namespace cs

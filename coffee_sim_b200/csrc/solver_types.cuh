@@ -7,27 +7,41 @@
 
 namespace cs {
 
-constexpr int SC_CAP = 4095;           // cells per CTA (12-bit local index, 0xFFFF reserved)
+constexpr int SC_CAP = 4095;           // owned cells per CTA (12-bit local index, 0xFFFF reserved)
 constexpr int SC_MAX_RANKS = 16;
 constexpr uint16_t SC_NONE = 0xFFFF;
 constexpr int SC_THREADS = 1024;
+// Slots of a CTA's correction array: owned cells [0, SC_CAP), halo copies of other
+// CTAs' cells [SC_HALO0, SC_HALO0 + SC_HALO), and one slot that always holds zero.
+constexpr int SC_HALO0 = 4096;
+constexpr int SC_HALO = 4095;
+constexpr uint16_t SC_DUMMY = 8191;
+constexpr int SC_SLOTS = 8192;
+constexpr int SC_SEND = 2048;          // halo updates a CTA sends after one colour
 
-// per-CTA shared memory: SoA arrays of SC_CAP entries
+// per-CTA shared memory
 struct ScLayout {
-    static constexpr size_t dfill = 0;                                  // float2 (d, fill code)
-    static constexpr size_t g = dfill + sizeof(float2) * SC_CAP;        // float residual
-    static constexpr size_t invW = g + sizeof(float) * SC_CAP;          // float 1/W (0: no faces)
-    static constexpr size_t ph = invW + sizeof(float) * SC_CAP;         // float
-    static constexpr size_t pl = ph + sizeof(float) * SC_CAP;           // float
-    static constexpr size_t b = pl + sizeof(float) * SC_CAP;            // float dx^2 rhs
-    static constexpr size_t ref = b + sizeof(float) * SC_CAP;           // uint16 x 6, cell-major
-    static constexpr size_t flags = ref + sizeof(uint16_t) * 6 * SC_CAP;  // uint8
-    static constexpr size_t part = (flags + SC_CAP + 15) & ~size_t(15);   // double[2 slots][2][SC_MAX_RANKS]
+    static constexpr size_t dval = 0;                                    // float correction x SC_SLOTS
+    static constexpr size_t fcode = dval + sizeof(float) * SC_SLOTS;     // float fill code x SC_SLOTS
+    static constexpr size_t g = fcode + sizeof(float) * SC_SLOTS;        // float residual
+    static constexpr size_t invW = g + sizeof(float) * 4096;             // float 1/W (0: no faces)
+    static constexpr size_t ph = invW + sizeof(float) * 4096;            // float
+    static constexpr size_t pl = ph + sizeof(float) * 4096;              // float
+    static constexpr size_t b = pl + sizeof(float) * 4096;               // float dx^2 rhs
+    static constexpr size_t ref = b + sizeof(float) * 4096;              // uint32 [3][4096]: face pairs
+    static constexpr size_t snd = ref + sizeof(uint32_t) * 3 * 4096;     // uint32 [2][SC_SEND]
+    static constexpr size_t flags = snd + sizeof(uint32_t) * 2 * SC_SEND;  // uint8 x 4096
+    static constexpr size_t part = flags + 4096;                         // double[2 slots][2][SC_MAX_RANKS]
     static constexpr size_t red = part + sizeof(double) * 4 * SC_MAX_RANKS;  // double[2][32]
     static constexpr size_t bytes = red + sizeof(double) * 64;
 };
-// flags byte: bits 0-2 air faces, bit 6 all fluid-face weights are 1, bit 7 no faces
-constexpr uint8_t SC_UNIT = 0x40, SC_EMPTY = 0x80;
+static_assert(ScLayout::bytes <= 232448, "cluster solve state exceeds the 227 KB shared-memory limit");
+// A face reference is a 13-bit slot index; bit 15 of the first word marks a cell
+// whose fluid faces all have weight 1.
+constexpr uint32_t SC_SLOT_MASK = 0x1fffu, SC_REF_UNIT = 0x8000u;
+// flags byte: bits 0-2 air faces, bit 5 held as halo by another CTA, bit 6 all
+// fluid-face weights are 1, bit 7 no faces
+constexpr uint8_t SC_SENT = 0x20, SC_UNIT = 0x40, SC_EMPTY = 0x80;
 
 
 // Solver bookkeeping written by the prep kernels and read by the cluster kernel.
@@ -40,15 +54,88 @@ struct ScResult {
     uint32_t sweeps, evals, status, pad;
     double r0, r1;
 };
+// counters: halo size per rank, then send-list length per (rank, colour)
+constexpr int SC_COUNTS = SC_MAX_RANKS * 3;
 
 struct ScBuffers {
     unsigned long long* flags;   // Morton codes: fluid | red << 32
     unsigned long long* scan;    // exclusive scan of flags
-    uint16_t* ref_of_cell;       // cells
-    uint32_t* cell_of;           // SC_MAX_RANKS * 4096
+    uint16_t* ref_of_cell;       // per grid cell: rank << 12 | local, SC_NONE if not fluid
+    uint32_t* cell_of;           // [rank][4096] grid cell of each owned slot
+    uint16_t* slot_ref;          // [rank][3 face pairs][4096][2] neighbour slot per face
+    float4* slot_coef;           // [rank][4096] (1/W, fill code, dx^2 rhs, flags bits)
+    float* halo_fill;            // [rank][SC_HALO] fill code of each halo slot
+    uint32_t* send;              // [rank][colour][SC_SEND] src | dest rank << 12 | halo slot << 16
+    uint32_t* counts;            // SC_COUNTS
     ScInfo* info;
     ScResult* result;
+    void* cub_temp;
+    size_t cub_bytes;
+    size_t stride;               // bytes between the scratch of consecutive instances
 };
 
+// Byte offsets of every solver scratch buffer inside one allocation.
+struct ScScratch {
+    size_t flags, scan, ref_of_cell, cell_of, slot_ref, slot_coef, halo_fill, send, counts, info, result, cub, total;
+};
+constexpr size_t sc_align(size_t n) { return (n + 255) & ~size_t(255); }
+constexpr ScScratch sc_scratch_layout(size_t cells, size_t codes, size_t cub_bytes) {
+    ScScratch s{};
+    s.flags = 0;
+    s.scan = s.flags + sc_align(codes * sizeof(unsigned long long));
+    s.ref_of_cell = s.scan + sc_align(codes * sizeof(unsigned long long));
+    s.cell_of = s.ref_of_cell + sc_align(cells * sizeof(uint16_t));
+    s.slot_ref = s.cell_of + sc_align((size_t)SC_MAX_RANKS * 4096 * sizeof(uint32_t));
+    s.slot_coef = s.slot_ref + sc_align((size_t)SC_MAX_RANKS * 3 * 4096 * 2 * sizeof(uint16_t));
+    s.halo_fill = s.slot_coef + sc_align((size_t)SC_MAX_RANKS * 4096 * sizeof(float4));
+    s.send = s.halo_fill + sc_align((size_t)SC_MAX_RANKS * SC_HALO * sizeof(float));
+    s.counts = s.send + sc_align((size_t)SC_MAX_RANKS * 2 * SC_SEND * sizeof(uint32_t));
+    s.info = s.counts + sc_align(SC_COUNTS * sizeof(uint32_t));
+    s.result = s.info + sc_align(sizeof(ScInfo));
+    s.cub = s.result + sc_align(sizeof(ScResult));
+    s.total = s.cub + sc_align(cub_bytes);
+    return s;
+}
+inline ScBuffers sc_buffers_at(unsigned char* base, const ScScratch& s, size_t cub_bytes) {
+    ScBuffers b;
+    b.flags = reinterpret_cast<unsigned long long*>(base + s.flags);
+    b.scan = reinterpret_cast<unsigned long long*>(base + s.scan);
+    b.ref_of_cell = reinterpret_cast<uint16_t*>(base + s.ref_of_cell);
+    b.cell_of = reinterpret_cast<uint32_t*>(base + s.cell_of);
+    b.slot_ref = reinterpret_cast<uint16_t*>(base + s.slot_ref);
+    b.slot_coef = reinterpret_cast<float4*>(base + s.slot_coef);
+    b.halo_fill = reinterpret_cast<float*>(base + s.halo_fill);
+    b.send = reinterpret_cast<uint32_t*>(base + s.send);
+    b.counts = reinterpret_cast<uint32_t*>(base + s.counts);
+    b.info = reinterpret_cast<ScInfo*>(base + s.info);
+    b.result = reinterpret_cast<ScResult*>(base + s.result);
+    b.cub_temp = base + s.cub;
+    b.cub_bytes = cub_bytes;
+    b.stride = s.total;
+    return b;
+}
+
+// The buffers of instance k of an ensemble whose scratch blocks are laid out back to back.
+template <class T>
+__host__ __device__ __forceinline__ T* sc_shift(T* p, size_t bytes) {
+    return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(p) + bytes);
+}
+__host__ __device__ __forceinline__ ScBuffers sc_instance(const ScBuffers& b, uint32_t k) {
+    const size_t o = b.stride * k;
+    ScBuffers r = b;
+    r.flags = sc_shift(b.flags, o);
+    r.scan = sc_shift(b.scan, o);
+    r.ref_of_cell = sc_shift(b.ref_of_cell, o);
+    r.cell_of = sc_shift(b.cell_of, o);
+    r.slot_ref = sc_shift(b.slot_ref, o);
+    r.slot_coef = sc_shift(b.slot_coef, o);
+    r.halo_fill = sc_shift(b.halo_fill, o);
+    r.send = sc_shift(b.send, o);
+    r.counts = sc_shift(b.counts, o);
+    r.info = sc_shift(b.info, o);
+    r.result = sc_shift(b.result, o);
+    r.cub_temp = sc_shift(reinterpret_cast<unsigned char*>(b.cub_temp), o);
+    return r;
+}
 
 }  // namespace cs

@@ -191,10 +191,13 @@ def test_cluster_solver_matches_per_colour_launches(engine):
         sim = MpmSim3D(s, engine)
         scenes.populate_c2(sim)
         sims.append(sim)
+    sims[1].profile_enable(True)
     for k in range(3):
         for sim in sims:
             sim.step_substep(scenes.C2_DT)
         ma, mb = sims[0].latest_metrics(), sims[1].latest_metrics()
+        # the cluster path ran: one launch in the sweep phase of each substep
+        assert sims[1].profile_read().phase_launches[4] == k + 1
         assert ma.last_sweeps == mb.last_sweeps
         assert mb.last_residual <= 1e-5
         assert mismatch(sims[0].read_pressure(), sims[1].read_pressure()) == 0
