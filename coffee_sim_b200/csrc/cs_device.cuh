@@ -42,7 +42,8 @@ struct Params {
     float nu_m2s, absorption_rate, max_saturation, min_perm;
     float extraction_rate, compaction_rate, bed_damping, bed_impact;
     float pore_capacity_scale, pore_overfill_alpha;
-    float div_clamp, p_clamp;
+    float div_clamp, p_clamp;  // fixed-point lane limits (state.rs:18)
+    float p_limit;             // pressure limit: p_clamp with fixed-point storage, none with FP32
     float j_alpha, j_expand_alpha, max_rest_frac, surface_void_scale;
     float water_r_dx, bed_r_dx, filter_absorption;
     // geometry

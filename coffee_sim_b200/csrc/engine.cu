@@ -248,6 +248,9 @@ void Engine::fill_params(Params& u, float dt) const {
     u.pore_overfill_alpha = s.brew.bed_pore_overfill_alpha;
     u.div_clamp = std::fmin(4.0f * s.max_velocity * inv_dx, FP_VALUE_LIMIT - 1.0f);
     u.p_clamp = FP_VALUE_LIMIT - 1.0f;
+    // i32 lanes hold p * 2^18, so fixed-point storage clamps at the lane limit; FP32
+    // storage has no such range and does not clamp
+    u.p_limit = s.pressure_storage == CS_PRESSURE_FIXED_POINT ? u.p_clamp : 3.0e38f;
     u.j_alpha = 32.0f;
     u.j_expand_alpha = 2.0f;
     u.max_rest_frac = 1.20f;

@@ -562,7 +562,7 @@ __global__ void k_refine_accumulate(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const int32_t* kl = lane(c, 3);
-    const double lim = (double)u.p_clamp;
+    const double lim = (double)u.p_limit;
     CS_FOR(i, u.cells) {
         if (!is_fluid(kl[i])) continue;
         double p = ((double)c.pf[i] + (double)c.plo[i]) + (double)c.pd[i];

@@ -14,7 +14,7 @@ __device__ __forceinline__ float pressure_load(const Ctx& c, uint32_t i) {
     return c.u.fixed_point ? (float)lane(c, 0)[i] * INV_FP_SCALE : c.pf[i];
 }
 __device__ __forceinline__ void pressure_store(const Ctx& c, uint32_t i, float v) {
-    float lim = c.u.p_clamp;
+    float lim = c.u.p_limit;
     float cl = wclamp(v, -lim, lim);
     if (cl != v) atomicAdd(&c.metrics[M_P_CLAMP], 1u);
     if (c.u.fixed_point) lane(c, 0)[i] = to_i32(cl * FP_SCALE);

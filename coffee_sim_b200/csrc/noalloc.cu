@@ -126,6 +126,7 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
     u.dt = dt;
     u.omega = omega;
     u.p_clamp = cs::FP_VALUE_LIMIT - 1.0f;
+    u.p_limit = 3.0e38f;  // FP32 storage: no fixed-point range to respect
     u.fixed_point = 0;
     // the solver reads the cell kind as lane 3 of the grid lanes
     ctx.lanes = reinterpret_cast<int32_t*>(reinterpret_cast<uintptr_t>(kind) - 3 * (uintptr_t)cells * sizeof(int32_t));

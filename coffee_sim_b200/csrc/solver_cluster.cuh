@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     // p <- p + d in FP64, split back into hi/lo.  Cells other CTAs hold as halo are
     // published to the global arrays for the next residual (all cells at the end).
     auto accumulate = [&]() {
-        const double lim = (double)u.p_clamp;
+        const double lim = (double)u.p_limit;
         for (uint32_t i = threadIdx.x; i < n_loc; i += blockDim.x) {
             double p = ((double)ph[i] + (double)pl[i]) + (double)dval[i];
             if (p > lim || p < -lim) {

@@ -108,6 +108,7 @@ struct Sim : SimBase {
         R extraction_rate, compaction_rate, bed_damping, bed_impact;
         R pore_capacity_scale, pore_overfill_alpha;
         R div_clamp, p_clamp, mdiv_scale, mdiv_inv;
+        R p_limit;  // pressure limit: p_clamp with fixed-point storage, none with FP32
         R j_alpha, j_expand_alpha, max_rest_frac, surface_void_scale;
         R water_r_dx, bed_r_dx, filter_absorption;
         R omega;
@@ -213,6 +214,7 @@ struct Sim : SimBase {
         u.bed_damping = R(8.5f); u.bed_impact = R(s.brew.bed_impact_rate);
         u.pore_capacity_scale = R(s.brew.bed_pore_capacity_scale); u.pore_overfill_alpha = R(s.brew.bed_pore_overfill_alpha);
         u.div_clamp = R(div_clamp); u.p_clamp = R(FP_VALUE_LIMIT - 1.0f);
+        u.p_limit = s.pressure_storage == CS_PRESSURE_FIXED_POINT ? u.p_clamp : R(3.0e38f);
         u.mdiv_scale = R(METRICS_DIV_FP_SCALE); u.mdiv_inv = R(1.0f / METRICS_DIV_FP_SCALE);
         u.j_alpha = R(32.0f); u.j_expand_alpha = R(2.0f); u.max_rest_frac = R(1.20f);
         u.surface_void_scale = R(s.brew.bed_surface_void_scale);
@@ -257,7 +259,7 @@ struct Sim : SimBase {
         return pf[c];
     }
     void pressure_store(uint32_t c, R v) {
-        R lim = u.p_clamp;
+        R lim = u.p_limit;
         R cl = wclamp(v, -lim, lim);
         if (cl != v) atomic_add_u32(&metrics[M_P_CLAMP], 1u);
         if (fixed_point()) lane(0)[c] = to_i32(cl * u.fp_scale);
@@ -1114,7 +1116,7 @@ struct Sim : SimBase {
     }
     void refine_accumulate() {
         int n = (int)cells;
-        R lim = u.p_clamp;
+        R lim = u.p_limit;
 #pragma omp parallel for schedule(static)
         for (int idx = 0; idx < n; ++idx) {
             if (!is_fluid(kind_load(idx))) continue;
