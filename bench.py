@@ -126,31 +126,31 @@ def algorithmic_bytes(n_p, n_c, pairs, evals, n_bed):
     return b
 
 
-def cpu_baseline(args, threads=None, steps=None, warm=None):
-    """Time the CPU oracle on the same workload (bounded sample)."""
+def cpu_baseline(args, steps, warm):
+    """Time the CPU oracle (all host threads) on the substeps the GPU arm times: the
+    same scene, `warm` untimed substeps, then the first `steps` of the timed window."""
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_lib
     lib = oracle_lib.oracle_library()
-    if threads:
-        oracle_lib.set_threads(threads)
     nthreads = int(lib.lib.oracle_get_threads())
     sim = build_scene(lib, args)
-    n_p = sim.particle_count()
     from coffee_sim_b200 import scenes
-    for _ in range(warm if warm is not None else args.cpu_warmup):
+    for _ in range(warm):
         sim.step_substep(scenes.C2_DT)
-    k = steps if steps is not None else args.cpu_steps
-    t = time.perf_counter()
+    n0 = sim.particle_count()
+    particle_steps = 0
     sweeps = 0
-    for _ in range(k):
+    t = time.perf_counter()
+    for _ in range(steps):
+        particle_steps += sim.particle_count()
         sim.step_substep(scenes.C2_DT)
         sweeps += sim.latest_metrics().last_sweeps
     dt = time.perf_counter() - t
-    return {"value": n_p * k / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": f"{k} substeps of the same V60 64^3 mid-pour state ({n_p} samples) after "
-                      f"{warm if warm is not None else args.cpu_warmup} warm-up substeps; {sweeps / max(k, 1):.0f} "
-                      f"RBGS pairs per substep; oracle/ C++ restatement, OpenMP, -O3",
-            "seconds": dt, "particles": n_p}
+    return {"value": particle_steps / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"substeps {warm + 1}..{warm + steps} of the V60 64^3 pour ({n0} samples at the start; "
+                      f"{sweeps / max(steps, 1):.0f} red-black pairs per substep), the first {steps} of the GPU "
+                      f"arm's timed substeps; oracle/ C++ restatement, OpenMP on {nthreads} threads, -O3",
+            "seconds": dt, "particles": n0}
 
 
 def run_reference(args, rank):
@@ -180,8 +180,7 @@ def main():
     ap.add_argument("--omega", type=float, default=1.9)
     ap.add_argument("--max-sweeps", type=int, default=4000)
     ap.add_argument("--check-every", type=int, default=10)
-    ap.add_argument("--cpu-steps", type=int, default=4)
-    ap.add_argument("--cpu-warmup", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -212,9 +211,11 @@ def main():
     n_bed = sim.num_bed
     dt = scenes.C2_DT
 
+    # warm-up substeps bring the pour to its mid-pour state; both timed loops replay
+    # the same K substeps from a snapshot of that state
     for _ in range(args.warmup):
         sim.step_substep(dt)
-    sim.sync()
+    state = sim.snapshot()
 
     def barrier():
         if dist:
@@ -223,11 +224,14 @@ def main():
             torch.cuda.synchronize()
 
     # ---- device-timed region: K substeps, L2 flushed before each ----
+    sim.restore(state)
     sim.profile_enable(True)
     step_ms = []
+    particle_steps = 0
     barrier()
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
+            particle_steps += sim.particle_count()
             sim.flush_l2()
             sim.timer_start()
             sim.step_substep(dt)
@@ -241,10 +245,13 @@ def main():
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = n_p * args.steps * world / (total_ms * 1e-3)
+    value = particle_steps * world / (total_ms * 1e-3)
 
-    # ---- end to end through the public API (host emission upload + metrics readback) ----
+    # ---- end to end through the public API: the same K substeps, each with its host
+    # emission upload and the metrics readback ----
+    sim.restore(state)
     sim.profile_enable(True)
+    barrier()
     sim.sync()
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -257,7 +264,7 @@ def main():
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = n_p * args.steps * world / e2e_s
+    e2e_value = particle_steps * world / e2e_s
 
     # ---- roofline of the dominant kernel ----
     # The cluster-resident solve (k_sc_solve) is one launch per substep and the only
@@ -279,7 +286,7 @@ def main():
         per_launch_bytes = 8.5 * n_c
     launch_ms = sweep_ms / sweep_launches
     achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9 if sweep_ms > 0 else 0.0
-    step_bytes = algorithmic_bytes(n_p, n_c, pairs_per_step, evals_per_step, n_bed)
+    step_bytes = algorithmic_bytes(particle_steps / args.steps, n_c, pairs_per_step, evals_per_step, n_bed)
     step_gbs = step_bytes / (total_ms / args.steps * 1e-3) / 1e9
     traffic = ncu_traffic(kernel)
 
@@ -288,7 +295,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded V60 scene generator; no dataset)",
-        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "particles": n_p, "bed_particles": n_bed,
+        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "particles": n_p, "particles_mean": particle_steps / args.steps,
+                   "bed_particles": n_bed, "timed_substeps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "substep_dt_s": dt, "residual_tol": 1e-5, "omega": args.omega, "warm_start": "previous substep",
                    "check_every_pairs": args.check_every, "l2": "flushed (512 MB write) before each timed step",
                    "parallelism": f"replicas x{world}"},
@@ -314,7 +322,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            line["cpu_baseline"] = cpu_baseline(args)
+            line["cpu_baseline"] = cpu_baseline(args, steps=min(args.steps, args.cpu_steps), warm=args.warmup)
             line["cpu_baseline"].pop("seconds", None)
             line["cpu_baseline"].pop("particles", None)
         except Exception as e:  # the oracle is test infrastructure; report its absence

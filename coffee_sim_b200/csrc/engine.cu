@@ -755,7 +755,7 @@ static const uint64_t kSnapMagic = 0x43534e4150423230ull;  // "CSNAPB20"
 
 int Engine::snapshot_size(uint64_t* bytes) {
     const uint64_t mp = settings.max_particles;
-    *bytes = sizeof(SnapHeader) + mp * sizeof(float4) * 7 + mp * 4 * sizeof(int32_t) + cells_ * sizeof(float);
+    *bytes = sizeof(SnapHeader) + mp * sizeof(float4) * 7 + mp * 4 * sizeof(int32_t) + cells_ * 2 * sizeof(float);
     return CS_OK;
 }
 
@@ -769,7 +769,7 @@ int Engine::snapshot_save(void* buf, uint64_t bytes) {
     SnapHeader h;
     std::memset(&h, 0, sizeof(h));
     h.magic = kSnapMagic;
-    h.version = 1;
+    h.version = 2;
     h.max_p = settings.max_particles;
     h.cells = cells_;
     h.num_water = num_water;
@@ -793,6 +793,9 @@ int Engine::snapshot_save(void* buf, uint64_t bytes) {
         return rc;
     p += delta_.bytes;
     if ((rc = check(cudaMemcpyAsync(p, pf_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "snapshot"))) return rc;
+    p += cells_ * 4;
+    // low word of the FP32-storage pressure (the warm start of the next solve)
+    if ((rc = check(cudaMemcpyAsync(p, plo_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "snapshot"))) return rc;
     return sync();
 }
 
@@ -805,7 +808,7 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
         return CS_ERR_INVALID_ARG;
     }
     std::memcpy(&h, buf, sizeof(h));
-    if (h.magic != kSnapMagic || h.version != 1 || h.max_p != settings.max_particles || h.cells != cells_ ||
+    if (h.magic != kSnapMagic || h.version != 2 || h.max_p != settings.max_particles || h.cells != cells_ ||
         bytes < need) {
         set_error("snapshot does not match this simulation's sizes");
         return CS_ERR_INVALID_ARG;
@@ -822,6 +825,8 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
         return rc;
     p += delta_.bytes;
     if ((rc = check(cudaMemcpyAsync(pf_.ptr, p, cells_ * 4, cudaMemcpyHostToDevice, stream_), "restore"))) return rc;
+    p += cells_ * 4;
+    if ((rc = check(cudaMemcpyAsync(plo_.ptr, p, cells_ * 4, cudaMemcpyHostToDevice, stream_), "restore"))) return rc;
     num_water = h.num_water;
     num_bed = h.num_bed;
     total_time = h.total_time;

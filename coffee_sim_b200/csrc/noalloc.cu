@@ -11,7 +11,7 @@
 // references, chunk tables, CUB scan storage, the solver context and result, the
 // clamp counters) lives in one file-scope __device__ array sized for grids of at
 // most 64 cells per side.  Every GPU that loads this library keeps that array
-// (about 4.9 MB) until the process exits.  Calls share it and it keeps the previous
+// (about 7.6 MB) until the process exits.  Calls share it and it keeps the previous
 // call's contents: each call rewrites or clears everything it reads, and calls that
 // overlap on the GPU race with each other.
 #include <cuda_runtime.h>

@@ -383,7 +383,7 @@ int32_t cs_sync(CsSim* sim);
  * kind (CELL kinds 0..4 as classify writes them), fill (liquid fill fraction),
  * div (classify's divergence minus target), p_hi/p_lo (pressure words: warm start
  * in, solution out).  Scratch lives in a static device array reserved when the
- * library is loaded (about 4.9 MB per GPU, held until exit), so grids are limited to
+ * library is loaded (about 7.6 MB per GPU, held until exit), so grids are limited to
  * 64 cells per side and 16 x 4095 fluid cells; larger inputs return CS_ERR_CAPACITY.
  * The first call on a device looks up that array's device address; make it before
  * any stream capture.  Calls share the array: calls that overlap on the GPU race.
