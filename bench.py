@@ -99,6 +99,7 @@ def build_scene(lib, args, device=0):
     s.raw.rbgs_omega = args.omega
     s.raw.max_sweeps = args.max_sweeps
     s.raw.check_every = args.check_every
+    s.raw.p2g_mode = {"atomic": 0, "sorted": 1}[args.p2g]
     sim = MpmSim3D(s, lib)
     scenes.populate_c2(sim)
     return sim
@@ -180,6 +181,8 @@ def main():
     ap.add_argument("--omega", type=float, default=1.9)
     ap.add_argument("--max-sweeps", type=int, default=4000)
     ap.add_argument("--check-every", type=int, default=10)
+    ap.add_argument("--p2g", default="sorted", choices=["atomic", "sorted"],
+                    help="P2G accumulation: per-particle global atomics or tile-sorted shared memory")
     ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -298,7 +301,7 @@ def main():
         "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "particles": n_p, "particles_mean": particle_steps / args.steps,
                    "bed_particles": n_bed, "timed_substeps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "substep_dt_s": dt, "residual_tol": 1e-5, "omega": args.omega, "warm_start": "previous substep",
-                   "check_every_pairs": args.check_every, "l2": "flushed (512 MB write) before each timed step",
+                   "check_every_pairs": args.check_every, "p2g": args.p2g, "l2": "flushed (512 MB write) before each timed step",
                    "parallelism": f"replicas x{world}"},
         "pressure_solve_ms": (prof.phase_ms[4] + prof.phase_ms[5]) / max(prof.substeps, 1),
         "sweeps_per_step": pairs_per_step,

@@ -55,6 +55,7 @@ struct Params {
     // modes
     uint32_t fixed_point;      // pressure/divergence stored as i32*2^18
     uint32_t int64_grid;       // P2G accumulators are i64*2^32
+    uint32_t ntx, nty, ntz;    // P2G tile grid (tiles of P2G_TILE^3 cells over base cells -1..g-1)
     uint32_t warm;             // keep last substep's pressure in fluid cells
     float omega;               // red-black over-relaxation (1 = plain Gauss-Seidel)
 };
@@ -76,6 +77,12 @@ struct Ctx {
     // grid
     int32_t* lanes;   // 6 x cells, reference aliasing (shader.rs:152-164)
     long long* lanes64;  // 6 x cells in int64 mode
+    // sorted P2G (CS_P2G_SORTED_SHARED): particles counting-sorted by 4^3-cell tile
+    uint32_t* p2g_key;     // max_p: tile of each particle (P2G_NO_TILE if it deposits nothing)
+    uint32_t* p2g_rank;    // max_p: position inside its tile
+    uint32_t* p2g_sorted;  // max_p: particle ids in tile order
+    uint32_t* tile_count;  // tiles + 1
+    uint32_t* tile_start;  // tiles + 1 (exclusive scan of tile_count)
     float4* gvel;     // v.xyz, mass
     float* pf;        // FP32 pressure (persistent across substeps for warm start)
     float* divf;      // FP32 divergence

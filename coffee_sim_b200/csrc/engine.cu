@@ -94,6 +94,20 @@ int Engine::init() {
     if ((rc = alloc(delta_, mp * 4 * sizeof(int32_t)))) return rc;
     if ((rc = alloc(lanes_, cells_ * 6 * sizeof(int32_t)))) return rc;
     if ((rc = alloc(lanes64_, settings.p2g_mode == CS_P2G_INT64 ? cells_ * 6 * sizeof(long long) : 0))) return rc;
+    if (settings.p2g_mode == CS_P2G_SORTED_SHARED) {
+        uint32_t nt[3];
+        for (int a = 0; a < 3; ++a) nt[a] = (settings.grid_dims[a] + 1 + P2G_TILE - 1) / P2G_TILE;
+        p2g_tiles_ = nt[0] * nt[1] * nt[2];
+        if ((rc = alloc(p2g_key_, (size_t)mp * sizeof(uint32_t)))) return rc;
+        if ((rc = alloc(p2g_rank_, (size_t)mp * sizeof(uint32_t)))) return rc;
+        if ((rc = alloc(p2g_sorted_, (size_t)mp * sizeof(uint32_t)))) return rc;
+        if ((rc = alloc(tile_count_, ((size_t)p2g_tiles_ + 1) * sizeof(uint32_t)))) return rc;
+        if ((rc = alloc(tile_start_, ((size_t)p2g_tiles_ + 1) * sizeof(uint32_t)))) return rc;
+        size_t temp = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, temp, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)p2g_tiles_ + 1,
+                                      stream_);
+        if ((rc = alloc(tile_temp_, temp))) return rc;
+    }
     if ((rc = alloc(gvel_, cells_ * f4))) return rc;
     if ((rc = alloc(pf_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(divf_, cells_ * sizeof(float)))) return rc;
@@ -134,6 +148,11 @@ int Engine::init() {
     ctx_.delta = (int32_t*)delta_.ptr;
     ctx_.lanes = (int32_t*)lanes_.ptr;
     ctx_.lanes64 = (long long*)lanes64_.ptr;
+    ctx_.p2g_key = (uint32_t*)p2g_key_.ptr;
+    ctx_.p2g_rank = (uint32_t*)p2g_rank_.ptr;
+    ctx_.p2g_sorted = (uint32_t*)p2g_sorted_.ptr;
+    ctx_.tile_count = (uint32_t*)tile_count_.ptr;
+    ctx_.tile_start = (uint32_t*)tile_start_.ptr;
     ctx_.gvel = (float4*)gvel_.ptr;
     ctx_.pf = (float*)pf_.ptr;
     ctx_.divf = (float*)divf_.ptr;
@@ -275,6 +294,9 @@ void Engine::fill_params(Params& u, float dt) const {
     u.bed_surface_span = g.bed_surface_span;
     u.fixed_point = s.pressure_storage == CS_PRESSURE_FIXED_POINT ? 1u : 0u;
     u.int64_grid = s.p2g_mode == CS_P2G_INT64 ? 1u : 0u;
+    u.ntx = (u.gx + 1 + P2G_TILE - 1) / P2G_TILE;
+    u.nty = (u.gy + 1 + P2G_TILE - 1) / P2G_TILE;
+    u.ntz = (u.gz + 1 + P2G_TILE - 1) / P2G_TILE;
     u.warm = (s.warm_start != CS_WARM_NONE && !u.fixed_point && have_prev_p) ? 1u : 0u;
     u.omega = s.rbgs_omega > 0.0f ? s.rbgs_omega : 1.0f;
 }
@@ -455,7 +477,20 @@ int Engine::substep(float sub_dt, uint32_t P) {
     if (P > 1) cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_);
     if (P > 2 && num_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc));
     mark(CS_PHASE_P2G);
-    if (P > 3 && np) CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    if (P > 3 && np) {
+        if (settings.p2g_mode == CS_P2G_SORTED_SHARED) {
+            cudaMemsetAsync(tile_count_.ptr, 0, tile_count_.bytes, stream_);
+            CS_LAUNCH(k_p2g_keys<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+            size_t temp = tile_temp_.bytes;
+            cub::DeviceScan::ExclusiveSum(tile_temp_.ptr, temp, (const uint32_t*)tile_count_.ptr,
+                                          (uint32_t*)tile_start_.ptr, (int)p2g_tiles_ + 1, stream_);
+            CS_LAUNCH(k_p2g_scatter<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+            const int tb = (int)std::min<uint32_t>(p2g_tiles_, (uint32_t)sms_ * 16);
+            CS_LAUNCH(k_p2g_tiles<<<dim3(tb, 1), P2G_THREADS, 0, stream_>>>(dc));
+        } else {
+            CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+        }
+    }
     mark(CS_PHASE_GRID);
     if (P > 4) CS_LAUNCH(k_grid_update<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 5 ? 1 : 0));
     if (P > 6) CS_LAUNCH(k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc));
@@ -958,6 +993,17 @@ static int validate(const CsSettings* s) {
     if (s->num_obstacles > CS_MAX_OBSTACLES) {
         set_error("too many obstacles");
         return CS_ERR_INVALID_ARG;
+    }
+    if (s->p2g_mode > CS_P2G_INT64 || s->warm_start > CS_WARM_LEARNED || s->pressure_storage > CS_PRESSURE_FP32 ||
+        s->solve_mode > CS_SOLVE_RESIDUAL || s->rbgs_kernel > 2) {
+        set_error("unknown mode value in settings");
+        return CS_ERR_INVALID_ARG;
+    }
+    // modes declared by the ABI whose engine path is not built yet
+    if (s->p2g_mode == CS_P2G_INT64 || s->warm_start == CS_WARM_LEARNED || s->device_emission || s->use_graph) {
+        set_error("settings request a mode this engine build does not implement "
+                  "(int64 P2G, learned warm start, device emission or graph capture)");
+        return CS_ERR_UNSUPPORTED;
     }
     if (s->warm_start != CS_WARM_NONE && s->pressure_storage == CS_PRESSURE_FIXED_POINT) {
         set_error("warm start needs CS_PRESSURE_FP32 storage");

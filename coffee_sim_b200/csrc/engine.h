@@ -73,6 +73,9 @@ private:
     DeviceBuffer d_ctx_, pos_, vel_, c0_, c1_, c2_, bedA_, bedB_, render_, snap_, delta_;
     DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, plo_, pd_, gres_, lookup_, sdf_, cls_, metrics_, resid_;
     DeviceBuffer staging_;  // AoS upload/readback staging
+    // sorted P2G
+    DeviceBuffer p2g_key_, p2g_rank_, p2g_sorted_, tile_count_, tile_start_, tile_temp_;
+    uint32_t p2g_tiles_ = 0;
     // cluster-resident solver
     DeviceBuffer sc_scratch_;  // every solver scratch buffer, laid out by sc_scratch_layout
     ScBuffers sc_buf_{};

@@ -98,26 +98,45 @@ __global__ void k_bed_lookup_scatter(const Ctx* __restrict__ cp) {
     }
 }
 
-// ---------------- p2g (shader.rs:955-1052), one global atomic per node and lane ----
-__device__ __forceinline__ void p2g_particle(const Ctx& c, uint32_t pid) {
+// ---------------- p2g (shader.rs:955-1052) ----------------
+// The deposit of one particle: B-spline weights, APIC momentum, rest and current volume,
+// each contribution rounded to i32 * 2^18 and handed to `add(node x, y, z, lane, value)`.
+// Integer sums do not depend on order, so every accumulation strategy below produces
+// the same lanes bit for bit.
+struct P2GSample {
+    int bx, by, bz;
+    float fx, fy, fz, mp, rpv, cpv;
+    float wx[3], wy[3], wz[3];
+    f3 a0, a1, a2, mv;
+};
+__device__ __forceinline__ bool p2g_prepare(const Ctx& c, uint32_t pid, P2GSample& q) {
     const Params& u = c.u;
     float4 P = c.pos[pid], Vv = c.vel[pid], A0 = c.c0[pid];
-    float mp = Vv.w;
-    if (!is_water_phase(A0.w) || mp <= inactive_mass(u)) return;
+    q.mp = Vv.w;
+    if (!is_water_phase(A0.w) || q.mp <= inactive_mass(u)) return false;
     float4 A1 = c.c1[pid], A2 = c.c2[pid];
     float gx = (P.x - u.ox) * u.inv_dx, gy = (P.y - u.oy) * u.inv_dx, gz = (P.z - u.oz) * u.inv_dx;
-    int bx = (int)floorf(gx - 0.5f), by = (int)floorf(gy - 0.5f), bz = (int)floorf(gz - 0.5f);
-    float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
-    float wx[3], wy[3], wz[3];
-    bspline(fx, wx);
-    bspline(fy, wy);
-    bspline(fz, wz);
-    f3 a0 = mk(mp * A0.x, mp * A0.y, mp * A0.z);
-    f3 a1 = mk(mp * A1.x, mp * A1.y, mp * A1.z);
-    f3 a2 = mk(mp * A2.x, mp * A2.y, mp * A2.z);
-    f3 mv = mk(mp * Vv.x, mp * Vv.y, mp * Vv.z);
-    float rpv = u.p_vol * mp / wmax(u.nominal_mass, 1e-6f);
-    float cpv = rpv * clamp_j(P.w);
+    q.bx = (int)floorf(gx - 0.5f);
+    q.by = (int)floorf(gy - 0.5f);
+    q.bz = (int)floorf(gz - 0.5f);
+    q.fx = gx - (float)q.bx;
+    q.fy = gy - (float)q.by;
+    q.fz = gz - (float)q.bz;
+    bspline(q.fx, q.wx);
+    bspline(q.fy, q.wy);
+    bspline(q.fz, q.wz);
+    const float mp = q.mp;
+    q.a0 = mk(mp * A0.x, mp * A0.y, mp * A0.z);
+    q.a1 = mk(mp * A1.x, mp * A1.y, mp * A1.z);
+    q.a2 = mk(mp * A2.x, mp * A2.y, mp * A2.z);
+    q.mv = mk(mp * Vv.x, mp * Vv.y, mp * Vv.z);
+    q.rpv = u.p_vol * mp / wmax(u.nominal_mass, 1e-6f);
+    q.cpv = q.rpv * clamp_j(P.w);
+    return true;
+}
+template <class Add>
+__device__ __forceinline__ void p2g_deposit(const Ctx& c, const P2GSample& q, Add add) {
+    const Params& u = c.u;
     const float lim = 1.0e9f;
     bool overflow = false;
 #pragma unroll
@@ -126,25 +145,24 @@ __device__ __forceinline__ void p2g_particle(const Ctx& c, uint32_t pid) {
         for (int j = 0; j < 3; ++j)
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                int cx = bx + i, cy = by + j, cz = bz + k;
+                int cx = q.bx + i, cy = q.by + j, cz = q.bz + k;
                 if (!in_grid(u, cx, cy, cz)) continue;
-                float w = wx[i] * wy[j] * wz[k];
-                f3 dpos = mk(((float)i - fx) * u.dx, ((float)j - fy) * u.dx, ((float)k - fz) * u.dx);
-                float mfp = (w * mp) * FP_SCALE;
-                float rfp = (w * rpv) * FP_SCALE;
-                float cfp = (w * cpv) * FP_SCALE;
-                float mx = (w * (mv.x + dot3(a0, dpos))) * FP_SCALE;
-                float my = (w * (mv.y + dot3(a1, dpos))) * FP_SCALE;
-                float mz = (w * (mv.z + dot3(a2, dpos))) * FP_SCALE;
+                float w = q.wx[i] * q.wy[j] * q.wz[k];
+                f3 dpos = mk(((float)i - q.fx) * u.dx, ((float)j - q.fy) * u.dx, ((float)k - q.fz) * u.dx);
+                float mfp = (w * q.mp) * FP_SCALE;
+                float rfp = (w * q.rpv) * FP_SCALE;
+                float cfp = (w * q.cpv) * FP_SCALE;
+                float mx = (w * (q.mv.x + dot3(q.a0, dpos))) * FP_SCALE;
+                float my = (w * (q.mv.y + dot3(q.a1, dpos))) * FP_SCALE;
+                float mz = (w * (q.mv.z + dot3(q.a2, dpos))) * FP_SCALE;
                 overflow |= fabsf(mfp) > lim || fabsf(mx) > lim || fabsf(my) > lim || fabsf(mz) > lim ||
                             fabsf(rfp) > lim || fabsf(cfp) > lim;
-                uint32_t ci = cidx(u, cx, cy, cz);
-                atomicAdd(&c.lanes[ci], to_i32(mfp));
-                atomicAdd(&c.lanes[(size_t)u.cells + ci], to_i32(mx));
-                atomicAdd(&c.lanes[2 * (size_t)u.cells + ci], to_i32(my));
-                atomicAdd(&c.lanes[3 * (size_t)u.cells + ci], to_i32(mz));
-                atomicAdd(&c.lanes[4 * (size_t)u.cells + ci], to_i32(rfp));
-                atomicAdd(&c.lanes[5 * (size_t)u.cells + ci], to_i32(cfp));
+                add(cx, cy, cz, 0, to_i32(mfp));
+                add(cx, cy, cz, 1, to_i32(mx));
+                add(cx, cy, cz, 2, to_i32(my));
+                add(cx, cy, cz, 3, to_i32(mz));
+                add(cx, cy, cz, 4, to_i32(rfp));
+                add(cx, cy, cz, 5, to_i32(cfp));
                 if (overflow) {
                     atomicAdd(&c.metrics[M_OVERFLOW], 1u);
                     overflow = false;
@@ -152,10 +170,108 @@ __device__ __forceinline__ void p2g_particle(const Ctx& c, uint32_t pid) {
             }
 }
 
+// One global atomic per node and lane (the reference's scheme).
 __global__ void k_p2g_atomic(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    uint32_t n = u.num_water + u.num_bed;
+    CS_FOR(pid, n) {
+        P2GSample q;
+        if (!p2g_prepare(c, pid, q)) continue;
+        p2g_deposit(c, q, [&](int x, int y, int z, int l, int32_t v) {
+            atomicAdd(&c.lanes[(size_t)l * u.cells + cidx(u, x, y, z)], v);
+        });
+    }
+}
+
+// ---- sorted P2G: counting sort by tile, shared-memory accumulation per tile ----
+// A particle whose base cell is b (its stencil covers b..b+2, b >= -1 inside the
+// domain) belongs to tile t = (b + 1) / P2G_TILE per axis; the tile's shared-memory
+// block covers nodes t*P2G_TILE - 1 .. t*P2G_TILE + P2G_TILE, so every node of its
+// particles lands in it.  A particle outside the domain (clamped key) falls back to
+// global atomics.
+constexpr int P2G_TILE = 4;
+constexpr int P2G_SPAN = P2G_TILE + 2;
+constexpr int P2G_NODES = P2G_SPAN * P2G_SPAN * P2G_SPAN;
+constexpr uint32_t P2G_NO_TILE = 0xffffffffu;
+constexpr int P2G_THREADS = 128;
+
+__device__ __forceinline__ uint32_t p2g_tile_axis(int b, uint32_t nt) {
+    int q = b + 1;
+    q = q < 0 ? 0 : q;
+    uint32_t t = (uint32_t)q / P2G_TILE;
+    return t < nt ? t : nt - 1;
+}
+
+__global__ void k_p2g_keys(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    uint32_t n = u.num_water + u.num_bed;
+    CS_FOR(pid, n) {
+        const float4 P = c.pos[pid], Vv = c.vel[pid];
+        const float ph = c.c0[pid].w;
+        uint32_t key = P2G_NO_TILE, rank = 0;
+        if (is_water_phase(ph) && !(Vv.w <= inactive_mass(u))) {
+            const int bx = (int)floorf((P.x - u.ox) * u.inv_dx - 0.5f);
+            const int by = (int)floorf((P.y - u.oy) * u.inv_dx - 0.5f);
+            const int bz = (int)floorf((P.z - u.oz) * u.inv_dx - 0.5f);
+            key = (p2g_tile_axis(bz, u.ntz) * u.nty + p2g_tile_axis(by, u.nty)) * u.ntx + p2g_tile_axis(bx, u.ntx);
+            rank = atomicAdd(&c.tile_count[key], 1u);
+        }
+        c.p2g_key[pid] = key;
+        c.p2g_rank[pid] = rank;
+    }
+}
+
+__global__ void k_p2g_scatter(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
     uint32_t n = c.u.num_water + c.u.num_bed;
-    CS_FOR(pid, n) p2g_particle(c, pid);
+    CS_FOR(pid, n) {
+        const uint32_t key = c.p2g_key[pid];
+        if (key != P2G_NO_TILE) c.p2g_sorted[c.tile_start[key] + c.p2g_rank[pid]] = pid;
+    }
+}
+
+__global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict__ cp) {
+    __shared__ int32_t acc[6][P2G_NODES];
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const uint32_t ntiles = u.ntx * u.nty * u.ntz;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t first = c.tile_start[t], last = c.tile_start[t + 1];
+        if (first == last) continue;  // uniform across the block
+        const uint32_t tx = t % u.ntx, ty = (t / u.ntx) % u.nty, tz = t / (u.ntx * u.nty);
+        const int ox = (int)(tx * P2G_TILE) - 1, oy = (int)(ty * P2G_TILE) - 1, oz = (int)(tz * P2G_TILE) - 1;
+        for (int i = threadIdx.x; i < 6 * P2G_NODES; i += blockDim.x) (&acc[0][0])[i] = 0;
+        __syncthreads();
+        for (uint32_t k = first + threadIdx.x; k < last; k += blockDim.x) {
+            P2GSample q;
+            if (!p2g_prepare(c, c.p2g_sorted[k], q)) continue;
+            const bool inside = q.bx >= ox && q.by >= oy && q.bz >= oz && q.bx + 2 < ox + P2G_SPAN &&
+                                q.by + 2 < oy + P2G_SPAN && q.bz + 2 < oz + P2G_SPAN;
+            if (inside) {
+                p2g_deposit(c, q, [&](int x, int y, int z, int l, int32_t v) {
+                    atomicAdd(&acc[l][((z - oz) * P2G_SPAN + (y - oy)) * P2G_SPAN + (x - ox)], v);
+                });
+            } else {
+                p2g_deposit(c, q, [&](int x, int y, int z, int l, int32_t v) {
+                    atomicAdd(&c.lanes[(size_t)l * u.cells + cidx(u, x, y, z)], v);
+                });
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < P2G_NODES; i += blockDim.x) {
+            const int x = ox + i % P2G_SPAN, y = oy + (i / P2G_SPAN) % P2G_SPAN, z = oz + i / (P2G_SPAN * P2G_SPAN);
+            if (!in_grid(u, x, y, z)) continue;
+            const uint32_t ci = cidx(u, x, y, z);
+#pragma unroll
+            for (int l = 0; l < 6; ++l) {
+                const int32_t v = acc[l][i];
+                if (v != 0) atomicAdd(&c.lanes[(size_t)l * u.cells + ci], v);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------- grid_update (shader.rs:1056-1082) [+ boundary_project] ----------------

@@ -219,11 +219,11 @@ typedef struct CsSettings {
     uint32_t check_every;         /* pairs between residual evaluations */
     uint32_t warm_start;          /* CS_WARM_* */
     uint32_t p2g_mode;            /* CS_P2G_* */
-    uint32_t sort_every;          /* substeps between cell-key sorts (sorted modes) */
+    uint32_t sort_every;          /* reserved: the sorted P2G mode sorts every substep */
     uint32_t device_emission;     /* 1: emit jet particles with a kernel (graph-capturable) */
     uint32_t use_graph;           /* 1: capture the substep in a CUDA graph */
     int32_t device;               /* CUDA device ordinal */
-    uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 persistent tiled */
+    uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 cluster-resident solve */
     float flow_override_ml_s;     /* >0: constant flow instead of the kettle-angle model */
     float exit_speed_override;    /* >0 with flow override: jet speed */
     float rbgs_omega;             /* red-black over-relaxation; 0 or 1 = plain Gauss-Seidel */

@@ -8,7 +8,7 @@ comparison asserts exact equality and prints the first mismatching pass otherwis
 import numpy as np
 import pytest
 
-from coffee_sim_b200 import scenes
+from coffee_sim_b200 import _ffi, scenes
 from coffee_sim_b200.sim import MpmSettings, MpmSim3D
 from helpers import copy_state, mismatch, pair, relerr
 
@@ -202,3 +202,40 @@ def test_cluster_solver_matches_per_colour_launches(engine):
         assert mb.last_residual <= 1e-5
         assert mismatch(sims[0].read_pressure(), sims[1].read_pressure()) == 0
         assert mismatch(sims[0].read_particles(), sims[1].read_particles()) == 0
+
+
+@pytest.mark.parametrize("passes", [AFTER_P2G, ALL])
+def test_sorted_p2g_matches_oracle(engine, oracle, center_pour_state, passes):
+    """Tile-sorted P2G with shared-memory accumulation (CS_P2G_SORTED_SHARED): the same
+    integer lanes as the oracle's per-particle atomics, bit for bit."""
+    settings, src = center_pour_state
+    settings.raw.p2g_mode = _ffi.CS_P2G_SORTED_SHARED
+    try:
+        e, o = pair(settings, engine, oracle)
+    finally:
+        settings.raw.p2g_mode = _ffi.CS_P2G_ATOMIC32
+    copy_state(src, e)
+    copy_state(src, o)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+        sim.step_substep_partial(FRAME / 10, passes)
+    _assert_same(_state(e), _state(o), f"sorted P2G after {passes} passes",
+                 ["particles", "affine", "bed_extract", "grid_vel", "lanes"])
+
+
+def test_sorted_p2g_matches_atomic_on_v60(engine):
+    """The dense V60 pour (8 samples per cell, a carafe pool): sorted and atomic P2G give
+    identical states over three substeps."""
+    sims = []
+    for mode in (_ffi.CS_P2G_ATOMIC32, _ffi.CS_P2G_SORTED_SHARED):
+        s = scenes.c2_v60(engine)
+        s.raw.rbgs_omega = 1.9
+        s.raw.p2g_mode = mode
+        sim = MpmSim3D(s, engine)
+        scenes.populate_c2(sim)
+        sims.append(sim)
+    for k in range(3):
+        for sim in sims:
+            sim.step_substep(scenes.C2_DT)
+        _assert_same(_state(sims[0]), _state(sims[1]), f"V60 substep {k}",
+                     ["particles", "affine", "bed_extract", "grid_vel", "pressure"])
