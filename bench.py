@@ -100,6 +100,7 @@ def build_scene(lib, args, device=0):
     s.raw.max_sweeps = args.max_sweeps
     s.raw.check_every = args.check_every
     s.raw.p2g_mode = {"atomic": 0, "sorted": 1}[args.p2g]
+    s.raw.device_emission = 1  # jet samples built on the device (the oracle matches this mode)
     sim = MpmSim3D(s, lib)
     scenes.populate_c2(sim)
     return sim
@@ -185,6 +186,7 @@ def main():
                     help="P2G accumulation: per-particle global atomics or tile-sorted shared memory")
     ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="end-to-end loop without CUDA-graph replay")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -252,6 +254,12 @@ def main():
 
     # ---- end to end through the public API: the same K substeps, each with its host
     # emission upload and the metrics readback ----
+    if not args.no_graph:
+        # capture and instantiate the substep graph outside the timed loop
+        sim.set_graph_mode(True)
+        sim.restore(state)
+        sim.step_substep(dt)
+        sim.sync()
     sim.restore(state)
     sim.profile_enable(True)
     barrier()
@@ -262,6 +270,8 @@ def main():
         sim.latest_metrics()
     e2e_s = time.perf_counter() - t0
     prof_e2e = sim.profile_read()
+    if not args.no_graph:
+        sim.set_graph_mode(False)
     if dist:
         import torch
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -301,7 +311,8 @@ def main():
         "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "particles": n_p, "particles_mean": particle_steps / args.steps,
                    "bed_particles": n_bed, "timed_substeps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "substep_dt_s": dt, "residual_tol": 1e-5, "omega": args.omega, "warm_start": "previous substep",
-                   "check_every_pairs": args.check_every, "p2g": args.p2g, "l2": "flushed (512 MB write) before each timed step",
+                   "check_every_pairs": args.check_every, "p2g": args.p2g,
+                   "emission": "device kernel", "e2e_launch": "direct" if args.no_graph else "CUDA graph replay", "l2": "flushed (512 MB write) before each timed step",
                    "parallelism": f"replicas x{world}"},
         "pressure_solve_ms": (prof.phase_ms[4] + prof.phase_ms[5]) / max(prof.substeps, 1),
         "sweeps_per_step": pairs_per_step,

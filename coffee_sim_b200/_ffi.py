@@ -5,7 +5,7 @@ return types to every exported function of a library that implements the C ABI.
 """
 import ctypes as C
 
-CS_ABI_VERSION = 4
+CS_ABI_VERSION = 5
 CS_MAX_OBSTACLES = 4
 
 STATUS = {
@@ -19,6 +19,8 @@ STATUS = {
     7: "CS_ERR_UNSUPPORTED",
     8: "CS_ERR_NO_DEVICE",
 }
+CS_OK, CS_ERR_INVALID_ARG, CS_ERR_CAPACITY, CS_ERR_CUDA, CS_ERR_NAN = 0, 1, 2, 3, 4
+CS_ERR_OVERFLOW, CS_ERR_TIMEOUT, CS_ERR_UNSUPPORTED, CS_ERR_NO_DEVICE = 5, 6, 7, 8
 
 CS_OBSTACLE_TRUNCATED_CONE = 0
 CS_OBSTACLE_CYLINDER = 1
@@ -224,6 +226,19 @@ class CsProfile(C.Structure):
     ]
 
 
+
+class CsTuneResult(C.Structure):
+    _fields_ = [
+        ("omega", C.c_float),
+        ("check_every", C.c_uint32),
+        ("p2g_mode", C.c_uint32),
+        ("trials", C.c_uint32),
+        ("best_ms", C.c_float),
+        ("initial_ms", C.c_float),
+        ("reserved", C.c_uint32 * 2),
+    ]
+
+
 P = C.c_void_p
 I32, U32, U64, F32 = C.c_int32, C.c_uint32, C.c_uint64, C.c_float
 PF = C.POINTER(C.c_float)
@@ -298,6 +313,10 @@ PROTOTYPES = {
     "cs_timer_stop": (I32, [P, PF]),
     "cs_flush_l2": (I32, [P]),
     "cs_sync": (I32, [P]),
+    "cs_set_solver": (I32, [P, F32, U32, U32]),
+    "cs_set_p2g_mode": (I32, [P, U32]),
+    "cs_set_graph_mode": (I32, [P, U32]),
+    "cs_autotune": (I32, [P, F32, U32, C.POINTER(CsTuneResult)]),
     "cs_pressure_solve_noalloc": (I32, [U32, U32, U32, F32, F32, F32, F32, U32, U32, P, P, P, P, P, P, PU32,
                                        C.POINTER(C.c_double)]),
 }

@@ -27,6 +27,14 @@ constexpr float BED_REACTION_ALPHA = 0.04f;      // shader.rs:76
 constexpr float BED_REACTION_IMPULSE_CAP = 0.012f;
 constexpr int SDF_RES = 128;                     // state.rs:20
 
+// One substep's jet emission, planned on the host (inflow.rs:133-189) and built on
+// the device (inflow.rs:196-218).
+struct JetPlan {
+    float t1[3], t2[3], vel[3], origin[3];
+    float jet_radius, dt, particle_mass;
+    uint32_t first_sequence, count, first_slot;
+};
+
 // Uniform block of one substep (the values of mod.rs:569-670; names follow
 // shader.rs:81-134).  Constants the reference hard-codes in the WGSL come from
 // CsGeometry so other cones can be simulated.
@@ -56,6 +64,7 @@ struct Params {
     uint32_t fixed_point;      // pressure/divergence stored as i32*2^18
     uint32_t int64_grid;       // P2G accumulators are i64*2^32
     uint32_t ntx, nty, ntz;    // P2G tile grid (tiles of P2G_TILE^3 cells over base cells -1..g-1)
+    JetPlan jet;               // device emission of this substep (count 0: none)
     uint32_t warm;             // keep last substep's pressure in fluid cells
     float omega;               // red-black over-relaxation (1 = plain Gauss-Seidel)
 };

@@ -37,6 +37,7 @@ Engine::Engine(const CsSettings& s) : settings(s) {
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
+    if (gexec_) cudaGraphExecDestroy(gexec_);
     for (auto& sp : spans_) {
         free_events_.push_back(sp.a);
         free_events_.push_back(sp.b);
@@ -94,7 +95,7 @@ int Engine::init() {
     if ((rc = alloc(delta_, mp * 4 * sizeof(int32_t)))) return rc;
     if ((rc = alloc(lanes_, cells_ * 6 * sizeof(int32_t)))) return rc;
     if ((rc = alloc(lanes64_, settings.p2g_mode == CS_P2G_INT64 ? cells_ * 6 * sizeof(long long) : 0))) return rc;
-    if (settings.p2g_mode == CS_P2G_SORTED_SHARED) {
+    {  // sort buffers: also used when the mode is switched at run time
         uint32_t nt[3];
         for (int a = 0; a < 3; ++a) nt[a] = (settings.grid_dims[a] + 1 + P2G_TILE - 1) / P2G_TILE;
         p2g_tiles_ = nt[0] * nt[1] * nt[2];
@@ -120,6 +121,8 @@ int Engine::init() {
     if ((rc = alloc(cls_, cells_))) return rc;
     if ((rc = alloc(metrics_, 8 * sizeof(uint32_t)))) return rc;
     if ((rc = alloc(resid_, 4 * sizeof(double)))) return rc;
+    if ((rc = alloc(sc_totals_, sizeof(ScTotals)))) return rc;
+    cudaMemsetAsync(sc_totals_.ptr, 0, sizeof(ScTotals), stream_);
     if ((rc = alloc(d_ctx_, sizeof(Ctx)))) return rc;
     if ((rc = alloc(staging_, std::max<size_t>(mp * 12 * sizeof(float), cells_ * 6 * sizeof(int32_t))))) return rc;
     // cluster-resident solver: buffers and the largest launchable cluster size
@@ -219,7 +222,11 @@ int Engine::reset() {
     return sync();
 }
 
-int Engine::sync() { return check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"); }
+int Engine::sync() {
+    int rc = check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    if (rc) return rc;
+    return collect();
+}
 
 // mod.rs:569-670 (write_uniforms), plus the WGSL constants of CsGeometry.
 void Engine::fill_params(Params& u, float dt) const {
@@ -313,8 +320,29 @@ int Engine::emit(float dt) {
     uint32_t count = inflow.plan(settings, dt, live, &dropped);
     frame_dropped += dropped;
     total_dropped += dropped;
+    jet_.count = 0;
     if (count == 0) return CS_OK;
     host::JetFrame jf = host::jet_frame(settings, inflow, dt, count, live);
+    if (settings.device_emission) {
+        // built by k_emit_jet after the context upload of this substep
+        for (int k = 0; k < 3; ++k) {
+            jet_.t1[k] = jf.t1[k];
+            jet_.t2[k] = jf.t2[k];
+            jet_.vel[k] = jf.vel[k];
+            jet_.origin[k] = jf.origin[k];
+        }
+        jet_.jet_radius = jf.jet_radius;
+        jet_.dt = jf.dt;
+        jet_.particle_mass = jf.particle_mass;
+        jet_.first_sequence = jf.first_sequence;
+        jet_.count = jf.count;
+        jet_.first_slot = jf.first_slot;
+        inflow.sequence += count;
+        frame_emitted_mass += (float)count * jf.particle_mass;
+        total_emitted_mass += (float)count * jf.particle_mass;
+        num_water += count;
+        return CS_OK;
+    }
     std::vector<float> parts((size_t)count * 8), affs((size_t)count * 12);
     host::emit_host(jf, parts.data(), affs.data());
     inflow.sequence += count;
@@ -451,33 +479,65 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
 }
 
 // mod.rs:271-419, one substep.  `passes` limits how many reference dispatches run
-// (numbered in the order of mod.rs:317-414, each number fixed).
+// (numbered in the order of mod.rs:317-414, each number fixed).  The host part (jet
+// plan, uniforms, context upload) runs here; the device work is enqueued directly or,
+// in graph mode, replayed from a captured graph.
 int Engine::substep(float sub_dt, uint32_t P) {
     int rc;
-    mark(CS_PHASE_EMIT);
+    const bool graph = settings.use_graph && P == 0xffffffffu;
+    if (!graph) mark(CS_PHASE_EMIT);
     if ((rc = emit(sub_dt))) return rc;
     fill_params(ctx_.u, sub_dt);
+    ctx_.u.jet = jet_;
     if ((rc = upload_ctx())) return rc;
+    if (graph) return substep_graph(sub_dt);
+    uint32_t sweeps = 0;
+    double r0 = -1.0, r1 = -1.0;
+    if ((rc = enqueue(P, false, sweeps, r0, r1))) return rc;
+    total_time += sub_dt;
+    last.last_sweeps = sweeps;
+    last.last_residual = r1;
+    last.initial_residual = r0;
+    prof_.sweeps += sweeps;
+    prof_.substeps += 1;
+    return CS_OK;
+}
+
+// The device work of one substep.  With `capture`, the stream is being captured into a
+// graph that later substeps replay: launch shapes then cover max_particles, every
+// kernel launches (particle counts live in the uploaded context), phases are not
+// marked, and the solve's result goes to the running totals instead of the host.
+int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, double& r1) {
+    int rc;
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
-    const uint32_t np = num_water + num_bed;
+    const uint32_t np = capture ? settings.max_particles : num_water + num_bed;
+    const bool any_p = capture || np > 0, any_bed = capture || num_bed > 0;
     const int cb = launch_cells_blocks();
     const int pb = launch_particle_blocks(np);
-    const int bb = launch_particle_blocks(num_bed);
+    const int bb = launch_particle_blocks(capture ? settings.max_particles : num_bed);
     const dim3 T(kThreads);
+    auto ph = [&](int phase) {
+        if (!capture) mark(phase);
+    };
 #define CS_LAUNCH(...)  \
     do {                \
         __VA_ARGS__;    \
         count_launch(); \
     } while (0)
-    mark(CS_PHASE_CLEAR);
+    if (capture) {
+        CS_LAUNCH(k_emit_jet<<<dim3(16, 1), T, 0, stream_>>>(dc));
+    } else if (jet_.count) {
+        CS_LAUNCH(k_emit_jet<<<dim3(launch_particle_blocks(jet_.count), 1), T, 0, stream_>>>(dc));
+    }
+    ph(CS_PHASE_CLEAR);
     // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309)
     cudaMemsetAsync(lanes_.ptr, 0, lanes_.bytes, stream_);
     cudaMemsetAsync(gvel_.ptr, 0, gvel_.bytes, stream_);
     if (P > 0) cudaMemsetAsync(metrics_.ptr, 0, metrics_.bytes, stream_);
     if (P > 1) cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_);
-    if (P > 2 && num_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc));
-    mark(CS_PHASE_P2G);
-    if (P > 3 && np) {
+    if (P > 2 && any_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    ph(CS_PHASE_P2G);
+    if (P > 3 && any_p) {
         if (settings.p2g_mode == CS_P2G_SORTED_SHARED) {
             cudaMemsetAsync(tile_count_.ptr, 0, tile_count_.bytes, stream_);
             CS_LAUNCH(k_p2g_keys<<<dim3(pb, 1), T, 0, stream_>>>(dc));
@@ -491,36 +551,136 @@ int Engine::substep(float sub_dt, uint32_t P) {
             CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc));
         }
     }
-    mark(CS_PHASE_GRID);
+    ph(CS_PHASE_GRID);
     if (P > 4) CS_LAUNCH(k_grid_update<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 5 ? 1 : 0));
     if (P > 6) CS_LAUNCH(k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc));
-    uint32_t sweeps = 0;
-    double r0 = -1.0, r1 = -1.0;
     if (P > 7) {
-        if ((rc = solve_pressure(sweeps, r0, r1))) return rc;
+        if (capture) {
+            const CsSettings& s = settings;
+            if (s.solve_mode == CS_SOLVE_RESIDUAL) {
+                if ((rc = sc_launch_prep(dc, sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_))) return rc;
+                count_launch(kScPrepLaunches);
+                if ((rc = sc_launch_cluster(dc, sc_buf_, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
+                                            stream_)))
+                    return rc;
+                count_launch();
+                CS_LAUNCH(k_sc_account<<<1, 1, 0, stream_>>>(sc_buf_.result, (ScTotals*)sc_totals_.ptr));
+            } else {
+                const uint32_t half = (s.grid_dims[0] + 1) / 2;
+                const size_t ncol = (size_t)half * s.grid_dims[1] * s.grid_dims[2];
+                const int blocks = (int)std::min<size_t>((ncol + kThreads - 1) / kThreads, (size_t)sms_ * 16);
+                for (uint32_t k = 0; k < s.pressure_rbgs_pairs; ++k) {
+                    CS_LAUNCH(k_rbgs_colour<<<dim3(blocks, 1), T, 0, stream_>>>(dc, 0u));
+                    CS_LAUNCH(k_rbgs_colour<<<dim3(blocks, 1), T, 0, stream_>>>(dc, 1u));
+                }
+            }
+        } else if ((rc = solve_pressure(sweeps, r0, r1))) {
+            return rc;
+        }
         have_prev_p = true;
     }
-    mark(CS_PHASE_PROJECT);
+    ph(CS_PHASE_PROJECT);
     if (P > 8) CS_LAUNCH(k_project<<<dim3(cb, 1), T, 0, stream_>>>(dc, 1 | (P > 9 ? 2 : 0) | (P > 10 ? 4 : 0)));
     if (P > 11) CS_LAUNCH(k_packing_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 12 ? 1 : 0));
     if (P > 13) CS_LAUNCH(k_viscosity_prepare<<<dim3(cb, 1), T, 0, stream_>>>(dc));
     if (P > 14) CS_LAUNCH(k_viscosity_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 15 ? 1 : 0));
-    mark(CS_PHASE_G2P);
-    if (P > 16 && np) CS_LAUNCH(k_g2p<<<dim3(pb, 1), T, 0, stream_>>>(dc));
-    mark(CS_PHASE_BED);
-    if (P > 17 && np) CS_LAUNCH(k_bed_coupling<<<dim3(pb, 1), T, 0, stream_>>>(dc));
-    if (P > 18 && num_bed) CS_LAUNCH(k_extraction_advect<<<dim3(bb, 1), T, 0, stream_>>>(dc));
-    if (P > 19 && num_bed) CS_LAUNCH(k_bed_dynamics<<<dim3(bb, 1), T, 0, stream_>>>(dc));
-    mark(CS_PHASE_RENDER);
-    if (P > 20 && np) CS_LAUNCH(k_prepare_render<<<dim3(pb, 1), T, 0, stream_>>>(dc));
-    mark(-1);
-    if ((rc = check(cudaGetLastError(), "substep launch"))) return rc;
-    total_time += sub_dt;
-    last.last_sweeps = sweeps;
-    last.last_residual = r1;
-    last.initial_residual = r0;
-    prof_.sweeps += sweeps;
+    ph(CS_PHASE_G2P);
+    if (P > 16 && any_p) CS_LAUNCH(k_g2p<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    ph(CS_PHASE_BED);
+    if (P > 17 && any_p) CS_LAUNCH(k_bed_coupling<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    if (P > 18 && any_bed) CS_LAUNCH(k_extraction_advect<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    if (P > 19 && any_bed) CS_LAUNCH(k_bed_dynamics<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    ph(CS_PHASE_RENDER);
+    if (P > 20 && any_p) CS_LAUNCH(k_prepare_render<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+#undef CS_LAUNCH
+    ph(-1);
+    return check(cudaGetLastError(), "substep launch");
+}
+
+Engine::GraphKey Engine::graph_key() const {
+    GraphKey k;
+    std::memset(&k, 0, sizeof(k));
+    const CsSettings& s = settings;
+    k.p2g_mode = s.p2g_mode;
+    k.check_every = s.check_every;
+    k.max_sweeps = s.max_sweeps;
+    k.solve_mode = s.solve_mode;
+    k.pressure_storage = s.pressure_storage;
+    k.rbgs_kernel = s.rbgs_kernel;
+    k.rbgs_pairs = s.pressure_rbgs_pairs;
+    k.residual_tol = s.residual_tol;
+    k.num_bed = num_bed;
+    k.max_particles = s.max_particles;
+    return k;
+}
+
+// Graph mode: capture the device work once (again when a captured setting changes)
+// and replay it; the host does not wait for the substep.
+int Engine::substep_graph(float sub_dt) {
+    int rc;
+    const GraphKey key = graph_key();
+    if (!gexec_ || !(key == gkey_)) {
+        if (gexec_) {
+            cudaGraphExecDestroy(gexec_);
+            gexec_ = nullptr;
+        }
+        if (settings.solve_mode == CS_SOLVE_RESIDUAL && sc_ranks_ == 0) {
+            set_error("graph mode needs the cluster-resident solve, which this device cannot launch");
+            return CS_ERR_UNSUPPORTED;
+        }
+        const uint64_t before = prof_.launches;
+        if ((rc = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture")))
+            return rc;
+        uint32_t sweeps = 0;
+        double r0 = -1.0, r1 = -1.0;
+        const int erc = enqueue(0xffffffffu, true, sweeps, r0, r1);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+        graph_launches_ = (uint32_t)(prof_.launches - before);
+        prof_.launches = before;
+        if (erc) {
+            if (g) cudaGraphDestroy(g);
+            return erc;
+        }
+        if ((rc = check(ce, "end capture"))) return rc;
+        rc = check(cudaGraphInstantiate(&gexec_, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        if (rc) return rc;
+        gkey_ = key;
+    }
+    if ((rc = check(cudaGraphLaunch(gexec_, stream_), "graph launch"))) return rc;
+    prof_.launches += graph_launches_;
     prof_.substeps += 1;
+    total_time += sub_dt;
+    have_prev_p = true;
+    graph_pending_ = true;
+    return CS_OK;
+}
+
+// Solve totals of the replayed substeps since the last call: sweep and residual
+// counters, the latest substep's metrics, and an error if a solve did not complete.
+int Engine::collect() {
+    if (!graph_pending_) return CS_OK;
+    graph_pending_ = false;
+    ScTotals t;
+    int rc = check(cudaMemcpyAsync(&t, sc_totals_.ptr, sizeof(t), cudaMemcpyDeviceToHost, stream_), "totals");
+    if (rc) return rc;
+    prof_.d2h_bytes += sizeof(t);
+    if ((rc = check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"))) return rc;
+    prof_.sweeps += t.sweeps - seen_.sweeps;
+    prof_.residual_evals += t.evals - seen_.evals;
+    const bool failed = t.failed != seen_.failed;
+    seen_ = t;
+    if (t.runs) {
+        last.last_sweeps = t.last.sweeps;
+        last.last_residual = t.last.r1;
+        last.initial_residual = t.last.r0;
+    }
+    if (failed) {
+        set_error("a replayed substep's pressure solve did not fit the thread-block cluster "
+                  "(16 x 4095 fluid cells); run this scene with use_graph = 0");
+        return CS_ERR_CAPACITY;
+    }
     return CS_OK;
 }
 
@@ -872,6 +1032,93 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
     return sync();
 }
 
+// ---- autotuner: time candidate configurations from one saved state ----
+int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
+    CsSettings& s = settings;
+    if (s.solve_mode != CS_SOLVE_RESIDUAL || s.pressure_storage == CS_PRESSURE_FIXED_POINT) {
+        set_error("the autotuner needs the residual-mode FP32 solve");
+        return CS_ERR_UNSUPPORTED;
+    }
+    if (substeps == 0 || !(sub_dt > 0.0f)) {
+        set_error("autotune: substeps and sub_dt must be positive");
+        return CS_ERR_INVALID_ARG;
+    }
+    uint64_t bytes = 0;
+    snapshot_size(&bytes);
+    std::vector<unsigned char> state(bytes);
+    int rc = snapshot_save(state.data(), bytes);
+    if (rc) return rc;
+    const CsSettings entry = s;
+    const float fe = frame_emitted_mass;
+    const uint32_t fd = frame_dropped;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    auto trial = [&](float omega, uint32_t ce, uint32_t p2g, float& ms) -> int {
+        int r = snapshot_load(state.data(), bytes);
+        if (r) return r;
+        s.rbgs_omega = omega;
+        s.check_every = ce;
+        s.p2g_mode = p2g;
+        bool converged = true;
+        cudaEventRecord(a, stream_);
+        for (uint32_t k = 0; k < substeps; ++k) {
+            if ((r = substep(sub_dt, 0xffffffffu))) return r;
+            converged = converged && last.last_residual >= 0.0 && last.last_residual <= (double)s.residual_tol;
+        }
+        cudaEventRecord(b, stream_);
+        if ((r = sync())) return r;
+        cudaEventElapsedTime(&ms, a, b);
+        ms /= (float)substeps;
+        if (!converged) ms = INFINITY;
+        return CS_OK;
+    };
+    CsTuneResult res{};
+    float ms = 0.0f;
+    if ((rc = trial(entry.rbgs_omega, entry.check_every, entry.p2g_mode, ms))) goto done;
+    res.initial_ms = ms;
+    res.best_ms = ms;
+    res.omega = entry.rbgs_omega;
+    res.check_every = entry.check_every;
+    res.p2g_mode = entry.p2g_mode;
+    res.trials = 1;
+    // P2G mode at the entry solver settings, then the solver at the chosen mode
+    for (uint32_t m : {(uint32_t)CS_P2G_ATOMIC32, (uint32_t)CS_P2G_SORTED_SHARED}) {
+        if (m == entry.p2g_mode) continue;
+        if ((rc = trial(entry.rbgs_omega, entry.check_every, m, ms))) goto done;
+        ++res.trials;
+        if (ms < res.best_ms) {
+            res.best_ms = ms;
+            res.p2g_mode = m;
+        }
+    }
+    for (float omega : {1.80f, 1.85f, 1.88f, 1.90f, 1.92f, 1.94f, 1.96f})
+        for (uint32_t ce : {5u, 10u, 20u}) {
+            if (omega == res.omega && ce == res.check_every) continue;
+            if ((rc = trial(omega, ce, res.p2g_mode, ms))) goto done;
+            ++res.trials;
+            if (ms < res.best_ms) {
+                res.best_ms = ms;
+                res.omega = omega;
+                res.check_every = ce;
+            }
+        }
+done:
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const int rc2 = snapshot_load(state.data(), bytes);
+    s = entry;
+    frame_emitted_mass = fe;
+    frame_dropped = fd;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    s.rbgs_omega = res.omega;
+    s.check_every = res.check_every;
+    s.p2g_mode = res.p2g_mode;
+    if (out) *out = res;
+    return CS_OK;
+}
+
 // ---- launch helpers shared by Engine and noalloc.cu ----
 // Largest cluster size the solve kernel can be launched with on the current device
 // (16 with the non-portable opt-in, else 8), 0 when neither fits.
@@ -1000,9 +1247,15 @@ static int validate(const CsSettings* s) {
         return CS_ERR_INVALID_ARG;
     }
     // modes declared by the ABI whose engine path is not built yet
-    if (s->p2g_mode == CS_P2G_INT64 || s->warm_start == CS_WARM_LEARNED || s->device_emission || s->use_graph) {
+    if (s->use_graph && (!s->device_emission || (s->solve_mode == CS_SOLVE_RESIDUAL &&
+                                                  (s->pressure_storage != CS_PRESSURE_FP32 || s->rbgs_kernel == 1)))) {
+        set_error("use_graph needs device_emission = 1 and, in residual mode, FP32 storage with the "
+                  "cluster-resident solve");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (s->p2g_mode == CS_P2G_INT64 || s->warm_start == CS_WARM_LEARNED) {
         set_error("settings request a mode this engine build does not implement "
-                  "(int64 P2G, learned warm start, device emission or graph capture)");
+                  "(int64 P2G or learned warm start)");
         return CS_ERR_UNSUPPORTED;
     }
     if (s->warm_start != CS_WARM_NONE && s->pressure_storage == CS_PRESSURE_FIXED_POINT) {
@@ -1117,6 +1370,41 @@ int32_t cs_set_flow_override(CsSim* sim, float flow, float speed) {
     sim->e->inflow.flow_override = flow > 0.0f ? flow : 0.0f;
     sim->e->inflow.speed_override = flow > 0.0f ? speed : 0.0f;
     return CS_OK;
+}
+int32_t cs_set_solver(CsSim* sim, float omega, uint32_t check_every, uint32_t max_sweeps) {
+    CS_SIM(sim);
+    if (omega != 0.0f && !(omega > 0.0f && omega < 2.0f)) {
+        set_error("omega must lie in (0, 2)");
+        return CS_ERR_INVALID_ARG;
+    }
+    CsSettings& s = sim->e->settings;
+    if (omega != 0.0f) s.rbgs_omega = omega;
+    if (check_every) s.check_every = check_every;
+    if (max_sweeps) s.max_sweeps = max_sweeps;
+    return CS_OK;
+}
+int32_t cs_set_p2g_mode(CsSim* sim, uint32_t mode) {
+    CS_SIM(sim);
+    if (mode != CS_P2G_ATOMIC32 && mode != CS_P2G_SORTED_SHARED) {
+        set_error("P2G mode must be CS_P2G_ATOMIC32 or CS_P2G_SORTED_SHARED");
+        return CS_ERR_INVALID_ARG;
+    }
+    sim->e->settings.p2g_mode = mode;
+    return CS_OK;
+}
+int32_t cs_set_graph_mode(CsSim* sim, uint32_t use_graph) {
+    CS_SIM(sim);
+    CsSettings t = sim->e->settings;
+    t.use_graph = use_graph ? 1u : 0u;
+    int rc = validate(&t);
+    if (rc) return rc;
+    if ((rc = sim->e->sync())) return rc;
+    sim->e->settings.use_graph = t.use_graph;
+    return CS_OK;
+}
+int32_t cs_autotune(CsSim* sim, float sub_dt, uint32_t substeps, CsTuneResult* out) {
+    CS_SIM(sim);
+    return sim->e->autotune(sub_dt, substeps, out);
 }
 int32_t cs_get_counts(const CsSim* sim, uint32_t* nw, uint32_t* nb, uint32_t* mp) {
     CS_SIM(sim);

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -76,6 +77,24 @@ private:
     // sorted P2G
     DeviceBuffer p2g_key_, p2g_rank_, p2g_sorted_, tile_count_, tile_start_, tile_temp_;
     uint32_t p2g_tiles_ = 0;
+    JetPlan jet_{};         // device emission planned for the current substep
+    // graph mode: the substep's device work captured once and replayed
+    int enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, double& r1);
+    int substep_graph(float sub_dt);
+    int collect();          // read the solve totals of replayed substeps
+    struct GraphKey {
+        uint32_t p2g_mode, check_every, max_sweeps, solve_mode, pressure_storage, rbgs_kernel, rbgs_pairs;
+        float residual_tol;
+        uint32_t num_bed, max_particles;
+        bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+    };
+    GraphKey graph_key() const;
+    cudaGraphExec_t gexec_ = nullptr;
+    GraphKey gkey_{};
+    uint32_t graph_launches_ = 0;  // own kernels per replay
+    bool graph_pending_ = false;   // replays whose solve totals are not yet read
+    DeviceBuffer sc_totals_;
+    ScTotals seen_{};              // totals at the last collect()
     // cluster-resident solver
     DeviceBuffer sc_scratch_;  // every solver scratch buffer, laid out by sc_scratch_layout
     ScBuffers sc_buf_{};
@@ -93,6 +112,7 @@ public:
     int timer_start();
     int timer_stop(float* ms);
     int flush_l2();
+    int autotune(float sub_dt, uint32_t substeps, CsTuneResult* out);
     void mark(int phase);      // close the open phase and open `phase` (-1 closes only)
     void count_launch(uint32_t n = 1) {
         prof_.launches += n;

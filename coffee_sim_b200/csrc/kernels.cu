@@ -194,7 +194,7 @@ constexpr int P2G_TILE = 4;
 constexpr int P2G_SPAN = P2G_TILE + 2;
 constexpr int P2G_NODES = P2G_SPAN * P2G_SPAN * P2G_SPAN;
 constexpr uint32_t P2G_NO_TILE = 0xffffffffu;
-constexpr int P2G_THREADS = 128;
+constexpr int P2G_THREADS = 256;
 
 __device__ __forceinline__ uint32_t p2g_tile_axis(int b, uint32_t nt) {
     int q = b + 1;
@@ -206,20 +206,36 @@ __device__ __forceinline__ uint32_t p2g_tile_axis(int b, uint32_t nt) {
 __global__ void k_p2g_keys(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
-    uint32_t n = u.num_water + u.num_bed;
-    CS_FOR(pid, n) {
-        const float4 P = c.pos[pid], Vv = c.vel[pid];
-        const float ph = c.c0[pid].w;
+    const uint32_t n = u.num_water + u.num_bed;
+    const uint32_t lane = threadIdx.x & 31u;
+    // warp-uniform loop (blockDim.x is a multiple of 32) so the warp votes below see
+    // every lane
+    for (uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; w0 < n; w0 += gridDim.x * blockDim.x) {
+        const uint32_t pid = w0 + lane;
         uint32_t key = P2G_NO_TILE, rank = 0;
-        if (is_water_phase(ph) && !(Vv.w <= inactive_mass(u))) {
-            const int bx = (int)floorf((P.x - u.ox) * u.inv_dx - 0.5f);
-            const int by = (int)floorf((P.y - u.oy) * u.inv_dx - 0.5f);
-            const int bz = (int)floorf((P.z - u.oz) * u.inv_dx - 0.5f);
-            key = (p2g_tile_axis(bz, u.ntz) * u.nty + p2g_tile_axis(by, u.nty)) * u.ntx + p2g_tile_axis(bx, u.ntx);
-            rank = atomicAdd(&c.tile_count[key], 1u);
+        if (pid < n) {
+            const float4 P = c.pos[pid], Vv = c.vel[pid];
+            const float ph = c.c0[pid].w;
+            if (is_water_phase(ph) && !(Vv.w <= inactive_mass(u))) {
+                const int bx = (int)floorf((P.x - u.ox) * u.inv_dx - 0.5f);
+                const int by = (int)floorf((P.y - u.oy) * u.inv_dx - 0.5f);
+                const int bz = (int)floorf((P.z - u.oz) * u.inv_dx - 0.5f);
+                key = (p2g_tile_axis(bz, u.ntz) * u.nty + p2g_tile_axis(by, u.nty)) * u.ntx +
+                      p2g_tile_axis(bx, u.ntx);
+            }
         }
-        c.p2g_key[pid] = key;
-        c.p2g_rank[pid] = rank;
+        // one counter atomic per distinct tile in the warp (neighbouring particles
+        // usually share a tile); ranks inside the warp follow lane order
+        const uint32_t same = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = __ffs(same) - 1;
+        uint32_t base = 0;
+        if (key != P2G_NO_TILE && lane == leader) base = atomicAdd(&c.tile_count[key], (uint32_t)__popc(same));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (key != P2G_NO_TILE) rank = base + __popc(same & ((1u << lane) - 1u));
+        if (pid < n) {
+            c.p2g_key[pid] = key;
+            c.p2g_rank[pid] = rank;
+        }
     }
 }
 
@@ -244,7 +260,12 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
         const int ox = (int)(tx * P2G_TILE) - 1, oy = (int)(ty * P2G_TILE) - 1, oz = (int)(tz * P2G_TILE) - 1;
         for (int i = threadIdx.x; i < 6 * P2G_NODES; i += blockDim.x) (&acc[0][0])[i] = 0;
         __syncthreads();
-        for (uint32_t k = first + threadIdx.x; k < last; k += blockDim.x) {
+        // Particles of one cell are mostly adjacent in the tile list; visiting each block
+        // of P2G_THREADS entries in an odd-stride order gives a warp particles of
+        // different cells, so its shared-memory atomics rarely hit one address.
+        for (uint32_t blk = first; blk < last; blk += P2G_THREADS) {
+            const uint32_t k = blk + ((threadIdx.x * 41u) & (P2G_THREADS - 1));
+            if (k >= last) continue;
             P2GSample q;
             if (!p2g_prepare(c, c.p2g_sorted[k], q)) continue;
             const bool inside = q.bx >= ox && q.by >= oy && q.bz >= oz && q.bx + 2 < ox + P2G_SPAN &&
@@ -1388,6 +1409,38 @@ __global__ void k_pack_particles(const Ctx* __restrict__ cp, uint32_t first, uin
         }
     }
 }
+// Device jet emission (inflow.rs:196-218): sample i of the substep at golden-angle
+// position first_sequence + i on the nozzle disk, back-dated by its age.  cos/sin are
+// the double-precision values rounded to float (the oracle's device-emission mode does
+// the same; inflow.rs evaluates them in f32).
+__global__ void k_emit_jet(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const JetPlan& j = c.u.jet;
+    const float golden = 2.399963f, radial = 0.7548777f;
+    CS_FOR(i, j.count) {
+        const float sf = (float)(uint32_t)(j.first_sequence + i);
+        float ru = (sf + 0.5f) * radial;
+        ru = ru - truncf(ru);
+        const float r = j.jet_radius * sqrtf(ru);
+        const float theta = sf * golden;
+        const float age = (((float)i + 0.5f) / (float)j.count) * j.dt;
+        const float ct = (float)cos((double)theta), st = (float)sin((double)theta);
+        float p[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float off = j.t1[k] * r * ct + j.t2[k] * r * st;
+            p[k] = j.origin[k] + off - j.vel[k] * age;
+        }
+        const uint32_t s = j.first_slot + i;
+        c.pos[s] = make_float4(p[0], p[1], p[2], 1.0f);
+        c.vel[s] = make_float4(j.vel[0], j.vel[1], j.vel[2], j.particle_mass);
+        const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        c.c0[s] = z;
+        c.c1[s] = z;
+        c.c2[s] = z;
+    }
+}
+
 __global__ void k_unpack_particles(const Ctx* __restrict__ cp, uint32_t first, uint32_t count, const float* in, int what) {
     const Ctx& c = cp[blockIdx.y];
     CS_FOR(k, count) {

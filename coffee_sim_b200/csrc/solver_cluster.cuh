@@ -489,4 +489,18 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     cluster.sync();  // keep every CTA's shared memory alive until remote accesses end
 }
 
+// Adds one solve's result to the running totals (one thread; graph mode, where the
+// host does not read each substep's result).
+__global__ void k_sc_account(const ScResult* __restrict__ res, ScTotals* __restrict__ tot) {
+    const ScResult r = *res;
+    tot->runs += 1;
+    if (r.status != 1) {
+        tot->failed += 1;
+    } else {
+        tot->sweeps += r.sweeps;
+        tot->evals += r.evals;
+    }
+    tot->last = r;
+}
+
 }  // namespace cs

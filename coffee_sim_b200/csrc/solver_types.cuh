@@ -54,6 +54,11 @@ struct ScResult {
     uint32_t sweeps, evals, status, pad;
     double r0, r1;
 };
+// Running totals of the solves of replayed substeps (graph mode reads them lazily).
+struct ScTotals {
+    unsigned long long sweeps, evals, failed, runs;
+    ScResult last;
+};
 // counters: halo size per rank, then send-list length per (rank, colour)
 constexpr int SC_COUNTS = SC_MAX_RANKS * 3;
 

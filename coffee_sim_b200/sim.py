@@ -317,6 +317,30 @@ class MpmSim3D:
         return added.value
 
     # -- device timing / profiling --
+    def current_settings(self):
+        """The simulation's settings as they are now (the tuner and setters change them)."""
+        st = _ffi.CsSettings()
+        self.lib.call("cs_get_settings", self._h, C.byref(st))
+        return st
+
+    def set_solver(self, omega=0.0, check_every=0, max_sweeps=0):
+        """Residual-mode solver parameters from the next substep on (0 keeps a value)."""
+        self.lib.call("cs_set_solver", self._h, C.c_float(omega), check_every, max_sweeps)
+
+    def set_p2g_mode(self, mode):
+        self.lib.call("cs_set_p2g_mode", self._h, mode)
+
+    def set_graph_mode(self, on):
+        """Capture the substep in a CUDA graph and replay it (needs device emission)."""
+        self.lib.call("cs_set_graph_mode", self._h, 1 if on else 0)
+
+    def autotune(self, sub_dt, substeps=4):
+        """Time candidate solver / P2G configurations from the current state and keep
+        the fastest that converges; the state itself is left unchanged."""
+        r = _ffi.CsTuneResult()
+        self.lib.call("cs_autotune", self._h, C.c_float(sub_dt), substeps, C.byref(r))
+        return r
+
     def profile_enable(self, on=True):
         self.lib.call("cs_profile_enable", self._h, 1 if on else 0)
 

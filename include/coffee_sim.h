@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define CS_ABI_VERSION 4u
+#define CS_ABI_VERSION 5u
 
 typedef enum CsStatus {
     CS_OK = 0,
@@ -370,6 +370,33 @@ typedef struct CsProfile {
 } CsProfile;
 int32_t cs_profile_enable(CsSim* sim, int32_t on);   /* resets the counters */
 int32_t cs_profile_read(CsSim* sim, CsProfile* out); /* synchronises */
+
+/* ---- Solver parameters and autotuner (no counterpart in the reference) ---- */
+
+/* Change the residual-mode solver between substeps: over-relaxation (0 keeps the current
+ * value), pairs between residual checks (0 keeps), cap on pairs (0 keeps). */
+int32_t cs_set_solver(CsSim* sim, float omega, uint32_t check_every, uint32_t max_sweeps);
+/* P2G accumulation (CS_P2G_ATOMIC32 or CS_P2G_SORTED_SHARED) from the next substep on. */
+int32_t cs_set_p2g_mode(CsSim* sim, uint32_t mode);
+/* Graph mode from the next substep on (same conditions as settings.use_graph). */
+int32_t cs_set_graph_mode(CsSim* sim, uint32_t use_graph);
+
+typedef struct CsTuneResult {
+    float omega;           /* chosen over-relaxation */
+    uint32_t check_every;  /* chosen pairs between residual checks */
+    uint32_t p2g_mode;     /* chosen P2G accumulation */
+    uint32_t trials;       /* configurations timed */
+    float best_ms;         /* device ms per substep with the chosen configuration */
+    float initial_ms;      /* device ms per substep with the configuration at entry */
+    uint32_t reserved[2];
+} CsTuneResult;
+
+/* Time `substeps` substeps of length sub_dt from the current state for each candidate
+ * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 5/10/20),
+ * restoring the state after every trial; keep the fastest whose every substep reached
+ * the residual target.  The simulation ends in the state it had at entry with the
+ * chosen configuration applied.  Residual-mode solves only (CS_ERR_UNSUPPORTED else). */
+int32_t cs_autotune(CsSim* sim, float sub_dt, uint32_t substeps, CsTuneResult* out);
 int32_t cs_timer_start(CsSim* sim);                  /* CUDA event on the sim's stream */
 int32_t cs_timer_stop(CsSim* sim, float* ms);        /* device ms since cs_timer_start; synchronises */
 int32_t cs_flush_l2(CsSim* sim);                     /* overwrite a buffer larger than L2 on the sim's stream */

@@ -1709,7 +1709,16 @@ struct Sim : SimBase {
             float r = jr * std::sqrt(ru);
             float theta = sf * golden;
             float age = (((float)i + 0.5f) / (float)count) * dt;
-            float ct = std::cos(theta), st = std::sin(theta);
+            // inflow.rs:205 uses f32 cos/sin; the device emission mode rounds the double-precision
+            // values instead (the same on the GPU and here)
+            float ct, st;
+            if (settings.device_emission) {
+                ct = (float)std::cos((double)theta);
+                st = (float)std::sin((double)theta);
+            } else {
+                ct = std::cos(theta);
+                st = std::sin(theta);
+            }
             float off[3];
             for (int c = 0; c < 3; ++c) off[c] = t1[c] * r * ct + t2[c] * r * st;
             size_t slot = (size_t)total + i;
@@ -1991,6 +2000,29 @@ int32_t cs_set_flow_override(CsSim* sim, float flow, float speed) {
     sim->impl->flow_override = flow > 0.0f ? flow : 0.0f;
     sim->impl->speed_override = flow > 0.0f ? speed : 0.0f;
     return CS_OK;
+}
+int32_t cs_set_solver(CsSim* sim, float omega, uint32_t check_every, uint32_t max_sweeps) {
+    if (!sim) return fail(CS_ERR_INVALID_ARG, "null sim");
+    if (omega != 0.0f && !(omega > 0.0f && omega < 2.0f)) return fail(CS_ERR_INVALID_ARG, "omega must lie in (0, 2)");
+    CsSettings& s = sim->impl->settings;
+    if (omega != 0.0f) s.rbgs_omega = omega;
+    if (check_every) s.check_every = check_every;
+    if (max_sweeps) s.max_sweeps = max_sweeps;
+    return CS_OK;
+}
+int32_t cs_set_p2g_mode(CsSim* sim, uint32_t mode) {
+    if (!sim) return fail(CS_ERR_INVALID_ARG, "null sim");
+    if (mode != CS_P2G_ATOMIC32 && mode != CS_P2G_SORTED_SHARED) return fail(CS_ERR_INVALID_ARG, "bad P2G mode");
+    sim->impl->settings.p2g_mode = mode;  // the oracle's deposit is order-independent either way
+    return CS_OK;
+}
+int32_t cs_set_graph_mode(CsSim* sim, uint32_t use_graph) {
+    if (!sim) return fail(CS_ERR_INVALID_ARG, "null sim");
+    sim->impl->settings.use_graph = use_graph ? 1u : 0u;  // nothing to capture on the CPU
+    return CS_OK;
+}
+int32_t cs_autotune(CsSim*, float, uint32_t, CsTuneResult*) {
+    return fail(CS_ERR_UNSUPPORTED, "the oracle has no autotuner (it times nothing)");
 }
 int32_t cs_get_counts(const CsSim* sim, uint32_t* nw, uint32_t* nb, uint32_t* mp) {
     if (!sim) return fail(CS_ERR_INVALID_ARG, "null sim");

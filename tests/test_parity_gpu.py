@@ -239,3 +239,58 @@ def test_sorted_p2g_matches_atomic_on_v60(engine):
             sim.step_substep(scenes.C2_DT)
         _assert_same(_state(sims[0]), _state(sims[1]), f"V60 substep {k}",
                      ["particles", "affine", "bed_extract", "grid_vel", "pressure"])
+
+
+def test_device_emission_matches_oracle(engine, oracle):
+    """Jet samples built by a kernel (device_emission = 1): ten frames of the centre
+    pour, bit-exact against the oracle's matching emission mode."""
+    s = MpmSettings.benchmark_center_pour(engine)
+    s.raw.device_emission = 1
+    e, o = pair(s, engine, oracle)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+    for f in range(10):
+        e.step_frame(FRAME)
+        o.step_frame(FRAME)
+        assert e.particle_count() == o.particle_count()
+        _assert_same(_state(e, cells=False), _state(o, cells=False), f"device emission frame {f}")
+    assert e.total_emitted_mass() == o.total_emitted_mass()
+    assert e.particle_count() > 12000
+
+
+def test_graph_replay_matches_direct_launches_v60(engine):
+    """use_graph = 1: the substep captured once and replayed gives the same states, sweep
+    counts and residuals as launching it directly (V60 pour, cluster solve)."""
+    sims = []
+    for graph in (0, 1):
+        s = scenes.c2_v60(engine)
+        s.raw.rbgs_omega = 1.9
+        s.raw.device_emission = 1
+        s.raw.use_graph = graph
+        sim = MpmSim3D(s, engine)
+        scenes.populate_c2(sim)
+        sim.set_flow_override(4.0, 0.8 * s.sim_units_per_meter)
+        sims.append(sim)
+    for k in range(4):
+        for sim in sims:
+            sim.step_substep(scenes.C2_DT)
+        ma, mb = sims[0].latest_metrics(), sims[1].latest_metrics()
+        assert ma.last_sweeps == mb.last_sweeps and ma.last_residual == mb.last_residual
+        assert sims[0].particle_count() == sims[1].particle_count()
+        _assert_same(_state(sims[0]), _state(sims[1]), f"graph substep {k}",
+                     ["particles", "affine", "bed_extract", "grid_vel", "pressure"])
+
+
+def test_graph_frames_match_oracle_reference_mode(engine, oracle):
+    """Reference configuration (fixed-point pressure, 40 pairs) in graph mode with
+    device emission: ten frames bit-exact against the oracle."""
+    s = MpmSettings.benchmark_center_pour(engine)
+    s.raw.device_emission = 1
+    s.raw.use_graph = 1
+    e, o = pair(s, engine, oracle)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+    for f in range(10):
+        e.step_frame(FRAME)
+        o.step_frame(FRAME)
+        _assert_same(_state(e, cells=False), _state(o, cells=False), f"graph frame {f}")
