@@ -281,6 +281,7 @@ PROTOTYPES = {
     "cs_read_affine": (I32, [P, U32, U32, PF]),
     "cs_read_bed_extract": (I32, [P, U32, U32, PF]),
     "cs_read_grid_lanes": (I32, [P, PI32]),
+    "cs_read_grid_lanes64": (I32, [P, C.POINTER(C.c_int64)]),
     "cs_read_grid_vel": (I32, [P, PF]),
     "cs_read_pressure": (I32, [P, PF]),
     "cs_read_cell_kind": (I32, [P, PI32]),

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/coffee_sim.h"
+#include "solver_types.cuh"
 
 namespace cs {
 
@@ -20,6 +21,8 @@ enum : int32_t { CELL_AIR = 0, CELL_SURFACE = 1, CELL_INTERIOR = 2, CELL_BED = 3
 enum : int { M_MAX_DIV = 0, M_FLUID = 1, M_DIV_CLAMP = 2, M_P_CLAMP = 3, M_OVERFLOW = 4, M_NAN = 5, M_TIMEOUT = 6 };
 constexpr float FP_SCALE = 262144.0f;            // state.rs:13, 2^18
 constexpr float INV_FP_SCALE = 1.0f / 262144.0f;
+constexpr float FP_SCALE64 = 4294967296.0f;      // int64 P2G mode, 2^32
+constexpr float INV_FP_SCALE64 = 1.0f / 4294967296.0f;
 constexpr float FP_VALUE_LIMIT = 8192.0f;        // state.rs:18
 constexpr float METRICS_DIV_FP_SCALE = 1024.0f;  // state.rs:28
 constexpr double FP64_SCALE = 4294967296.0;      // 2^32, int64 P2G mode
@@ -104,6 +107,7 @@ struct Ctx {
     const uint8_t* cls;     // cells, 1 = solid
     uint32_t* metrics;      // 8 counters
     double* resid;          // [0] sum r^2, [1] sum b^2
+    ScBuffers sb;           // cluster-resident pressure solve scratch of this instance
 };
 
 // ---------------- math with WGSL semantics ----------------
@@ -132,6 +136,7 @@ __device__ __forceinline__ float smoothstepf(float lo, float hi, float x) {
 }
 __device__ __forceinline__ float wfract(float x) { return x - floorf(x); }
 __device__ __forceinline__ int32_t to_i32(float x) { return __float2int_rz(x); }  // saturating, NaN -> 0
+__device__ __forceinline__ long long to_i64(float x) { return __float2ll_rz(x); }  // saturating, NaN -> 0
 __device__ __forceinline__ uint32_t to_u32(float x) { return __float2uint_rz(x); }
 __device__ __forceinline__ f3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 

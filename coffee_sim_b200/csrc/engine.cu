@@ -136,6 +136,7 @@ int Engine::init() {
         const ScScratch lay = sc_scratch_layout(cells_, sc_codes_, cub);
         if ((rc = alloc(sc_scratch_, lay.total))) return rc;
         sc_buf_ = sc_buffers_at((unsigned char*)sc_scratch_.ptr, lay, cub);
+        ctx_.sb = sc_buf_;
         sc_ranks_ = sc_max_cluster_ranks();
     }
 
@@ -393,12 +394,12 @@ int Engine::solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done) 
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
     const uint32_t codes = (uint32_t)sc_codes_;
     mark(CS_PHASE_RESIDUAL);
-    int rc = sc_launch_prep(dc, sc_buf_, codes, sc_ranks_, 1, stream_, sms_);
+    int rc = sc_launch_prep(dc, &sc_buf_, codes, sc_ranks_, 1, stream_, sms_);
     if (rc) return rc;
     count_launch(kScPrepLaunches);
     mark(CS_PHASE_SWEEPS);
     const CsSettings& s = settings;
-    if ((rc = sc_launch_cluster(dc, sc_buf_, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every, stream_)))
+    if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every, stream_)))
         return rc;
     count_launch();
     ScResult res;
@@ -533,12 +534,13 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309)
     cudaMemsetAsync(lanes_.ptr, 0, lanes_.bytes, stream_);
     cudaMemsetAsync(gvel_.ptr, 0, gvel_.bytes, stream_);
+    if (settings.p2g_mode == CS_P2G_INT64) cudaMemsetAsync(lanes64_.ptr, 0, lanes64_.bytes, stream_);
     if (P > 0) cudaMemsetAsync(metrics_.ptr, 0, metrics_.bytes, stream_);
     if (P > 1) cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_);
     if (P > 2 && any_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc));
     ph(CS_PHASE_P2G);
     if (P > 3 && any_p) {
-        if (settings.p2g_mode == CS_P2G_SORTED_SHARED) {
+        if (settings.p2g_mode != CS_P2G_ATOMIC32) {
             cudaMemsetAsync(tile_count_.ptr, 0, tile_count_.bytes, stream_);
             CS_LAUNCH(k_p2g_keys<<<dim3(pb, 1), T, 0, stream_>>>(dc));
             size_t temp = tile_temp_.bytes;
@@ -546,7 +548,10 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
                                           (uint32_t*)tile_start_.ptr, (int)p2g_tiles_ + 1, stream_);
             CS_LAUNCH(k_p2g_scatter<<<dim3(pb, 1), T, 0, stream_>>>(dc));
             const int tb = (int)std::min<uint32_t>(p2g_tiles_, (uint32_t)sms_ * 16);
-            CS_LAUNCH(k_p2g_tiles<<<dim3(tb, 1), P2G_THREADS, 0, stream_>>>(dc));
+            if (settings.p2g_mode == CS_P2G_INT64)
+                CS_LAUNCH(k_p2g_tiles<unsigned long long><<<dim3(tb, 1), P2G_THREADS, 0, stream_>>>(dc));
+            else
+                CS_LAUNCH(k_p2g_tiles<int32_t><<<dim3(tb, 1), P2G_THREADS, 0, stream_>>>(dc));
         } else {
             CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc));
         }
@@ -558,9 +563,9 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
         if (capture) {
             const CsSettings& s = settings;
             if (s.solve_mode == CS_SOLVE_RESIDUAL) {
-                if ((rc = sc_launch_prep(dc, sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_))) return rc;
+                if ((rc = sc_launch_prep(dc, &sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_))) return rc;
                 count_launch(kScPrepLaunches);
-                if ((rc = sc_launch_cluster(dc, sc_buf_, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
+                if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
                                             stream_)))
                     return rc;
                 count_launch();
@@ -749,6 +754,12 @@ int Engine::write_particles(int what, uint32_t first, uint32_t count, const floa
     k_unpack_particles<<<dim3(launch_particle_blocks(count), 1), kThreads, 0, stream_>>>(
         (const Ctx*)d_ctx_.ptr, first, count, (const float*)staging_.ptr, what);
     // the staging buffer is reused by the next upload: wait for this one
+    return sync();
+}
+
+int Engine::read_lanes64(int64_t* out) {
+    int rc = check(cudaMemcpyAsync(out, lanes64_.ptr, lanes64_.bytes, cudaMemcpyDeviceToHost, stream_), "lanes64");
+    if (rc) return rc;
     return sync();
 }
 
@@ -1032,6 +1043,217 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
     return sync();
 }
 
+// ---- batched ensemble ----
+Ensemble::~Ensemble() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (Engine* e : eng) delete e;
+    if (d_ctx) cudaFree(d_ctx);
+    if (d_results) cudaFree(d_results);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Ensemble::init(const CsSettings* s, uint32_t n) {
+    if (n == 0) {
+        set_error("an ensemble needs at least one instance");
+        return CS_ERR_INVALID_ARG;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        CsSettings t = s[i];
+        t.device_emission = 1;  // jet samples are built by the batched emission kernel
+        t.use_graph = 0;
+        int rc = validate_settings(&t);
+        if (rc) return rc;
+        const CsSettings& a = s[0];
+        if (t.grid_dims[0] != a.grid_dims[0] || t.grid_dims[1] != a.grid_dims[1] || t.grid_dims[2] != a.grid_dims[2] ||
+            t.p2g_mode != a.p2g_mode || t.solve_mode != a.solve_mode || t.pressure_storage != a.pressure_storage ||
+            t.device != a.device || t.pressure_rbgs_pairs != a.pressure_rbgs_pairs || t.max_sweeps != a.max_sweeps ||
+            t.check_every != a.check_every || t.residual_tol != a.residual_tol) {
+            set_error("ensemble instances must share grid dims, device, P2G mode and solver settings");
+            return CS_ERR_INVALID_ARG;
+        }
+        Engine* e = new Engine(t);
+        eng.push_back(e);
+        if ((rc = e->init())) return rc;
+    }
+    Engine& e0 = *eng[0];
+    if (e0.settings.solve_mode == CS_SOLVE_RESIDUAL &&
+        (e0.settings.pressure_storage != CS_PRESSURE_FP32 || e0.sc_ranks_ == 0)) {
+        set_error("ensembles in residual mode need FP32 storage and the cluster-resident solve");
+        return CS_ERR_UNSUPPORTED;
+    }
+    ranks = e0.sc_ranks_;
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&d_ctx, sizeof(Ctx) * n) != cudaSuccess || cudaMalloc(&d_results, sizeof(ScResult) * n) != cudaSuccess) {
+        set_error("ensemble allocation failed");
+        return CS_ERR_CUDA;
+    }
+    hctx.resize(n);
+    hsb.resize(n);
+    results.resize(n);
+    for (uint32_t i = 0; i < n; ++i) hsb[i] = eng[i]->sc_buf_;
+    return CS_OK;
+}
+
+int Ensemble::sync() {
+    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+        set_error(std::string("ensemble stream: ") + cudaGetErrorString(cudaGetLastError()));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+
+// One substep of every instance: host prologues (jet plans, uniforms), one context
+// upload, then each pass as a single launch over all instances.
+int Ensemble::substep(float sub_dt) {
+    int rc;
+    const uint32_t n = size();
+    for (uint32_t i = 0; i < n; ++i) {
+        Engine& e = *eng[i];
+        if ((rc = e.sync())) return rc;  // no work of its own may be in flight
+        if ((rc = e.emit(sub_dt))) return rc;
+        e.fill_params(e.ctx_.u, sub_dt);
+        e.ctx_.u.jet = e.jet_;
+        hctx[i] = e.ctx_;
+    }
+    if (cudaMemcpyAsync(d_ctx, hctx.data(), sizeof(Ctx) * n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+        set_error("ensemble context upload failed");
+        return CS_ERR_CUDA;
+    }
+    if ((rc = enqueue())) return rc;
+    for (uint32_t i = 0; i < n; ++i) {
+        Engine& e = *eng[i];
+        e.total_time += sub_dt;
+        e.have_prev_p = true;
+        e.prof_.substeps += 1;
+    }
+    return CS_OK;
+}
+
+int Ensemble::enqueue() {
+    int rc;
+    const uint32_t n = size();
+    Engine& e0 = *eng[0];
+    const CsSettings& s = e0.settings;
+    const Ctx* dc = (const Ctx*)d_ctx;
+    uint32_t max_np = 0, max_bed = 0, max_jet = 0;
+    for (Engine* e : eng) {
+        max_np = std::max(max_np, e->num_water + e->num_bed);
+        max_bed = std::max(max_bed, e->num_bed);
+        max_jet = std::max(max_jet, e->jet_.count);
+    }
+    const int cb = e0.launch_cells_blocks();
+    const int pb = e0.launch_particle_blocks(max_np);
+    const int bb = e0.launch_particle_blocks(max_bed);
+    const dim3 T(kThreads);
+    cudaStream_t st = stream;
+    if (max_jet) k_emit_jet<<<dim3(e0.launch_particle_blocks(max_jet), n), T, 0, st>>>(dc);
+    k_clear_batch<<<dim3(cb, n), T, 0, st>>>(dc, e0.p2g_tiles_ + 1);
+    if (max_bed) k_bed_lookup_scatter<<<dim3(bb, n), T, 0, st>>>(dc);
+    if (max_np) {
+        if (s.p2g_mode != CS_P2G_ATOMIC32) {
+            k_p2g_keys<<<dim3(pb, n), T, 0, st>>>(dc);
+            for (Engine* e : eng) {
+                size_t temp = e->tile_temp_.bytes;
+                cub::DeviceScan::ExclusiveSum(e->tile_temp_.ptr, temp, (const uint32_t*)e->tile_count_.ptr,
+                                              (uint32_t*)e->tile_start_.ptr, (int)e->p2g_tiles_ + 1, st);
+            }
+            k_p2g_scatter<<<dim3(pb, n), T, 0, st>>>(dc);
+            const int tb = (int)std::min<uint32_t>(e0.p2g_tiles_, (uint32_t)e0.sms_ * 16);
+            if (s.p2g_mode == CS_P2G_INT64)
+                k_p2g_tiles<unsigned long long><<<dim3(tb, n), P2G_THREADS, 0, st>>>(dc);
+            else
+                k_p2g_tiles<int32_t><<<dim3(tb, n), P2G_THREADS, 0, st>>>(dc);
+        } else {
+            k_p2g_atomic<<<dim3(pb, n), T, 0, st>>>(dc);
+        }
+    }
+    k_grid_update<<<dim3(cb, n), T, 0, st>>>(dc, 1);
+    k_classify<<<dim3(cb, n), T, 0, st>>>(dc);
+    if (s.solve_mode == CS_SOLVE_RESIDUAL) {
+        if ((rc = sc_launch_prep(dc, hsb.data(), (uint32_t)e0.sc_codes_, ranks, n, st, e0.sms_))) return rc;
+        if ((rc = sc_launch_cluster(dc, ranks, n, s.residual_tol, s.max_sweeps, s.check_every, st))) return rc;
+        k_gather_results<<<1, 256, 0, st>>>(dc, n, (ScResult*)d_results);
+        if (cudaMemcpyAsync(results.data(), d_results, sizeof(ScResult) * n, cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            (rc = sync()))
+            return rc ? rc : CS_ERR_CUDA;
+        for (uint32_t i = 0; i < n; ++i) {
+            Engine& e = *eng[i];
+            const ScResult& r = results[i];
+            if (r.status != 1) {
+                // this instance's fluid does not fit the cluster: solve it alone with
+                // per-colour launches on its own stream
+                if ((rc = e.upload_ctx())) return rc;
+                const int keep = e.sc_ranks_;
+                e.sc_ranks_ = 0;
+                uint32_t sw = 0;
+                double r0 = -1.0, r1 = -1.0;
+                rc = e.solve_pressure(sw, r0, r1);
+                e.sc_ranks_ = keep;
+                if (rc) return rc;
+                if ((rc = e.sync())) return rc;
+                e.last.last_sweeps = sw;
+                e.last.initial_residual = r0;
+                e.last.last_residual = r1;
+                e.prof_.sweeps += sw;
+                continue;
+            }
+            e.last.last_sweeps = r.sweeps;
+            e.last.initial_residual = r.r0;
+            e.last.last_residual = r.r1;
+            e.prof_.sweeps += r.sweeps;
+            e.prof_.residual_evals += r.evals;
+        }
+    } else {
+        const uint32_t half = (s.grid_dims[0] + 1) / 2;
+        const size_t ncol = (size_t)half * s.grid_dims[1] * s.grid_dims[2];
+        const int blocks = (int)std::min<size_t>((ncol + kThreads - 1) / kThreads, (size_t)e0.sms_ * 16);
+        for (uint32_t k = 0; k < s.pressure_rbgs_pairs; ++k) {
+            k_rbgs_colour<<<dim3(blocks, n), T, 0, st>>>(dc, 0u);
+            k_rbgs_colour<<<dim3(blocks, n), T, 0, st>>>(dc, 1u);
+        }
+        for (Engine* e : eng) {
+            e->last.last_sweeps = s.pressure_rbgs_pairs;
+            e->prof_.sweeps += s.pressure_rbgs_pairs;
+        }
+    }
+    k_project<<<dim3(cb, n), T, 0, st>>>(dc, 1 | 2 | 4);
+    k_packing_apply<<<dim3(cb, n), T, 0, st>>>(dc, 1);
+    k_viscosity_prepare<<<dim3(cb, n), T, 0, st>>>(dc);
+    k_viscosity_apply<<<dim3(cb, n), T, 0, st>>>(dc, 1);
+    if (max_np) {
+        k_g2p<<<dim3(pb, n), T, 0, st>>>(dc);
+        k_bed_coupling<<<dim3(pb, n), T, 0, st>>>(dc);
+    }
+    if (max_bed) {
+        k_extraction_advect<<<dim3(bb, n), T, 0, st>>>(dc);
+        k_bed_dynamics<<<dim3(bb, n), T, 0, st>>>(dc);
+    }
+    if (max_np) k_prepare_render<<<dim3(pb, n), T, 0, st>>>(dc);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {
+        set_error(std::string("ensemble substep launch: ") + cudaGetErrorString(err));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+
+int Ensemble::step_frame(float dt) {
+    const CsSettings& s = eng[0]->settings;
+    const float fdt = std::fmin(dt, s.max_frame_dt);
+    const uint32_t k = s.substeps > 1 ? s.substeps : 1;
+    const float sdt = fdt / (float)k;
+    for (Engine* e : eng) {
+        e->frame_emitted_mass = 0.0f;
+        e->frame_dropped = 0;
+    }
+    for (uint32_t j = 0; j < k; ++j) {
+        int rc = substep(sdt);
+        if (rc) return rc;
+    }
+    return CS_OK;
+}
+
 // ---- autotuner: time candidate configurations from one saved state ----
 int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     CsSettings& s = settings;
@@ -1084,7 +1306,7 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     res.trials = 1;
     // P2G mode at the entry solver settings, then the solver at the chosen mode
     for (uint32_t m : {(uint32_t)CS_P2G_ATOMIC32, (uint32_t)CS_P2G_SORTED_SHARED}) {
-        if (m == entry.p2g_mode) continue;
+        if (m == entry.p2g_mode || entry.p2g_mode == CS_P2G_INT64) continue;  // int64 changes the numerics
         if ((rc = trial(entry.rbgs_omega, entry.check_every, m, ms))) goto done;
         ++res.trials;
         if (ms < res.best_ms) {
@@ -1158,22 +1380,22 @@ size_t sc_scan_temp_bytes(uint32_t codes) {
 // Morton scan, chunking, neighbour slots, halo/send lists and coefficients for
 // `instances` solves whose scratch blocks lie back to back (kScPrepLaunches launches
 // for one instance).
-int sc_launch_prep(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, uint32_t instances,
+int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ranks, uint32_t instances,
                    cudaStream_t stream, int sms) {
     const int cb = (int)std::min<size_t>((codes + kThreads - 1) / kThreads, (size_t)sms * 16);
-    k_sc_flags<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb, codes);
+    k_sc_flags<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, codes);
     for (uint32_t k = 0; k < instances; ++k) {
-        const ScBuffers b = sc_instance(sb, k);
-        size_t temp = b.cub_bytes;
-        if (cub::DeviceScan::ExclusiveSum(b.cub_temp, temp, b.flags, b.scan, (int)codes, stream) != cudaSuccess) {
+        size_t temp = sb[k].cub_bytes;
+        if (cub::DeviceScan::ExclusiveSum(sb[k].cub_temp, temp, sb[k].flags, sb[k].scan, (int)codes, stream) !=
+            cudaSuccess) {
             set_error("scan launch failed");
             return CS_ERR_CUDA;
         }
     }
-    k_sc_totals<<<dim3(1, instances), 1, 0, stream>>>(d_ctx, sb, (uint32_t)ranks, codes);
-    k_sc_starts<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb, codes);
-    k_sc_map<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb, codes);
-    k_sc_halo<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, sb);
+    k_sc_totals<<<dim3(1, instances), 1, 0, stream>>>(d_ctx, (uint32_t)ranks, codes);
+    k_sc_starts<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, codes);
+    k_sc_map<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, codes);
+    k_sc_halo<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("solver prep launch: ") + cudaGetErrorString(e));
@@ -1183,8 +1405,8 @@ int sc_launch_prep(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ra
 }
 
 // The cluster solve of `instances` independent systems: one cluster of `ranks` CTAs each.
-int sc_launch_cluster(const Ctx* d_ctx, const ScBuffers& sb, int ranks, uint32_t instances, float tol,
-                      uint32_t max_pairs, uint32_t check_every, cudaStream_t stream) {
+int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,
+                      uint32_t check_every, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ranks, instances, 1);
     cfg.blockDim = dim3(SC_THREADS, 1, 1);
@@ -1197,7 +1419,7 @@ int sc_launch_cluster(const Ctx* d_ctx, const ScBuffers& sb, int ranks, uint32_t
     attr.val.clusterDim.z = 1;
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_sc_solve, d_ctx, sb, tol, max_pairs, check_every);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_sc_solve, d_ctx, tol, max_pairs, check_every);
     if (e != cudaSuccess) {
         set_error(std::string("cluster solve launch: ") + cudaGetErrorString(e));
         return CS_ERR_CUDA;
@@ -1253,9 +1475,8 @@ static int validate(const CsSettings* s) {
                   "cluster-resident solve");
         return CS_ERR_INVALID_ARG;
     }
-    if (s->p2g_mode == CS_P2G_INT64 || s->warm_start == CS_WARM_LEARNED) {
-        set_error("settings request a mode this engine build does not implement "
-                  "(int64 P2G or learned warm start)");
+    if (s->warm_start == CS_WARM_LEARNED) {
+        set_error("settings request a mode this engine build does not implement (learned warm start)");
         return CS_ERR_UNSUPPORTED;
     }
     if (s->warm_start != CS_WARM_NONE && s->pressure_storage == CS_PRESSURE_FIXED_POINT) {
@@ -1268,6 +1489,10 @@ static int validate(const CsSettings* s) {
     }
     return CS_OK;
 }
+
+namespace cs {
+int validate_settings(const CsSettings* s) { return ::validate(s); }
+}  // namespace cs
 
 #define CS_SIM(sim)                          \
     if (!(sim) || !(sim)->e) {               \
@@ -1385,8 +1610,13 @@ int32_t cs_set_solver(CsSim* sim, float omega, uint32_t check_every, uint32_t ma
 }
 int32_t cs_set_p2g_mode(CsSim* sim, uint32_t mode) {
     CS_SIM(sim);
-    if (mode != CS_P2G_ATOMIC32 && mode != CS_P2G_SORTED_SHARED) {
-        set_error("P2G mode must be CS_P2G_ATOMIC32 or CS_P2G_SORTED_SHARED");
+    if (mode != CS_P2G_ATOMIC32 && mode != CS_P2G_SORTED_SHARED &&
+        !(mode == CS_P2G_INT64 && sim->e->settings.p2g_mode == CS_P2G_INT64)) {
+        set_error("P2G mode must be CS_P2G_ATOMIC32 or CS_P2G_SORTED_SHARED (int64 is chosen at creation)");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (sim->e->settings.p2g_mode == CS_P2G_INT64 && mode != CS_P2G_INT64) {
+        set_error("a simulation created with int64 P2G keeps it");
         return CS_ERR_INVALID_ARG;
     }
     sim->e->settings.p2g_mode = mode;
@@ -1487,6 +1717,15 @@ int32_t cs_read_grid_lanes(CsSim* s, int32_t* o) {
     CS_SIM(s);
     CS_PTR(o);
     return s->e->read_lanes(o);
+}
+int32_t cs_read_grid_lanes64(CsSim* s, int64_t* o) {
+    CS_SIM(s);
+    CS_PTR(o);
+    if (s->e->settings.p2g_mode != CS_P2G_INT64) {
+        set_error("not an int64 P2G simulation");
+        return CS_ERR_INVALID_ARG;
+    }
+    return s->e->read_lanes64(o);
 }
 int32_t cs_read_grid_vel(CsSim* s, float* o) {
     CS_SIM(s);

@@ -18,7 +18,11 @@ struct DeviceBuffer {
     size_t bytes = 0;
 };
 
+class Ensemble;
+
 class Engine {
+    friend class Ensemble;
+
 public:
     explicit Engine(const CsSettings& s);
     ~Engine();
@@ -32,6 +36,7 @@ public:
     int read_particles(int what, uint32_t first, uint32_t count, float* out);
     int write_particles(int what, uint32_t first, uint32_t count, const float* in);
     int read_lanes(int32_t* out);
+    int read_lanes64(int64_t* out);
     int read_gvel(float* out);
     int read_pressure(float* out);
     int read_kind(int32_t* out);
@@ -135,5 +140,32 @@ private:
 };
 
 void set_error(const std::string& msg);
+int validate_settings(const CsSettings* s);
+
+// n independent pours with the same grid, stepped together: every pass is one launch
+// with gridDim.y = n over a device array of the instances' contexts (no counterpart in
+// the reference).  Each instance keeps its own Engine (buffers, host state, readback);
+// the ensemble's stream runs the batched substeps.
+class Ensemble {
+public:
+    ~Ensemble();
+    int init(const CsSettings* settings, uint32_t n);
+    int substep(float sub_dt);
+    int step_frame(float dt);
+    int sync();
+    Engine& at(uint32_t i) { return *eng[i]; }
+    uint32_t size() const { return (uint32_t)eng.size(); }
+
+private:
+    int enqueue();
+    std::vector<Engine*> eng;
+    cudaStream_t stream = nullptr;
+    void* d_ctx = nullptr;       // n x Ctx
+    void* d_results = nullptr;   // n x ScResult
+    std::vector<Ctx> hctx;
+    std::vector<ScBuffers> hsb;
+    std::vector<ScResult> results;
+    int ranks = 0;
+};
 
 }  // namespace cs

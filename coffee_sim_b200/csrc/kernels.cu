@@ -134,10 +134,11 @@ __device__ __forceinline__ bool p2g_prepare(const Ctx& c, uint32_t pid, P2GSampl
     q.cpv = q.rpv * clamp_j(P.w);
     return true;
 }
-template <class Add>
+template <bool I64, class Add>
 __device__ __forceinline__ void p2g_deposit(const Ctx& c, const P2GSample& q, Add add) {
     const Params& u = c.u;
-    const float lim = 1.0e9f;
+    const float scale = I64 ? FP_SCALE64 : FP_SCALE;
+    const float lim = I64 ? 1.0e18f : 1.0e9f;
     bool overflow = false;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -149,20 +150,29 @@ __device__ __forceinline__ void p2g_deposit(const Ctx& c, const P2GSample& q, Ad
                 if (!in_grid(u, cx, cy, cz)) continue;
                 float w = q.wx[i] * q.wy[j] * q.wz[k];
                 f3 dpos = mk(((float)i - q.fx) * u.dx, ((float)j - q.fy) * u.dx, ((float)k - q.fz) * u.dx);
-                float mfp = (w * q.mp) * FP_SCALE;
-                float rfp = (w * q.rpv) * FP_SCALE;
-                float cfp = (w * q.cpv) * FP_SCALE;
-                float mx = (w * (q.mv.x + dot3(q.a0, dpos))) * FP_SCALE;
-                float my = (w * (q.mv.y + dot3(q.a1, dpos))) * FP_SCALE;
-                float mz = (w * (q.mv.z + dot3(q.a2, dpos))) * FP_SCALE;
+                float mfp = (w * q.mp) * scale;
+                float rfp = (w * q.rpv) * scale;
+                float cfp = (w * q.cpv) * scale;
+                float mx = (w * (q.mv.x + dot3(q.a0, dpos))) * scale;
+                float my = (w * (q.mv.y + dot3(q.a1, dpos))) * scale;
+                float mz = (w * (q.mv.z + dot3(q.a2, dpos))) * scale;
                 overflow |= fabsf(mfp) > lim || fabsf(mx) > lim || fabsf(my) > lim || fabsf(mz) > lim ||
                             fabsf(rfp) > lim || fabsf(cfp) > lim;
-                add(cx, cy, cz, 0, to_i32(mfp));
-                add(cx, cy, cz, 1, to_i32(mx));
-                add(cx, cy, cz, 2, to_i32(my));
-                add(cx, cy, cz, 3, to_i32(mz));
-                add(cx, cy, cz, 4, to_i32(rfp));
-                add(cx, cy, cz, 5, to_i32(cfp));
+                if (I64) {
+                    add(cx, cy, cz, 0, to_i64(mfp));
+                    add(cx, cy, cz, 1, to_i64(mx));
+                    add(cx, cy, cz, 2, to_i64(my));
+                    add(cx, cy, cz, 3, to_i64(mz));
+                    add(cx, cy, cz, 4, to_i64(rfp));
+                    add(cx, cy, cz, 5, to_i64(cfp));
+                } else {
+                    add(cx, cy, cz, 0, to_i32(mfp));
+                    add(cx, cy, cz, 1, to_i32(mx));
+                    add(cx, cy, cz, 2, to_i32(my));
+                    add(cx, cy, cz, 3, to_i32(mz));
+                    add(cx, cy, cz, 4, to_i32(rfp));
+                    add(cx, cy, cz, 5, to_i32(cfp));
+                }
                 if (overflow) {
                     atomicAdd(&c.metrics[M_OVERFLOW], 1u);
                     overflow = false;
@@ -178,7 +188,7 @@ __global__ void k_p2g_atomic(const Ctx* __restrict__ cp) {
     CS_FOR(pid, n) {
         P2GSample q;
         if (!p2g_prepare(c, pid, q)) continue;
-        p2g_deposit(c, q, [&](int x, int y, int z, int l, int32_t v) {
+        p2g_deposit<false>(c, q, [&](int x, int y, int z, int l, int32_t v) {
             atomicAdd(&c.lanes[(size_t)l * u.cells + cidx(u, x, y, z)], v);
         });
     }
@@ -248,10 +258,15 @@ __global__ void k_p2g_scatter(const Ctx* __restrict__ cp) {
     }
 }
 
+// T = int32_t (reference lanes) or unsigned long long (int64 mode; two's-complement
+// sums are the same as signed ones)
+template <class T>
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict__ cp) {
-    __shared__ int32_t acc[6][P2G_NODES];
+    constexpr bool I64 = sizeof(T) == 8;
+    __shared__ T acc[6][P2G_NODES];
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
+    T* glanes = I64 ? reinterpret_cast<T*>(c.lanes64) : reinterpret_cast<T*>(c.lanes);
     const uint32_t ntiles = u.ntx * u.nty * u.ntz;
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const uint32_t first = c.tile_start[t], last = c.tile_start[t + 1];
@@ -271,12 +286,12 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
             const bool inside = q.bx >= ox && q.by >= oy && q.bz >= oz && q.bx + 2 < ox + P2G_SPAN &&
                                 q.by + 2 < oy + P2G_SPAN && q.bz + 2 < oz + P2G_SPAN;
             if (inside) {
-                p2g_deposit(c, q, [&](int x, int y, int z, int l, int32_t v) {
-                    atomicAdd(&acc[l][((z - oz) * P2G_SPAN + (y - oy)) * P2G_SPAN + (x - ox)], v);
+                p2g_deposit<I64>(c, q, [&](int x, int y, int z, int l, auto v) {
+                    atomicAdd(&acc[l][((z - oz) * P2G_SPAN + (y - oy)) * P2G_SPAN + (x - ox)], (T)v);
                 });
             } else {
-                p2g_deposit(c, q, [&](int x, int y, int z, int l, int32_t v) {
-                    atomicAdd(&c.lanes[(size_t)l * u.cells + cidx(u, x, y, z)], v);
+                p2g_deposit<I64>(c, q, [&](int x, int y, int z, int l, auto v) {
+                    atomicAdd(&glanes[(size_t)l * u.cells + cidx(u, x, y, z)], (T)v);
                 });
             }
         }
@@ -287,8 +302,8 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
             const uint32_t ci = cidx(u, x, y, z);
 #pragma unroll
             for (int l = 0; l < 6; ++l) {
-                const int32_t v = acc[l][i];
-                if (v != 0) atomicAdd(&c.lanes[(size_t)l * u.cells + ci], v);
+                const T v = acc[l][i];
+                if (v != 0) atomicAdd(&glanes[(size_t)l * u.cells + ci], v);
             }
         }
         __syncthreads();
@@ -300,11 +315,9 @@ __global__ void k_grid_update(const Ctx* __restrict__ cp, int with_boundary) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     CS_FOR(i, u.cells) {
-        float mass = (float)c.lanes[i] * INV_FP_SCALE;
+        float mass = p2g_lane(c, 0, i);
         if (mass < 1e-6f) continue;
-        f3 v = mk((float)c.lanes[(size_t)u.cells + i] * INV_FP_SCALE / mass,
-                  (float)c.lanes[2 * (size_t)u.cells + i] * INV_FP_SCALE / mass,
-                  (float)c.lanes[3 * (size_t)u.cells + i] * INV_FP_SCALE / mass);
+        f3 v = mk(p2g_lane(c, 1, i) / mass, p2g_lane(c, 2, i) / mass, p2g_lane(c, 3, i) / mass);
         v.y += u.gravity * u.dt;
         float sp = len3(v);
         if (sp > u.vel_cap) v = v * (u.vel_cap / sp);
@@ -1439,6 +1452,28 @@ __global__ void k_emit_jet(const Ctx* __restrict__ cp) {
         c.c1[s] = z;
         c.c2[s] = z;
     }
+}
+
+// Per-substep clears of every ensemble instance in one launch (the memsets of the
+// single-simulation path): P2G lanes, grid velocity, bed lookup, metrics, tile counts.
+__global__ void k_clear_batch(const Ctx* __restrict__ cp, uint32_t tiles) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    CS_FOR(i, u.cells) {
+#pragma unroll
+        for (int l = 0; l < 6; ++l) c.lanes[(size_t)l * u.cells + i] = 0;
+        if (u.int64_grid)
+#pragma unroll
+            for (int l = 0; l < 6; ++l) c.lanes64[(size_t)l * u.cells + i] = 0;
+        c.gvel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        c.lookup[i] = -1;
+    }
+    CS_FOR(t, tiles) c.tile_count[t] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x < 8) c.metrics[threadIdx.x] = 0u;
+}
+// Copy each instance's solve result into one array (one readback for the ensemble).
+__global__ void k_gather_results(const Ctx* __restrict__ cp, uint32_t n, ScResult* __restrict__ out) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = *cp[i].sb.result;
 }
 
 __global__ void k_unpack_particles(const Ctx* __restrict__ cp, uint32_t first, uint32_t count, const float* in, int what) {

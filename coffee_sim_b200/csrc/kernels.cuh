@@ -47,8 +47,13 @@ __device__ __forceinline__ void vscratch_store(const Ctx& c, uint32_t i, f3 v) {
     lane(c, 2)[i] = to_i32(v.y * FP_SCALE);
     lane(c, 3)[i] = to_i32(v.z * FP_SCALE);
 }
-__device__ __forceinline__ float rest_vol(const Ctx& c, uint32_t i) { return (float)lane(c, 4)[i] * INV_FP_SCALE; }
-__device__ __forceinline__ float cur_vol(const Ctx& c, uint32_t i) { return (float)lane(c, 5)[i] * INV_FP_SCALE; }
+// P2G lanes 0-5: i32 * 2^18 (the reference), or i64 * 2^32 in the int64 mode
+__device__ __forceinline__ float p2g_lane(const Ctx& c, int l, uint32_t i) {
+    if (c.u.int64_grid) return (float)c.lanes64[(size_t)l * c.u.cells + i] * INV_FP_SCALE64;
+    return (float)lane(c, l)[i] * INV_FP_SCALE;
+}
+__device__ __forceinline__ float rest_vol(const Ctx& c, uint32_t i) { return p2g_lane(c, 4, i); }
+__device__ __forceinline__ float cur_vol(const Ctx& c, uint32_t i) { return p2g_lane(c, 5, i); }
 
 // shader.rs:293-304; evaluated once per cell by classify and stored in c.fill
 __device__ __forceinline__ float liquid_fill(const Ctx& c, uint32_t i, int32_t kind) {

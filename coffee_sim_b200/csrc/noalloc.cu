@@ -137,6 +137,7 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
     ctx.metrics = reinterpret_cast<uint32_t*>(base + kOffMetrics);
 
     const cs::ScBuffers sb = cs::sc_buffers_at(base + kOffSolver, kSolver, kCubBytes);
+    ctx.sb = sb;
     const cs::Ctx* dctx = reinterpret_cast<const cs::Ctx*>(base + kOffCtx);
 
     cudaError_t e = cudaMemcpyAsync(base + kOffCtx, &ctx, sizeof(ctx), cudaMemcpyHostToDevice, st);
@@ -146,8 +147,8 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
         cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
         return CS_ERR_CUDA;
     }
-    if ((rc = cs::sc_launch_prep(dctx, sb, codes, slot->ranks, 1, st, slot->sms))) return rc;
-    if ((rc = cs::sc_launch_cluster(dctx, sb, slot->ranks, 1, residual_tol, max_pairs, check_every, st))) return rc;
+    if ((rc = cs::sc_launch_prep(dctx, &sb, codes, slot->ranks, 1, st, slot->sms))) return rc;
+    if ((rc = cs::sc_launch_cluster(dctx, slot->ranks, 1, residual_tol, max_pairs, check_every, st))) return rc;
     cs::ScResult res;
     e = cudaMemcpyAsync(&res, sb.result, sizeof(res), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

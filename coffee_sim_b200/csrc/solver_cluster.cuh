@@ -64,8 +64,8 @@ __device__ __forceinline__ bool sc_cell_of_code(const Params& u, uint32_t m, uin
     return true;
 }
 
-__global__ void k_sc_flags(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t codes) {
-    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
+__global__ void k_sc_flags(const Ctx* __restrict__ cp, uint32_t codes) {
+    const ScBuffers& sb = cp[blockIdx.y].sb;
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const int32_t* kl = c.lanes + 3 * (size_t)u.cells;
@@ -78,8 +78,8 @@ __global__ void k_sc_flags(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t c
 }
 
 // Totals and chunking (one thread), then the red count before each chunk's first cell.
-__global__ void k_sc_totals(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t ranks, uint32_t codes) {
-    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
+__global__ void k_sc_totals(const Ctx* __restrict__ cp, uint32_t ranks, uint32_t codes) {
+    const ScBuffers& sb = cp[blockIdx.y].sb;
     unsigned long long last = sb.scan[codes - 1] + sb.flags[codes - 1];
     uint32_t nf = (uint32_t)(last & 0xffffffffull), nr = (uint32_t)(last >> 32);
     uint32_t chunk = (nf + ranks - 1) / ranks;
@@ -91,8 +91,8 @@ __global__ void k_sc_totals(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t 
     for (int k = 0; k < SC_COUNTS; ++k) sb.counts[k] = 0u;
 }
 
-__global__ void k_sc_starts(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t codes) {
-    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
+__global__ void k_sc_starts(const Ctx* __restrict__ cp, uint32_t codes) {
+    const ScBuffers& sb = cp[blockIdx.y].sb;
     const uint32_t chunk = sb.info->chunk;
     if (chunk == 0) return;
     CS_FOR(m, codes) {
@@ -102,8 +102,8 @@ __global__ void k_sc_starts(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t 
     }
 }
 
-__global__ void k_sc_map(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t codes) {
-    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
+__global__ void k_sc_map(const Ctx* __restrict__ cp, uint32_t codes) {
+    const ScBuffers& sb = cp[blockIdx.y].sb;
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const ScInfo& inf = *sb.info;
@@ -137,8 +137,8 @@ __global__ void k_sc_map(const Ctx* __restrict__ cp, ScBuffers sb0, uint32_t cod
 // send list for its colour.  Validity of a fluid face is symmetric (face_weight of
 // two fluid cells is 1 or min of the fills), so both sides agree on which faces exist.
 // Halo slot order comes from atomics and differs between runs; it only places copies.
-__global__ void k_sc_halo(const Ctx* __restrict__ cp, ScBuffers sb0) {
-    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
+__global__ void k_sc_halo(const Ctx* __restrict__ cp) {
+    const ScBuffers& sb = cp[blockIdx.y].sb;
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     const ScInfo& inf = *sb.info;
@@ -235,11 +235,11 @@ __device__ __forceinline__ float sc_weight(float fc_i, float fc_j) {
 
 // One cluster per instance (blockIdx.y); R = cluster size along x.
 __global__ void __launch_bounds__(SC_THREADS, 1)
-    k_sc_solve(const Ctx* __restrict__ cp, ScBuffers sb0, float tol, uint32_t max_pairs, uint32_t check_every) {
+    k_sc_solve(const Ctx* __restrict__ cp, float tol, uint32_t max_pairs, uint32_t check_every) {
     extern __shared__ __align__(16) unsigned char smem[];
     cg::cluster_group cluster = cg::this_cluster();
-    const ScBuffers sb = sc_instance(sb0, blockIdx.y);
     const Ctx& c = cp[blockIdx.y];
+    const ScBuffers& sb = c.sb;
     const Params& u = c.u;
     const uint32_t R = cluster.num_blocks();
     const uint32_t rank = cluster.block_rank();

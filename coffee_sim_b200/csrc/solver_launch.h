@@ -15,9 +15,11 @@ constexpr uint32_t kScPrepLaunches = 5;  // own kernels of sc_launch_prep per ca
 void set_error(const std::string& msg);
 int sc_max_cluster_ranks();
 size_t sc_scan_temp_bytes(uint32_t codes);
-int sc_launch_prep(const Ctx* d_ctx, const ScBuffers& sb, uint32_t codes, int ranks, uint32_t instances,
+// d_ctx: device array of `instances` contexts (each carrying its ScBuffers); sb: the
+// same ScBuffers on the host, for the CUB scans launched from the host.
+int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ranks, uint32_t instances,
                    cudaStream_t stream, int sms);
-int sc_launch_cluster(const Ctx* d_ctx, const ScBuffers& sb, int ranks, uint32_t instances, float tol,
-                      uint32_t max_pairs, uint32_t check_every, cudaStream_t stream);
+int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,
+                      uint32_t check_every, cudaStream_t stream);
 
 }  // namespace cs

@@ -74,9 +74,8 @@ struct ScBuffers {
     uint32_t* counts;            // SC_COUNTS
     ScInfo* info;
     ScResult* result;
-    void* cub_temp;
+    void* cub_temp;              // CUB scan storage (host-side launches)
     size_t cub_bytes;
-    size_t stride;               // bytes between the scratch of consecutive instances
 };
 
 // Byte offsets of every solver scratch buffer inside one allocation.
@@ -116,31 +115,7 @@ inline ScBuffers sc_buffers_at(unsigned char* base, const ScScratch& s, size_t c
     b.result = reinterpret_cast<ScResult*>(base + s.result);
     b.cub_temp = base + s.cub;
     b.cub_bytes = cub_bytes;
-    b.stride = s.total;
     return b;
-}
-
-// The buffers of instance k of an ensemble whose scratch blocks are laid out back to back.
-template <class T>
-__host__ __device__ __forceinline__ T* sc_shift(T* p, size_t bytes) {
-    return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(p) + bytes);
-}
-__host__ __device__ __forceinline__ ScBuffers sc_instance(const ScBuffers& b, uint32_t k) {
-    const size_t o = b.stride * k;
-    ScBuffers r = b;
-    r.flags = sc_shift(b.flags, o);
-    r.scan = sc_shift(b.scan, o);
-    r.ref_of_cell = sc_shift(b.ref_of_cell, o);
-    r.cell_of = sc_shift(b.cell_of, o);
-    r.slot_ref = sc_shift(b.slot_ref, o);
-    r.slot_coef = sc_shift(b.slot_coef, o);
-    r.halo_fill = sc_shift(b.halo_fill, o);
-    r.send = sc_shift(b.send, o);
-    r.counts = sc_shift(b.counts, o);
-    r.info = sc_shift(b.info, o);
-    r.result = sc_shift(b.result, o);
-    r.cub_temp = sc_shift(reinterpret_cast<unsigned char*>(b.cub_temp), o);
-    return r;
 }
 
 }  // namespace cs

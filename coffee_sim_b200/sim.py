@@ -264,6 +264,12 @@ class MpmSim3D:
     def read_grid_lanes(self):
         return self._read_cells("cs_read_grid_lanes", np.int32, 6).reshape(6, -1)
 
+    def read_grid_lanes64(self):
+        """P2G lanes of an int64-mode simulation: (6, cells) int64, value * 2^32."""
+        out = np.zeros(6 * self.settings.cells, dtype=np.int64)
+        self.lib.call("cs_read_grid_lanes64", self._h, out.ctypes.data_as(C.POINTER(C.c_int64)))
+        return out.reshape(6, -1)
+
     def read_grid_vel(self):
         return self._read_cells("cs_read_grid_vel", np.float32, 4).reshape(-1, 4)
 
@@ -374,3 +380,85 @@ class MpmSim3D:
     def restore(self, blob):
         buf = (C.c_uint8 * len(blob)).from_buffer_copy(blob)
         self.lib.call("cs_snapshot_load", self._h, buf, len(blob))
+
+
+class MpmEnsemble:
+    """n independent pours with one grid size stepped together on one GPU (the batched
+    engine: every pass is one launch over all instances).  Engine extension without a
+    reference counterpart; each instance reads back like an MpmSim3D."""
+
+    def __init__(self, settings_list, lib=None):
+        self.lib = lib if lib is not None else engine_library()
+        self.settings = [s.copy() if isinstance(s, MpmSettings) else MpmSettings(s) for s in settings_list]
+        arr = (_ffi.CsSettings * len(self.settings))(*[s.raw for s in self.settings])
+        self._h = C.c_void_p()
+        self.lib.call("cs_ensemble_create", arr, len(self.settings), C.byref(self._h))
+
+    def __len__(self):
+        return len(self.settings)
+
+    def close(self):
+        if self._h:
+            self.lib.lib.cs_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step_substep(self, sub_dt):
+        self.lib.call("cs_ensemble_step_substep", self._h, C.c_float(sub_dt))
+
+    def step_frame(self, dt):
+        self.lib.call("cs_ensemble_step_frame", self._h, C.c_float(dt))
+
+    def member(self, i):
+        """A view of instance i with the add_water_block / settings interface that the
+        scene builders use."""
+        return _EnsembleMember(self, i)
+
+    def add_water_block(self, i, lo, hi, per_axis=2, jitter=0.25, seed=0, require_open_sdf=False):
+        lo_a = (C.c_float * 3)(*lo)
+        hi_a = (C.c_float * 3)(*hi)
+        added = C.c_uint32()
+        self.lib.call("cs_ensemble_add_water_block", self._h, i, lo_a, hi_a, per_axis, C.c_float(jitter), seed,
+                      1 if require_open_sdf else 0, C.byref(added))
+        return added.value
+
+    def set_kettle_angle(self, i, deg):
+        self.lib.call("cs_ensemble_set_kettle_angle", self._h, i, C.c_float(deg))
+
+    def set_flow_override(self, i, flow_ml_s, exit_speed):
+        self.lib.call("cs_ensemble_set_flow_override", self._h, i, C.c_float(flow_ml_s), C.c_float(exit_speed))
+
+    def counts(self, i):
+        nw, nb = C.c_uint32(), C.c_uint32()
+        self.lib.call("cs_ensemble_get_counts", self._h, i, C.byref(nw), C.byref(nb))
+        return nw.value, nb.value
+
+    def particle_count(self, i):
+        return sum(self.counts(i))
+
+    def read_particles(self, i, first=0, count=None):
+        if count is None:
+            count = self.particle_count(i) - first
+        out = np.zeros((count, 8), dtype=np.float32)
+        self.lib.call("cs_ensemble_read_particles", self._h, i, first, count,
+                      out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def metrics(self, i):
+        m = _ffi.CsMetrics()
+        self.lib.call("cs_ensemble_get_metrics", self._h, i, C.byref(m))
+        return m
+
+
+class _EnsembleMember:
+    def __init__(self, ens, i):
+        self.ens, self.i = ens, i
+        self.settings = ens.settings[i]
+
+    def add_water_block(self, lo, hi, per_axis=2, jitter=0.25, seed=0, require_open_sdf=False):
+        return self.ens.add_water_block(self.i, lo, hi, per_axis, jitter, seed, require_open_sdf)

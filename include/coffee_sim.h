@@ -301,6 +301,7 @@ int32_t cs_read_particles(CsSim* sim, uint32_t first, uint32_t count, float* out
 int32_t cs_read_affine(CsSim* sim, uint32_t first, uint32_t count, float* out);        /* 12 f32 each */
 int32_t cs_read_bed_extract(CsSim* sim, uint32_t first, uint32_t count, float* out);   /* 8 f32 each */
 int32_t cs_read_grid_lanes(CsSim* sim, int32_t* out);       /* 6 x cells, reference lane aliasing */
+int32_t cs_read_grid_lanes64(CsSim* sim, int64_t* out);     /* 6 x cells, i64 * 2^32 P2G lanes (int64 mode) */
 int32_t cs_read_grid_vel(CsSim* sim, float* out);           /* 4 x cells */
 int32_t cs_read_pressure(CsSim* sim, float* out);           /* cells, decoded to f32 */
 int32_t cs_read_cell_kind(CsSim* sim, int32_t* out);        /* cells, kind after classify */

@@ -89,7 +89,7 @@ struct SimBase {
     virtual float sample_sdf_pub(float x, float y, float z) = 0;
 };
 
-enum { RD_PART, RD_AFF, RD_BEDX, RD_LANES, RD_GVEL, RD_P, RD_KIND, RD_LOOKUP, RD_DELTA, RD_RENDER, RD_SDF, RD_CLASS };
+enum { RD_PART, RD_AFF, RD_BEDX, RD_LANES, RD_GVEL, RD_P, RD_KIND, RD_LOOKUP, RD_DELTA, RD_RENDER, RD_SDF, RD_CLASS, RD_LANES64 };
 
 template <class R>
 struct Sim : SimBase {
@@ -117,6 +117,7 @@ struct Sim : SimBase {
 
     std::vector<R> part, aff, bedx, render;  // reference AoS layouts
     std::vector<int32_t> grid;                // 6 lanes
+    std::vector<int64_t> grid64;              // 6 lanes, i64 * 2^32 (int64 P2G mode)
     std::vector<R> gvel;                      // 4 per cell
     std::vector<R> pf, divf;                  // FP32-storage pressure/divergence
     std::vector<R> plo, pd, gres;             // refinement: pressure low part, correction, residual
@@ -137,6 +138,7 @@ struct Sim : SimBase {
         bedx.assign(mp * 8, R(0));
         render.assign(mp * 8, R(0));
         grid.assign(cells * 6, 0);
+        grid64.assign(settings.p2g_mode == CS_P2G_INT64 ? cells * 6 : 0, 0);
         gvel.assign(cells * 4, R(0));
         pf.assign(cells, R(0));
         divf.assign(cells, R(0));
@@ -165,6 +167,7 @@ struct Sim : SimBase {
         std::fill(bedx.begin(), bedx.end(), R(0));
         std::fill(render.begin(), render.end(), R(0));
         std::fill(grid.begin(), grid.end(), 0);
+        std::fill(grid64.begin(), grid64.end(), 0);
         std::fill(gvel.begin(), gvel.end(), R(0));
         std::fill(pf.begin(), pf.end(), R(0));
         std::fill(divf.begin(), divf.end(), R(0));
@@ -297,8 +300,14 @@ struct Sim : SimBase {
         lane(2)[c] = to_i32(cl.y * u.fp_scale);
         lane(3)[c] = to_i32(cl.z * u.fp_scale);
     }
-    R rest_vol(uint32_t c) { return R(lane(4)[c]) * u.inv_fp; }
-    R cur_vol(uint32_t c) { return R(lane(5)[c]) * u.inv_fp; }
+    // P2G lanes 0-5: i32 * 2^18, or i64 * 2^32 in the int64 mode
+    bool int64_grid() const { return settings.p2g_mode == CS_P2G_INT64; }
+    R p2g_lane(int l, uint32_t c) {
+        if (int64_grid()) return R((float)grid64[(size_t)l * cells + c]) * R(1.0f / 4294967296.0f);
+        return R(lane(l)[c]) * u.inv_fp;
+    }
+    R rest_vol(uint32_t c) { return p2g_lane(4, c); }
+    R cur_vol(uint32_t c) { return p2g_lane(5, c); }
     static bool is_fluid(int32_t k) { return k == CELL_INTERIOR || k == CELL_SURFACE || k == CELL_BED; }
     static bool is_solid(int32_t k) { return k == CELL_SOLID; }
     static bool is_water_phase(R ph) { return ph < R(0.5); }
@@ -746,12 +755,23 @@ struct Sim : SimBase {
                         V inner = mp * vp + V3<R>(dot(a0, dpos), dot(a1, dpos), dot(a2, dpos));
                         V mom = w * inner;
                         uint32_t ci = cell_index(cx, cy, cz);
-                        R lim = R(1.0e9);
+                        const bool i64 = int64_grid();
+                        if (i64) fp = R(4294967296.0f);
+                        R lim = i64 ? R(1.0e18f) : R(1.0e9);
                         R mfp = mc * fp, rfp = rvc * fp, cfp = cvc * fp;
                         R mxf = mom.x * fp, myf = mom.y * fp, mzf = mom.z * fp;
                         if (std::fabs(mfp) > lim || std::fabs(mxf) > lim || std::fabs(myf) > lim ||
                             std::fabs(mzf) > lim || std::fabs(rfp) > lim || std::fabs(cfp) > lim)
                             atomic_add_u32(&metrics[M_OVERFLOW], 1u);
+                        if (i64) {
+                            const R vals[6] = {mfp, mxf, myf, mzf, rfp, cfp};
+                            for (int l = 0; l < 6; ++l) {
+                                // two's-complement sum, like the device's u64 atomics
+                                __atomic_fetch_add(reinterpret_cast<uint64_t*>(&grid64[(size_t)l * cells + ci]),
+                                                   (uint64_t)to_i64(vals[l]), __ATOMIC_RELAXED);
+                            }
+                            continue;
+                        }
                         atomic_add_i32(&lane(0)[ci], to_i32(mfp));
                         atomic_add_i32(&lane(1)[ci], to_i32(mxf));
                         atomic_add_i32(&lane(2)[ci], to_i32(myf));
@@ -766,10 +786,9 @@ struct Sim : SimBase {
         int n = (int)cells;
 #pragma omp parallel for schedule(static)
         for (int idx = 0; idx < n; ++idx) {
-            R inv_fp = u.inv_fp;
-            R mass = R(lane(0)[idx]) * inv_fp;
+            R mass = p2g_lane(0, idx);
             if (mass < R(1e-6)) continue;
-            V v = V3<R>(R(lane(1)[idx]) * inv_fp / mass, R(lane(2)[idx]) * inv_fp / mass, R(lane(3)[idx]) * inv_fp / mass);
+            V v = V3<R>(p2g_lane(1, idx) / mass, p2g_lane(2, idx) / mass, p2g_lane(3, idx) / mass);
             v.y += u.gravity * u.dt;
             R sp = length(v);
             if (sp > u.vel_cap) v = v * (u.vel_cap / sp);
@@ -1749,6 +1768,7 @@ struct Sim : SimBase {
         bool warm = s.warm_start != CS_WARM_NONE && !fixed_point() && have_prev_p;
         // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309)
         std::fill(grid.begin(), grid.end(), 0);
+        std::fill(grid64.begin(), grid64.end(), 0);
         std::fill(gvel.begin(), gvel.end(), R(0));
         uint32_t np = num_particles();
         uint32_t pass = 0;
@@ -1846,6 +1866,9 @@ struct Sim : SimBase {
                     for (size_t c = 0; c < cells; ++c) i[c] = to_i32((float)pf[c] * FP_SCALE);
                 break;
             case RD_GVEL: for (size_t k = 0; k < cells * 4; ++k) f[k] = (float)gvel[k]; break;
+            case RD_LANES64:
+                for (size_t k = 0; k < grid64.size(); ++k) reinterpret_cast<int64_t*>(out)[k] = grid64[k];
+                break;
             case RD_P:
                 for (size_t c = 0; c < cells; ++c)
                     f[c] = fixed_point() ? (float)(R(grid[c]) * R(1.0f / FP_SCALE)) : (float)pf[c];
@@ -2089,6 +2112,11 @@ int32_t cs_read_particles(CsSim* s, uint32_t f, uint32_t c, float* o) { return r
 int32_t cs_read_affine(CsSim* s, uint32_t f, uint32_t c, float* o) { return rd(s, RD_AFF, f, c, o); }
 int32_t cs_read_bed_extract(CsSim* s, uint32_t f, uint32_t c, float* o) { return rd(s, RD_BEDX, f, c, o); }
 int32_t cs_read_grid_lanes(CsSim* s, int32_t* o) { return rd(s, RD_LANES, 0, 0, o); }
+int32_t cs_read_grid_lanes64(CsSim* s, int64_t* o) {
+    if (!s) return fail(CS_ERR_INVALID_ARG, "null sim");
+    if (s->impl->settings.p2g_mode != CS_P2G_INT64) return fail(CS_ERR_INVALID_ARG, "not an int64 P2G simulation");
+    return rd(s, RD_LANES64, 0, 0, o);
+}
 int32_t cs_read_grid_vel(CsSim* s, float* o) { return rd(s, RD_GVEL, 0, 0, o); }
 int32_t cs_read_pressure(CsSim* s, float* o) { return rd(s, RD_P, 0, 0, o); }
 int32_t cs_read_cell_kind(CsSim* s, int32_t* o) { return rd(s, RD_KIND, 0, 0, o); }

@@ -56,6 +56,12 @@ template <class R> inline int32_t to_i32(R x) {
     if (x <= R(-2147483648.0)) return INT32_MIN;
     return (int32_t)x;
 }
+template <class R> inline int64_t to_i64(R x) {
+    if (x != x) return 0;
+    if (x >= R(9223372036854775807.0)) return INT64_MAX;
+    if (x <= R(-9223372036854775808.0)) return INT64_MIN;
+    return (int64_t)x;
+}
 template <class R> inline uint32_t to_u32(R x) {
     if (x != x || x <= R(0)) return 0u;
     if (x >= R(4294967295.0)) return UINT32_MAX;
