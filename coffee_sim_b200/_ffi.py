@@ -318,6 +318,9 @@ PROTOTYPES = {
     "cs_set_p2g_mode": (I32, [P, U32]),
     "cs_set_graph_mode": (I32, [P, U32]),
     "cs_autotune": (I32, [P, F32, U32, C.POINTER(CsTuneResult)]),
+    "cs_nn_conv3d": (I32, [P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P]),
+    "cs_nn_conv3d_wgrad": (I32, [P, P, P, I32, I32, I32, I32, I32, I32, P, P]),
+    "cs_nn_pack_weights": (I32, [P, P, I32, I32, I32, I32, I32, P]),
     "cs_pressure_solve_noalloc": (I32, [U32, U32, U32, F32, F32, F32, F32, U32, U32, P, P, P, P, P, P, PU32,
                                        C.POINTER(C.c_double)]),
 }

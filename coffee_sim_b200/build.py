@@ -34,7 +34,7 @@ def nvcc_path():
 
 
 def sources():
-    return [CSRC / "engine.cu", CSRC / "ensemble.cu", CSRC / "noalloc.cu", CSRC / "host_scene.cpp"]
+    return [CSRC / "engine.cu", CSRC / "ensemble.cu", CSRC / "noalloc.cu", CSRC / "nn.cu", CSRC / "host_scene.cpp"]
 
 
 def deps():

@@ -1,0 +1,376 @@
+// nn.cu — BF16 3-D convolution on the tcgen05 tensor cores, and the elementwise pieces
+// of the pressure-guess U-Net (learned warm start; no counterpart in the reference).
+//
+// Activations are channels-last bf16, [voxel][C] with C a multiple of 8, voxel =
+// (z * gy + y) * gx + x.  A 3x3x3 "same" convolution is one GEMM per 128-voxel tile:
+//   Y[v][co] = b[co] + sum_{t, ci} W[co][t * Cin + ci] * X[v + off_t][ci]
+// with M = 128 voxels, N = Cout, K = 27 * Cin taken 64 at a time.  The A operand is
+// gathered straight from X into shared memory (implicit im2col: one 16-byte load per
+// tap and 8 channels, zero outside the grid), B is the weight matrix, the accumulator
+// lives in TMEM, and the epilogue adds the bias, applies ReLU and stores bf16 (and
+// optionally f32).  The gradient w.r.t. the input is the same convolution with flipped,
+// transposed weights.  The weight gradient is a second GEMM,
+//   dW^T[t * Cin + ci][co] = sum_v X[v + off_t][ci] * dY[v][co],
+// with M = 27 * Cin, N = Cout and K = voxels split over CTAs; both operands are loaded
+// 8 voxels x 8 channels at a time and transposed in registers into K-major form.
+//
+// Every mbarrier wait is bounded; on a timeout the kernel raises a flag in `err`,
+// waits (bounded) for its own MMAs, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/coffee_sim.h"
+#include "umma.cuh"
+
+namespace cs {
+void set_error(const std::string& msg);
+
+namespace nn {
+
+constexpr int BM = 128;       // voxels (rows) per tile
+constexpr int BKC = 8;        // 16-byte K chunks per stage (64 bf16)
+constexpr int THREADS = 128;  // 4 warps: warp w owns TMEM lanes 32w..32w+31
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+
+struct Grid3 {
+    int gx, gy, gz;
+    __host__ __device__ int voxels() const { return gx * gy * gz; }
+};
+
+__device__ __forceinline__ int tap_dx(int t) { return t % 3 - 1; }
+__device__ __forceinline__ int tap_dy(int t) { return (t / 3) % 3 - 1; }
+__device__ __forceinline__ int tap_dz(int t) { return t / 9 - 1; }
+
+// voxel v shifted by tap t, or -1 outside the grid
+__device__ __forceinline__ int shifted(const Grid3& g, int v, int t) {
+    const int x = v % g.gx, y = (v / g.gx) % g.gy, z = v / (g.gx * g.gy);
+    const int xs = x + tap_dx(t), ys = y + tap_dy(t), zs = z + tap_dz(t);
+    if (xs < 0 || ys < 0 || zs < 0 || xs >= g.gx || ys >= g.gy || zs >= g.gz) return -1;
+    return (zs * g.gy + ys) * g.gx + xs;
+}
+
+// byte offset of (row, k chunk) in a K-major no-swizzle operand of `rows` rows and
+// BKC chunks: core matrix (group = row / 8, chunk) at (chunk * rows / 8 + group) * 128
+__device__ __forceinline__ uint32_t core_off(int row, int chunk, int rows) {
+    return (uint32_t)((chunk * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16);
+}
+
+// 8x8 transpose of bf16: in[j] holds 8 values of row j; out[r] gets column r.
+__device__ __forceinline__ void transpose8(const uint4 (&in)[8], uint4 (&out)[8]) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t a = (&in[2 * q].x)[r >> 1], b = (&in[2 * q + 1].x)[r >> 1];
+            w[q] = __byte_perm(a, b, (r & 1) ? 0x7632 : 0x5410);
+        }
+        out[r] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+struct ConvArgs {
+    Grid3 g;
+    const __nv_bfloat16* x;  // [vox][cin]
+    const __nv_bfloat16* w;  // [cout_pad][kpad], K = t * cin + ci, zero padded
+    const float* bias;       // [cout] or null
+    __nv_bfloat16* y;        // [vox][cout_store] or null
+    float* y32;              // [vox][cout] or null
+    int cin, cout_pad, cout_store, kpad, relu;
+    const __nv_bfloat16* dy;  // weight gradient: [vox][cout_pad]
+    float* dwt;               // weight gradient: [27 * cin][cout_pad], accumulated
+    int m_rows;               // weight gradient: 27 * cin
+    int k_per_split;          // weight gradient: voxels per CTA (multiple of 64)
+    uint32_t* err;
+};
+
+// MODE 0: convolution (forward / input gradient); MODE 1: weight gradient.
+template <int MODE>
+__global__ void __launch_bounds__(THREADS) k_conv_umma(ConvArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmem_base;
+    const int N = a.cout_pad;
+    const int a_bytes = BM * BKC * 16, b_bytes = N * BKC * 16;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+
+    if (warp == 0) {
+        umma::tmem_alloc(&tmem_base, ncols);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        umma::mbar_init(&bars[0], 1);
+        umma::mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+
+    const int nvox = a.g.voxels();
+    const int m0 = blockIdx.x * BM;
+    int nstages, k0 = 0;
+    if (MODE == 0) {
+        nstages = a.kpad / (BKC * 8);
+    } else {
+        k0 = blockIdx.y * a.k_per_split;
+        const int kend = min(k0 + a.k_per_split, nvox);
+        nstages = kend > k0 ? (kend - k0 + BKC * 8 - 1) / (BKC * 8) : 0;
+    }
+    const uint32_t idesc = umma::idesc_bf16_f32((uint32_t)N);
+    uint32_t phase0 = 0u, phase1 = 0u;  // completed-phase parity of each buffer's barrier
+    bool ok = true;
+
+    for (int s = 0; s < nstages && ok; ++s) {
+        const int buf = s & 1;
+        if (s >= 2) {  // the MMAs of stage s-2 read this buffer
+            const bool w = umma::mbar_wait(&bars[buf], buf ? phase1 : phase0, WAIT_LIMIT);
+            if (buf) phase1 ^= 1u; else phase0 ^= 1u;
+            ok = __syncthreads_and(w ? 1 : 0) != 0;  // one decision for the whole CTA
+            if (!ok) break;
+        }
+        unsigned char* A = buf ? sm + a_bytes + b_bytes : sm;
+        unsigned char* B = A + a_bytes;
+        if (MODE == 0) {
+            const int cgroups = a.cin >> 3;
+            const int kchunks = 27 * cgroups;
+            // A: 128 rows x 8 chunks, 8 per thread
+            for (int i = tid; i < BM * BKC; i += THREADS) {
+                const int row = i / BKC, c = i % BKC;
+                const int kc = s * BKC + c;
+                uint4 val = make_uint4(0u, 0u, 0u, 0u);
+                const int v = m0 + row;
+                if (v < nvox && kc < kchunks) {
+                    const int src = shifted(a.g, v, kc / cgroups);
+                    if (src >= 0)
+                        val = *reinterpret_cast<const uint4*>(a.x + (size_t)src * a.cin + (kc % cgroups) * 8);
+                }
+                *reinterpret_cast<uint4*>(A + core_off(row, c, BM)) = val;
+            }
+            for (int i = tid; i < N * BKC; i += THREADS) {
+                const int row = i / BKC, c = i % BKC;
+                const uint4 val =
+                    *reinterpret_cast<const uint4*>(a.w + (size_t)row * a.kpad + (size_t)(s * BKC + c) * 8);
+                *reinterpret_cast<uint4*>(B + core_off(row, c, N)) = val;
+            }
+        } else {
+            const int vbase = k0 + s * BKC * 8;
+            // A: rows (t, ci) x 8 voxel chunks; one 8x8 block per task
+            for (int task = tid; task < (BM >> 3) * BKC; task += THREADS) {
+                const int rg = task / BKC, c = task % BKC;
+                const int m = m0 + rg * 8;  // first row of the group: (t, ci0)
+                uint4 in[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    in[j] = make_uint4(0u, 0u, 0u, 0u);
+                    const int v = vbase + c * 8 + j;
+                    if (m < a.m_rows && v < nvox && v < k0 + a.k_per_split) {
+                        const int t = m / a.cin, ci0 = m % a.cin;
+                        const int src = shifted(a.g, v, t);
+                        if (src >= 0) in[j] = *reinterpret_cast<const uint4*>(a.x + (size_t)src * a.cin + ci0);
+                    }
+                }
+                uint4 out[8];
+                transpose8(in, out);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) *reinterpret_cast<uint4*>(A + core_off(rg * 8 + r, c, BM)) = out[r];
+            }
+            for (int task = tid; task < (N >> 3) * BKC; task += THREADS) {
+                const int rg = task / BKC, c = task % BKC;
+                uint4 in[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int v = vbase + c * 8 + j;
+                    in[j] = (v < nvox && v < k0 + a.k_per_split)
+                                ? *reinterpret_cast<const uint4*>(a.dy + (size_t)v * N + rg * 8)
+                                : make_uint4(0u, 0u, 0u, 0u);
+                }
+                uint4 out[8];
+                transpose8(in, out);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) *reinterpret_cast<uint4*>(B + core_off(rg * 8 + r, c, N)) = out[r];
+            }
+        }
+        umma::fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after_sync();
+            const uint32_t a_addr = umma::smem_addr(A), b_addr = umma::smem_addr(B);
+#pragma unroll
+            for (int j = 0; j < BKC / 2; ++j) {
+                const uint64_t da = umma::smem_desc(a_addr + j * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
+                const uint64_t db = umma::smem_desc(b_addr + j * 2 * (N / 8) * 128, (N / 8) * 128, 128);
+                umma::mma_bf16(tmem, da, db, idesc, (s > 0 || j > 0) ? 1u : 0u);
+            }
+            umma::commit(&bars[buf]);
+        }
+        __syncthreads();
+    }
+    // the last commit covers every MMA of this CTA
+    if (nstages > 0) {
+        const int lb = (nstages - 1) & 1;
+        const bool done = umma::mbar_wait(&bars[lb], lb ? phase1 : phase0, WAIT_LIMIT);
+        ok = __syncthreads_and((done && ok) ? 1 : 0) != 0;
+        if (!ok && tid == 0) atomicOr(a.err, 1u);
+    }
+    umma::fence_after_sync();
+    if (ok && nstages > 0) {
+        const int row = warp * 32 + (tid & 31);
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < N; c0 += 8) {
+            float v[8];
+            umma::tmem_ld8(lane_addr + (uint32_t)c0, v);
+            umma::tmem_wait_ld();
+            if (MODE == 0) {
+                const int vox = m0 + row;
+                if (vox >= nvox) continue;
+                for (int q = 0; q < 8; ++q) {
+                    const int co = c0 + q;
+                    float r = v[q] + ((a.bias && co < a.cout_store) ? a.bias[co] : 0.0f);
+                    if (a.relu) r = fmaxf(r, 0.0f);
+                    v[q] = co < a.cout_store ? r : 0.0f;
+                }
+                if (a.y && c0 < a.cout_store) {
+                    __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(v[q]);
+                    *reinterpret_cast<uint4*>(a.y + (size_t)vox * a.cout_store + c0) =
+                        *reinterpret_cast<const uint4*>(h);
+                }
+                if (a.y32)
+                    for (int q = 0; q < 8 && c0 + q < a.cout_store; ++q) a.y32[(size_t)vox * a.cout_store + c0 + q] = v[q];
+            } else {
+                const int m = m0 + row;
+                if (m >= a.m_rows) continue;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (v[q] != 0.0f) atomicAdd(&a.dwt[(size_t)m * N + c0 + q], v[q]);
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, ncols);
+}
+
+static size_t conv_smem(int n) { return (size_t)2 * (BM + n) * BKC * 16; }
+
+template <int MODE>
+static int launch(const ConvArgs& a, dim3 grid, cudaStream_t st) {
+    const size_t smem = conv_smem(a.cout_pad);
+    static bool attr[2] = {false, false};
+    if (!attr[MODE]) {
+        cudaFuncSetAttribute(k_conv_umma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        attr[MODE] = true;
+    }
+    k_conv_umma<MODE><<<grid, THREADS, smem, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("conv launch: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+
+// ---- elementwise pieces ----
+// master weights f32 [cout][27][cin] -> bf16 [cout_pad][kpad] (K = t * cin_pad + ci);
+// flip != 0 builds the input-gradient weights W'[ci][t][co] = W[co][26 - t][ci].
+__global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ out, int cin, int cin_pad,
+                               int cout, int rows_pad, int kpad, int flip) {
+    const int total = rows_pad * kpad;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int row = i / kpad, k = i % kpad;
+        float val = 0.0f;
+        if (!flip) {
+            const int t = k / cin_pad, ci = k % cin_pad;
+            if (row < cout && t < 27 && ci < cin) val = w[((size_t)row * 27 + t) * cin + ci];
+        } else {  // row = ci, K = t * cout_pad(=cin_pad here) + co
+            const int t = k / cin_pad, co = k % cin_pad;
+            if (row < cin && t < 27 && co < cout) val = w[((size_t)co * 27 + (26 - t)) * cin + row];
+        }
+        out[i] = __float2bfloat16(val);
+    }
+}
+
+}  // namespace nn
+}  // namespace cs
+
+using namespace cs::nn;
+
+static cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+
+extern "C" {
+
+// Y = relu?(conv3x3x3(X, W) + b).  x: bf16 [vox][cin_pad]; w: bf16 [cout_pad][kpad] from
+// cs_nn_pack_weights; y: bf16 [vox][cout_pad] (channels >= cout zero), y32: f32
+// [vox][cout_pad] or null.  err: device flag set on a wait timeout.
+int32_t cs_nn_conv3d(const void* x, const void* w, const float* bias, void* y, float* y32, int32_t gx, int32_t gy,
+                     int32_t gz, int32_t cin_pad, int32_t cout_pad, int32_t relu, uint32_t* err, void* stream) {
+    if (cin_pad % 8 || cout_pad % 16 || cout_pad > 256 || cout_pad < 16 || gx < 1 || gy < 1 || gz < 1 || !x || !w ||
+        !err) {
+        cs::set_error("cs_nn_conv3d: channels must be multiples of 8 (input) and 16 (output, <= 256)");
+        return CS_ERR_INVALID_ARG;
+    }
+    ConvArgs a{};
+    a.g = Grid3{gx, gy, gz};
+    a.x = (const __nv_bfloat16*)x;
+    a.w = (const __nv_bfloat16*)w;
+    a.bias = bias;
+    a.y = (__nv_bfloat16*)y;
+    a.y32 = y32;
+    a.cin = cin_pad;
+    a.cout_pad = cout_pad;
+    a.cout_store = cout_pad;
+    a.kpad = ((27 * cin_pad + 63) / 64) * 64;
+    a.relu = relu;
+    a.err = err;
+    const int tiles = (a.g.voxels() + BM - 1) / BM;
+    return launch<0>(a, dim3(tiles, 1), as_stream(stream));
+}
+
+// dWt[t * cin_pad + ci][co] += sum_v X[v + off_t][ci] * dY[v][co]  (f32, accumulated).
+int32_t cs_nn_conv3d_wgrad(const void* x, const void* dy, float* dwt, int32_t gx, int32_t gy, int32_t gz,
+                           int32_t cin_pad, int32_t cout_pad, int32_t splits, uint32_t* err, void* stream) {
+    if (cin_pad % 8 || cout_pad % 16 || cout_pad > 256 || cout_pad < 16 || splits < 1 || !x || !dy || !dwt || !err) {
+        cs::set_error("cs_nn_conv3d_wgrad: bad arguments");
+        return CS_ERR_INVALID_ARG;
+    }
+    ConvArgs a{};
+    a.g = Grid3{gx, gy, gz};
+    a.x = (const __nv_bfloat16*)x;
+    a.dy = (const __nv_bfloat16*)dy;
+    a.dwt = dwt;
+    a.cin = cin_pad;
+    a.cout_pad = cout_pad;
+    a.m_rows = 27 * cin_pad;
+    const int nvox = a.g.voxels();
+    int per = (nvox + splits - 1) / splits;
+    per = ((per + 63) / 64) * 64;
+    a.k_per_split = per;
+    a.err = err;
+    const int tiles = (a.m_rows + BM - 1) / BM;
+    const int ns = (nvox + per - 1) / per;
+    return launch<1>(a, dim3(tiles, ns), as_stream(stream));
+}
+
+// Pack f32 master weights [cout][27][cin] into the bf16 GEMM layout; flip = 1 gives the
+// input-gradient operator (rows = cin, K = t * cout_pad + co).
+int32_t cs_nn_pack_weights(const float* w, void* out, int32_t cin, int32_t cin_pad, int32_t cout, int32_t cout_pad,
+                           int32_t flip, void* stream) {
+    if (!w || !out) {
+        cs::set_error("cs_nn_pack_weights: null pointer");
+        return CS_ERR_INVALID_ARG;
+    }
+    const int rows = flip ? ((cin + 15) / 16) * 16 : cout_pad;
+    const int kin = flip ? cout_pad : cin_pad;
+    const int kpad = ((27 * kin + 63) / 64) * 64;
+    k_pack_weights<<<256, 256, 0, as_stream(stream)>>>(w, (__nv_bfloat16*)out, cin, kin, cout, rows, kpad, flip);
+    return cudaGetLastError() == cudaSuccess ? CS_OK : CS_ERR_CUDA;
+}
+
+}  // extern "C"

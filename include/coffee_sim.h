@@ -372,6 +372,16 @@ typedef struct CsProfile {
 int32_t cs_profile_enable(CsSim* sim, int32_t on);   /* resets the counters */
 int32_t cs_profile_read(CsSim* sim, CsProfile* out); /* synchronises */
 
+/* ---- BF16 3-D convolution on the tensor cores (tcgen05), the layers of the pressure-guess
+ * U-Net (no counterpart in the reference).  Device pointers, channels-last bf16
+ * activations [voxel][C]; `err` is a device flag raised if a wait times out. ---- */
+int32_t cs_nn_conv3d(const void* x, const void* w, const float* bias, void* y, float* y32, int32_t gx, int32_t gy,
+                     int32_t gz, int32_t cin_pad, int32_t cout_pad, int32_t relu, uint32_t* err, void* stream);
+int32_t cs_nn_conv3d_wgrad(const void* x, const void* dy, float* dwt, int32_t gx, int32_t gy, int32_t gz,
+                           int32_t cin_pad, int32_t cout_pad, int32_t splits, uint32_t* err, void* stream);
+int32_t cs_nn_pack_weights(const float* w, void* out, int32_t cin, int32_t cin_pad, int32_t cout, int32_t cout_pad,
+                           int32_t flip, void* stream);
+
 /* ---- Solver parameters and autotuner (no counterpart in the reference) ---- */
 
 /* Change the residual-mode solver between substeps: over-relaxation (0 keeps the current
