@@ -321,6 +321,14 @@ PROTOTYPES = {
     "cs_nn_conv3d": (I32, [P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P]),
     "cs_nn_conv3d_wgrad": (I32, [P, P, P, I32, I32, I32, I32, I32, I32, P, P]),
     "cs_nn_pack_weights": (I32, [P, P, I32, I32, I32, I32, I32, P]),
+    "cs_nn_pool": (I32, [P, P, P, P, I32, I32, I32, I32, I32, P]),
+    "cs_nn_upcat": (I32, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P]),
+    "cs_nn_relu_grad": (I32, [P, P, P, P, C.c_int64, I32, P]),
+    "cs_nn_head": (I32, [P, P, P, P, P, P, C.c_int64, I32, I32, P]),
+    "cs_nn_mse": (I32, [P, P, P, P, P, C.c_int64, F32, P]),
+    "cs_nn_wgrad_master": (I32, [P, P, I32, I32, I32, P]),
+    "cs_nn_adam": (I32, [P, P, P, P, C.c_int64, F32, F32, F32, F32, I32, P]),
+    "cs_nn_axpy": (I32, [P, P, F32, C.c_int64, P]),
     "cs_pressure_solve_noalloc": (I32, [U32, U32, U32, F32, F32, F32, F32, U32, U32, P, P, P, P, P, P, PU32,
                                        C.POINTER(C.c_double)]),
 }

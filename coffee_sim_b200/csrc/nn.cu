@@ -19,6 +19,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <string>
 
@@ -297,6 +299,139 @@ __global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __res
     }
 }
 
+// ---- U-Net glue (CUDA cores) ----
+#define NN_FOR(i, n) for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); \
+                          i += (long long)gridDim.x * blockDim.x)
+
+// 2x2x2 average pool of a channels-last tensor; fine grid (gx, gy, gz) even.
+__global__ void k_pool_fwd(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y, Grid3 f, int c) {
+    const int hx = f.gx / 2, hy = f.gy / 2, hz = f.gz / 2;
+    const long long n = (long long)hx * hy * hz * c;
+    NN_FOR(i, n) {
+        const int ch = (int)(i % c);
+        const long long v = i / c;
+        const int x0 = (int)(v % hx) * 2, y0 = (int)((v / hx) % hy) * 2, z0 = (int)(v / ((long long)hx * hy)) * 2;
+        float acc = 0.0f;
+        for (int dz = 0; dz < 2; ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    acc += __bfloat162float(x[((size_t)((z0 + dz) * f.gy + y0 + dy) * f.gx + x0 + dx) * c + ch]);
+        y[i] = __float2bfloat16(acc * 0.125f);
+    }
+}
+// gradient of the pool: dx[v] += dy[parent(v)] / 8 (f32)
+__global__ void k_pool_bwd(const float* __restrict__ dy, float* __restrict__ dx, Grid3 f, int c) {
+    const long long n = (long long)f.voxels() * c;
+    NN_FOR(i, n) {
+        const int ch = (int)(i % c);
+        const long long v = i / c;
+        const int x = (int)(v % f.gx), y = (int)((v / f.gx) % f.gy), z = (int)(v / ((long long)f.gx * f.gy));
+        const long long pv = ((long long)(z / 2) * (f.gy / 2) + y / 2) * (f.gx / 2) + x / 2;
+        dx[i] += dy[pv * c + ch] * 0.125f;
+    }
+}
+// out[v] = [low[parent(v)] (c1 channels), skip[v] (c2 channels)] on the fine grid
+__global__ void k_upcat_fwd(const __nv_bfloat16* __restrict__ low, const __nv_bfloat16* __restrict__ skip,
+                            __nv_bfloat16* __restrict__ out, Grid3 f, int c1, int c2) {
+    const int c = c1 + c2;
+    const long long n = (long long)f.voxels() * c;
+    NN_FOR(i, n) {
+        const int ch = (int)(i % c);
+        const long long v = i / c;
+        if (ch < c1) {
+            const int x = (int)(v % f.gx), y = (int)((v / f.gx) % f.gy), z = (int)(v / ((long long)f.gx * f.gy));
+            const long long pv = ((long long)(z / 2) * (f.gy / 2) + y / 2) * (f.gx / 2) + x / 2;
+            out[i] = low[pv * c1 + ch];
+        } else {
+            out[i] = skip[v * c2 + (ch - c1)];
+        }
+    }
+}
+// gradient of upcat: dlow[p] += sum over its 8 children, dskip[v] += its part (f32)
+__global__ void k_upcat_bwd(const float* __restrict__ dout, float* __restrict__ dlow, float* __restrict__ dskip,
+                            Grid3 f, int c1, int c2) {
+    const int c = c1 + c2;
+    const int hx = f.gx / 2, hy = f.gy / 2, hz = f.gz / 2;
+    const long long nlow = (long long)hx * hy * hz * c1;
+    NN_FOR(i, nlow) {
+        const int ch = (int)(i % c1);
+        const long long pv = i / c1;
+        const int x0 = (int)(pv % hx) * 2, y0 = (int)((pv / hx) % hy) * 2, z0 = (int)(pv / ((long long)hx * hy)) * 2;
+        float acc = 0.0f;
+        for (int dz = 0; dz < 2; ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    acc += dout[((size_t)((z0 + dz) * f.gy + y0 + dy) * f.gx + x0 + dx) * c + ch];
+        dlow[i] += acc;
+    }
+    const long long nskip = (long long)f.voxels() * c2;
+    NN_FOR(i, nskip) {
+        const long long v = i / c2;
+        dskip[i] += dout[v * c + c1 + (int)(i % c2)];
+    }
+}
+// gradient g (f32) masked by the ReLU of the layer output y -> bf16 operand of the
+// backward convolutions; accumulates the bias gradient.
+__global__ void k_relu_grad(const float* __restrict__ g, const __nv_bfloat16* __restrict__ y,
+                            __nv_bfloat16* __restrict__ out, float* __restrict__ db, long long n, int c) {
+    NN_FOR(i, n) {
+        const float v = __bfloat162float(y[i]) > 0.0f ? g[i] : 0.0f;
+        out[i] = __float2bfloat16(v);
+        if (db && v != 0.0f) atomicAdd(&db[i % c], v);
+    }
+}
+// 1x1x1 output layer: out[v] = w[c] + sum_k w[k] x[v][k]
+__global__ void k_head_fwd(const __nv_bfloat16* __restrict__ x, const float* __restrict__ w, float* __restrict__ out,
+                           long long nv, int c) {
+    NN_FOR(v, nv) {
+        float acc = w[c];
+        for (int k = 0; k < c; ++k) acc += w[k] * __bfloat162float(x[v * c + k]);
+        out[v] = acc;
+    }
+}
+__global__ void k_head_bwd(const __nv_bfloat16* __restrict__ x, const float* __restrict__ w,
+                           const float* __restrict__ dout, float* __restrict__ dx, float* __restrict__ dw, long long nv,
+                           int c) {
+    NN_FOR(v, nv) {
+        const float d = dout[v];
+        for (int k = 0; k < c; ++k) dx[v * c + k] = w[k] * d;
+        if (d == 0.0f) continue;
+        for (int k = 0; k < c; ++k) atomicAdd(&dw[k], __bfloat162float(x[v * c + k]) * d);
+        atomicAdd(&dw[c], d);
+    }
+}
+// masked mean squared error: loss[0] += sum m (o - t)^2 / count, dout = 2 m (o - t) / count
+__global__ void k_mse(const float* __restrict__ o, const float* __restrict__ t, const float* __restrict__ m,
+                      float* __restrict__ dout, float* __restrict__ loss, long long nv, float inv_count) {
+    NN_FOR(v, nv) {
+        const float e = (o[v] - t[v]) * m[v];
+        dout[v] = 2.0f * e * inv_count;
+        if (e != 0.0f) atomicAdd(loss, e * e * inv_count);
+    }
+}
+// dW^T [(t, ci)][co] (cout_pad columns) -> master layout gW[co][t][ci]
+__global__ void k_wgrad_master(const float* __restrict__ dwt, float* __restrict__ gw, int cin, int cout, int cout_pad) {
+    const long long n = (long long)cout * 27 * cin;
+    NN_FOR(i, n) {
+        const int ci = (int)(i % cin), t = (int)((i / cin) % 27), co = (int)(i / (27LL * cin));
+        gw[i] = dwt[((long long)t * cin + ci) * cout_pad + co];
+    }
+}
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    NN_FOR(i, n) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+__global__ void k_axpy(float* __restrict__ y, const float* __restrict__ x, float a, long long n) {
+    NN_FOR(i, n) y[i] += a * x[i];
+}
+
 }  // namespace nn
 }  // namespace cs
 
@@ -371,6 +506,78 @@ int32_t cs_nn_pack_weights(const float* w, void* out, int32_t cin, int32_t cin_p
     const int kpad = ((27 * kin + 63) / 64) * 64;
     k_pack_weights<<<256, 256, 0, as_stream(stream)>>>(w, (__nv_bfloat16*)out, cin, kin, cout, rows, kpad, flip);
     return cudaGetLastError() == cudaSuccess ? CS_OK : CS_ERR_CUDA;
+}
+
+
+static int nn_check(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cs::set_error(std::string(what) + ": " + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+static int nn_blocks(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 32)); }
+
+int32_t cs_nn_pool(const void* x, void* y, const float* dy, float* dx, int32_t gx, int32_t gy, int32_t gz, int32_t c,
+                   int32_t backward, void* stream) {
+    const Grid3 f{gx, gy, gz};
+    if (gx % 2 || gy % 2 || gz % 2 || c < 1) {
+        cs::set_error("cs_nn_pool: grid dims must be even");
+        return CS_ERR_INVALID_ARG;
+    }
+    const long long n = (long long)f.voxels() * c;
+    if (!backward)
+        k_pool_fwd<<<nn_blocks(n / 8), 256, 0, as_stream(stream)>>>((const __nv_bfloat16*)x, (__nv_bfloat16*)y, f, c);
+    else
+        k_pool_bwd<<<nn_blocks(n), 256, 0, as_stream(stream)>>>(dy, dx, f, c);
+    return nn_check("cs_nn_pool");
+}
+int32_t cs_nn_upcat(const void* low, const void* skip, void* out, const float* dout, float* dlow, float* dskip,
+                    int32_t gx, int32_t gy, int32_t gz, int32_t c1, int32_t c2, int32_t backward, void* stream) {
+    const Grid3 f{gx, gy, gz};
+    if (gx % 2 || gy % 2 || gz % 2) {
+        cs::set_error("cs_nn_upcat: grid dims must be even");
+        return CS_ERR_INVALID_ARG;
+    }
+    const long long n = (long long)f.voxels() * (c1 + c2);
+    if (!backward)
+        k_upcat_fwd<<<nn_blocks(n), 256, 0, as_stream(stream)>>>((const __nv_bfloat16*)low, (const __nv_bfloat16*)skip,
+                                                                  (__nv_bfloat16*)out, f, c1, c2);
+    else
+        k_upcat_bwd<<<nn_blocks(n), 256, 0, as_stream(stream)>>>(dout, dlow, dskip, f, c1, c2);
+    return nn_check("cs_nn_upcat");
+}
+int32_t cs_nn_relu_grad(const float* g, const void* y, void* out, float* db, int64_t n, int32_t c, void* stream) {
+    k_relu_grad<<<nn_blocks(n), 256, 0, as_stream(stream)>>>(g, (const __nv_bfloat16*)y, (__nv_bfloat16*)out, db, n, c);
+    return nn_check("cs_nn_relu_grad");
+}
+int32_t cs_nn_head(const void* x, const float* w, float* out, const float* dout, float* dx, float* dw, int64_t nv,
+                   int32_t c, int32_t backward, void* stream) {
+    if (!backward)
+        k_head_fwd<<<nn_blocks(nv), 256, 0, as_stream(stream)>>>((const __nv_bfloat16*)x, w, out, nv, c);
+    else
+        k_head_bwd<<<nn_blocks(nv), 256, 0, as_stream(stream)>>>((const __nv_bfloat16*)x, w, dout, dx, dw, nv, c);
+    return nn_check("cs_nn_head");
+}
+int32_t cs_nn_mse(const float* o, const float* t, const float* m, float* dout, float* loss, int64_t nv,
+                  float inv_count, void* stream) {
+    k_mse<<<nn_blocks(nv), 256, 0, as_stream(stream)>>>(o, t, m, dout, loss, nv, inv_count);
+    return nn_check("cs_nn_mse");
+}
+int32_t cs_nn_wgrad_master(const float* dwt, float* gw, int32_t cin, int32_t cout, int32_t cout_pad, void* stream) {
+    k_wgrad_master<<<nn_blocks((long long)cout * 27 * cin), 256, 0, as_stream(stream)>>>(dwt, gw, cin, cout, cout_pad);
+    return nn_check("cs_nn_wgrad_master");
+}
+int32_t cs_nn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                   int32_t step, void* stream) {
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_adam<<<nn_blocks(n), 256, 0, as_stream(stream)>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2);
+    return nn_check("cs_nn_adam");
+}
+int32_t cs_nn_axpy(float* y, const float* x, float a, int64_t n, void* stream) {
+    k_axpy<<<nn_blocks(n), 256, 0, as_stream(stream)>>>(y, x, a, n);
+    return nn_check("cs_nn_axpy");
 }
 
 }  // extern "C"

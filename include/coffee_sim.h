@@ -381,6 +381,26 @@ int32_t cs_nn_conv3d_wgrad(const void* x, const void* dy, float* dwt, int32_t gx
                            int32_t cin_pad, int32_t cout_pad, int32_t splits, uint32_t* err, void* stream);
 int32_t cs_nn_pack_weights(const float* w, void* out, int32_t cin, int32_t cin_pad, int32_t cout, int32_t cout_pad,
                            int32_t flip, void* stream);
+/* 2x2x2 average pool (bf16 forward; f32 gradient accumulated into dx). */
+int32_t cs_nn_pool(const void* x, void* y, const float* dy, float* dx, int32_t gx, int32_t gy, int32_t gz, int32_t c,
+                   int32_t backward, void* stream);
+/* Nearest x2 upsample of `low` concatenated with `skip` (bf16); the gradient accumulates
+ * into dlow / dskip (f32). */
+int32_t cs_nn_upcat(const void* low, const void* skip, void* out, const float* dout, float* dlow, float* dskip,
+                    int32_t gx, int32_t gy, int32_t gz, int32_t c1, int32_t c2, int32_t backward, void* stream);
+/* ReLU-masked gradient to bf16, accumulating the bias gradient db (may be null). */
+int32_t cs_nn_relu_grad(const float* g, const void* y, void* out, float* db, int64_t n, int32_t c, void* stream);
+/* 1x1x1 output layer with c inputs: w holds c weights then the bias. */
+int32_t cs_nn_head(const void* x, const float* w, float* out, const float* dout, float* dx, float* dw, int64_t nv,
+                   int32_t c, int32_t backward, void* stream);
+/* Masked mean squared error and its gradient (loss accumulated into loss[0]). */
+int32_t cs_nn_mse(const float* o, const float* t, const float* m, float* dout, float* loss, int64_t nv,
+                  float inv_count, void* stream);
+/* Weight gradient from the GEMM layout [(tap, ci)][co] to the master layout [co][tap][ci]. */
+int32_t cs_nn_wgrad_master(const float* dwt, float* gw, int32_t cin, int32_t cout, int32_t cout_pad, void* stream);
+int32_t cs_nn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                   int32_t step, void* stream);
+int32_t cs_nn_axpy(float* y, const float* x, float a, int64_t n, void* stream);
 
 /* ---- Solver parameters and autotuner (no counterpart in the reference) ---- */
 
