@@ -210,7 +210,7 @@ class CsMetrics(C.Structure):
 
 
 CS_PHASE_COUNT = 16
-PHASE_NAMES = ["emit", "clear", "p2g", "grid", "sweeps", "residual", "project", "g2p", "bed", "render"]
+PHASE_NAMES = ["emit", "clear", "p2g", "grid", "sweeps", "residual", "project", "g2p", "bed", "render", "learned"]
 
 
 class CsProfile(C.Structure):
@@ -314,6 +314,9 @@ PROTOTYPES = {
     "cs_timer_stop": (I32, [P, PF]),
     "cs_flush_l2": (I32, [P]),
     "cs_sync": (I32, [P]),
+    "cs_set_learned_weights": (I32, [P, PF, U64]),
+    "cs_learned_capture": (I32, [P, U32]),
+    "cs_learned_read_sample": (I32, [P, P, P, P, PF]),
     "cs_set_solver": (I32, [P, F32, U32, U32]),
     "cs_set_p2g_mode": (I32, [P, U32]),
     "cs_set_graph_mode": (I32, [P, U32]),

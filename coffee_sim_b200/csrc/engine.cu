@@ -579,8 +579,10 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
                     CS_LAUNCH(k_rbgs_colour<<<dim3(blocks, 1), T, 0, stream_>>>(dc, 1u));
                 }
             }
-        } else if ((rc = solve_pressure(sweeps, r0, r1))) {
-            return rc;
+        } else {
+            if ((rc = learned_before_solve())) return rc;
+            if ((rc = solve_pressure(sweeps, r0, r1))) return rc;
+            if ((rc = learned_after_solve())) return rc;
         }
         have_prev_p = true;
     }
@@ -1063,6 +1065,10 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
         t.use_graph = 0;
         int rc = validate_settings(&t);
         if (rc) return rc;
+        if (t.warm_start == CS_WARM_LEARNED) {
+            set_error("ensembles run the previous-substep warm start (no learned guess)");
+            return CS_ERR_UNSUPPORTED;
+        }
         const CsSettings& a = s[0];
         if (t.grid_dims[0] != a.grid_dims[0] || t.grid_dims[1] != a.grid_dims[1] || t.grid_dims[2] != a.grid_dims[2] ||
             t.p2g_mode != a.p2g_mode || t.solve_mode != a.solve_mode || t.pressure_storage != a.pressure_storage ||
@@ -1252,6 +1258,220 @@ int Ensemble::step_frame(float dt) {
         if (rc) return rc;
     }
     return CS_OK;
+}
+
+// ---- learned warm start ----
+// The network of coffee_sim_b200/unet.py: per layer (level, input, output channels);
+// parameters in order, each layer's weights [cout][27][cin] then its bias, then the
+// 1x1x1 output layer's 16 weights and bias.
+namespace {
+struct UnetLayer {
+    int level, cin, cout;
+};
+constexpr UnetLayer kUnet[9] = {{0, 8, 16}, {0, 16, 16}, {1, 16, 32}, {1, 32, 32}, {2, 32, 64},
+                                {1, 96, 32}, {1, 32, 32}, {0, 48, 16}, {0, 16, 16}};
+constexpr int kHeadC = 16;
+uint64_t unet_param_count() {
+    uint64_t n = 0;
+    for (const UnetLayer& l : kUnet) n += (uint64_t)l.cout * 27 * l.cin + l.cout;
+    return n + kHeadC + 1;
+}
+uint64_t unet_layer_offset(int k) {
+    uint64_t n = 0;
+    for (int i = 0; i < k; ++i) n += (uint64_t)kUnet[i].cout * 27 * kUnet[i].cin + kUnet[i].cout;
+    return n;
+}
+int r16(int c) { return (c + 15) / 16 * 16; }
+}  // namespace
+
+int Engine::learned_alloc() {
+    if (l_ready_) return CS_OK;
+    const CsSettings& s = settings;
+    for (int a = 0; a < 3; ++a)
+        if (s.grid_dims[a] % 4) {
+            set_error("the learned warm start needs grid dims that are multiples of 4");
+            return CS_ERR_INVALID_ARG;
+        }
+    const size_t v0 = cells_, v1 = v0 / 8, v2 = v1 / 8;
+    int rc;
+    if ((rc = alloc(l_params_, unet_param_count() * sizeof(float)))) return rc;
+    for (int k = 0; k < 9; ++k) {
+        const size_t kpad = (size_t)((27 * kUnet[k].cin + 63) / 64 * 64);
+        if ((rc = alloc(l_wf_[k], (size_t)r16(kUnet[k].cout) * kpad * 2))) return rc;
+    }
+    // activations (bf16): e1a e1b p1 e2a e2b p2 e3a u2 d2a d2b u1 d1a d1b
+    const size_t sizes[13] = {v0 * 16, v0 * 16, v1 * 16, v1 * 32, v1 * 32, v2 * 32, v2 * 64,
+                              v1 * 96, v1 * 32, v1 * 32, v0 * 48, v0 * 16, v0 * 16};
+    for (int k = 0; k < 13; ++k)
+        if ((rc = alloc(l_act_[k], sizes[k] * 2))) return rc;
+    if ((rc = alloc(l_feat_, v0 * 8 * 2))) return rc;
+    if ((rc = alloc(l_out_, v0 * sizeof(float)))) return rc;
+    if ((rc = alloc(l_stats_, 2 * sizeof(double)))) return rc;
+    if ((rc = alloc(l_scale_, sizeof(float)))) return rc;
+    if ((rc = alloc(l_bak_hi_, v0 * sizeof(float)))) return rc;
+    if ((rc = alloc(l_bak_lo_, v0 * sizeof(float)))) return rc;
+    if ((rc = alloc(l_target_, v0 * sizeof(float)))) return rc;
+    if ((rc = alloc(l_mask_, v0 * sizeof(float)))) return rc;
+    if ((rc = alloc(l_err_, sizeof(uint32_t)))) return rc;
+    cudaMemsetAsync(l_err_.ptr, 0, sizeof(uint32_t), stream_);
+    l_ready_ = true;
+    return CS_OK;
+}
+
+int Engine::set_learned_weights(const float* params, uint64_t count) {
+    if (count != unet_param_count()) {
+        set_error("learned weights: expected " + std::to_string(unet_param_count()) + " parameters");
+        return CS_ERR_INVALID_ARG;
+    }
+    int rc = learned_alloc();
+    if (rc) return rc;
+    if ((rc = check(cudaMemcpyAsync(l_params_.ptr, params, count * sizeof(float), cudaMemcpyHostToDevice, stream_),
+                    "weights upload")))
+        return rc;
+    const float* dp = (const float*)l_params_.ptr;
+    for (int k = 0; k < 9; ++k) {
+        const UnetLayer& l = kUnet[k];
+        if ((rc = cs_nn_pack_weights(dp + unet_layer_offset(k), l_wf_[k].ptr, l.cin, l.cin, l.cout, r16(l.cout), 0,
+                                     stream_)))
+            return rc;
+    }
+    l_weights_ = true;
+    return sync();
+}
+
+int Engine::learned_features() {
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    cudaMemsetAsync(l_stats_.ptr, 0, 2 * sizeof(double), stream_);
+    k_learned_stats<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc, (double*)l_stats_.ptr);
+    k_learned_features<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(
+        dc, (const double*)l_stats_.ptr, (__nv_bfloat16*)l_feat_.ptr, (float*)l_scale_.ptr);
+    count_launch(2);
+    return check(cudaGetLastError(), "learned features");
+}
+
+int Engine::learned_forward() {
+    const CsSettings& s = settings;
+    const int d[3][3] = {{(int)s.grid_dims[0], (int)s.grid_dims[1], (int)s.grid_dims[2]},
+                         {(int)s.grid_dims[0] / 2, (int)s.grid_dims[1] / 2, (int)s.grid_dims[2] / 2},
+                         {(int)s.grid_dims[0] / 4, (int)s.grid_dims[1] / 4, (int)s.grid_dims[2] / 4}};
+    const float* dp = (const float*)l_params_.ptr;
+    uint32_t* err = (uint32_t*)l_err_.ptr;
+    void* a[13];
+    for (int k = 0; k < 13; ++k) a[k] = l_act_[k].ptr;
+    enum { E1A, E1B, P1, E2A, E2B, P2, E3A, U2, D2A, D2B, U1, D1A, D1B };
+    int rc;
+    auto conv = [&](int k, const void* x, void* y) {
+        const UnetLayer& l = kUnet[k];
+        const int* g = d[l.level];
+        const float* bias = dp + unet_layer_offset(k) + (uint64_t)l.cout * 27 * l.cin;
+        count_launch();
+        return cs_nn_conv3d(x, l_wf_[k].ptr, bias, y, nullptr, g[0], g[1], g[2], l.cin, r16(l.cout), 1, err, stream_);
+    };
+    if ((rc = conv(0, l_feat_.ptr, a[E1A])) || (rc = conv(1, a[E1A], a[E1B]))) return rc;
+    if ((rc = cs_nn_pool(a[E1B], a[P1], nullptr, nullptr, d[0][0], d[0][1], d[0][2], 16, 0, stream_))) return rc;
+    if ((rc = conv(2, a[P1], a[E2A])) || (rc = conv(3, a[E2A], a[E2B]))) return rc;
+    if ((rc = cs_nn_pool(a[E2B], a[P2], nullptr, nullptr, d[1][0], d[1][1], d[1][2], 32, 0, stream_))) return rc;
+    if ((rc = conv(4, a[P2], a[E3A]))) return rc;
+    if ((rc = cs_nn_upcat(a[E3A], a[E2B], a[U2], nullptr, nullptr, nullptr, d[1][0], d[1][1], d[1][2], 64, 32, 0,
+                          stream_)))
+        return rc;
+    if ((rc = conv(5, a[U2], a[D2A])) || (rc = conv(6, a[D2A], a[D2B]))) return rc;
+    if ((rc = cs_nn_upcat(a[D2B], a[E1B], a[U1], nullptr, nullptr, nullptr, d[0][0], d[0][1], d[0][2], 32, 16, 0,
+                          stream_)))
+        return rc;
+    if ((rc = conv(7, a[U1], a[D1A])) || (rc = conv(8, a[D1A], a[D1B]))) return rc;
+    const float* head = dp + unet_layer_offset(9);
+    count_launch(5);
+    return cs_nn_head(a[D1B], head, (float*)l_out_.ptr, nullptr, nullptr, nullptr, (int64_t)cells_, kHeadC, 0,
+                      stream_);
+}
+
+// Before the solve: the FP64 residual r of the previous-substep pressure p and the
+// network inputs built from it; with the learned warm start, p + (network output) * s
+// replaces p when that has the smaller FP64 residual.
+int Engine::learned_before_solve() {
+    const bool learned = settings.warm_start == CS_WARM_LEARNED;
+    last.learned_used = 0;
+    if (!learned && !l_capture_) return CS_OK;
+    if (learned && !l_weights_) {
+        set_error("CS_WARM_LEARNED needs weights (cs_set_learned_weights)");
+        return CS_ERR_INVALID_ARG;
+    }
+    int rc;
+    if ((rc = learned_alloc())) return rc;
+    const double r_prev = refine_residual();  // leaves the residual in gres for the inputs
+    mark(CS_PHASE_LEARNED);
+    if ((rc = learned_features())) return rc;
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    k_learned_save<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc, (float*)l_bak_hi_.ptr,
+                                                                          (float*)l_bak_lo_.ptr);
+    count_launch();
+    if (!learned) return CS_OK;
+    mark(CS_PHASE_LEARNED);
+    if ((rc = learned_forward())) return rc;
+    k_learned_apply<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(
+        dc, (const float*)l_out_.ptr, (const float*)l_scale_.ptr, (const float*)l_bak_hi_.ptr,
+        (const float*)l_bak_lo_.ptr);
+    count_launch();
+    const double r_guess = refine_residual();
+    mark(CS_PHASE_LEARNED);
+    uint32_t err = 0;
+    cudaMemcpy(&err, l_err_.ptr, sizeof(err), cudaMemcpyDeviceToHost);
+    if (err) {
+        set_error("a tensor-core convolution of the learned warm start timed out");
+        return CS_ERR_TIMEOUT;
+    }
+    // a clear improvement only: the FP64 norms are reduced with atomics, so equal
+    // pressures can differ in their last bits
+    if (r_guess < 0.999 * r_prev) {
+        last.learned_used = 1;
+    } else {
+        k_learned_restore<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc, (const float*)l_bak_hi_.ptr,
+                                                                                    (const float*)l_bak_lo_.ptr);
+        count_launch();
+    }
+    return check(cudaGetLastError(), "learned warm start");
+}
+
+int Engine::learned_after_solve() {
+    if (!l_capture_) return CS_OK;
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    k_learned_target<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(
+        dc, (const float*)l_scale_.ptr, (const float*)l_bak_hi_.ptr, (const float*)l_bak_lo_.ptr,
+        (float*)l_target_.ptr, (float*)l_mask_.ptr);
+    count_launch();
+    l_have_sample_ = true;
+    return check(cudaGetLastError(), "learned target");
+}
+
+int Engine::learned_capture(bool on) {
+    if (on) {
+        int rc = learned_alloc();
+        if (rc) return rc;
+    }
+    l_capture_ = on;
+    if (on) l_have_sample_ = false;  // turning capture off keeps the last pair readable
+    return CS_OK;
+}
+
+int Engine::learned_read_sample(void* feat, float* target, float* mask, float* scale) {
+    if (!l_have_sample_) {
+        set_error("no captured sample: enable cs_learned_capture and step a substep first");
+        return CS_ERR_INVALID_ARG;
+    }
+    int rc;
+    if (feat && (rc = check(cudaMemcpyAsync(feat, l_feat_.ptr, cells_ * 16, cudaMemcpyDeviceToDevice, stream_),
+                            "sample features")))
+        return rc;
+    if (target && (rc = check(cudaMemcpyAsync(target, l_target_.ptr, cells_ * 4, cudaMemcpyDeviceToDevice, stream_),
+                              "sample target")))
+        return rc;
+    if (mask && (rc = check(cudaMemcpyAsync(mask, l_mask_.ptr, cells_ * 4, cudaMemcpyDeviceToDevice, stream_),
+                            "sample mask")))
+        return rc;
+    if (scale && (rc = check(cudaMemcpyAsync(scale, l_scale_.ptr, 4, cudaMemcpyDeviceToHost, stream_), "scale")))
+        return rc;
+    return sync();
 }
 
 // ---- autotuner: time candidate configurations from one saved state ----
@@ -1475,9 +1695,10 @@ static int validate(const CsSettings* s) {
                   "cluster-resident solve");
         return CS_ERR_INVALID_ARG;
     }
-    if (s->warm_start == CS_WARM_LEARNED) {
-        set_error("settings request a mode this engine build does not implement (learned warm start)");
-        return CS_ERR_UNSUPPORTED;
+    if (s->warm_start == CS_WARM_LEARNED &&
+        (s->use_graph || s->pressure_storage != CS_PRESSURE_FP32 || s->solve_mode != CS_SOLVE_RESIDUAL)) {
+        set_error("the learned warm start needs the residual-mode FP32 solve and no graph capture");
+        return CS_ERR_INVALID_ARG;
     }
     if (s->warm_start != CS_WARM_NONE && s->pressure_storage == CS_PRESSURE_FIXED_POINT) {
         set_error("warm start needs CS_PRESSURE_FP32 storage");
@@ -1631,6 +1852,19 @@ int32_t cs_set_graph_mode(CsSim* sim, uint32_t use_graph) {
     if ((rc = sim->e->sync())) return rc;
     sim->e->settings.use_graph = t.use_graph;
     return CS_OK;
+}
+int32_t cs_set_learned_weights(CsSim* sim, const float* params, uint64_t count) {
+    CS_SIM(sim);
+    CS_PTR(params);
+    return sim->e->set_learned_weights(params, count);
+}
+int32_t cs_learned_capture(CsSim* sim, uint32_t on) {
+    CS_SIM(sim);
+    return sim->e->learned_capture(on != 0);
+}
+int32_t cs_learned_read_sample(CsSim* sim, void* feat, float* target, float* mask, float* scale) {
+    CS_SIM(sim);
+    return sim->e->learned_read_sample(feat, target, mask, scale);
 }
 int32_t cs_autotune(CsSim* sim, float sub_dt, uint32_t substeps, CsTuneResult* out) {
     CS_SIM(sim);

@@ -83,6 +83,15 @@ private:
     DeviceBuffer p2g_key_, p2g_rank_, p2g_sorted_, tile_count_, tile_start_, tile_temp_;
     uint32_t p2g_tiles_ = 0;
     JetPlan jet_{};         // device emission planned for the current substep
+    // learned warm start: flat f32 parameters, packed bf16 layers, activations
+    int learned_alloc();
+    int learned_features();
+    int learned_forward();
+    int learned_before_solve();
+    int learned_after_solve();
+    DeviceBuffer l_params_, l_feat_, l_out_, l_stats_, l_scale_, l_bak_hi_, l_bak_lo_, l_target_, l_mask_, l_err_;
+    DeviceBuffer l_wf_[9], l_act_[13];
+    bool l_weights_ = false, l_capture_ = false, l_have_sample_ = false, l_ready_ = false;
     // graph mode: the substep's device work captured once and replayed
     int enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, double& r1);
     int substep_graph(float sub_dt);
@@ -118,6 +127,10 @@ public:
     int timer_stop(float* ms);
     int flush_l2();
     int autotune(float sub_dt, uint32_t substeps, CsTuneResult* out);
+    // learned warm start (CS_WARM_LEARNED) and training-sample capture
+    int set_learned_weights(const float* params, uint64_t count);
+    int learned_capture(bool on);
+    int learned_read_sample(void* feat, float* target, float* mask, float* scale);
     void mark(int phase);      // close the open phase and open `phase` (-1 closes only)
     void count_launch(uint32_t n = 1) {
         prof_.launches += n;

@@ -6,6 +6,8 @@
 // instance, so a batched ensemble runs every member in the same launch.  Element
 // loops are grid-stride so launch shapes do not depend on the particle count (a
 // captured CUDA graph stays valid while particles are emitted).
+#include <cuda_bf16.h>
+
 #include "kernels.cuh"
 #include "kernels_api.h"
 
@@ -1474,6 +1476,106 @@ __global__ void k_clear_batch(const Ctx* __restrict__ cp, uint32_t tiles) {
 // Copy each instance's solve result into one array (one readback for the ensemble).
 __global__ void k_gather_results(const Ctx* __restrict__ cp, uint32_t n, ScResult* __restrict__ out) {
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = *cp[i].sb.result;
+}
+
+// ---- learned warm start: network inputs, guess, training targets ----
+// The inputs come after an FP64 residual evaluation of the previous-substep pressure
+// (k_refine_residual leaves r in gres): the network maps the residual to a pressure
+// correction, an approximate inverse of the pressure operator.
+// acc[0] += r^2, acc[1] += 1 over fluid cells
+__global__ void k_learned_stats(const Ctx* __restrict__ cp, double* __restrict__ acc) {
+    const Ctx& c = cp[blockIdx.y];
+    const int32_t* kl = lane(c, 3);
+    double r2 = 0.0, n = 0.0;
+    CS_FOR(i, c.u.cells) {
+        if (!is_fluid(kl[i])) continue;
+        const double r = (double)c.gres[i];
+        r2 += r * r;
+        n += 1.0;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        n += __shfl_down_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], r2);
+        atomicAdd(&acc[1], n);
+    }
+}
+// 8 channels per cell: r / s, fill, fluid, bed, solid, 0, 0, 0 with s the RMS of the
+// residual over the fluid cells (written to scale[0])
+__global__ void k_learned_features(const Ctx* __restrict__ cp, const double* __restrict__ acc,
+                                   __nv_bfloat16* __restrict__ feat, float* __restrict__ scale) {
+    const Ctx& c = cp[blockIdx.y];
+    const int32_t* kl = lane(c, 3);
+    const double ms = acc[1] > 0.0 ? acc[0] / acc[1] : 0.0;
+    const float sc = ms > 0.0 ? (float)sqrt(ms) : 1.0f;
+    const float inv = 1.0f / sc;
+    if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = sc;
+    CS_FOR(i, c.u.cells) {
+        const int32_t k = kl[i];
+        const bool fl = is_fluid(k);
+        float f[8];
+        f[0] = fl ? c.gres[i] * inv : 0.0f;
+        f[1] = fl ? c.fill[i] : 0.0f;
+        f[2] = fl ? 1.0f : 0.0f;
+        f[3] = k == CELL_BED ? 1.0f : 0.0f;
+        f[4] = is_solid(k) ? 1.0f : 0.0f;
+        f[5] = 0.0f;
+        f[6] = 0.0f;
+        f[7] = 0.0f;
+        __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(f[q]);
+        *reinterpret_cast<uint4*>(feat + (size_t)i * 8) = *reinterpret_cast<const uint4*>(h);
+    }
+}
+// the previous-substep pressure (the plain warm start) kept for the correction
+// target and for the rule that keeps whichever start has the smaller residual
+__global__ void k_learned_save(const Ctx* __restrict__ cp, float* __restrict__ bak_hi, float* __restrict__ bak_lo) {
+    const Ctx& c = cp[blockIdx.y];
+    CS_FOR(i, c.u.cells) {
+        bak_hi[i] = c.pf[i];
+        bak_lo[i] = c.plo[i];
+    }
+}
+// guess = previous pressure + out * s on fluid cells (the network predicts the change
+// of the pressure over the substep in units of s), split into hi/lo words
+__global__ void k_learned_apply(const Ctx* __restrict__ cp, const float* __restrict__ out,
+                                const float* __restrict__ scale, const float* __restrict__ bak_hi,
+                                const float* __restrict__ bak_lo) {
+    const Ctx& c = cp[blockIdx.y];
+    const int32_t* kl = lane(c, 3);
+    const double sc = (double)scale[0];
+    CS_FOR(i, c.u.cells) {
+        if (!is_fluid(kl[i])) continue;
+        const double p = ((double)bak_hi[i] + (double)bak_lo[i]) + (double)out[i] * sc;
+        const float hi = (float)p;
+        c.pf[i] = hi;
+        c.plo[i] = (float)(p - (double)hi);
+    }
+}
+__global__ void k_learned_restore(const Ctx* __restrict__ cp, const float* __restrict__ bak_hi,
+                                  const float* __restrict__ bak_lo) {
+    const Ctx& c = cp[blockIdx.y];
+    CS_FOR(i, c.u.cells) {
+        c.pf[i] = bak_hi[i];
+        c.plo[i] = bak_lo[i];
+    }
+}
+// training pair of this substep: target = (solved - previous pressure) / s, mask = fluid
+__global__ void k_learned_target(const Ctx* __restrict__ cp, const float* __restrict__ scale,
+                                 const float* __restrict__ bak_hi, const float* __restrict__ bak_lo,
+                                 float* __restrict__ target, float* __restrict__ mask) {
+    const Ctx& c = cp[blockIdx.y];
+    const int32_t* kl = lane(c, 3);
+    const double inv = 1.0 / (double)scale[0];
+    CS_FOR(i, c.u.cells) {
+        const bool fl = is_fluid(kl[i]);
+        const double d = ((double)c.pf[i] + (double)c.plo[i]) - ((double)bak_hi[i] + (double)bak_lo[i]);
+        target[i] = fl ? (float)(d * inv) : 0.0f;
+        mask[i] = fl ? 1.0f : 0.0f;
+    }
 }
 
 __global__ void k_unpack_particles(const Ctx* __restrict__ cp, uint32_t first, uint32_t count, const float* in, int what) {

@@ -36,6 +36,7 @@ constexpr int BM = 128;       // voxels (rows) per tile
 constexpr int BKC = 8;        // 16-byte K chunks per stage (64 bf16)
 constexpr int THREADS = 128;  // 4 warps: warp w owns TMEM lanes 32w..32w+31
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
+static_assert(BM == 128 && BKC == 8 && THREADS == 128, "loader thread mapping assumes 128 x 8 chunks, 128 threads");
 
 struct Grid3 {
     int gx, gy, gz;
@@ -45,14 +46,6 @@ struct Grid3 {
 __device__ __forceinline__ int tap_dx(int t) { return t % 3 - 1; }
 __device__ __forceinline__ int tap_dy(int t) { return (t / 3) % 3 - 1; }
 __device__ __forceinline__ int tap_dz(int t) { return t / 9 - 1; }
-
-// voxel v shifted by tap t, or -1 outside the grid
-__device__ __forceinline__ int shifted(const Grid3& g, int v, int t) {
-    const int x = v % g.gx, y = (v / g.gx) % g.gy, z = v / (g.gx * g.gy);
-    const int xs = x + tap_dx(t), ys = y + tap_dy(t), zs = z + tap_dz(t);
-    if (xs < 0 || ys < 0 || zs < 0 || xs >= g.gx || ys >= g.gy || zs >= g.gz) return -1;
-    return (zs * g.gy + ys) * g.gx + xs;
-}
 
 // byte offset of (row, k chunk) in a K-major no-swizzle operand of `rows` rows and
 // BKC chunks: core matrix (group = row / 8, chunk) at (chunk * rows / 8 + group) * 128
@@ -128,6 +121,19 @@ __global__ void __launch_bounds__(THREADS) k_conv_umma(ConvArgs a) {
     uint32_t phase0 = 0u, phase1 = 0u;  // completed-phase parity of each buffer's barrier
     bool ok = true;
 
+    // MODE 0 loader: thread tid always fills K chunk (tid & 7) of rows (tid >> 3) + 16 k,
+    // k = 0..7; their voxel coordinates are decoded once (x < 0 marks a row past the end)
+    int rx[8], ry[8], rz[8];
+    if (MODE == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int v = m0 + (tid >> 3) + 16 * k;
+            rx[k] = v < nvox ? v % a.g.gx : -1;
+            ry[k] = (v / a.g.gx) % a.g.gy;
+            rz[k] = v / (a.g.gx * a.g.gy);
+        }
+    }
+
     for (int s = 0; s < nstages && ok; ++s) {
         const int buf = s & 1;
         if (s >= 2) {  // the MMAs of stage s-2 read this buffer
@@ -141,16 +147,21 @@ __global__ void __launch_bounds__(THREADS) k_conv_umma(ConvArgs a) {
         if (MODE == 0) {
             const int cgroups = a.cin >> 3;
             const int kchunks = 27 * cgroups;
-            // A: 128 rows x 8 chunks, 8 per thread
-            for (int i = tid; i < BM * BKC; i += THREADS) {
-                const int row = i / BKC, c = i % BKC;
-                const int kc = s * BKC + c;
+            // A: 128 rows x 8 chunks; this thread's chunk is one (tap, 8-channel group)
+            const int c = tid & (BKC - 1);
+            const int kc = s * BKC + c;
+            const int t = kc / cgroups, cg = kc - t * cgroups;
+            const int dx = tap_dx(t), dy = tap_dy(t), dz = tap_dz(t);
+            const bool live = kc < kchunks;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int row = (tid >> 3) + 16 * k;
+                const int xs = rx[k] + dx, ys = ry[k] + dy, zs = rz[k] + dz;
                 uint4 val = make_uint4(0u, 0u, 0u, 0u);
-                const int v = m0 + row;
-                if (v < nvox && kc < kchunks) {
-                    const int src = shifted(a.g, v, kc / cgroups);
-                    if (src >= 0)
-                        val = *reinterpret_cast<const uint4*>(a.x + (size_t)src * a.cin + (kc % cgroups) * 8);
+                if (live && rx[k] >= 0 && xs >= 0 && ys >= 0 && zs >= 0 && xs < a.g.gx && ys < a.g.gy &&
+                    zs < a.g.gz) {
+                    const int src = (zs * a.g.gy + ys) * a.g.gx + xs;
+                    val = *reinterpret_cast<const uint4*>(a.x + (size_t)src * a.cin + cg * 8);
                 }
                 *reinterpret_cast<uint4*>(A + core_off(row, c, BM)) = val;
             }
@@ -167,14 +178,27 @@ __global__ void __launch_bounds__(THREADS) k_conv_umma(ConvArgs a) {
                 const int rg = task / BKC, c = task % BKC;
                 const int m = m0 + rg * 8;  // first row of the group: (t, ci0)
                 uint4 in[8];
+                const int t = m / a.cin, ci0 = m % a.cin;
+                const int dx = tap_dx(t), dy = tap_dy(t), dz = tap_dz(t);
+                // the 8 voxels are consecutive: decode the first, then step along x
+                const int v0 = vbase + c * 8;
+                int x = v0 % a.g.gx, y = (v0 / a.g.gx) % a.g.gy, z = v0 / (a.g.gx * a.g.gy);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     in[j] = make_uint4(0u, 0u, 0u, 0u);
-                    const int v = vbase + c * 8 + j;
+                    const int v = v0 + j;
                     if (m < a.m_rows && v < nvox && v < k0 + a.k_per_split) {
-                        const int t = m / a.cin, ci0 = m % a.cin;
-                        const int src = shifted(a.g, v, t);
-                        if (src >= 0) in[j] = *reinterpret_cast<const uint4*>(a.x + (size_t)src * a.cin + ci0);
+                        const int xs = x + dx, ys = y + dy, zs = z + dz;
+                        if (xs >= 0 && ys >= 0 && zs >= 0 && xs < a.g.gx && ys < a.g.gy && zs < a.g.gz)
+                            in[j] = *reinterpret_cast<const uint4*>(
+                                a.x + (size_t)((zs * a.g.gy + ys) * a.g.gx + xs) * a.cin + ci0);
+                    }
+                    if (++x == a.g.gx) {
+                        x = 0;
+                        if (++y == a.g.gy) {
+                            y = 0;
+                            ++z;
+                        }
                     }
                 }
                 uint4 out[8];

@@ -336,6 +336,21 @@ class MpmSim3D:
     def set_p2g_mode(self, mode):
         self.lib.call("cs_set_p2g_mode", self._h, mode)
 
+    def set_learned_weights(self, params):
+        """Weights of the pressure-guess U-Net (flat f32 vector, coffee_sim_b200.unet layout)."""
+        a = np.ascontiguousarray(params, dtype=np.float32)
+        self.lib.call("cs_set_learned_weights", self._h, a.ctypes.data_as(C.POINTER(C.c_float)), a.size)
+
+    def learned_capture(self, on=True):
+        self.lib.call("cs_learned_capture", self._h, 1 if on else 0)
+
+    def learned_read_sample(self, feat, target, mask):
+        """Copy the last captured (inputs, target, mask) into torch CUDA tensors; returns s."""
+        sc = C.c_float()
+        self.lib.call("cs_learned_read_sample", self._h, C.c_void_p(feat.data_ptr()), C.c_void_p(target.data_ptr()),
+                      C.c_void_p(mask.data_ptr()), C.byref(sc))
+        return sc.value
+
     def set_graph_mode(self, on):
         """Capture the substep in a CUDA graph and replay it (needs device emission)."""
         self.lib.call("cs_set_graph_mode", self._h, 1 if on else 0)

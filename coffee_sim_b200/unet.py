@@ -8,10 +8,12 @@ the tcgen05 tensor cores through the engine library (`cs_nn_*`), and the glue
 (pooling, concatenation, ReLU masks, loss, Adam) through its CUDA-core kernels.
 torch only allocates the device memory and supplies the stream.
 
-Inputs (8 channels per cell): dx^2 * rhs / s, previous pressure / s, fill fraction,
-fluid, bed and solid masks, two zero channels; s is the RMS of dx^2 * rhs over the
-fluid cells, so the network works in units where the right-hand side is O(1) and its
-output times s is the pressure guess.  No counterpart in the reference.
+Inputs (8 channels per cell): r / s, fill fraction, fluid, bed and solid masks, three
+zero channels, where r is the FP64 residual of the previous-substep pressure under the
+pressure operator and s its RMS over the fluid cells.  The output times s is the
+predicted pressure correction, so the network is a learned approximate inverse of the
+operator; the guess is the previous pressure plus the correction (a zero output is the
+plain warm start).  No counterpart in the reference.
 """
 import ctypes as C
 import math
@@ -28,7 +30,7 @@ LAYERS = [
 ]
 HEAD_C = 16
 FEATURES = 8
-REAL_INPUTS = 6
+REAL_INPUTS = 5
 
 
 def param_count():
@@ -275,3 +277,45 @@ def reference_forward(params, feat, dims):
     a, b, _ = sl["head"]
     out = torch.einsum("bczyx,c->bzyx", d1, p[a:b]) + p[b]
     return out.reshape(-1)
+
+
+# ---- training on solver-generated pairs ----
+def collect_samples(sim, sub_dt, substeps, torch_mod=None):
+    """Step `sim` (an engine MpmSim3D) `substeps` times with sample capture on and return
+    the (inputs, target, mask) pairs as CUDA tensors: network inputs before each solve,
+    (solved - previous pressure) / s after it, and the fluid mask."""
+    import torch
+
+    n = sim.settings.cells
+    out = []
+    sim.learned_capture(True)
+    try:
+        for _ in range(substeps):
+            sim.step_substep(sub_dt)
+            feat = torch.empty(n, FEATURES, dtype=torch.bfloat16, device="cuda")
+            target = torch.empty(n, dtype=torch.float32, device="cuda")
+            mask = torch.empty(n, dtype=torch.float32, device="cuda")
+            sim.learned_read_sample(feat, target, mask)
+            out.append((feat, target, mask))
+    finally:
+        sim.learned_capture(False)
+    return out
+
+
+def train(samples, dims, lib, steps=1000, lr=1e-3, seed=0, params=None, log_every=0):
+    """Adam on the masked MSE between the guess and the solved pressure (units of s),
+    one pair per step in a seeded random order.  Returns (flat params, loss history)."""
+    import torch
+
+    net = UNet(dims, lib, params=params, seed=seed)
+    rng = np.random.default_rng(seed)
+    hist = []
+    for k in range(steps):
+        f, t, m = samples[int(rng.integers(len(samples)))]
+        step_lr = lr * (0.1 ** (k / max(steps, 1)))  # exponential decay to lr / 10
+        loss = net.train_step(f, t, m, lr=step_lr)
+        if log_every and (k % log_every == 0 or k == steps - 1):
+            hist.append((k, float(loss.item())))
+    torch.cuda.synchronize()
+    net.check_errors()
+    return net.params_numpy(), hist

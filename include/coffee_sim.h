@@ -358,6 +358,7 @@ enum {
     CS_PHASE_G2P = 7,
     CS_PHASE_BED = 8,       /* bed coupling, extraction, bed dynamics */
     CS_PHASE_RENDER = 9,
+    CS_PHASE_LEARNED = 10,  /* learned warm start: inputs, U-Net guess, residual comparison */
     CS_PHASE_COUNT = 16
 };
 typedef struct CsProfile {
@@ -401,6 +402,20 @@ int32_t cs_nn_wgrad_master(const float* dwt, float* gw, int32_t cin, int32_t cou
 int32_t cs_nn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
                    int32_t step, void* stream);
 int32_t cs_nn_axpy(float* y, const float* x, float a, int64_t n, void* stream);
+
+/* ---- Learned warm start (CS_WARM_LEARNED; no counterpart in the reference) ----
+ * Weights of the pressure-guess U-Net (coffee_sim_b200/unet.py layout, f32, host memory).
+ * From the FP64 residual of the previous-substep pressure the network predicts a pressure
+ * correction; before each solve the previous pressure plus that correction replaces it
+ * when its FP64 residual is smaller (CsMetrics.learned_used).  Grid dims must be
+ * multiples of 4. */
+int32_t cs_set_learned_weights(CsSim* sim, const float* params, uint64_t count);
+/* Capture one training pair per substep: network inputs before the solve (bf16
+ * [cells][8]) and (solved - previous pressure) / s with its fluid mask (f32 [cells]). */
+int32_t cs_learned_capture(CsSim* sim, uint32_t on);
+/* Copy the last captured pair into device buffers of the caller (any may be null);
+ * scale (host) receives s. */
+int32_t cs_learned_read_sample(CsSim* sim, void* feat, float* target, float* mask, float* scale);
 
 /* ---- Solver parameters and autotuner (no counterpart in the reference) ---- */
 

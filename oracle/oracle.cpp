@@ -2044,6 +2044,13 @@ int32_t cs_set_graph_mode(CsSim* sim, uint32_t use_graph) {
     sim->impl->settings.use_graph = use_graph ? 1u : 0u;  // nothing to capture on the CPU
     return CS_OK;
 }
+int32_t cs_set_learned_weights(CsSim*, const float*, uint64_t) {
+    return fail(CS_ERR_UNSUPPORTED, "the oracle has no learned warm start (it runs the previous-substep start)");
+}
+int32_t cs_learned_capture(CsSim*, uint32_t) { return fail(CS_ERR_UNSUPPORTED, "the oracle captures no samples"); }
+int32_t cs_learned_read_sample(CsSim*, void*, float*, float*, float*) {
+    return fail(CS_ERR_UNSUPPORTED, "the oracle captures no samples");
+}
 int32_t cs_autotune(CsSim*, float, uint32_t, CsTuneResult*) {
     return fail(CS_ERR_UNSUPPORTED, "the oracle has no autotuner (it times nothing)");
 }
