@@ -1,5 +1,7 @@
-"""Benchmark: particle-steps/s of the MLS-MPM substep with the pressure solve swept to
-a relative residual of 1e-5 (the BASELINE metric), on the V60 pour-over scene at 64^3.
+"""Benchmark: particle-steps/s and pressure-solve ms of the MLS-MPM substep with the
+pressure swept to a relative residual of 1e-5, on the V60 pour-over scene at 64^3, with
+the previous-substep warm start ("plain", the headline value) and with the learned
+warm start ("learned").
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -25,7 +27,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "particle-steps/sec at 1e-5 pressure residual (V60 64^3)"
+METRIC = "particle-steps/sec & pressure-solve ms at 1e-5 residual: learned vs plain RBGS"
 UNIT = "particle-steps/s"
 WORKLOAD = "c2_v60_midpour_64cube"
 
@@ -91,10 +93,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def build_scene(lib, args, device=0):
-    from coffee_sim_b200 import scenes
+def build_scene(lib, args, device=0, learned=False, populate=True):
+    from coffee_sim_b200 import _ffi, scenes
     from coffee_sim_b200.sim import MpmSim3D
     s = scenes.c2_v60(lib, grid=args.grid)
+    if learned:
+        s.raw.warm_start = _ffi.CS_WARM_LEARNED
     s.raw.device = device
     s.raw.rbgs_omega = args.omega
     s.raw.max_sweeps = args.max_sweeps
@@ -102,7 +106,8 @@ def build_scene(lib, args, device=0):
     s.raw.p2g_mode = {"atomic": 0, "sorted": 1}[args.p2g]
     s.raw.device_emission = 1  # jet samples built on the device (the oracle matches this mode)
     sim = MpmSim3D(s, lib)
-    scenes.populate_c2(sim)
+    if populate:
+        scenes.populate_c2(sim)
     return sim
 
 
@@ -126,6 +131,46 @@ def algorithmic_bytes(n_p, n_c, pairs, evals, n_bed):
     if n_bed:
         b += 4 * n_c + 200 * n_bed
     return b
+
+
+def learned_arm(lib, args, device, state, dt, barrier, dist):
+    """The same timed substeps with the learned warm start (U-Net guess on the tensor
+    cores, kept when its FP64 residual beats the previous-substep pressure)."""
+    import numpy as np
+
+    wfile = ROOT / "coffee_sim_b200" / "weights" / "unet_v60_64.npy"
+    if args.grid % 4 or not wfile.exists():
+        return {"unavailable": "needs grid dims divisible by 4 and coffee_sim_b200/weights/unet_v60_64.npy"}
+    sim = build_scene(lib, args, device=device, learned=True, populate=False)
+    sim.set_learned_weights(np.load(wfile))
+    sim.restore(state)
+    sim.profile_enable(True)
+    step_ms, particle_steps, used = [], 0, 0
+    barrier()
+    for _ in range(args.steps):
+        particle_steps += sim.particle_count()
+        sim.flush_l2()
+        sim.timer_start()
+        sim.step_substep(dt)
+        step_ms.append(sim.timer_stop())
+        used += int(sim.latest_metrics().learned_used)
+    barrier()
+    prof = sim.profile_read()
+    total_ms = sum(step_ms)
+    if dist:
+        import torch
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    world = dist.get_world_size() if dist else 1
+    n = max(prof.substeps, 1)
+    out = {"value": particle_steps * world / (total_ms * 1e-3), "ms_per_step": total_ms / args.steps,
+           "pressure_solve_ms": (prof.phase_ms[4] + prof.phase_ms[5] + prof.phase_ms[10]) / n,
+           "learned_guess_ms": prof.phase_ms[10] / n, "sweeps_per_step": prof.sweeps / n,
+           "guess_kept_fraction": used / args.steps, "final_residual": sim.latest_metrics().last_residual,
+           "weights": "coffee_sim_b200/weights/unet_v60_64.npy (python -m coffee_sim_b200.train_unet)"}
+    sim.close()
+    return out
 
 
 def cpu_baseline(args, steps, warm):
@@ -187,6 +232,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="end-to-end loop without CUDA-graph replay")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-warm-start arm")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -319,7 +365,7 @@ def main():
         "final_residual": metrics.last_residual,
         "phase_ms_per_step": {n: prof.phase_ms[i] / max(prof.substeps, 1)
                               for i, n in enumerate(["emit", "clear", "p2g", "grid", "sweeps", "residual",
-                                                     "project", "g2p", "bed", "render"])},
+                                                     "project", "g2p", "bed", "render", "learned"])},
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
@@ -334,6 +380,10 @@ def main():
         "gpu_launches": int(prof.launches),
         "clocks": clocks.summary(),
     }
+    line["plain"] = {"value": value, "pressure_solve_ms": line["pressure_solve_ms"],
+                      "sweeps_per_step": pairs_per_step, "warm_start": "previous substep"}
+    if not args.no_learned:
+        line["learned"] = learned_arm(lib, args, local, state, dt, barrier, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(args, steps=min(args.steps, args.cpu_steps), warm=args.warmup)
