@@ -284,6 +284,156 @@ __global__ void __launch_bounds__(THREADS) k_conv_umma(ConvArgs a) {
     if (warp == 0) umma::tmem_dealloc(tmem, ncols);
 }
 
+// ---- forward convolution with an asynchronous copy pipeline ----
+// Same GEMM as k_conv_umma<0>, with NBUF stage buffers: the 16-byte operand chunks of
+// stage s + LOOKAHEAD are copied with cp.async (zero-filled outside the grid) while the
+// tensor cores work on stage s, so the gathers' latency overlaps the MMAs.  A buffer is
+// refilled only after the MMAs of the stage that last used it have completed (mbarrier).
+constexpr int NBUF = 4, LOOKAHEAD = 2;
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_addr(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(THREADS) k_conv_fwd(ConvArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bars[NBUF];
+    __shared__ uint32_t tmem_base;
+    const int N = a.cout_pad;
+    const int a_bytes = BM * BKC * 16, b_bytes = N * BKC * 16, stage_bytes = a_bytes + b_bytes;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+    if (warp == 0) {
+        umma::tmem_alloc(&tmem_base, ncols);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int b = 0; b < NBUF; ++b) umma::mbar_init(&bars[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+
+    const int nvox = a.g.voxels();
+    const int m0 = blockIdx.x * BM;
+    const int nstages = a.kpad / (BKC * 8);
+    const int cgroups = a.cin >> 3;
+    const int kchunks = 27 * cgroups;
+    const uint32_t idesc = umma::idesc_bf16_f32((uint32_t)N);
+    // thread tid fills K chunk (tid & 7) of rows (tid >> 3) + 16 k of every A stage
+    const int c = tid & (BKC - 1);
+    int rx[8], ry[8], rz[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int v = m0 + (tid >> 3) + 16 * k;
+        rx[k] = v < nvox ? v % a.g.gx : -1;
+        ry[k] = (v / a.g.gx) % a.g.gy;
+        rz[k] = v / (a.g.gx * a.g.gy);
+    }
+    auto issue = [&](int st) {
+        unsigned char* A = sm + (st % NBUF) * stage_bytes;
+        unsigned char* B = A + a_bytes;
+        const int kc = st * BKC + c;
+        const int t = kc / cgroups, cg = kc - t * cgroups;
+        const int dx = tap_dx(t), dy = tap_dy(t), dz = tap_dz(t);
+        const bool live = kc < kchunks;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int xs = rx[k] + dx, ys = ry[k] + dy, zs = rz[k] + dz;
+            const bool ok = live && rx[k] >= 0 && xs >= 0 && ys >= 0 && zs >= 0 && xs < a.g.gx && ys < a.g.gy &&
+                            zs < a.g.gz;
+            const __nv_bfloat16* src = ok ? a.x + (size_t)((zs * a.g.gy + ys) * a.g.gx + xs) * a.cin + cg * 8 : a.x;
+            cp_async16(A + core_off((tid >> 3) + 16 * k, c, BM), src, ok);
+        }
+        for (int i = tid; i < N * BKC; i += THREADS) {
+            const int row = i / BKC, cc = i % BKC;
+            cp_async16(B + core_off(row, cc, N), a.w + (size_t)row * a.kpad + (size_t)(st * BKC + cc) * 8, true);
+        }
+    };
+
+    bool ok = true;
+    // one copy group per stage (empty past the end), so that waiting until at most
+    // LOOKAHEAD groups are pending means stage s has landed
+    for (int st = 0; st < LOOKAHEAD; ++st) {
+        if (st < nstages) issue(st);
+        cp_async_commit();
+    }
+    for (int s = 0; s < nstages; ++s) {
+        const int next = s + LOOKAHEAD;
+        if (next < nstages) {
+            const int prev = next - NBUF;  // the stage that last used this buffer
+            bool w = true;
+            if (prev >= 0) w = umma::mbar_wait(&bars[next % NBUF], (uint32_t)((prev / NBUF) & 1), WAIT_LIMIT);
+            if (!__syncthreads_and(w ? 1 : 0)) {
+                ok = false;
+                break;
+            }
+            issue(next);
+        }
+        cp_async_commit();  // (possibly empty) group keeps the group count aligned with stages
+        cp_async_wait<LOOKAHEAD>();
+        umma::fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after_sync();
+            unsigned char* A = sm + (s % NBUF) * stage_bytes;
+            const uint32_t a_addr = umma::smem_addr(A), b_addr = umma::smem_addr(A + a_bytes);
+#pragma unroll
+            for (int j = 0; j < BKC / 2; ++j) {
+                const uint64_t da = umma::smem_desc(a_addr + j * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
+                const uint64_t db = umma::smem_desc(b_addr + j * 2 * (N / 8) * 128, (N / 8) * 128, 128);
+                umma::mma_bf16(tmem, da, db, idesc, (s > 0 || j > 0) ? 1u : 0u);
+            }
+            umma::commit(&bars[s % NBUF]);
+        }
+    }
+    cp_async_wait<0>();
+    if (nstages > 0) {
+        const int last = nstages - 1;
+        const bool done = umma::mbar_wait(&bars[last % NBUF], (uint32_t)((last / NBUF) & 1), WAIT_LIMIT);
+        ok = __syncthreads_and((done && ok) ? 1 : 0) != 0;
+        if (!ok && tid == 0) atomicOr(a.err, 1u);
+    }
+    umma::fence_after_sync();
+    if (ok && nstages > 0) {
+        const int row = warp * 32 + (tid & 31);
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        const int vox = m0 + row;
+        for (int c0 = 0; c0 < N; c0 += 8) {
+            float v[8];
+            umma::tmem_ld8(lane_addr + (uint32_t)c0, v);
+            umma::tmem_wait_ld();
+            if (vox >= nvox) continue;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                float r = v[q] + (a.bias ? a.bias[c0 + q] : 0.0f);
+                v[q] = a.relu ? fmaxf(r, 0.0f) : r;
+            }
+            if (a.y) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(v[q]);
+                *reinterpret_cast<uint4*>(a.y + (size_t)vox * N + c0) = *reinterpret_cast<const uint4*>(h);
+            }
+            if (a.y32)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) a.y32[(size_t)vox * N + c0 + q] = v[q];
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, ncols);
+}
+
 static size_t conv_smem(int n) { return (size_t)2 * (BM + n) * BKC * 16; }
 
 template <int MODE>
@@ -489,7 +639,19 @@ int32_t cs_nn_conv3d(const void* x, const void* w, const float* bias, void* y, f
     a.relu = relu;
     a.err = err;
     const int tiles = (a.g.voxels() + BM - 1) / BM;
-    return launch<0>(a, dim3(tiles, 1), as_stream(stream));
+    static bool attr = false;
+    const size_t smem = (size_t)NBUF * (BM + cout_pad) * BKC * 16;
+    if (!attr) {
+        cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+    }
+    k_conv_fwd<<<dim3(tiles, 1), THREADS, smem, as_stream(stream)>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cs::set_error(std::string("conv launch: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
 }
 
 // dWt[t * cin_pad + ci][co] += sum_v X[v + off_t][ci] * dY[v][co]  (f32, accumulated).

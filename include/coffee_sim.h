@@ -376,6 +376,8 @@ int32_t cs_profile_read(CsSim* sim, CsProfile* out); /* synchronises */
 /* ---- BF16 3-D convolution on the tensor cores (tcgen05), the layers of the pressure-guess
  * U-Net (no counterpart in the reference).  Device pointers, channels-last bf16
  * activations [voxel][C]; `err` is a device flag raised if a wait times out. ---- */
+/* Y = relu?(conv3x3x3(X) + bias): x bf16 [vox][cin_pad], w packed by cs_nn_pack_weights,
+ * bias cout_pad floats or null, y bf16 / y32 f32 [vox][cout_pad] (either may be null). */
 int32_t cs_nn_conv3d(const void* x, const void* w, const float* bias, void* y, float* y32, int32_t gx, int32_t gy,
                      int32_t gz, int32_t cin_pad, int32_t cout_pad, int32_t relu, uint32_t* err, void* stream);
 int32_t cs_nn_conv3d_wgrad(const void* x, const void* dy, float* dwt, int32_t gx, int32_t gy, int32_t gz,
