@@ -21,6 +21,7 @@ configuration text.  Two conventions hold everywhere:
   4 * rho * V_sample kg, so only mass ratios enter the solve.
 """
 import math
+import random
 
 import numpy as np
 
@@ -205,3 +206,24 @@ def spiral_spout(t, radius=0.015, hz=0.5, y=V60_TOP_Y + 0.015, U=V60_U):
     """Spout origin on the spiral pour path (radius 1.5 cm, 0.5 Hz), in scene units."""
     a = 2.0 * math.pi * hz * t
     return (radius * math.cos(a) * U, y * U, radius * math.sin(a) * U)
+
+
+def c4_ensemble(lib=None, n=64, seed=3, grid=64, max_particles=340000):
+    """Batched ensemble: n independent V60 pours at 64^3 with seeded per-instance
+    parameters — water fill height and carafe pool depth (sample counts spread over
+    about 20k-300k), flow rate U[2, 6] ml/s, kettle angle U[10, 35] deg, and bed
+    log-permeability mean U[ln 5e-10, ln 2e-9] m^2.  Returns (settings list, per-instance
+    populate arguments)."""
+    rng = random.Random(seed)
+    settings, fills = [], []
+    bed_top = V60_BOT_Y + 0.3 * (V60_TOP_Y - V60_BOT_Y)
+    for i in range(n):
+        s = c2_v60(lib, grid=grid, max_particles=max_particles, seed=seed * 1000 + i)
+        r = s.raw
+        r.bed.initial_permeability = math.exp(rng.uniform(math.log(5e-10), math.log(2e-9)))
+        r.initial_kettle_angle_deg = rng.uniform(10.0, 35.0)
+        r.flow_override_ml_s = rng.uniform(2.0, 6.0)
+        settings.append(s)
+        fills.append({"fill_top": rng.uniform(bed_top + 0.006, 0.05), "pool_depth": rng.uniform(0.0, 0.012),
+                      "seed": seed * 1000 + i})
+    return settings, fills
