@@ -44,37 +44,91 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    """SM clocks and clock-event (throttle) reasons sampled while the timed region runs:
+    NVML read every 5 ms from a thread (read-only queries), with one sample taken on entry
+    and one on exit; `nvidia-smi -lms 200` when NVML is unavailable."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.005):
         self.index = index
-        self.rows = []
+        self.period = period_s
+        self.samples = []  # (sm_mhz, max_mhz, [reason names])
+        self.source = None
         self.proc = None
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _nvml_sample(self):
+        nv, h = self.nvml, self.handle
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        names = sorted({name for name, attr in self.REASONS if bits & getattr(nv, attr, 0)})
+        self.samples.append((float(sm), float(mx), names))
+
+    def _nvml_loop(self):
+        while not self.stop.wait(self.period):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+
+    def _smi_loop(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.proc.stdout:
+            r = [x.strip() for x in line.split(",")]
+            if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                self.samples.append((float(r[1]), float(r[2]),
+                                     [names[k] for k in range(4) if r[5 + k].lower() == "active"]))
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            self.nvml, self.handle = self._nvml_handle()
+            self._nvml_sample()
+            self.source = "nvml every 5 ms"
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
         except Exception:
-            self.proc = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                     "--format=csv,noheader,nounits", "-lms", "200"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi every 200 ms"
+                self.thread = threading.Thread(target=self._smi_loop, daemon=True)
+            except Exception:
+                self.thread = None
+        if self.thread:
+            self.thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
-
     def __exit__(self, *a):
-        if self.proc:
+        if self.proc is None and self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
+        elif self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
             try:
@@ -83,14 +137,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted({n for s in self.samples for n in s[2]}),
+                "samples": len(self.samples), "source": self.source}
 
 
 def build_scene(lib, args, device=0, learned=False, populate=True):
@@ -245,12 +297,13 @@ def run_c4(args, rank, world, local, dist):
     if dist:
         dist.barrier()
     particle_steps = 0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        particle_steps += sum(ens.particle_count(k) for k in range(len(mine)))
-        ens.step_substep(dt)
-    pairs = [ens.metrics(k).last_sweeps for k in range(len(mine))]  # synchronises
-    elapsed = time.perf_counter() - t0
+    with ClockSampler(local) as clocks:
+        ens.timer_start()
+        for _ in range(args.steps):
+            particle_steps += sum(ens.particle_count(k) for k in range(len(mine)))
+            ens.step_substep(dt)
+        elapsed = ens.timer_stop() * 1e-3  # CUDA events on the ensemble's stream
+    pairs = [ens.metrics(k).last_sweeps for k in range(len(mine))]
     stats = shard.gather_statistics({i: [float(ens.particle_count(k)), float(pairs[k])] for k, i in enumerate(mine)})
     if dist:
         import torch
@@ -265,8 +318,11 @@ def run_c4(args, rank, world, local, dist):
             "config": {"workload": f"c4_ensemble_{args.instances}x64cube", "instances": args.instances,
                        "particles_min": min(counts), "particles_max": max(counts), "particles_total": sum(counts),
                        "pairs_mean": sum(v[1] for v in stats.values()) / len(stats), "residual_tol": 1e-5,
-                       "omega": args.omega, "timing": "host wall clock around synchronised substeps",
-                       "parallelism": f"instances sharded over {world} GPU(s)"}}
+                       "omega": args.omega, "timing": "CUDA events on the ensemble stream, max over ranks",
+                       "l2": "not flushed: 64 resident pours' particle and grid arrays exceed the 126 MB L2 many times over"
+                             if args.instances >= 16 else "not flushed",
+                       "parallelism": f"instances sharded over {world} GPU(s)"},
+            "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ens.close()

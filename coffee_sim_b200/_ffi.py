@@ -308,6 +308,8 @@ PROTOTYPES = {
     "cs_ensemble_get_counts": (I32, [P, U32, PU32, PU32]),
     "cs_ensemble_read_particles": (I32, [P, U32, U32, U32, PF]),
     "cs_ensemble_get_metrics": (I32, [P, U32, PM]),
+    "cs_ensemble_timer_start": (I32, [P]),
+    "cs_ensemble_timer_stop": (I32, [P, C.POINTER(C.c_float)]),
     "cs_profile_enable": (I32, [P, I32]),
     "cs_profile_read": (I32, [P, C.POINTER(CsProfile)]),
     "cs_timer_start": (I32, [P]),

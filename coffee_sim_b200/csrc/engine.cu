@@ -1051,7 +1051,33 @@ Ensemble::~Ensemble() {
     for (Engine* e : eng) delete e;
     if (d_ctx) cudaFree(d_ctx);
     if (d_results) cudaFree(d_results);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
     if (stream) cudaStreamDestroy(stream);
+}
+
+static int ens_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CS_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return CS_ERR_CUDA;
+}
+
+int Ensemble::timer_start() {
+    int rc;
+    if (!t0 && (rc = ens_check(cudaEventCreate(&t0), "ensemble timer"))) return rc;
+    if (!t1 && (rc = ens_check(cudaEventCreate(&t1), "ensemble timer"))) return rc;
+    return ens_check(cudaEventRecord(t0, stream), "ensemble timer start");
+}
+
+int Ensemble::timer_stop(float* ms) {
+    if (!t0) {
+        set_error("timer not started");
+        return CS_ERR_INVALID_ARG;
+    }
+    int rc = ens_check(cudaEventRecord(t1, stream), "ensemble timer stop");
+    if (rc) return rc;
+    if ((rc = ens_check(cudaEventSynchronize(t1), "ensemble timer sync"))) return rc;
+    return ens_check(cudaEventElapsedTime(ms, t0, t1), "ensemble timer elapsed");
 }
 
 int Ensemble::init(const CsSettings* s, uint32_t n) {

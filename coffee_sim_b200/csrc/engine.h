@@ -166,6 +166,8 @@ public:
     int substep(float sub_dt);
     int step_frame(float dt);
     int sync();
+    int timer_start();            // CUDA event on the ensemble's stream
+    int timer_stop(float* ms);    // device ms since timer_start; synchronises
     Engine& at(uint32_t i) { return *eng[i]; }
     uint32_t size() const { return (uint32_t)eng.size(); }
 
@@ -179,6 +181,7 @@ private:
     std::vector<ScBuffers> hsb;
     std::vector<ScResult> results;
     int ranks = 0;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
 };
 
 }  // namespace cs

@@ -58,6 +58,20 @@ int32_t cs_ensemble_step_frame(CsEnsemble* e, float dt) {
     return e->ens->step_frame(dt);
 }
 
+int32_t cs_ensemble_timer_start(CsEnsemble* e) {
+    CS_ENS(e, 0u);
+    return e->ens->timer_start();
+}
+
+int32_t cs_ensemble_timer_stop(CsEnsemble* e, float* ms) {
+    CS_ENS(e, 0u);
+    if (!ms) {
+        cs::set_error("null output pointer");
+        return CS_ERR_INVALID_ARG;
+    }
+    return e->ens->timer_stop(ms);
+}
+
 int32_t cs_ensemble_add_water_block(CsEnsemble* e, uint32_t i, const float lo[3], const float hi[3],
                                     uint32_t per_axis, float jitter, uint32_t seed, uint32_t require_open_sdf,
                                     uint32_t* added) {

@@ -469,6 +469,15 @@ class MpmEnsemble:
         self.lib.call("cs_ensemble_get_metrics", self._h, i, C.byref(m))
         return m
 
+    def timer_start(self):
+        self.lib.call("cs_ensemble_timer_start", self._h)
+
+    def timer_stop(self):
+        """Device milliseconds since timer_start (CUDA events on the ensemble's stream)."""
+        ms = C.c_float()
+        self.lib.call("cs_ensemble_timer_stop", self._h, C.byref(ms))
+        return ms.value
+
 
 class _EnsembleMember:
     def __init__(self, ens, i):

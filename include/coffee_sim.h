@@ -344,6 +344,8 @@ int32_t cs_ensemble_set_flow_override(CsEnsemble* ens, uint32_t i, float flow_ml
 int32_t cs_ensemble_get_counts(CsEnsemble* ens, uint32_t i, uint32_t* num_water, uint32_t* num_bed);
 int32_t cs_ensemble_read_particles(CsEnsemble* ens, uint32_t i, uint32_t first, uint32_t count, float* out);
 int32_t cs_ensemble_get_metrics(CsEnsemble* ens, uint32_t i, CsMetrics* out);
+int32_t cs_ensemble_timer_start(CsEnsemble* ens);           /* CUDA event on the ensemble's stream */
+int32_t cs_ensemble_timer_stop(CsEnsemble* ens, float* ms); /* device ms since the start; synchronises */
 
 /* ---- device timing and profiling (no counterpart: the reference defers timestamp
  * queries, mod.rs:313 `timestamp_writes: None`) ---- */

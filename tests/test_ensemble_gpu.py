@@ -68,3 +68,15 @@ def test_ensemble_rejects_mixed_grids(engine):
     b = scenes.c2_v60(engine, grid=48, max_particles=60000)
     with pytest.raises(_ffi.CsError):
         MpmEnsemble([a, b], engine)
+
+
+def test_ensemble_device_timer(engine):
+    ens = MpmEnsemble([_v60(engine, 4.0)], engine)
+    scenes.populate_c2(ens.member(0), seed=2)
+    with pytest.raises(_ffi.CsError):
+        ens.timer_stop()  # not started
+    ens.timer_start()
+    ens.step_substep(scenes.C2_DT)
+    ms = ens.timer_stop()
+    assert 0.0 < ms < 5000.0
+    ens.close()
