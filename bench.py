@@ -155,6 +155,7 @@ def build_scene(lib, args, device=0, learned=False, populate=True):
     s.raw.rbgs_omega = args.omega
     s.raw.max_sweeps = args.max_sweeps
     s.raw.check_every = args.check_every
+    s.raw.rbgs_kernel = {"p2p": 2, "cluster": 3}[args.solve_sync]
     s.raw.p2g_mode = {"atomic": 0, "sorted": 1}[args.p2g]
     s.raw.device_emission = 1  # jet samples built on the device (the oracle matches this mode)
     sim = MpmSim3D(s, lib)
@@ -220,7 +221,9 @@ def learned_arm(lib, args, device, state, dt, barrier, dist):
            "pressure_solve_ms": (prof.phase_ms[4] + prof.phase_ms[5] + prof.phase_ms[10]) / n,
            "learned_guess_ms": prof.phase_ms[10] / n, "sweeps_per_step": prof.sweeps / n,
            "guess_kept_fraction": used / args.steps, "final_residual": sim.latest_metrics().last_residual,
-           "weights": "coffee_sim_b200/weights/unet_v60_64.npy (python -m coffee_sim_b200.train_unet)"}
+           "weights": "coffee_sim_b200/weights/unet_v60_64.npy (python -m coffee_sim_b200.train_unet)",
+           "launch": "direct launches with per-phase CUDA events (the learned warm start has no graph "
+                     "mode); compare with plain.value_direct_launches"}
     sim.close()
     return out
 
@@ -286,6 +289,7 @@ def run_c4(args, rank, world, local, dist):
         settings[i].raw.p2g_mode = 1
         settings[i].raw.rbgs_omega = args.omega
         settings[i].raw.max_sweeps = args.max_sweeps
+        settings[i].raw.rbgs_kernel = {"p2p": 2, "cluster": 3}[args.solve_sync]
     ens = MpmEnsemble([settings[i] for i in mine], lib)
     for k, i in enumerate(mine):
         f = fills[i]
@@ -339,6 +343,9 @@ def main():
     # defaults chosen by cs_autotune on this scene (omega 1.80-1.96 x checks every 5/10/20 pairs)
     ap.add_argument("--omega", type=float, default=1.92)
     ap.add_argument("--max-sweeps", type=int, default=4000)
+    ap.add_argument("--solve-sync", default="p2p", choices=["p2p", "cluster"],
+                    help="colour separation inside the cluster solve: point-to-point mbarrier waits "
+                         "or cluster barriers")
     ap.add_argument("--check-every", type=int, default=20)
     ap.add_argument("--p2g", default="sorted", choices=["atomic", "sorted"],
                     help="P2G accumulation: per-particle global atomics or tile-sorted shared memory")
@@ -395,9 +402,30 @@ def main():
             dist.barrier()
             torch.cuda.synchronize()
 
-    # ---- device-timed region: K substeps, L2 flushed before each ----
+    # ---- profiling pass: the K substeps with direct launches and CUDA events around
+    # every phase (phase breakdown, sweep counts, the solve kernel's launch times) ----
     sim.restore(state)
     sim.profile_enable(True)
+    prof_ms = 0.0
+    for _ in range(args.steps):
+        sim.flush_l2()
+        sim.timer_start()
+        sim.step_substep(dt)
+        prof_ms += sim.timer_stop()
+    prof = sim.profile_read()
+    metrics = sim.latest_metrics()
+
+    # ---- device-timed region: the same K substeps replayed as the captured substep
+    # graph (no per-phase events), L2 flushed before each ----
+    use_graph = not args.no_graph
+    if use_graph:
+        # capture and instantiate the substep graph outside the timed loops
+        sim.set_graph_mode(True)
+        sim.restore(state)
+        sim.step_substep(dt)
+        sim.sync()
+    sim.restore(state)
+    sim.profile_enable(True)  # counts launches; graph replays record no phase events
     step_ms = []
     particle_steps = 0
     barrier()
@@ -409,8 +437,8 @@ def main():
             sim.step_substep(dt)
             step_ms.append(sim.timer_stop())
     barrier()
-    prof = sim.profile_read()
-    metrics = sim.latest_metrics()
+    prof_timed = sim.profile_read()
+    timed_metrics = sim.latest_metrics()
     total_ms = sum(step_ms)
     if dist:
         import torch
@@ -421,12 +449,6 @@ def main():
 
     # ---- end to end through the public API: the same K substeps, each with its host
     # emission upload and the metrics readback ----
-    if not args.no_graph:
-        # capture and instantiate the substep graph outside the timed loop
-        sim.set_graph_mode(True)
-        sim.restore(state)
-        sim.step_substep(dt)
-        sim.sync()
     sim.restore(state)
     sim.profile_enable(True)
     barrier()
@@ -437,7 +459,7 @@ def main():
         sim.latest_metrics()
     e2e_s = time.perf_counter() - t0
     prof_e2e = sim.profile_read()
-    if not args.no_graph:
+    if use_graph:
         sim.set_graph_mode(False)
     if dist:
         import torch
@@ -479,11 +501,18 @@ def main():
                    "bed_particles": n_bed, "timed_substeps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "substep_dt_s": dt, "residual_tol": 1e-5, "omega": args.omega, "warm_start": "previous substep",
                    "check_every_pairs": args.check_every, "p2g": args.p2g,
-                   "emission": "device kernel", "e2e_launch": "direct" if args.no_graph else "CUDA graph replay", "l2": "flushed (512 MB write) before each timed step",
+                   "solve_sync": {"p2p": "point-to-point mbarrier waits", "cluster": "cluster barriers"}[args.solve_sync],
+                   "emission": "device kernel",
+                   "timed_launch": "CUDA graph replay" if use_graph else "direct launches",
+                   "e2e_launch": "CUDA graph replay" if use_graph else "direct launches",
+                   "l2": "flushed (512 MB write) before each timed step",
                    "parallelism": f"replicas x{world}"},
         "pressure_solve_ms": (prof.phase_ms[4] + prof.phase_ms[5]) / max(prof.substeps, 1),
         "sweeps_per_step": pairs_per_step,
-        "final_residual": metrics.last_residual,
+        "sweeps_per_step_timed": prof_timed.sweeps / max(prof_timed.substeps, 1),
+        "final_residual": timed_metrics.last_residual,
+        "profile_pass": {"ms_per_step": prof_ms / args.steps, "launch": "direct, CUDA events around every phase",
+                         "value": particle_steps * world / (prof_ms * 1e-3)},
         "phase_ms_per_step": {n: prof.phase_ms[i] / max(prof.substeps, 1)
                               for i, n in enumerate(["emit", "clear", "p2g", "grid", "sweeps", "residual",
                                                      "project", "g2p", "bed", "render", "learned"])},
@@ -492,17 +521,20 @@ def main():
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
                      "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": launch_ms,
+                     "kernel_timing": "CUDA events around each launch on the engine stream, profiling pass "
+                                      "over the same K substeps",
                      "launches": int(prof.phase_launches[4]),
                      "step_algorithmic_bytes": step_bytes,
                      "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": prof_e2e.h2d_bytes / args.steps,
                 "d2h_bytes_per_step": prof_e2e.d2h_bytes / args.steps},
-        "gpu_launches": int(prof.launches),
+        "gpu_launches": int(prof_timed.launches),
         "clocks": clocks.summary(),
     }
     line["plain"] = {"value": value, "pressure_solve_ms": line["pressure_solve_ms"],
-                      "sweeps_per_step": pairs_per_step, "warm_start": "previous substep"}
+                      "sweeps_per_step": pairs_per_step, "warm_start": "previous substep",
+                      "value_direct_launches": line["profile_pass"]["value"]}
     if not args.no_learned:
         line["learned"] = learned_arm(lib, args, local, state, dt, barrier, dist)
     if rank == 0 and world == 1 and not args.no_cpu:

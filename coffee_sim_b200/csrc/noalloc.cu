@@ -148,7 +148,8 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
         return CS_ERR_CUDA;
     }
     if ((rc = cs::sc_launch_prep(dctx, &sb, codes, slot->ranks, 1, st, slot->sms))) return rc;
-    if ((rc = cs::sc_launch_cluster(dctx, slot->ranks, 1, residual_tol, max_pairs, check_every, st))) return rc;
+    if ((rc = cs::sc_launch_cluster(dctx, slot->ranks, 1, residual_tol, max_pairs, check_every, st, 1u)))
+        return rc;
     cs::ScResult res;
     e = cudaMemcpyAsync(&res, sb.result, sizeof(res), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -45,6 +45,45 @@ __device__ __forceinline__ void sc_st(uint32_t addr, float v) {
     asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
 }
 
+// Point-to-point halo exchange.  The value goes out as an asynchronous remote store
+// whose completion counts 4 bytes on an mbarrier of the receiving CTA; the receiver
+// arms that mbarrier with the byte count it expects for the colour and waits for the
+// phase to complete.  A store may land before the receiver arms the phase (the
+// transaction count goes negative until the expect-tx arrives).
+__device__ __forceinline__ void sc_st_async(uint32_t addr, float v, uint32_t mbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];" ::"r"(addr),
+                 "r"(__float_as_uint(v)), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void sc_mbar_init(uint32_t a) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void sc_mbar_expect(uint32_t a, uint32_t bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(a),
+        "r"(bytes)
+        : "memory");
+}
+// Waits for the phase of parity `parity`; gives up (false) once `cycles` SM clock
+// cycles have passed since the first poll.
+__device__ __forceinline__ bool sc_mbar_wait(uint32_t a, uint32_t parity, long long cycles) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > cycles) return false;
+    }
+}
+constexpr long long kScWaitCycles = 1ll << 30;  // ~0.5 s at 2 GHz
+
 // Cells are numbered along a Morton (Z-order) curve over the grid padded to a power
 // of two per side, so each CTA's contiguous chunk is a compact 3-D block and few of
 // its neighbours live in other CTAs.
@@ -205,6 +244,7 @@ __global__ void k_sc_halo(const Ctx* __restrict__ cp) {
                 hs[f] = h;
                 if (h < (uint32_t)SC_HALO) {
                     sb.halo_fill[(size_t)q * SC_HALO + h] = fci;
+                    atomicAdd(&sb.counts[SC_RECV0 + q * 2 + par], 1u);
                     const uint32_t e = atomicAdd(&sb.counts[SC_MAX_RANKS + r * 2 + par], 1u);
                     if (e < (uint32_t)SC_SEND) sb.send[((size_t)r * 2 + par) * SC_SEND + e] = i | (q << 12) | (h << 16);
                 }
@@ -233,9 +273,17 @@ __device__ __forceinline__ float sc_weight(float fc_i, float fc_j) {
     return (fc_i > 1.5f || fc_j > 1.5f) ? 1.0f : fminf(fc_i, fc_j);
 }
 
-// One cluster per instance (blockIdx.y); R = cluster size along x.
+// One cluster per instance (blockIdx.y); R = cluster size along x.  With `p2p` the
+// two colours of a red-black pair are separated by point-to-point waits (each CTA waits
+// only for the halo values it receives, counted on its mbarriers) instead of cluster
+// barriers.  Either way a CTA starts a colour only after every neighbour finished the
+// other colour, so the values are the same.  The neighbour relation is symmetric with
+// opposite colours (a black cell of CTA i next to a cell of CTA j makes that cell red and
+// held by i), so a CTA can only send a colour after receiving the other colour from each
+// receiver, which that receiver sent after it finished reading its old halo values:
+// no store overwrites a halo value before it was read.
 __global__ void __launch_bounds__(SC_THREADS, 1)
-    k_sc_solve(const Ctx* __restrict__ cp, float tol, uint32_t max_pairs, uint32_t check_every) {
+    k_sc_solve(const Ctx* __restrict__ cp, float tol, uint32_t max_pairs, uint32_t check_every, uint32_t p2p) {
     extern __shared__ __align__(16) unsigned char smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const Ctx& c = cp[blockIdx.y];
@@ -259,6 +307,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     const uint32_t n_red = inf.red_before[rank + 1] - inf.red_before[rank];
     const uint32_t n_halo = sb.counts[rank];
     const uint32_t n_send[2] = {sb.counts[SC_MAX_RANKS + 2 * rank], sb.counts[SC_MAX_RANKS + 2 * rank + 1]};
+    const uint32_t n_recv[2] = {sb.counts[SC_RECV0 + 2 * rank], sb.counts[SC_RECV0 + 2 * rank + 1]};
 
     float* dval = sc_arr<float>(smem, ScLayout::dval);
     float* fcode = sc_arr<float>(smem, ScLayout::fcode);
@@ -272,7 +321,14 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     uint8_t* flg = sc_arr<uint8_t>(smem, ScLayout::flags);
     double* part = sc_arr<double>(smem, ScLayout::part);
     double* red = sc_arr<double>(smem, ScLayout::red);
+    uint32_t* abortf = sc_arr<uint32_t>(smem, ScLayout::abortf);
     const uint32_t a_dval = (uint32_t)__cvta_generic_to_shared(dval);
+    const uint32_t a_mbar = (uint32_t)__cvta_generic_to_shared(smem + ScLayout::mbar);  // 8 bytes per colour
+    if (p2p && threadIdx.x == 0) {
+        sc_mbar_init(a_mbar);
+        sc_mbar_init(a_mbar + 8u);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     const uint32_t* cell_of = sb.cell_of + rank * 4096u;
     const uint32_t sy = u.gx, sz = u.gx * u.gy;
 
@@ -310,6 +366,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         }
     }
     cluster.sync();
+
+    bool timed_out = false;  // a point-to-point wait of this thread ran out
+    bool abort_all = false;  // some CTA timed out (uniform: read from the reduction)
 
     // FP64 residual of the current pressure; g <- residual, d <- 0 (halo copies too).
     // Neighbour pressures come from this CTA's shared memory or, for halo cells, from
@@ -364,7 +423,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             red[warp] = r2;
             red[32 + warp] = b2;
         }
-        __syncthreads();
+        const uint32_t cta_timed_out = __syncthreads_or(timed_out ? 1 : 0) ? 1u : 0u;
         if (threadIdx.x < R) {
             double a = 0.0, bsum = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
@@ -374,12 +433,15 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             double* dst = cluster.map_shared_rank(part, threadIdx.x);
             dst[slot * 2 * SC_MAX_RANKS + rank] = a;
             dst[slot * 2 * SC_MAX_RANKS + SC_MAX_RANKS + rank] = bsum;
+            uint32_t* fdst = cluster.map_shared_rank(abortf, threadIdx.x);
+            fdst[slot * SC_MAX_RANKS + rank] = cta_timed_out;
         }
         cluster.sync();
         double a = 0.0, bsum = 0.0;
         for (uint32_t q = 0; q < R; ++q) {
             a += part[slot * 2 * SC_MAX_RANKS + q];
             bsum += part[slot * 2 * SC_MAX_RANKS + SC_MAX_RANKS + q];
+            abort_all = abort_all || abortf[slot * SC_MAX_RANKS + q] != 0u;
         }
         if (bsum <= 0.0) return 0.0;
         return sqrt(a) / sqrt(bsum);
@@ -416,16 +478,32 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         if (omega != 1.0f) dn = me + omega * (dn - me);
         dval[i] = dn;
     };
-    auto sweep = [&](uint32_t lo, uint32_t hi, uint32_t col) {
-        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) relax(i);
-        __syncthreads();
-        // push the new values of this colour to the CTAs that hold them as halo
+    // push the new values of colour `col` to the CTAs that hold them as halo
+    auto push = [&](uint32_t col) {
         const uint32_t* list = snd + col * SC_SEND;
         for (uint32_t e = threadIdx.x; e < n_send[col]; e += blockDim.x) {
             const uint32_t s = list[e];
             const uint32_t src = s & 4095u, q = (s >> 12) & 15u, h = s >> 16;
-            sc_st(sc_mapa(a_dval + (uint32_t)(SC_HALO0 + h) * 4u, q), dval[src]);
+            const uint32_t dst = sc_mapa(a_dval + (uint32_t)(SC_HALO0 + h) * 4u, q);
+            if (p2p)
+                sc_st_async(dst, dval[src], sc_mapa(a_mbar + col * 8u, q));
+            else
+                sc_st(dst, dval[src]);
         }
+    };
+    auto sweep = [&](uint32_t lo, uint32_t hi, uint32_t col) {
+        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) relax(i);
+        __syncthreads();
+        push(col);
+    };
+    // p2p: arm this CTA's mbarrier of colour `col` with the bytes it receives and wait
+    uint32_t phase_bits = 0;  // bit col: parity of the next phase of mbarrier col
+    auto wait_colour = [&](uint32_t col) {
+        const uint32_t a = a_mbar + col * 8u;
+        if (threadIdx.x == 0) sc_mbar_expect(a, 4u * n_recv[col]);
+        // after one timeout the remaining waits of the solve only poll once
+        if (!sc_mbar_wait(a, (phase_bits >> col) & 1u, timed_out ? 0ll : kScWaitCycles)) timed_out = true;
+        phase_bits ^= 1u << col;
     };
 
     // p <- p + d in FP64, split back into hi/lo.  Cells other CTAs hold as halo are
@@ -455,14 +533,21 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     double r0 = residual(slot);
     double r1 = r0;
     uint32_t pairs = 0, evals = 1;
-    while (!(r1 <= (double)tol) && pairs < max_pairs) {
+    while (!(r1 <= (double)tol) && pairs < max_pairs && !abort_all) {
         uint32_t k = min(ce, max_pairs - pairs);
         for (uint32_t j = 0; j < k; ++j) {
-            cluster.sync();
+            if (!p2p)
+                cluster.sync();
+            else if (j > 0)
+                wait_colour(1);  // black values of the previous pair
             sweep(0, n_red, 0);
-            cluster.sync();
+            if (!p2p)
+                cluster.sync();
+            else
+                wait_colour(0);  // red values of this pair
             sweep(n_red, n_loc, 1);
         }
+        if (p2p) wait_colour(1);
         pairs += k;
         __syncthreads();
         accumulate();
@@ -486,7 +571,21 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         sb.result->r0 = r0;
         sb.result->r1 = r1;
     }
+    const bool gave_up = __syncthreads_or(timed_out ? 1 : 0) != 0;
+    if (abort_all) {
+        // stores that were still travelling when a wait gave up land within microseconds;
+        // give them ~10 ms before the CTAs leave
+        const long long t0 = clock64();
+        while (clock64() - t0 < (1ll << 24)) {
+        }
+    }
     cluster.sync();  // keep every CTA's shared memory alive until remote accesses end
+    if (gave_up && threadIdx.x == 0) {
+        // a point-to-point wait ran out: the values are not trusted (the host falls
+        // back to per-colour launches) and the timeout is reported
+        atomicExch(&sb.result->status, 3u);
+        atomicOr(&c.metrics[M_TIMEOUT], 1u);
+    }
 }
 
 // Adds one solve's result to the running totals (one thread; graph mode, where the

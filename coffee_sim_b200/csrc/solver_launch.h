@@ -19,7 +19,9 @@ size_t sc_scan_temp_bytes(uint32_t codes);
 // same ScBuffers on the host, for the CUB scans launched from the host.
 int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ranks, uint32_t instances,
                    cudaStream_t stream, int sms);
+// p2p: 1 separates the colours with point-to-point mbarrier waits, 0 with cluster
+// barriers (rbgs_kernel = 3).
 int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,
-                      uint32_t check_every, cudaStream_t stream);
+                      uint32_t check_every, cudaStream_t stream, uint32_t p2p);
 
 }  // namespace cs

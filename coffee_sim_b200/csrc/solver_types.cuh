@@ -33,7 +33,9 @@ struct ScLayout {
     static constexpr size_t flags = snd + sizeof(uint32_t) * 2 * SC_SEND;  // uint8 x 4096
     static constexpr size_t part = flags + 4096;                         // double[2 slots][2][SC_MAX_RANKS]
     static constexpr size_t red = part + sizeof(double) * 4 * SC_MAX_RANKS;  // double[2][32]
-    static constexpr size_t bytes = red + sizeof(double) * 64;
+    static constexpr size_t mbar = red + sizeof(double) * 64;               // uint64 mbarrier per colour
+    static constexpr size_t abortf = mbar + sizeof(unsigned long long) * 2;  // uint32[2 slots][SC_MAX_RANKS]
+    static constexpr size_t bytes = abortf + sizeof(uint32_t) * 2 * SC_MAX_RANKS;
 };
 static_assert(ScLayout::bytes <= 232448, "cluster solve state exceeds the 227 KB shared-memory limit");
 // A face reference is a 13-bit slot index; bit 15 of the first word marks a cell
@@ -59,8 +61,10 @@ struct ScTotals {
     unsigned long long sweeps, evals, failed, runs;
     ScResult last;
 };
-// counters: halo size per rank, then send-list length per (rank, colour)
-constexpr int SC_COUNTS = SC_MAX_RANKS * 3;
+// counters: halo size per rank, send-list length per (rank, colour), then the halo
+// values each rank receives per colour (one per halo slot of a cell of that colour)
+constexpr int SC_COUNTS = SC_MAX_RANKS * 5;
+constexpr int SC_RECV0 = SC_MAX_RANKS * 3;
 
 struct ScBuffers {
     unsigned long long* flags;   // Morton codes: fluid | red << 32

@@ -180,11 +180,13 @@ def test_v60_refinement_solve_matches_oracle(engine, oracle, grid, omega):
         _assert_same(a, b, f"V60 {grid}^3 substep {k}", ["particles", "affine", "bed_extract", "grid_vel", "pressure"])
 
 
-def test_cluster_solver_matches_per_colour_launches(engine):
-    """The one-launch cluster-resident solve (solver_cluster.cuh) against the
-    per-colour launch path on the same state: identical sweep counts and pressures."""
+@pytest.mark.parametrize("cluster_kernel", [2, 3])
+def test_cluster_solver_matches_per_colour_launches(engine, cluster_kernel):
+    """The one-launch cluster-resident solve (solver_cluster.cuh; 2: point-to-point
+    mbarrier waits between the colours, 3: cluster barriers) against the per-colour launch
+    path on the same state: identical sweep counts and pressures."""
     sims = []
-    for kernel in (1, 2):
+    for kernel in (1, cluster_kernel):
         s = scenes.c2_v60(engine)
         s.raw.rbgs_omega = 1.9
         s.raw.rbgs_kernel = kernel
