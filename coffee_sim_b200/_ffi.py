@@ -255,6 +255,7 @@ PROTOTYPES = {
     "cs_abi_version": (U32, []),
     "cs_is_gpu_engine": (I32, []),
     "cs_settings_default_v60": (I32, [PS]),
+    "cs_kozeny_carman_permeability_m2": (F32, [F32, F32]),
     "cs_settings_benchmark_free_stream": (I32, [PS]),
     "cs_settings_benchmark_center_pour": (I32, [PS]),
     "cs_settings_aim_spout": (I32, [PS, F32, F32, F32]),

@@ -399,7 +399,8 @@ int Engine::solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done) 
     count_launch(kScPrepLaunches);
     mark(CS_PHASE_SWEEPS);
     const CsSettings& s = settings;
-    if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every, stream_)))
+    if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every, stream_,
+                                s.rbgs_kernel == 3 ? 0u : 1u)))
         return rc;
     count_launch();
     ScResult res;
@@ -566,7 +567,7 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
                 if ((rc = sc_launch_prep(dc, &sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_))) return rc;
                 count_launch(kScPrepLaunches);
                 if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
-                                            stream_)))
+                                            stream_, s.rbgs_kernel == 3 ? 0u : 1u)))
                     return rc;
                 count_launch();
                 CS_LAUNCH(k_sc_account<<<1, 1, 0, stream_>>>(sc_buf_.result, (ScTotals*)sc_totals_.ptr));
@@ -958,6 +959,7 @@ struct SnapHeader {
     float total_time, total_emitted_mass;
     uint32_t total_dropped, have_prev_p;
     host::Inflow inflow;
+    CsSpout spout;  // set_spout_position / set_spout_target move it (mod.rs:452-458)
 };
 static const uint64_t kSnapMagic = 0x43534e4150423230ull;  // "CSNAPB20"
 
@@ -977,7 +979,7 @@ int Engine::snapshot_save(void* buf, uint64_t bytes) {
     SnapHeader h;
     std::memset(&h, 0, sizeof(h));
     h.magic = kSnapMagic;
-    h.version = 2;
+    h.version = 3;
     h.max_p = settings.max_particles;
     h.cells = cells_;
     h.num_water = num_water;
@@ -987,6 +989,7 @@ int Engine::snapshot_save(void* buf, uint64_t bytes) {
     h.total_dropped = total_dropped;
     h.have_prev_p = have_prev_p ? 1 : 0;
     h.inflow = inflow;
+    h.spout = settings.spout;
     char* p = (char*)buf;
     std::memcpy(p, &h, sizeof(h));
     p += sizeof(h);
@@ -1016,7 +1019,7 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
         return CS_ERR_INVALID_ARG;
     }
     std::memcpy(&h, buf, sizeof(h));
-    if (h.magic != kSnapMagic || h.version != 2 || h.max_p != settings.max_particles || h.cells != cells_ ||
+    if (h.magic != kSnapMagic || h.version != 3 || h.max_p != settings.max_particles || h.cells != cells_ ||
         bytes < need) {
         set_error("snapshot does not match this simulation's sizes");
         return CS_ERR_INVALID_ARG;
@@ -1042,6 +1045,7 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
     total_dropped = h.total_dropped;
     have_prev_p = h.have_prev_p != 0;
     inflow = h.inflow;
+    settings.spout = h.spout;
     return sync();
 }
 
@@ -1203,7 +1207,9 @@ int Ensemble::enqueue() {
     k_classify<<<dim3(cb, n), T, 0, st>>>(dc);
     if (s.solve_mode == CS_SOLVE_RESIDUAL) {
         if ((rc = sc_launch_prep(dc, hsb.data(), (uint32_t)e0.sc_codes_, ranks, n, st, e0.sms_))) return rc;
-        if ((rc = sc_launch_cluster(dc, ranks, n, s.residual_tol, s.max_sweeps, s.check_every, st))) return rc;
+        if ((rc = sc_launch_cluster(dc, ranks, n, s.residual_tol, s.max_sweeps, s.check_every, st,
+                                    s.rbgs_kernel == 3 ? 0u : 1u)))
+            return rc;
         k_gather_results<<<1, 256, 0, st>>>(dc, n, (ScResult*)d_results);
         if (cudaMemcpyAsync(results.data(), d_results, sizeof(ScResult) * n, cudaMemcpyDeviceToHost, st) !=
                 cudaSuccess ||
@@ -1652,7 +1658,7 @@ int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ra
 
 // The cluster solve of `instances` independent systems: one cluster of `ranks` CTAs each.
 int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,
-                      uint32_t check_every, cudaStream_t stream) {
+                      uint32_t check_every, cudaStream_t stream, uint32_t p2p) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ranks, instances, 1);
     cfg.blockDim = dim3(SC_THREADS, 1, 1);
@@ -1665,7 +1671,7 @@ int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol
     attr.val.clusterDim.z = 1;
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_sc_solve, d_ctx, tol, max_pairs, check_every);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_sc_solve, d_ctx, tol, max_pairs, check_every, p2p);
     if (e != cudaSuccess) {
         set_error(std::string("cluster solve launch: ") + cudaGetErrorString(e));
         return CS_ERR_CUDA;
@@ -1710,7 +1716,7 @@ static int validate(const CsSettings* s) {
         return CS_ERR_INVALID_ARG;
     }
     if (s->p2g_mode > CS_P2G_INT64 || s->warm_start > CS_WARM_LEARNED || s->pressure_storage > CS_PRESSURE_FP32 ||
-        s->solve_mode > CS_SOLVE_RESIDUAL || s->rbgs_kernel > 2) {
+        s->solve_mode > CS_SOLVE_RESIDUAL || s->rbgs_kernel > 3) {
         set_error("unknown mode value in settings");
         return CS_ERR_INVALID_ARG;
     }
@@ -1777,6 +1783,9 @@ int32_t cs_settings_aim_spout(CsSettings* s, float x, float y, float z) {
     CS_PTR(s);
     cs::host::spout_aim_at(s->spout, x, y, z);
     return CS_OK;
+}
+float cs_kozeny_carman_permeability_m2(float grind_um, float porosity) {
+    return cs::host::kozeny_carman_m2(grind_um, porosity);
 }
 
 int32_t cs_create(const CsSettings* settings, CsSim** out) {

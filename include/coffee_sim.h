@@ -223,7 +223,8 @@ typedef struct CsSettings {
     uint32_t device_emission;     /* 1: emit jet particles with a kernel (graph-capturable) */
     uint32_t use_graph;           /* 1: capture the substep in a CUDA graph */
     int32_t device;               /* CUDA device ordinal */
-    uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 cluster-resident solve */
+    uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 cluster-resident solve,
+                                     3 cluster-resident with cluster barriers between colours */
     float flow_override_ml_s;     /* >0: constant flow instead of the kettle-angle model */
     float exit_speed_override;    /* >0 with flow override: jet speed */
     float rbgs_omega;             /* red-black over-relaxation; 0 or 1 = plain Gauss-Seidel */
@@ -262,6 +263,9 @@ int32_t cs_settings_benchmark_free_stream(CsSettings* out); /* MpmSettings::benc
 int32_t cs_settings_benchmark_center_pour(CsSettings* out); /* MpmSettings::benchmark_center_pour */
 /* SpoutSettings::aim_at / translate_origin_to on a settings value (inflow.rs:49-67). */
 int32_t cs_settings_aim_spout(CsSettings* s, float x, float y, float z);
+/* kozeny_carman_permeability_m2 (brew_config.rs:92-96): bed permeability in m^2 of a
+ * grind of mean particle diameter grind_um at the given porosity. */
+float cs_kozeny_carman_permeability_m2(float grind_um, float porosity);
 
 /* ---- lifetime (mod.rs:196-262, 432-446) ---- */
 int32_t cs_create(const CsSettings* settings, CsSim** out);   /* MpmSim3D::new */

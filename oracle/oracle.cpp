@@ -89,7 +89,8 @@ struct SimBase {
     virtual float sample_sdf_pub(float x, float y, float z) = 0;
 };
 
-enum { RD_PART, RD_AFF, RD_BEDX, RD_LANES, RD_GVEL, RD_P, RD_KIND, RD_LOOKUP, RD_DELTA, RD_RENDER, RD_SDF, RD_CLASS, RD_LANES64 };
+enum { RD_PART, RD_AFF, RD_BEDX, RD_LANES, RD_GVEL, RD_P, RD_KIND, RD_LOOKUP, RD_DELTA, RD_RENDER, RD_SDF, RD_CLASS, RD_LANES64,
+       RD_DIV };
 
 template <class R>
 struct Sim : SimBase {
@@ -1874,6 +1875,7 @@ struct Sim : SimBase {
                     f[c] = fixed_point() ? (float)(R(grid[c]) * R(1.0f / FP_SCALE)) : (float)pf[c];
                 break;
             case RD_KIND: for (size_t c = 0; c < cells; ++c) i[c] = grid[3 * cells + c]; break;
+            case RD_DIV: for (size_t c = 0; c < cells; ++c) f[c] = (float)div_load((uint32_t)c); break;
             case RD_LOOKUP: for (size_t c = 0; c < cells; ++c) i[c] = lookup[c]; break;
             case RD_DELTA: for (size_t k = 0; k < delta.size(); ++k) i[k] = delta[k]; break;
             case RD_SDF: std::memcpy(out, sdf.data(), sdf.size() * 4); break;
@@ -1956,6 +1958,9 @@ int32_t cs_settings_aim_spout(CsSettings* s, float x, float y, float z) {
     if (!s) return fail(CS_ERR_INVALID_ARG, "null");
     spout_aim_at(s->spout, x, y, z);
     return CS_OK;
+}
+float cs_kozeny_carman_permeability_m2(float grind_um, float porosity) {
+    return kozeny_carman(grind_um, porosity);
 }
 
 int32_t cs_create(const CsSettings* settings, CsSim** out) {
@@ -2249,6 +2254,15 @@ int32_t cs_sync(CsSim* s) { return s ? CS_OK : fail(CS_ERR_INVALID_ARG, "null si
 // 1 effective head, speed cap, exit speed, flow rate at angle a0 for settings s;
 // 2 exit_speed_from_head(a0 head, a1 cap, s gravity/units);
 // 3 flow_rate_from_speed(a0 speed, a1 nozzle, a2 cd, a3 vol_to_ml, a4 max).
+// Test-only: the solver's right-hand side input (classify's divergence minus its volume
+// target, per cell, as the pressure sweep reads it), valid after a partial substep that
+// ran classify.
+extern "C" int32_t oracle_read_divergence(CsSim* s, float* out) {
+    if (!s || !s->impl || !out) return fail(CS_ERR_INVALID_ARG, "null");
+    s->impl->read(RD_DIV, 0, 0, out);
+    return CS_OK;
+}
+
 extern "C" int32_t oracle_eval(int32_t fn, const CsSettings* s, const float* a, float* out) {
     if (!a || !out) return fail(CS_ERR_INVALID_ARG, "null");
     switch (fn) {

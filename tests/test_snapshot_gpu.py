@@ -62,3 +62,32 @@ def test_snapshot_rejects_other_sizes(engine):
         other.restore(blob)
     with pytest.raises(Exception):
         sim.restore(blob[:64])
+
+
+def test_snapshot_restores_the_spout_and_kettle(engine):
+    """The spout position and target (set_spout_position / set_spout_target, mod.rs:452-458)
+    and the kettle angle are part of the saved state: frames after a restore pour from
+    where the spout was when the snapshot was taken."""
+    from coffee_sim_b200.sim import MpmSettings
+    sim = MpmSim3D(MpmSettings.benchmark_free_stream(engine), engine)
+    sim.set_kettle_angle(36.0)
+    for _ in range(3):
+        sim.step_frame(1.0 / 60.0)
+    blob = sim.snapshot()
+    pos = sim.spout_position()
+    for f in range(3):
+        sim.set_spout_position(-0.1 * (f + 1), 6.8, 0.0)
+        sim.step_frame(1.0 / 60.0)
+    moved = _state(sim)
+    sim.restore(blob)
+    assert sim.spout_position() == pos
+    assert sim.kettle_angle() == 36.0
+    for f in range(3):
+        sim.set_spout_position(-0.1 * (f + 1), 6.8, 0.0)
+        sim.step_frame(1.0 / 60.0)
+    _same(moved, _state(sim))
+    sim.restore(blob)
+    for _ in range(3):
+        sim.step_frame(1.0 / 60.0)
+    still = _state(sim)
+    assert mismatch(still["particles"], moved["particles"]) > 0  # the spout did move
