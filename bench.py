@@ -316,6 +316,15 @@ def run_c4(args, rank, world, local, dist):
         dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
         elapsed, particle_steps = float(t[0].item()), float(t[1].item())
     counts = [v[0] for v in stats.values()]
+    # step roofline: compulsory bytes of every instance's substep (the bench's formula,
+    # dense 64^3 grid per instance) over the step time, against the measured HBM peak
+    # (pairs: each instance's last substep, standing in for the window's mean)
+    n_c = int(settings[0].cells)
+    n_bed = int(settings[0].raw.bed.num_particles)
+    step_bytes = sum(algorithmic_bytes(v[0], n_c, v[1], v[1] / max(args.check_every, 1) + 1, n_bed)
+                     for v in stats.values())
+    peak, peak_kind = load_peaks()
+    step_gbs = step_bytes / (elapsed / args.steps) / 1e9
     line = {"metric": METRIC, "value": particle_steps / elapsed, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ensemble generator)",
@@ -326,6 +335,11 @@ def run_c4(args, rank, world, local, dist):
                        "l2": "not flushed: 64 resident pours' particle and grid arrays exceed the 126 MB L2 many times over"
                              if args.instances >= 16 else "not flushed",
                        "parallelism": f"instances sharded over {world} GPU(s)"},
+            "roofline": {"bound": "hbm", "kernel": "whole batched substep", "achieved": step_gbs, "peak": peak,
+                         "unit": "GB/s", "frac": step_gbs / peak, "traffic": None,
+                         "algorithmic_bytes_per_step": step_bytes,
+                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s"},
             "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -99,6 +99,9 @@ struct Ctx {
     float* pf;        // FP32 pressure (persistent across substeps for warm start)
     float* divf;      // FP32 divergence
     float* fill;      // liquid fill fraction of each cell (written by classify)
+    // face-weight code of each cell (classify): -2 solid, -1 not fluid, 2 bed-coupled,
+    // else the liquid fill fraction; the per-colour sweep reads only this per face
+    float* fcode;
     float* plo;       // low word of the pressure (refinement mode: p = pf + plo)
     float* pd;        // pressure correction of the current refinement cycle
     float* gres;      // FP64 residual of the cycle, rounded to fp32

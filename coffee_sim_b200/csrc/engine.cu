@@ -113,6 +113,7 @@ int Engine::init() {
     if ((rc = alloc(pf_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(divf_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(fill_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(fcode_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(plo_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(pd_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(gres_, cells_ * sizeof(float)))) return rc;
@@ -161,6 +162,7 @@ int Engine::init() {
     ctx_.pf = (float*)pf_.ptr;
     ctx_.divf = (float*)divf_.ptr;
     ctx_.fill = (float*)fill_.ptr;
+    ctx_.fcode = (float*)fcode_.ptr;
     ctx_.plo = (float*)plo_.ptr;
     ctx_.pd = (float*)pd_.ptr;
     ctx_.gres = (float*)gres_.ptr;
@@ -203,7 +205,7 @@ int Engine::reset() {
     std::memset(&last, 0, sizeof(last));
     last.last_residual = last.initial_residual = -1.0;
     DeviceBuffer* zero[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_, &render_, &snap_, &delta_, &lanes_,
-                            &gvel_, &pf_, &divf_, &fill_, &plo_, &pd_, &gres_};
+                            &gvel_, &pf_, &divf_, &fill_, &fcode_, &plo_, &pd_, &gres_};
     int rc;
     for (DeviceBuffer* b : zero)
         if ((rc = check(cudaMemsetAsync(b->ptr, 0, b->bytes, stream_), "memset"))) return rc;

@@ -404,12 +404,14 @@ __global__ void k_classify(const Ctx* __restrict__ cp) {
             kl[i] = CELL_SOLID;
             div_store(c, i, 0.0f);
             c.fill[i] = 0.0f;
+            c.fcode[i] = -2.0f;
             continue;
         }
         if (mass <= occupancy_mass(u)) {
             kl[i] = CELL_AIR;
             div_store(c, i, 0.0f);
             c.fill[i] = 0.0f;
+            c.fcode[i] = -1.0f;
             continue;
         }
         int32_t kind;
@@ -427,6 +429,7 @@ __global__ void k_classify(const Ctx* __restrict__ cp) {
         }
         kl[i] = kind;
         c.fill[i] = liquid_fill(c, i, kind);
+        c.fcode[i] = kind == CELL_BED ? 2.0f : c.fill[i];
         if (u.warm && !u.fixed_point) {
             c.pf[i] = keep;
             c.plo[i] = keep_lo;
@@ -670,7 +673,7 @@ __global__ void k_refine_residual(const Ctx* __restrict__ cp) {
 __global__ void k_refine_sweep(const Ctx* __restrict__ cp, uint32_t parity) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
-    const int32_t* kl = lane(c, 3);
+    const float* fc = c.fcode;
     const uint32_t half = (u.gx + 1) / 2;
     const uint32_t n = half * u.gy * u.gz;
     CS_FOR(t, n) {
@@ -679,22 +682,25 @@ __global__ void k_refine_sweep(const Ctx* __restrict__ cp, uint32_t parity) {
         uint32_t ix = 2 * slot + ((iy + iz + parity) & 1u);
         if (ix >= u.gx) continue;
         uint32_t i = cidx(u, ix, iy, iz);
-        int32_t kind = kl[i];
-        if (!is_fluid(kind)) continue;
-        float sf = c.fill[i];
+        // one fill code per cell carries what face_weight needs (kind and fill): the
+        // same weights in the same face order as the kind/fill form
+        const float fi = fc[i];
+        if (fi < 0.0f) continue;  // not fluid
+        const bool bed = fi > 1.5f;
+        const float sf = bed ? 1.0f : fi;
         float nc = 0.0f, ds = 0.0f;
         const uint32_t sy = u.gx, sz = u.gx * u.gy;
-#define CS_DFACE(cond, off)                                     \
-    if (cond) {                                                 \
-        uint32_t ni = i + (off);                                \
-        int32_t nk = kl[ni];                                    \
-        if (!is_solid(nk)) {                                    \
-            float w = face_weight(kind, sf, nk, c.fill[ni]);    \
-            if (w > 0.0f) {                                     \
-                nc += w;                                        \
-                if (is_fluid(nk)) ds += w * c.pd[ni];           \
-            }                                                   \
-        }                                                       \
+#define CS_DFACE(cond, off)                                                   \
+    if (cond) {                                                               \
+        uint32_t ni = i + (off);                                              \
+        const float fj = fc[ni];                                              \
+        if (fj != -2.0f) {                                                    \
+            const float w = (bed || fj > 1.5f) ? 1.0f : (fj < 0.0f ? sf : wmin(sf, fj)); \
+            if (w > 0.0f) {                                                   \
+                nc += w;                                                      \
+                if (fj >= 0.0f) ds += w * c.pd[ni];                           \
+            }                                                                 \
+        }                                                                     \
     }
         CS_DFACE(ix > 0, (uint32_t)-1)
         CS_DFACE(ix + 1 < u.gx, 1u)

@@ -208,6 +208,35 @@ def spiral_spout(t, radius=0.015, hz=0.5, y=V60_TOP_Y + 0.015, U=V60_U):
     return (radius * math.cos(a) * U, y * U, radius * math.sin(a) * U)
 
 
+def c3_large(lib=None, grid=128, max_particles=2_700_000, bed_samples=24000, seed=2):
+    """Large V60 pour: 128^3 over the same 16 cm cube (dx = 1.25 mm) with the C2 cone,
+    bed and jet generators (seed 2); `populate_c2` gives ~2.2M samples at this grid.
+    The spout follows the spiral pour path: the caller moves it every substep with
+    set_spout_position(*spiral_spout(t)).  Bed samples scale with the cell count so
+    the bed keeps its sample density.  P2G runs cell-sorted with shared-memory tiles."""
+    s = c2_v60(lib, grid=grid, max_particles=max_particles, bed_samples=bed_samples, seed=seed)
+    s.raw.p2g_mode = _ffi.CS_P2G_SORTED_SHARED
+    return s
+
+
+def c5_scale(lib=None, grid=192, max_particles=8_600_000, bed_samples=81000, seed=4):
+    """Scale and reproducibility sweep: 192^3 (dx = 0.83 mm, ~7.6M samples from
+    `populate_c2`); two-layer bed split at its mid-height, porosity 0.45 above and 0.35
+    below with a 10x lower permeability below; the pour 1.2 cm off centre; int64
+    fixed-point P2G (bit-reproducible grid)."""
+    s = c2_v60(lib, grid=grid, max_particles=max_particles, bed_samples=bed_samples, seed=seed)
+    r = s.raw
+    U = float(r.sim_units_per_meter)
+    b = r.bed
+    b.layer_split_y = 0.5 * (b.bot_y + b.top_y)
+    b.initial_porosity = 0.45
+    b.lower_porosity_scale = 0.35 / 0.45
+    b.lower_permeability_scale = 0.1
+    r.spout.origin[0] = 0.012 * U
+    r.p2g_mode = _ffi.CS_P2G_INT64
+    return s
+
+
 def c4_ensemble(lib=None, n=64, seed=3, grid=64, max_particles=340000):
     """Batched ensemble: n independent V60 pours at 64^3 with seeded per-instance
     parameters — water fill height and carafe pool depth (sample counts spread over
