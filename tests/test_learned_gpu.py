@@ -63,3 +63,49 @@ def test_learned_mode_needs_weights(engine):
         sim.step_substep(scenes.C2_DT)
     with pytest.raises(_ffi.CsError):
         sim.set_learned_weights(np.zeros(10, dtype=np.float32))
+
+
+def test_trained_network_gain_over_previous_substep_start(engine):
+    """What the committed network gains on the V60 64^3 pour (substeps 6-25, replayed from
+    one snapshot for both warm starts): the guess is kept whenever its FP64 residual is
+    below 0.999x the previous-substep start's, which happens on a share of the substeps,
+    and every substep still reaches 1e-5.  The pair counts of both runs are printed (the
+    network does not shorten the solve materially at this size)."""
+    from pathlib import Path
+
+    wfile = Path(__file__).resolve().parent.parent / "coffee_sim_b200" / "weights" / "unet_v60_64.npy"
+    params = np.load(wfile)
+    runs = {}
+    base = None
+    for warm in (_ffi.CS_WARM_PREVIOUS, _ffi.CS_WARM_LEARNED):
+        s = scenes.c2_v60(engine, grid=64)
+        s.raw.rbgs_omega = 1.92
+        s.raw.check_every = 20
+        s.raw.max_sweeps = 4000
+        s.raw.device_emission = 1
+        s.raw.p2g_mode = _ffi.CS_P2G_SORTED_SHARED
+        s.raw.warm_start = warm
+        sim = MpmSim3D(s, engine)
+        if base is None:
+            scenes.populate_c2(sim)
+            for _ in range(5):
+                sim.step_substep(scenes.C2_DT)
+            base = sim.snapshot()
+        else:
+            sim.set_learned_weights(params)
+            sim.restore(base)
+        pairs, kept, r0 = [], 0, []
+        for _ in range(20):
+            sim.step_substep(scenes.C2_DT)
+            m = sim.latest_metrics()
+            assert m.last_residual <= 1e-5
+            pairs.append(int(m.last_sweeps))
+            kept += int(m.learned_used)
+            r0.append(float(m.initial_residual))
+        runs[warm] = (pairs, kept, r0)
+        sim.close()
+    plain, learned = runs[_ffi.CS_WARM_PREVIOUS], runs[_ffi.CS_WARM_LEARNED]
+    print(f"\nplain pairs {sum(plain[0]) / 20:.1f}, learned pairs {sum(learned[0]) / 20:.1f}, "
+          f"guess kept on {learned[1]}/20 substeps")
+    assert learned[1] > 0
+    assert plain[1] == 0
