@@ -354,13 +354,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--grid", type=int, default=64)
-    # defaults chosen by cs_autotune on this scene (omega 1.80-1.96 x checks every 5/10/20 pairs)
+    # omega chosen by cs_autotune on this scene (1.80-1.96); the check interval is the longest
+    # one: the solve predicts the pairs it still needs after each check (measured: 20 -> 330,
+    # 30 -> 340, 40 -> 345 M particle-steps/s)
     ap.add_argument("--omega", type=float, default=1.92)
     ap.add_argument("--max-sweeps", type=int, default=4000)
     ap.add_argument("--solve-sync", default="p2p", choices=["p2p", "cluster"],
                     help="colour separation inside the cluster solve: point-to-point mbarrier waits "
                          "or cluster barriers")
-    ap.add_argument("--check-every", type=int, default=20)
+    ap.add_argument("--check-every", type=int, default=40)
     ap.add_argument("--p2g", default="sorted", choices=["atomic", "sorted"],
                     help="P2G accumulation: per-particle global atomics or tile-sorted shared memory")
     ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")

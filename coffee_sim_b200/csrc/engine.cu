@@ -444,8 +444,9 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
         const uint32_t ce = s.check_every ? s.check_every : 10;
         r0 = refine_residual();
         r1 = r0;
+        uint32_t next = ce;
         while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
-            uint32_t k = std::min(ce, s.max_sweeps - sweeps);
+            uint32_t k = std::min(next, s.max_sweeps - sweeps);
             mark(CS_PHASE_SWEEPS);
             for (uint32_t j = 0; j < k; ++j) {
                 k_refine_sweep<<<dim3(blocks, 1), kThreads, 0, stream_>>>(dc, 0u);
@@ -456,7 +457,9 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
             mark(CS_PHASE_RESIDUAL);
             k_refine_accumulate<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc);
             count_launch();
+            const double r_before = r1;
             r1 = refine_residual();
+            next = sc_next_interval(r1, r_before, k, (double)s.residual_tol, ce);
         }
     } else if (s.solve_mode == CS_SOLVE_RESIDUAL) {
         uint32_t ce = s.check_every ? s.check_every : 1;
@@ -1569,7 +1572,7 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
         }
     }
     for (float omega : {1.80f, 1.85f, 1.88f, 1.90f, 1.92f, 1.94f, 1.96f})
-        for (uint32_t ce : {5u, 10u, 20u}) {
+        for (uint32_t ce : {10u, 20u, 30u, 40u}) {
             if (omega == res.omega && ce == res.check_every) continue;
             if ((rc = trial(omega, ce, res.p2g_mode, ms))) goto done;
             ++res.trials;

@@ -533,8 +533,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     double r0 = residual(slot);
     double r1 = r0;
     uint32_t pairs = 0, evals = 1;
+    uint32_t next = ce;  // pairs before the next check (same value on every CTA)
     while (!(r1 <= (double)tol) && pairs < max_pairs && !abort_all) {
-        uint32_t k = min(ce, max_pairs - pairs);
+        uint32_t k = min(next, max_pairs - pairs);
         for (uint32_t j = 0; j < k; ++j) {
             if (!p2p)
                 cluster.sync();
@@ -553,8 +554,10 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         accumulate();
         cluster.sync();
         slot ^= 1;
+        const double r_before = r1;
         r1 = residual(slot);
         ++evals;
+        next = sc_next_interval(r1, r_before, k, (double)tol, ce);
     }
     // publish every owned cell (the loop above published only halo-held ones)
     if (pairs > 0)

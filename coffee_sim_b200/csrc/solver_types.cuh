@@ -3,6 +3,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cmath>
 #include <vector_types.h>
 
 namespace cs {
@@ -51,6 +52,20 @@ struct ScInfo {
     uint32_t n_fluid, n_red, chunk, overflow;
     uint32_t red_before[SC_MAX_RANKS + 1];
 };
+// Pairs to run before the next residual check of the refinement loop.  The check that
+// just gave r_new (after k_last pairs that took the residual from r_old) predicts the
+// pairs still needed from the decay over that interval,
+// ceil(k_last * log(tol / r_new) / log(r_new / r_old)), and the next check comes then:
+// at least 2 pairs, at most ce (the configured check interval).  Without a measured
+// decay (first interval, or no decrease) the interval is ce.
+__host__ __device__ inline uint32_t sc_next_interval(double r_new, double r_old, uint32_t k_last, double tol,
+                                                     uint32_t ce) {
+    if (!(r_old > 0.0) || !(r_new > tol) || !(r_new < r_old) || k_last == 0) return ce;
+    const double n = ceil((double)k_last * log(tol / r_new) / log(r_new / r_old));
+    if (!(n < (double)ce)) return ce;
+    return n < 2.0 ? 2u : (uint32_t)n;
+}
+
 // Result of one solve.
 struct ScResult {
     uint32_t sweeps, evals, status, pad;

@@ -216,7 +216,9 @@ typedef struct CsSettings {
     uint32_t solve_mode;          /* CS_SOLVE_* */
     float residual_tol;           /* relative residual target (FP64 norm) */
     uint32_t max_sweeps;          /* cap on red+black pairs in residual mode */
-    uint32_t check_every;         /* pairs between residual evaluations */
+    uint32_t check_every;         /* pairs between residual evaluations; in FP32 residual mode
+                                     the longest interval: after each check the pairs still
+                                     needed are predicted from the decay rate (at least 2) */
     uint32_t warm_start;          /* CS_WARM_* */
     uint32_t p2g_mode;            /* CS_P2G_* */
     uint32_t sort_every;          /* reserved: the sorted P2G mode sorts every substep */
@@ -446,7 +448,7 @@ typedef struct CsTuneResult {
 } CsTuneResult;
 
 /* Time `substeps` substeps of length sub_dt from the current state for each candidate
- * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 5/10/20),
+ * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/30/40),
  * restoring the state after every trial; keep the fastest whose every substep reached
  * the residual target.  The simulation ends in the state it had at entry with the
  * chosen configuration applied.  Residual-mode solves only (CS_ERR_UNSUPPORTED else). */

@@ -37,6 +37,17 @@ namespace orc {
 
 static thread_local std::string g_err;
 static int g_precision_bits = 32;
+
+// Refinement-loop check schedule (engine extension, no reference counterpart): after a
+// residual check, the pairs still needed are predicted from the decay over the last
+// interval, ceil(k * log(tol / r_new) / log(r_new / r_old)); the next check comes after
+// that many pairs, at least 2 and at most ce; ce when no decay was measured.
+static uint32_t next_check_interval(double r_new, double r_old, uint32_t k, double tol, uint32_t ce) {
+    if (!(r_old > 0.0) || !(r_new > tol) || !(r_new < r_old) || k == 0) return ce;
+    const double n = std::ceil((double)k * std::log(tol / r_new) / std::log(r_new / r_old));
+    if (!(n < (double)ce)) return ce;
+    return n < 2.0 ? 2u : (uint32_t)n;
+}
 static int g_threads = 0;
 
 static int fail(int code, const std::string& msg) {
@@ -1793,15 +1804,18 @@ struct Sim : SimBase {
                 uint32_t ce = s.check_every ? s.check_every : 10;
                 r0 = refine_residual();
                 r1 = r0;
+                uint32_t next = ce;
                 while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
-                    uint32_t k = std::min(ce, s.max_sweeps - sweeps);
+                    uint32_t k = std::min(next, s.max_sweeps - sweeps);
                     for (uint32_t j = 0; j < k; ++j) {
                         refine_sweep(0);
                         refine_sweep(1);
                     }
                     sweeps += k;
                     refine_accumulate();
+                    const double r_before = r1;
                     r1 = refine_residual();
+                    next = next_check_interval(r1, r_before, k, (double)s.residual_tol, ce);
                 }
             } else if (s.solve_mode == CS_SOLVE_RESIDUAL) {
                 uint32_t ce = s.check_every ? s.check_every : 1;
