@@ -341,10 +341,56 @@ def run_c4(args, rank, world, local, dist):
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s"},
             "clocks": clocks.summary()}
+    ens.close()
+    if not args.no_learned:
+        line["learned"] = c4_learned_arm(args, lib, mine, settings, fills, local, dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ens.close()
     return 0
+
+
+def c4_learned_arm(args, lib, mine, settings, fills, local, dist):
+    """The same ensemble with the learned warm start: each instance's U-Net guess runs
+    between the batched classify and the batched solve, kept when its FP64 residual is
+    lower than the previous-substep start's."""
+    import numpy as np
+    from coffee_sim_b200 import _ffi, scenes
+    from coffee_sim_b200.sim import MpmEnsemble
+
+    wfile = ROOT / "coffee_sim_b200" / "weights" / "unet_v60_64.npy"
+    if not wfile.exists():
+        return {"unavailable": "coffee_sim_b200/weights/unet_v60_64.npy missing"}
+    for i in mine:
+        settings[i].raw.warm_start = _ffi.CS_WARM_LEARNED
+    ens = MpmEnsemble([settings[i] for i in mine], lib)
+    ens.set_learned_weights(np.load(wfile))
+    for k, i in enumerate(mine):
+        f = fills[i]
+        scenes.populate_c2(ens.member(k), fill_top=f["fill_top"], pool_depth=f["pool_depth"], seed=f["seed"])
+    dt = scenes.C2_DT
+    for _ in range(args.warmup):
+        ens.step_substep(dt)
+    ens.metrics(0)
+    if dist:
+        dist.barrier()
+    particle_steps, kept = 0, 0
+    ens.timer_start()
+    for _ in range(args.steps):
+        particle_steps += sum(ens.particle_count(k) for k in range(len(mine)))
+        ens.step_substep(dt)
+        kept += sum(int(ens.metrics(k).learned_used) for k in range(len(mine)))
+    elapsed = ens.timer_stop() * 1e-3
+    pairs = sum(ens.metrics(k).last_sweeps for k in range(len(mine))) / max(len(mine), 1)
+    ens.close()
+    if dist:
+        import torch
+        t = torch.tensor([elapsed, float(particle_steps), float(kept)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        elapsed, particle_steps, kept = float(t[0].item()), float(t[1].item()), float(t[2].item())
+    return {"value": particle_steps / elapsed, "ms_per_step": elapsed * 1e3 / args.steps,
+            "guess_kept_fraction": kept / (args.steps * args.instances), "pairs_mean_last_substep": pairs,
+            "timing": "CUDA events on the ensemble stream (the per-instance guesses synchronise the host)"}
 
 
 def main():

@@ -309,6 +309,7 @@ PROTOTYPES = {
     "cs_ensemble_get_counts": (I32, [P, U32, PU32, PU32]),
     "cs_ensemble_read_particles": (I32, [P, U32, U32, U32, PF]),
     "cs_ensemble_get_metrics": (I32, [P, U32, PM]),
+    "cs_ensemble_set_learned_weights": (I32, [P, PF, U64]),
     "cs_ensemble_timer_start": (I32, [P]),
     "cs_ensemble_timer_stop": (I32, [P, C.POINTER(C.c_float)]),
     "cs_profile_enable": (I32, [P, I32]),

@@ -1100,16 +1100,12 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
         t.use_graph = 0;
         int rc = validate_settings(&t);
         if (rc) return rc;
-        if (t.warm_start == CS_WARM_LEARNED) {
-            set_error("ensembles run the previous-substep warm start (no learned guess)");
-            return CS_ERR_UNSUPPORTED;
-        }
         const CsSettings& a = s[0];
         if (t.grid_dims[0] != a.grid_dims[0] || t.grid_dims[1] != a.grid_dims[1] || t.grid_dims[2] != a.grid_dims[2] ||
             t.p2g_mode != a.p2g_mode || t.solve_mode != a.solve_mode || t.pressure_storage != a.pressure_storage ||
             t.device != a.device || t.pressure_rbgs_pairs != a.pressure_rbgs_pairs || t.max_sweeps != a.max_sweeps ||
-            t.check_every != a.check_every || t.residual_tol != a.residual_tol) {
-            set_error("ensemble instances must share grid dims, device, P2G mode and solver settings");
+            t.check_every != a.check_every || t.residual_tol != a.residual_tol || t.warm_start != a.warm_start) {
+            set_error("ensemble instances must share grid dims, device, P2G mode, warm start and solver settings");
             return CS_ERR_INVALID_ARG;
         }
         Engine* e = new Engine(t);
@@ -1210,6 +1206,14 @@ int Ensemble::enqueue() {
     }
     k_grid_update<<<dim3(cb, n), T, 0, st>>>(dc, 1);
     k_classify<<<dim3(cb, n), T, 0, st>>>(dc);
+    if (s.warm_start == CS_WARM_LEARNED) {
+        // each instance's network guess (inputs from its residual, U-Net forward, FP64
+        // acceptance test) on its own stream, then the batched solve starts from it
+        if ((rc = sync())) return rc;
+        for (Engine* e : eng) {
+            if ((rc = e->upload_ctx()) || (rc = e->learned_before_solve()) || (rc = e->sync())) return rc;
+        }
+    }
     if (s.solve_mode == CS_SOLVE_RESIDUAL) {
         if ((rc = sc_launch_prep(dc, hsb.data(), (uint32_t)e0.sc_codes_, ranks, n, st, e0.sms_))) return rc;
         if ((rc = sc_launch_cluster(dc, ranks, n, s.residual_tol, s.max_sweeps, s.check_every, st,

@@ -58,6 +58,19 @@ int32_t cs_ensemble_step_frame(CsEnsemble* e, float dt) {
     return e->ens->step_frame(dt);
 }
 
+int32_t cs_ensemble_set_learned_weights(CsEnsemble* e, const float* params, uint64_t count) {
+    CS_ENS(e, 0u);
+    if (!params) {
+        cs::set_error("null weights");
+        return CS_ERR_INVALID_ARG;
+    }
+    int rc = e->ens->sync();
+    if (rc) return rc;
+    for (uint32_t i = 0; i < e->ens->size(); ++i)
+        if ((rc = e->ens->at(i).set_learned_weights(params, count))) return rc;
+    return CS_OK;
+}
+
 int32_t cs_ensemble_timer_start(CsEnsemble* e) {
     CS_ENS(e, 0u);
     return e->ens->timer_start();

@@ -469,6 +469,11 @@ class MpmEnsemble:
         self.lib.call("cs_ensemble_get_metrics", self._h, i, C.byref(m))
         return m
 
+    def set_learned_weights(self, params):
+        """One weight vector (coffee_sim_b200/unet.py layout) for every instance."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self.lib.call("cs_ensemble_set_learned_weights", self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size)
+
     def timer_start(self):
         self.lib.call("cs_ensemble_timer_start", self._h)
 

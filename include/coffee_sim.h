@@ -350,6 +350,9 @@ int32_t cs_ensemble_set_flow_override(CsEnsemble* ens, uint32_t i, float flow_ml
 int32_t cs_ensemble_get_counts(CsEnsemble* ens, uint32_t i, uint32_t* num_water, uint32_t* num_bed);
 int32_t cs_ensemble_read_particles(CsEnsemble* ens, uint32_t i, uint32_t first, uint32_t count, float* out);
 int32_t cs_ensemble_get_metrics(CsEnsemble* ens, uint32_t i, CsMetrics* out);
+/* The learned warm start's weights for every instance (CS_WARM_LEARNED ensembles: each
+ * instance's guess runs between the batched classify and the batched solve). */
+int32_t cs_ensemble_set_learned_weights(CsEnsemble* ens, const float* params, uint64_t count);
 int32_t cs_ensemble_timer_start(CsEnsemble* ens);           /* CUDA event on the ensemble's stream */
 int32_t cs_ensemble_timer_stop(CsEnsemble* ens, float* ms); /* device ms since the start; synchronises */
 

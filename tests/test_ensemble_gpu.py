@@ -80,3 +80,41 @@ def test_ensemble_device_timer(engine):
     ms = ens.timer_stop()
     assert 0.0 < ms < 5000.0
     ens.close()
+
+
+def test_ensemble_learned_warm_start_matches_single_pours(engine):
+    """CS_WARM_LEARNED in an ensemble: each instance's network guess and its acceptance
+    are those of the same pour stepped alone, bit for bit."""
+    from pathlib import Path
+
+    import numpy as np
+
+    params = np.load(Path(__file__).resolve().parent.parent / "coffee_sim_b200" / "weights" / "unet_v60_64.npy")
+    flows = [2.0, 5.0]
+    settings = []
+    for f in flows:
+        s = _v60(engine, f)
+        s.raw.warm_start = _ffi.CS_WARM_LEARNED
+        settings.append(s)
+    ens = MpmEnsemble(settings, engine)
+    ens.set_learned_weights(params)
+    singles = [MpmSim3D(s, engine) for s in settings]
+    for i, f in enumerate(flows):
+        U = float(settings[i].sim_units_per_meter)
+        scenes.populate_c2(ens.member(i), seed=i + 7)
+        scenes.populate_c2(singles[i], seed=i + 7)
+        ens.set_flow_override(i, f, 0.8 * U)
+        singles[i].set_flow_override(f, 0.8 * U)
+        singles[i].set_learned_weights(params)
+    used = 0
+    for k in range(4):
+        ens.step_substep(scenes.C2_DT)
+        for sim in singles:
+            sim.step_substep(scenes.C2_DT)
+        for i, sim in enumerate(singles):
+            me, ms = ens.metrics(i), sim.latest_metrics()
+            assert (me.learned_used, me.last_sweeps) == (ms.learned_used, ms.last_sweeps), (k, i)
+            assert me.last_residual <= 1e-5
+            assert mismatch(ens.read_particles(i), sim.read_particles()) == 0, (k, i)
+            used += me.learned_used
+    print(f"\nguess kept on {used} of 8 instance-substeps")
