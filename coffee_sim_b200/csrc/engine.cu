@@ -1347,7 +1347,7 @@ int Engine::learned_alloc() {
         if ((rc = alloc(l_act_[k], sizes[k] * 2))) return rc;
     if ((rc = alloc(l_feat_, v0 * 8 * 2))) return rc;
     if ((rc = alloc(l_out_, v0 * sizeof(float)))) return rc;
-    if ((rc = alloc(l_stats_, 2 * sizeof(double)))) return rc;
+    if ((rc = alloc(l_stats_, (2 * kLearnedStatBlocks + 3) * sizeof(double)))) return rc;  // zeroed
     if ((rc = alloc(l_scale_, sizeof(float)))) return rc;
     if ((rc = alloc(l_bak_hi_, v0 * sizeof(float)))) return rc;
     if ((rc = alloc(l_bak_lo_, v0 * sizeof(float)))) return rc;
@@ -1382,8 +1382,7 @@ int Engine::set_learned_weights(const float* params, uint64_t count) {
 
 int Engine::learned_features() {
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
-    cudaMemsetAsync(l_stats_.ptr, 0, 2 * sizeof(double), stream_);
-    k_learned_stats<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc, (double*)l_stats_.ptr);
+    k_learned_stats<<<dim3(kLearnedStatBlocks, 1), kThreads, 0, stream_>>>(dc, (double*)l_stats_.ptr);
     k_learned_features<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(
         dc, (const double*)l_stats_.ptr, (__nv_bfloat16*)l_feat_.ptr, (float*)l_scale_.ptr);
     count_launch(2);

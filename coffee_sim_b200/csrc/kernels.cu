@@ -1489,9 +1489,16 @@ __global__ void k_gather_results(const Ctx* __restrict__ cp, uint32_t n, ScResul
 // (k_refine_residual leaves r in gres): the network maps the residual to a pressure
 // correction, an approximate inverse of the pressure operator.
 // acc[0] += r^2, acc[1] += 1 over fluid cells
+// Per-block partial sums (sum r^2, fluid cells) of the residual over the fluid cells in
+// acc[2 * block], acc[2 * block + 1]; the last block to finish adds them in block order
+// into acc[2 * kLearnedStatBlocks], acc[2 * kLearnedStatBlocks + 1], so the totals do not
+// depend on the order blocks finish in.  The finish counter sits after them and is left
+// at zero.
+constexpr int kLearnedStatBlocks = 296;
 __global__ void k_learned_stats(const Ctx* __restrict__ cp, double* __restrict__ acc) {
     const Ctx& c = cp[blockIdx.y];
     const int32_t* kl = lane(c, 3);
+    __shared__ double part[2][32];
     double r2 = 0.0, n = 0.0;
     CS_FOR(i, c.u.cells) {
         if (!is_fluid(kl[i])) continue;
@@ -1503,9 +1510,43 @@ __global__ void k_learned_stats(const Ctx* __restrict__ cp, double* __restrict__
         r2 += __shfl_down_sync(0xffffffffu, r2, o);
         n += __shfl_down_sync(0xffffffffu, n, o);
     }
+    const int w = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&acc[0], r2);
-        atomicAdd(&acc[1], n);
+        part[0][w] = r2;
+        part[1][w] = n;
+    }
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            a += part[0][k];
+            b += part[1][k];
+        }
+        acc[2 * blockIdx.x] = a;
+        acc[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        unsigned int* done = reinterpret_cast<unsigned int*>(acc + 2 * kLearnedStatBlocks + 2);
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+        if (last) *done = 0u;
+    }
+    __syncthreads();
+    if (last && threadIdx.x < 32) {
+        // lane l adds partials l, l + 32, ... in order, then a fixed shuffle tree
+        __threadfence();
+        double ta = 0.0, tb = 0.0;
+        for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
+            ta += __ldcg(acc + 2 * k);
+            tb += __ldcg(acc + 2 * k + 1);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ta += __shfl_down_sync(0xffffffffu, ta, o);
+            tb += __shfl_down_sync(0xffffffffu, tb, o);
+        }
+        if (threadIdx.x == 0) {
+            acc[2 * kLearnedStatBlocks] = ta;
+            acc[2 * kLearnedStatBlocks + 1] = tb;
+        }
     }
 }
 // 8 channels per cell: r / s, fill, fluid, bed, solid, 0, 0, 0 with s the RMS of the
@@ -1514,7 +1555,8 @@ __global__ void k_learned_features(const Ctx* __restrict__ cp, const double* __r
                                    __nv_bfloat16* __restrict__ feat, float* __restrict__ scale) {
     const Ctx& c = cp[blockIdx.y];
     const int32_t* kl = lane(c, 3);
-    const double ms = acc[1] > 0.0 ? acc[0] / acc[1] : 0.0;
+    const double* tot = acc + 2 * kLearnedStatBlocks;
+    const double ms = tot[1] > 0.0 ? tot[0] / tot[1] : 0.0;
     const float sc = ms > 0.0 ? (float)sqrt(ms) : 1.0f;
     const float inv = 1.0f / sc;
     if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = sc;

@@ -16,6 +16,8 @@
 //
 // Every mbarrier wait is bounded; on a timeout the kernel raises a flag in `err`,
 // waits (bounded) for its own MMAs, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -434,6 +436,209 @@ __global__ void __launch_bounds__(THREADS) k_conv_fwd(ConvArgs a) {
     if (warp == 0) umma::tmem_dealloc(tmem, ncols);
 }
 
+// Halo-tiled convolution: a CTA computes an 8 (x) x 16 (y) x 1 (z) block of output voxels
+// (M = 128).  Its input block with a one-voxel halo, 10 x 18 x 3 voxels, is loaded once
+// by TMA (one tiled box per 8-channel block, zeros outside the grid) into shared memory
+// as [channel block][z][y][x][8 channels] (16 bytes per voxel and block; the channel
+// count is padded to a multiple of 16 with zero blocks).  In that layout the A operand of tap (dx, dy, dz) is the same block shifted:
+// a core matrix is 8 consecutive x voxels (128 contiguous bytes), consecutive 8-row
+// groups (y) are 10 * 16 = 160 bytes apart (SBO) and consecutive channel blocks one
+// block plane apart (LBO), so every tap's MMAs read the one copy through a descriptor
+// with a shifted start address.  The weights of each tap (N x Cpad) stream through a
+// ring of HB_SLOTS shared-memory slots with cp.async; a slot is refilled once the MMAs
+// that read it have completed (tcgen05.commit to the slot's mbarrier).
+constexpr int HX = 10, HY = 18, HZ = 3, HVOX = HX * HY * HZ, HB_PLANE = HVOX * 16, HB_SLOTS = 3;
+// channel-block planes start 128-byte aligned (a tiled TMA box lands at a 128-byte
+// aligned shared address): 8640 bytes of data in an 8704-byte stride
+constexpr int HB_PSTRIDE = (HB_PLANE + 127) / 128 * 128;
+
+// shared memory of the halo kernel: input block plus a ring of HB_SLOTS taps' weights
+// (`all_taps` false) or every tap's weights at once
+static size_t halo_smem(int cin_pad16, int n, bool all_taps) {
+    return (size_t)(cin_pad16 / 8) * HB_PSTRIDE + (size_t)(all_taps ? 27 : HB_SLOTS) * n * cin_pad16 * 2;
+}
+
+// all_taps: every tap's weights are resident (one copy group, all MMAs issued back to
+// back under one commit); otherwise they stream through the ring.
+template <bool ALL>
+__global__ void __launch_bounds__(THREADS) k_conv_halo(ConvArgs a, const __grid_constant__ CUtensorMap xmap) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bars[HB_SLOTS];
+    __shared__ uint64_t halo_bar;
+    __shared__ uint32_t tmem_base;
+    const int N = a.cout_pad;
+    const int cpad = (a.cin + 15) & ~15;  // channels as the MMAs see them (K = 16 per MMA)
+    const int ncb = cpad >> 3;            // 8-channel blocks, even
+    const int b_bytes = N * cpad * 2;     // one tap's weights
+    unsigned char* halo = sm;
+    unsigned char* bring = sm + (size_t)ncb * HB_PSTRIDE;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+    if (warp == 0) {
+        umma::tmem_alloc(&tmem_base, ncols);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int b = 0; b < HB_SLOTS; ++b) umma::mbar_init(&bars[b], 1);
+        umma::mbar_init(&halo_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+
+    const int tx = (a.g.gx + 7) >> 3, ty = (a.g.gy + 15) >> 4;
+    const int bx = blockIdx.x % tx, by = (blockIdx.x / tx) % ty, bz = blockIdx.x / (tx * ty);
+    const int x0 = bx * 8, y0 = by * 16, z0 = bz;
+    const uint32_t idesc = umma::idesc_bf16_f32((uint32_t)N);
+
+    // input block with halo: one TMA box (8 channels x 10 x 18 x 3 voxels, zeros outside
+    // the grid) per 8-channel block, landing as [z][y][x][8 channels]; channel blocks past
+    // cin (padding to a multiple of 16) are zeroed here
+    const int ncb_in = a.cin >> 3;
+    for (int e = ncb_in * HVOX + tid; e < ncb * HVOX; e += THREADS)
+        *reinterpret_cast<uint4*>(halo + (size_t)(e / HVOX) * HB_PSTRIDE + (e % HVOX) * 16) =
+            make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) {
+        const uint32_t bar = umma::smem_addr(&halo_bar);
+        asm volatile(
+            "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+            "r"((uint32_t)(ncb_in * HB_PLANE))
+            : "memory");
+        for (int cb = 0; cb < ncb_in; ++cb)
+            asm volatile(
+                "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+                "%4, %5}], [%6];" ::"r"(umma::smem_addr(halo + (size_t)cb * HB_PSTRIDE)),
+                "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(cb * 8), "r"(x0 - 1), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
+                : "memory");
+    }
+    // tap t's weights into its slot (ring slot t % HB_SLOTS, or slot t with every tap
+    // resident), as N x cpad K-major core matrices
+    auto slot_of = [&](int t) { return ALL ? t : t % HB_SLOTS; };
+    auto load_b = [&](int t) {
+        unsigned char* B = bring + (size_t)slot_of(t) * b_bytes;
+        for (int i = tid; i < N * ncb; i += THREADS) {
+            const int row = i / ncb, cb = i - row * ncb;
+            const bool ok = cb * 8 < a.cin;
+            const __nv_bfloat16* src = a.w + (size_t)row * a.kpad + (size_t)t * a.cin + cb * 8;
+            cp_async16(B + core_off(row, cb, N), ok ? src : a.w, ok);
+        }
+    };
+    bool ok = true;
+    int issued = -1;  // last tap whose MMAs were issued
+    // weights in flight first (every tap, or the first HB_SLOTS), then the input block
+    if (ALL) {
+        for (int t = 0; t < 27; ++t) load_b(t);
+        cp_async_commit();
+    } else {
+        for (int t = 0; t < HB_SLOTS; ++t) {
+            load_b(t);
+            cp_async_commit();
+        }
+    }
+    const bool halo_ok = umma::mbar_wait(&halo_bar, 0u, WAIT_LIMIT);
+    if (ALL) {
+        cp_async_wait<0>();
+        umma::fence_proxy_async();
+        ok = __syncthreads_and(halo_ok ? 1 : 0) != 0;
+    }
+    if (ALL && ok) {
+        if (tid == 0) {
+            umma::fence_after_sync();
+            for (int t = 0; t < 27; ++t) {
+                const int dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+                const uint32_t a_base = umma::smem_addr(halo) + (uint32_t)(((dz * HY + dy) * HX + dx) * 16);
+                const uint32_t b_base = umma::smem_addr(bring + (size_t)t * b_bytes);
+                for (int j = 0; j < ncb / 2; ++j) {
+                    const uint64_t da = umma::smem_desc(a_base + (uint32_t)(2 * j * HB_PSTRIDE), HB_PSTRIDE, HX * 16);
+                    const uint64_t db =
+                        umma::smem_desc(b_base + (uint32_t)(2 * j * (N / 8) * 128), (N / 8) * 128, 128);
+                    umma::mma_bf16(tmem, da, db, idesc, (t > 0 || j > 0) ? 1u : 0u);
+                }
+            }
+            umma::commit(&bars[0]);
+        }
+        issued = 26;
+    }
+    if (!ALL) ok = __syncthreads_and(halo_ok ? 1 : 0) != 0;
+    for (int t = 0; t < (ALL || !ok ? 0 : 27); ++t) {
+        // groups committed after tap t's weights: HB_SLOTS - 1 at t = 0, then one refill
+        // per iteration keeps it at one
+        if (t == 0)
+            cp_async_wait<HB_SLOTS - 1>();
+        else
+            cp_async_wait<1>();
+        umma::fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after_sync();
+            const int dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+            const uint32_t a_base = umma::smem_addr(halo) + (uint32_t)(((dz * HY + dy) * HX + dx) * 16);
+            const uint32_t b_base = umma::smem_addr(bring + (size_t)(t % HB_SLOTS) * b_bytes);
+            for (int j = 0; j < ncb / 2; ++j) {
+                const uint64_t da = umma::smem_desc(a_base + (uint32_t)(2 * j * HB_PSTRIDE), HB_PSTRIDE, HX * 16);
+                const uint64_t db = umma::smem_desc(b_base + (uint32_t)(2 * j * (N / 8) * 128), (N / 8) * 128, 128);
+                umma::mma_bf16(tmem, da, db, idesc, (t > 0 || j > 0) ? 1u : 0u);
+            }
+            umma::commit(&bars[t % HB_SLOTS]);
+        }
+        issued = t;
+        // refill the slot of tap t - 1 (its MMAs were issued one iteration ago) with tap
+        // t - 1 + HB_SLOTS; every iteration commits one group, empty past the last tap
+        const int prev = t - 1, next = prev + HB_SLOTS;
+        if (prev >= 0 && next < 27) {
+            const bool w = umma::mbar_wait(&bars[prev % HB_SLOTS], (uint32_t)((prev / HB_SLOTS) & 1), WAIT_LIMIT);
+            if (!__syncthreads_and(w ? 1 : 0)) {
+                ok = false;
+                break;
+            }
+            load_b(next);
+        }
+        if (t > 0) cp_async_commit();
+    }
+    cp_async_wait<0>();
+    // the last tap's commit covers every MMA issued before it
+    if (issued >= 0) {
+        const int sl = ALL ? 0 : issued % HB_SLOTS;
+        const uint32_t ph = ALL ? 0u : (uint32_t)((issued / HB_SLOTS) & 1);
+        const bool done = umma::mbar_wait(&bars[sl], ph, WAIT_LIMIT);
+        ok = __syncthreads_and((done && ok) ? 1 : 0) != 0;
+    }
+    if (!ok && tid == 0) atomicOr(a.err, 1u);
+    umma::fence_after_sync();
+    if (ok && issued == 26) {
+        const int row = warp * 32 + (tid & 31);  // M row: x = row % 8, y = row / 8
+        const int xo = x0 + (row & 7), yo = y0 + (row >> 3);
+        const bool inside = xo < a.g.gx && yo < a.g.gy;
+        const int vox = (z0 * a.g.gy + yo) * a.g.gx + xo;
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < N; c0 += 8) {
+            float v[8];
+            umma::tmem_ld8(lane_addr + (uint32_t)c0, v);
+            umma::tmem_wait_ld();
+            if (!inside) continue;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                float r = v[q] + (a.bias ? a.bias[c0 + q] : 0.0f);
+                v[q] = a.relu ? fmaxf(r, 0.0f) : r;
+            }
+            if (a.y) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(v[q]);
+                *reinterpret_cast<uint4*>(a.y + (size_t)vox * N + c0) = *reinterpret_cast<const uint4*>(h);
+            }
+            if (a.y32)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) a.y32[(size_t)vox * N + c0 + q] = v[q];
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, ncols);
+}
+
 static size_t conv_smem(int n) { return (size_t)2 * (BM + n) * BKC * 16; }
 
 template <int MODE>
@@ -507,18 +712,22 @@ __global__ void k_pool_bwd(const float* __restrict__ dy, float* __restrict__ dx,
 // out[v] = [low[parent(v)] (c1 channels), skip[v] (c2 channels)] on the fine grid
 __global__ void k_upcat_fwd(const __nv_bfloat16* __restrict__ low, const __nv_bfloat16* __restrict__ skip,
                             __nv_bfloat16* __restrict__ out, Grid3 f, int c1, int c2) {
-    const int c = c1 + c2;
-    const long long n = (long long)f.voxels() * c;
+    // one 16-byte chunk (8 channels) per thread; c1, c2 multiples of 8
+    const int q1 = c1 >> 3, q = (c1 + c2) >> 3;
+    const long long n = (long long)f.voxels() * q;
+    const int hx = f.gx / 2, hy = f.gy / 2;
     NN_FOR(i, n) {
-        const int ch = (int)(i % c);
-        const long long v = i / c;
-        if (ch < c1) {
+        const int ch = (int)(i % q);
+        const long long v = i / q;
+        uint4 val;
+        if (ch < q1) {
             const int x = (int)(v % f.gx), y = (int)((v / f.gx) % f.gy), z = (int)(v / ((long long)f.gx * f.gy));
-            const long long pv = ((long long)(z / 2) * (f.gy / 2) + y / 2) * (f.gx / 2) + x / 2;
-            out[i] = low[pv * c1 + ch];
+            const long long pv = ((long long)(z / 2) * hy + y / 2) * hx + x / 2;
+            val = reinterpret_cast<const uint4*>(low)[pv * q1 + ch];
         } else {
-            out[i] = skip[v * c2 + (ch - c1)];
+            val = reinterpret_cast<const uint4*>(skip)[v * (q - q1) + (ch - q1)];
         }
+        reinterpret_cast<uint4*>(out)[i] = val;
     }
 }
 // gradient of upcat: dlow[p] += sum over its 8 children, dskip[v] += its part (f32)
@@ -613,6 +822,31 @@ using namespace cs::nn;
 
 static cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
 
+// Tensor map of a channels-last bf16 activation [gz][gy][gx][cin] for the halo kernel's
+// TMA loads: dims (cin, gx, gy, gz), box 8 channels x 10 x 18 x 3 voxels, no swizzle,
+// zeros outside the tensor.  False when the driver entry point or the encoding fails
+// (the caller then uses the copy-gather kernel).
+static bool input_tensor_map(CUtensorMap* map, const void* x, int gx, int gy, int gz, int cin) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            encode = nullptr;
+        cudaGetLastError();
+    }
+    if (!encode || ((uintptr_t)x & 15u) || cin % 8) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)gx, (cuuint64_t)gy, (cuuint64_t)gz};
+    const cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)gx * cin * 2, (cuuint64_t)gx * gy * cin * 2};
+    const cuuint32_t box[4] = {8, HX, HY, HZ};
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estride,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 extern "C" {
 
 // Y = relu?(conv3x3x3(X, W) + b).  x: bf16 [vox][cin_pad]; w: bf16 [cout_pad][kpad] from
@@ -638,14 +872,29 @@ int32_t cs_nn_conv3d(const void* x, const void* w, const float* bias, void* y, f
     a.kpad = ((27 * cin_pad + 63) / 64) * 64;
     a.relu = relu;
     a.err = err;
-    const int tiles = (a.g.voxels() + BM - 1) / BM;
+    // dynamic shared memory cap of the halo kernel (its static part, ~1 KB, adds to it)
+    constexpr size_t kHaloSmemCap = 220 * 1024;
     static bool attr = false;
-    const size_t smem = (size_t)NBUF * (BM + cout_pad) * BKC * 16;
     if (!attr) {
         cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_conv_halo<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHaloSmemCap);
+        cudaFuncSetAttribute(k_conv_halo<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHaloSmemCap);
+        cudaGetLastError();  // a refused attribute shows up as a launch error below
         attr = true;
     }
-    k_conv_fwd<<<dim3(tiles, 1), THREADS, smem, as_stream(stream)>>>(a);
+    const int cp16 = (cin_pad + 15) & ~15;
+    const int tiles = ((gx + 7) / 8) * ((gy + 15) / 16) * gz;
+    CUtensorMap xmap;
+    const bool tma = input_tensor_map(&xmap, x, gx, gy, gz, cin_pad);
+    if (tma && halo_smem(cp16, cout_pad, true) <= kHaloSmemCap) {
+        k_conv_halo<true><<<dim3(tiles, 1), THREADS, halo_smem(cp16, cout_pad, true), as_stream(stream)>>>(a, xmap);
+    } else if (tma && halo_smem(cp16, cout_pad, false) <= kHaloSmemCap) {
+        k_conv_halo<false><<<dim3(tiles, 1), THREADS, halo_smem(cp16, cout_pad, false), as_stream(stream)>>>(a, xmap);
+    } else {
+        const int tiles = (a.g.voxels() + BM - 1) / BM;
+        const size_t smem = (size_t)NBUF * (BM + cout_pad) * BKC * 16;
+        k_conv_fwd<<<dim3(tiles, 1), THREADS, smem, as_stream(stream)>>>(a);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         cs::set_error(std::string("conv launch: ") + cudaGetErrorString(e));
@@ -722,14 +971,14 @@ int32_t cs_nn_pool(const void* x, void* y, const float* dy, float* dx, int32_t g
 int32_t cs_nn_upcat(const void* low, const void* skip, void* out, const float* dout, float* dlow, float* dskip,
                     int32_t gx, int32_t gy, int32_t gz, int32_t c1, int32_t c2, int32_t backward, void* stream) {
     const Grid3 f{gx, gy, gz};
-    if (gx % 2 || gy % 2 || gz % 2) {
-        cs::set_error("cs_nn_upcat: grid dims must be even");
+    if (gx % 2 || gy % 2 || gz % 2 || c1 % 8 || c2 % 8) {
+        cs::set_error("cs_nn_upcat: grid dims must be even and channel counts multiples of 8");
         return CS_ERR_INVALID_ARG;
     }
     const long long n = (long long)f.voxels() * (c1 + c2);
     if (!backward)
-        k_upcat_fwd<<<nn_blocks(n), 256, 0, as_stream(stream)>>>((const __nv_bfloat16*)low, (const __nv_bfloat16*)skip,
-                                                                  (__nv_bfloat16*)out, f, c1, c2);
+        k_upcat_fwd<<<nn_blocks(n / 8), 256, 0, as_stream(stream)>>>(
+            (const __nv_bfloat16*)low, (const __nv_bfloat16*)skip, (__nv_bfloat16*)out, f, c1, c2);
     else
         k_upcat_bwd<<<nn_blocks(n), 256, 0, as_stream(stream)>>>(dout, dlow, dskip, f, c1, c2);
     return nn_check("cs_nn_upcat");
