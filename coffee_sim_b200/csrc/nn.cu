@@ -529,7 +529,16 @@ __global__ void __launch_bounds__(THREADS) k_conv_halo(ConvArgs a, const __grid_
     int issued = -1;  // last tap whose MMAs were issued
     // weights in flight first (every tap, or the first HB_SLOTS), then the input block
     if (ALL) {
-        for (int t = 0; t < 27; ++t) load_b(t);
+        // each thread owns fixed (row, channel block) pairs and copies them for every tap:
+        // tap t's copy is t * b_bytes further in shared memory and t * cin further in
+        // the packed weights
+        for (int i = tid; i < N * ncb; i += THREADS) {
+            const int row = i / ncb, cb = i - row * ncb;
+            const bool ok = cb * 8 < a.cin;
+            unsigned char* dst = bring + core_off(row, cb, N);
+            const __nv_bfloat16* src = a.w + (size_t)row * a.kpad + cb * 8;
+            for (int t = 0; t < 27; ++t, dst += b_bytes, src += a.cin) cp_async16(dst, ok ? src : a.w, ok);
+        }
         cp_async_commit();
     } else {
         for (int t = 0; t < HB_SLOTS; ++t) {
