@@ -492,6 +492,10 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
 int Engine::substep(float sub_dt, uint32_t P) {
     int rc;
     const bool graph = settings.use_graph && P == 0xffffffffu;
+    if (graph && l_capture_) {
+        set_error("training-sample capture runs with use_graph = 0");
+        return CS_ERR_UNSUPPORTED;
+    }
     if (!graph) mark(CS_PHASE_EMIT);
     if ((rc = emit(sub_dt))) return rc;
     fill_params(ctx_.u, sub_dt);
@@ -569,6 +573,7 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
         if (capture) {
             const CsSettings& s = settings;
             if (s.solve_mode == CS_SOLVE_RESIDUAL) {
+                if (s.warm_start == CS_WARM_LEARNED && (rc = learned_enqueue(false))) return rc;
                 if ((rc = sc_launch_prep(dc, &sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_))) return rc;
                 count_launch(kScPrepLaunches);
                 if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
@@ -586,8 +591,9 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
                 }
             }
         } else {
-            if ((rc = learned_before_solve())) return rc;
+            if ((rc = learned_enqueue(true))) return rc;
             if ((rc = solve_pressure(sweeps, r0, r1))) return rc;
+            if ((rc = learned_collect())) return rc;
             if ((rc = learned_after_solve())) return rc;
         }
         have_prev_p = true;
@@ -620,6 +626,7 @@ Engine::GraphKey Engine::graph_key() const {
     k.solve_mode = s.solve_mode;
     k.pressure_storage = s.pressure_storage;
     k.rbgs_kernel = s.rbgs_kernel;
+    k.warm_start = s.warm_start;
     k.rbgs_pairs = s.pressure_rbgs_pairs;
     k.residual_tol = s.residual_tol;
     k.num_bed = num_bed;
@@ -694,7 +701,7 @@ int Engine::collect() {
                   "(16 x 4095 fluid cells); run this scene with use_graph = 0");
         return CS_ERR_CAPACITY;
     }
-    return CS_OK;
+    return learned_collect();
 }
 
 // mod.rs:264-270
@@ -1208,10 +1215,15 @@ int Ensemble::enqueue() {
     k_classify<<<dim3(cb, n), T, 0, st>>>(dc);
     if (s.warm_start == CS_WARM_LEARNED) {
         // each instance's network guess (inputs from its residual, U-Net forward, FP64
-        // acceptance test) on its own stream, then the batched solve starts from it
-        if ((rc = sync())) return rc;
+        // acceptance test on the device), enqueued on the ensemble stream ahead of the
+        // batched solve
         for (Engine* e : eng) {
-            if ((rc = e->upload_ctx()) || (rc = e->learned_before_solve()) || (rc = e->sync())) return rc;
+            cudaStream_t own = e->stream_;
+            e->stream_ = st;
+            rc = e->upload_ctx();
+            if (!rc) rc = e->learned_enqueue(false);
+            e->stream_ = own;
+            if (rc) return rc;
         }
     }
     if (s.solve_mode == CS_SOLVE_RESIDUAL) {
@@ -1227,6 +1239,7 @@ int Ensemble::enqueue() {
         for (uint32_t i = 0; i < n; ++i) {
             Engine& e = *eng[i];
             const ScResult& r = results[i];
+            if ((rc = e.learned_collect())) return rc;
             if (r.status != 1) {
                 // this instance's fluid does not fit the cluster: solve it alone with
                 // per-colour launches on its own stream
@@ -1354,6 +1367,8 @@ int Engine::learned_alloc() {
     if ((rc = alloc(l_target_, v0 * sizeof(float)))) return rc;
     if ((rc = alloc(l_mask_, v0 * sizeof(float)))) return rc;
     if ((rc = alloc(l_err_, sizeof(uint32_t)))) return rc;
+    if ((rc = alloc(l_rprev_, 2 * sizeof(double)))) return rc;
+    if ((rc = alloc(l_keep_, sizeof(uint32_t)))) return rc;
     cudaMemsetAsync(l_err_.ptr, 0, sizeof(uint32_t), stream_);
     l_ready_ = true;
     return CS_OK;
@@ -1428,10 +1443,12 @@ int Engine::learned_forward() {
 
 // Before the solve: the FP64 residual r of the previous-substep pressure p and the
 // network inputs built from it; with the learned warm start, p + (network output) * s
-// replaces p when that has the smaller FP64 residual.
-int Engine::learned_before_solve() {
+// replaces p when that has the smaller FP64 residual (below 0.999x).  Every step is
+// enqueued on the stream and the acceptance test runs on the device, so the sequence can
+// be captured in a graph; learned_collect reads the outcome once the solve has
+// synchronised.  `marks`: record the profiling phase.
+int Engine::learned_enqueue(bool marks) {
     const bool learned = settings.warm_start == CS_WARM_LEARNED;
-    last.learned_used = 0;
     if (!learned && !l_capture_) return CS_OK;
     if (learned && !l_weights_) {
         set_error("CS_WARM_LEARNED needs weights (cs_set_learned_weights)");
@@ -1439,38 +1456,48 @@ int Engine::learned_before_solve() {
     }
     int rc;
     if ((rc = learned_alloc())) return rc;
-    const double r_prev = refine_residual();  // leaves the residual in gres for the inputs
-    mark(CS_PHASE_LEARNED);
-    if ((rc = learned_features())) return rc;
     const Ctx* dc = (const Ctx*)d_ctx_.ptr;
-    k_learned_save<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc, (float*)l_bak_hi_.ptr,
-                                                                          (float*)l_bak_lo_.ptr);
+    const int cb = launch_cells_blocks();
+    if (marks) mark(CS_PHASE_LEARNED);
+    // residual of the previous pressure (left in gres for the inputs), its norms kept
+    cudaMemsetAsync(resid_.ptr, 0, 2 * sizeof(double), stream_);
+    k_refine_residual<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc);
+    cudaMemcpyAsync(l_rprev_.ptr, resid_.ptr, 2 * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
     count_launch();
-    if (!learned) return CS_OK;
-    mark(CS_PHASE_LEARNED);
+    prof_.residual_evals += 1;
+    if ((rc = learned_features())) return rc;
+    k_learned_save<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, (float*)l_bak_hi_.ptr, (float*)l_bak_lo_.ptr);
+    count_launch();
+    if (!learned) return check(cudaGetLastError(), "learned inputs");
     if ((rc = learned_forward())) return rc;
-    k_learned_apply<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(
-        dc, (const float*)l_out_.ptr, (const float*)l_scale_.ptr, (const float*)l_bak_hi_.ptr,
-        (const float*)l_bak_lo_.ptr);
-    count_launch();
-    const double r_guess = refine_residual();
-    mark(CS_PHASE_LEARNED);
-    uint32_t err = 0;
-    cudaMemcpy(&err, l_err_.ptr, sizeof(err), cudaMemcpyDeviceToHost);
+    k_learned_apply<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, (const float*)l_out_.ptr, (const float*)l_scale_.ptr,
+                                                        (const float*)l_bak_hi_.ptr, (const float*)l_bak_lo_.ptr);
+    cudaMemsetAsync(resid_.ptr, 0, 2 * sizeof(double), stream_);
+    k_refine_residual<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc);
+    k_learned_decide<<<1, 1, 0, stream_>>>((const double*)l_rprev_.ptr, (const double*)resid_.ptr,
+                                           (uint32_t*)l_keep_.ptr);
+    k_learned_restore<<<dim3(cb, 1), kThreads, 0, stream_>>>(dc, (const float*)l_bak_hi_.ptr,
+                                                            (const float*)l_bak_lo_.ptr, (const uint32_t*)l_keep_.ptr);
+    count_launch(4);
+    prof_.residual_evals += 1;
+    return check(cudaGetLastError(), "learned warm start");
+}
+
+int Engine::learned_collect() {
+    last.learned_used = 0;
+    if (settings.warm_start != CS_WARM_LEARNED || !l_ready_) return CS_OK;
+    uint32_t keep = 0, err = 0;
+    int rc;
+    if ((rc = check(cudaMemcpy(&keep, l_keep_.ptr, sizeof(keep), cudaMemcpyDeviceToHost), "learned outcome")) ||
+        (rc = check(cudaMemcpy(&err, l_err_.ptr, sizeof(err), cudaMemcpyDeviceToHost), "learned error flag")))
+        return rc;
+    prof_.d2h_bytes += 2 * sizeof(uint32_t);
     if (err) {
         set_error("a tensor-core convolution of the learned warm start timed out");
         return CS_ERR_TIMEOUT;
     }
-    // a clear improvement only: the FP64 norms are reduced with atomics, so equal
-    // pressures can differ in their last bits
-    if (r_guess < 0.999 * r_prev) {
-        last.learned_used = 1;
-    } else {
-        k_learned_restore<<<dim3(launch_cells_blocks(), 1), kThreads, 0, stream_>>>(dc, (const float*)l_bak_hi_.ptr,
-                                                                                    (const float*)l_bak_lo_.ptr);
-        count_launch();
-    }
-    return check(cudaGetLastError(), "learned warm start");
+    last.learned_used = keep;
+    return CS_OK;
 }
 
 int Engine::learned_after_solve() {
@@ -1736,8 +1763,8 @@ static int validate(const CsSettings* s) {
         return CS_ERR_INVALID_ARG;
     }
     if (s->warm_start == CS_WARM_LEARNED &&
-        (s->use_graph || s->pressure_storage != CS_PRESSURE_FP32 || s->solve_mode != CS_SOLVE_RESIDUAL)) {
-        set_error("the learned warm start needs the residual-mode FP32 solve and no graph capture");
+        (s->pressure_storage != CS_PRESSURE_FP32 || s->solve_mode != CS_SOLVE_RESIDUAL)) {
+        set_error("the learned warm start needs the residual-mode FP32 solve");
         return CS_ERR_INVALID_ARG;
     }
     if (s->warm_start != CS_WARM_NONE && s->pressure_storage == CS_PRESSURE_FIXED_POINT) {

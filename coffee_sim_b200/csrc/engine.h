@@ -88,9 +88,11 @@ private:
     int learned_alloc();
     int learned_features();
     int learned_forward();
-    int learned_before_solve();
+    int learned_enqueue(bool marks);  // residual, inputs, guess and its device-side acceptance
+    int learned_collect();            // outcome of the last guess, after the solve synchronised
     int learned_after_solve();
-    DeviceBuffer l_params_, l_feat_, l_out_, l_stats_, l_scale_, l_bak_hi_, l_bak_lo_, l_target_, l_mask_, l_err_;
+    DeviceBuffer l_params_, l_feat_, l_out_, l_stats_, l_scale_, l_bak_hi_, l_bak_lo_, l_target_, l_mask_, l_err_,
+        l_rprev_, l_keep_;
     DeviceBuffer l_wf_[9], l_act_[13];
     bool l_weights_ = false, l_capture_ = false, l_have_sample_ = false, l_ready_ = false;
     // graph mode: the substep's device work captured once and replayed
@@ -98,7 +100,7 @@ private:
     int substep_graph(float sub_dt);
     int collect();          // read the solve totals of replayed substeps
     struct GraphKey {
-        uint32_t p2g_mode, check_every, max_sweeps, solve_mode, pressure_storage, rbgs_kernel, rbgs_pairs;
+        uint32_t p2g_mode, check_every, max_sweeps, solve_mode, pressure_storage, rbgs_kernel, rbgs_pairs, warm_start;
         float residual_tol;
         uint32_t num_bed, max_particles;
         bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }

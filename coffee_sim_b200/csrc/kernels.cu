@@ -1603,9 +1603,22 @@ __global__ void k_learned_apply(const Ctx* __restrict__ cp, const float* __restr
         c.plo[i] = (float)(p - (double)hi);
     }
 }
+// The acceptance test of the learned guess, on the device: prev and guess hold the FP64
+// sums (r^2, b^2) of the residual before and after the guess; the guess is kept when its
+// relative residual is below 0.999x the previous one (the FP64 sums are reduced with
+// atomics, so equal pressures can differ in their last bits).
+__global__ void k_learned_decide(const double* __restrict__ prev, const double* __restrict__ guess,
+                                 uint32_t* __restrict__ keep) {
+    const double rp = prev[1] > 0.0 ? sqrt(prev[0]) / sqrt(prev[1]) : 0.0;
+    const double rg = guess[1] > 0.0 ? sqrt(guess[0]) / sqrt(guess[1]) : 0.0;
+    keep[0] = rg < 0.999 * rp ? 1u : 0u;
+}
+// previous-substep pressure back in place, unless the guess was kept (keep may be null:
+// always restore)
 __global__ void k_learned_restore(const Ctx* __restrict__ cp, const float* __restrict__ bak_hi,
-                                  const float* __restrict__ bak_lo) {
+                                  const float* __restrict__ bak_lo, const uint32_t* __restrict__ keep) {
     const Ctx& c = cp[blockIdx.y];
+    if (keep && keep[0]) return;
     CS_FOR(i, c.u.cells) {
         c.pf[i] = bak_hi[i];
         c.plo[i] = bak_lo[i];

@@ -109,3 +109,50 @@ def test_trained_network_gain_over_previous_substep_start(engine):
           f"guess kept on {learned[1]}/20 substeps")
     assert learned[1] > 0
     assert plain[1] == 0
+
+
+def test_learned_graph_replay_matches_direct_launches(engine):
+    """The learned substep (residual, inputs, U-Net forward, device-side acceptance test,
+    solve) replayed as a CUDA graph gives the direct-launch results bit for bit, with the
+    same accepted guesses (V60 64^3 from substep 6, where the guess is kept on some
+    substeps and rejected on others)."""
+    from pathlib import Path
+
+    params = np.load(Path(__file__).resolve().parent.parent / "coffee_sim_b200" / "weights" / "unet_v60_64.npy")
+
+    def v60(warm):
+        s = scenes.c2_v60(engine, grid=64)
+        s.raw.rbgs_omega = 1.92
+        s.raw.check_every = 40
+        s.raw.device_emission = 1
+        s.raw.p2g_mode = _ffi.CS_P2G_SORTED_SHARED
+        s.raw.warm_start = warm
+        return MpmSim3D(s, engine)
+
+    base = v60(_ffi.CS_WARM_PREVIOUS)
+    scenes.populate_c2(base)
+    for _ in range(5):
+        base.step_substep(scenes.C2_DT)
+    blob = base.snapshot()
+    base.close()
+    sims = []
+    for graph in (False, True):
+        sim = v60(_ffi.CS_WARM_LEARNED)
+        sim.set_learned_weights(params)
+        sim.restore(blob)
+        if graph:
+            sim.set_graph_mode(True)
+        sims.append(sim)
+    kept = []
+    for k in range(8):
+        for sim in sims:
+            sim.step_substep(scenes.C2_DT)
+        a, b = sims[0].latest_metrics(), sims[1].latest_metrics()
+        assert (a.learned_used, a.last_sweeps) == (b.learned_used, b.last_sweeps), k
+        assert b.last_residual <= 1e-5
+        kept.append(int(a.learned_used))
+        assert mismatch(sims[0].read_pressure(), sims[1].read_pressure()) == 0, k
+        n = sims[0].particle_count()
+        assert mismatch(sims[0].read_particles(0, n), sims[1].read_particles(0, n)) == 0, k
+    print(f"\nguess kept on substeps {kept}")
+    assert 0 < sum(kept) < len(kept)
