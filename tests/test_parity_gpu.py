@@ -147,7 +147,7 @@ def test_center_pour_frames_bit_exact(engine, oracle):
 
 
 def test_c1_water_block_200_steps(engine, oracle):
-    """the 32^3 water block, 200 substeps, compared every 50."""
+    """The C1 water block (32^3, 16.8k samples, 40 pairs): 200 substeps, compared every 50."""
     se = scenes.c1_water_block(engine)
     e, o = MpmSim3D(se, engine), MpmSim3D(se, oracle)
     assert scenes.populate_c1(e) == scenes.populate_c1(o)
