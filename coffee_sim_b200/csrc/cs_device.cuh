@@ -102,6 +102,10 @@ struct Ctx {
     // face-weight code of each cell (classify): -2 solid, -1 not fluid, 2 bed-coupled,
     // else the liquid fill fraction; the per-colour sweep reads only this per face
     float* fcode;
+    // bed-matrix velocity of each cell (mean velocity of the solid bed samples looked up in
+    // its 3x3x3 neighbourhood, shader.rs:380-407), computed once per substep for classify
+    // and project
+    float4* bedv;
     float* plo;       // low word of the pressure (refinement mode: p = pf + plo)
     float* pd;        // pressure correction of the current refinement cycle
     float* gres;      // FP64 residual of the cycle, rounded to fp32

@@ -114,6 +114,7 @@ int Engine::init() {
     if ((rc = alloc(divf_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(fill_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(fcode_, cells_ * sizeof(float)))) return rc;
+    if ((rc = alloc(bedv_, cells_ * f4))) return rc;
     if ((rc = alloc(plo_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(pd_, cells_ * sizeof(float)))) return rc;
     if ((rc = alloc(gres_, cells_ * sizeof(float)))) return rc;
@@ -163,6 +164,7 @@ int Engine::init() {
     ctx_.divf = (float*)divf_.ptr;
     ctx_.fill = (float*)fill_.ptr;
     ctx_.fcode = (float*)fcode_.ptr;
+    ctx_.bedv = (float4*)bedv_.ptr;
     ctx_.plo = (float*)plo_.ptr;
     ctx_.pd = (float*)pd_.ptr;
     ctx_.gres = (float*)gres_.ptr;
@@ -568,7 +570,10 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     }
     ph(CS_PHASE_GRID);
     if (P > 4) CS_LAUNCH(k_grid_update<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 5 ? 1 : 0));
-    if (P > 6) CS_LAUNCH(k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc));
+    if (P > 6) {
+        if (any_bed) CS_LAUNCH(k_bed_velocity<<<dim3(cb, 1), T, 0, stream_>>>(dc));
+        CS_LAUNCH(k_classify<<<dim3(cb, 1), T, 0, stream_>>>(dc));
+    }
     if (P > 7) {
         if (capture) {
             const CsSettings& s = settings;
@@ -1212,6 +1217,7 @@ int Ensemble::enqueue() {
         }
     }
     k_grid_update<<<dim3(cb, n), T, 0, st>>>(dc, 1);
+    if (max_bed) k_bed_velocity<<<dim3(cb, n), T, 0, st>>>(dc);
     k_classify<<<dim3(cb, n), T, 0, st>>>(dc);
     if (s.warm_start == CS_WARM_LEARNED) {
         // each instance's network guess (inputs from its residual, U-Net forward, FP64

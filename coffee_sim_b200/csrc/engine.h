@@ -77,8 +77,8 @@ private:
     int sms_ = 148;
     std::vector<DeviceBuffer*> owned_;
     DeviceBuffer d_ctx_, pos_, vel_, c0_, c1_, c2_, bedA_, bedB_, render_, snap_, delta_;
-    DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, fcode_, plo_, pd_, gres_, lookup_, sdf_, cls_, metrics_,
-        resid_;
+    DeviceBuffer lanes_, lanes64_, gvel_, pf_, divf_, fill_, fcode_, bedv_, plo_, pd_, gres_, lookup_, sdf_, cls_,
+        metrics_, resid_;
     DeviceBuffer staging_;  // AoS upload/readback staging
     // sorted P2G
     DeviceBuffer p2g_key_, p2g_rank_, p2g_sorted_, tile_count_, tile_start_, tile_temp_;

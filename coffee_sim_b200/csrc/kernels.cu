@@ -346,6 +346,26 @@ __global__ void k_boundary(const Ctx* __restrict__ cp) {
     }
 }
 
+// bed_matrix_velocity_cell (shader.rs:380-407) of every cell, once per substep: the bed
+// samples' velocities and the cell lookup do not change between bed_lookup_scatter and
+// bed_dynamics, so classify (six neighbours of each bed-coupled cell) and project (each
+// bed-coupled cell) read these instead of rescanning 27 cells per call.
+__global__ void k_bed_velocity(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    if (!c.bedv) return;
+    CS_FOR(i, u.cells) {
+        uint32_t ix, iy, iz;
+        decompose(u, i, ix, iy, iz);
+        const f3 v = bed_matrix_velocity(c, (int)ix, (int)iy, (int)iz);
+        c.bedv[i] = make_float4(v.x, v.y, v.z, 0.0f);
+    }
+}
+__device__ __forceinline__ f3 bed_velocity_at(const Ctx& c, int x, int y, int z) {
+    if (!in_grid(c.u, x, y, z)) return mk(0.0f, 0.0f, 0.0f);
+    return xyz(c.bedv[cidx(c.u, (uint32_t)x, (uint32_t)y, (uint32_t)z)]);
+}
+
 // ---------------- classify_cells (shader.rs:1181-1367) ----------------
 __device__ float volume_target(const Params& u, float rest, float cur) {
     float cv = u.dx * u.dx * u.dx;
@@ -389,6 +409,8 @@ __device__ __forceinline__ bool open_nb(const Ctx& c, f3 cc, uint32_t x, uint32_
 __global__ void k_classify(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
+    // the metrics' max |div| and fluid-cell count, per thread, then one atomic per warp
+    uint32_t max_fd = 0u, n_fluid = 0u;
     CS_FOR(i, u.cells) {
         float mass = c.gvel[i].w;
         float keep = (!u.fixed_point && u.warm) ? c.pf[i] : 0.0f;
@@ -453,17 +475,24 @@ __global__ void k_classify(const Ctx* __restrict__ cp) {
                 float poro = wclamp(compacted_porosity(c, (uint32_t)b), 0.08f, 1.0f);
                 float sfrac = 1.0f - poro;
                 int x = ix, y = iy, z = iz;
-                float bxm = bed_velocity_cell(c, x - 1, y, z).x, bxp = bed_velocity_cell(c, x + 1, y, z).x;
-                float bym = bed_velocity_cell(c, x, y - 1, z).y, byp = bed_velocity_cell(c, x, y + 1, z).y;
-                float bzm = bed_velocity_cell(c, x, y, z - 1).z, bzp = bed_velocity_cell(c, x, y, z + 1).z;
+                float bxm = bed_velocity_at(c, x - 1, y, z).x, bxp = bed_velocity_at(c, x + 1, y, z).x;
+                float bym = bed_velocity_at(c, x, y - 1, z).y, byp = bed_velocity_at(c, x, y + 1, z).y;
+                float bzm = bed_velocity_at(c, x, y, z - 1).z, bzp = bed_velocity_at(c, x, y, z + 1).z;
                 float sdiv = 0.5f * u.inv_dx * (((bxp - bxm) + (byp - bym)) + (bzp - bzm));
                 target = (pt - sfrac * sdiv) / poro;
             }
         }
         div_store(c, i, div - target);
         uint32_t fd = to_u32(wclamp(fabsf(div) * METRICS_DIV_FP_SCALE, 0.0f, 2147483648.0f));
-        atomicMax(&c.metrics[M_MAX_DIV], fd);
-        atomicAdd(&c.metrics[M_FLUID], 1u);
+        max_fd = max_fd > fd ? max_fd : fd;
+        n_fluid += 1u;
+    }
+    // every lane leaves the loop (blocks are whole warps and nothing returns early)
+    max_fd = __reduce_max_sync(0xffffffffu, max_fd);
+    n_fluid = __reduce_add_sync(0xffffffffu, n_fluid);
+    if ((threadIdx.x & 31u) == 0u && n_fluid) {
+        atomicMax(&c.metrics[M_MAX_DIV], max_fd);
+        atomicAdd(&c.metrics[M_FLUID], n_fluid);
     }
 }
 
@@ -787,7 +816,7 @@ __global__ void k_project(const Ctx* __restrict__ cp, int stages) {
                     float perm = compacted_permeability(c, (uint32_t)b);
                     float rate = u.nu_m2s / perm;
                     float damp = 1.0f / (1.0f + wmax(rate * u.dt, 0.0f));
-                    f3 bv = bed_matrix_velocity(c, ix, iy, iz);
+                    f3 bv = xyz(c.bedv[i]);
                     f3 before = v;
                     v = bv + (v - bv) * damp;
                     f3 wi = g.w * (v - before);
