@@ -425,7 +425,7 @@ def main():
     ap.add_argument("--solve-sync", default="p2p", choices=["p2p", "cluster"],
                     help="colour separation inside the cluster solve: point-to-point mbarrier waits "
                          "or cluster barriers")
-    ap.add_argument("--check-every", type=int, default=40)
+    ap.add_argument("--check-every", type=int, default=60)
     ap.add_argument("--p2g", default="sorted", choices=["atomic", "sorted"],
                     help="P2G accumulation: per-particle global atomics or tile-sorted shared memory")
     ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")

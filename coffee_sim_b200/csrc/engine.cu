@@ -1608,7 +1608,7 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
         }
     }
     for (float omega : {1.80f, 1.85f, 1.88f, 1.90f, 1.92f, 1.94f, 1.96f})
-        for (uint32_t ce : {10u, 20u, 30u, 40u}) {
+        for (uint32_t ce : {10u, 20u, 40u, 60u, 80u}) {
             if (omega == res.omega && ce == res.check_every) continue;
             if ((rc = trial(omega, ce, res.p2g_mode, ms))) goto done;
             ++res.trials;

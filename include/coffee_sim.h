@@ -451,7 +451,7 @@ typedef struct CsTuneResult {
 } CsTuneResult;
 
 /* Time `substeps` substeps of length sub_dt from the current state for each candidate
- * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/30/40),
+ * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/40/60/80),
  * restoring the state after every trial; keep the fastest whose every substep reached
  * the residual target.  The simulation ends in the state it had at entry with the
  * chosen configuration applied.  Residual-mode solves only (CS_ERR_UNSUPPORTED else). */
