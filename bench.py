@@ -324,8 +324,9 @@ def run_c4(args, rank, world, local, dist):
             particle_steps += sum(ens.particle_count(k) for k in range(len(mine)))
             ens.step_substep(dt)
         elapsed = ens.timer_stop() * 1e-3  # CUDA events on the ensemble's stream
-    pairs = [ens.metrics(k).last_sweeps for k in range(len(mine))]
-    stats = shard.gather_statistics({i: [float(ens.particle_count(k)), float(pairs[k])] for k, i in enumerate(mine)})
+    ms = [ens.metrics(k) for k in range(len(mine))]
+    stats = shard.gather_statistics({i: [float(ens.particle_count(k)), float(ms[k].last_sweeps),
+                                         float(ms[k].residual_checks)] for k, i in enumerate(mine)})
     if dist:
         import torch
         t = torch.tensor([elapsed, float(particle_steps)], dtype=torch.float64, device="cuda")
@@ -335,11 +336,11 @@ def run_c4(args, rank, world, local, dist):
     counts = [v[0] for v in stats.values()]
     # step roofline: compulsory bytes of every instance's substep (the bench's formula,
     # dense 64^3 grid per instance) over the step time, against the measured HBM peak
-    # (pairs: each instance's last substep, standing in for the window's mean)
+    # (pairs and FP64 residual checks: each instance's last substep, standing in for the
+    # window's mean)
     n_c = int(settings[0].cells)
     n_bed = int(settings[0].raw.bed.num_particles)
-    step_bytes = sum(algorithmic_bytes(v[0], n_c, v[1], v[1] / max(args.check_every, 1) + 1, n_bed)
-                     for v in stats.values())
+    step_bytes = sum(algorithmic_bytes(v[0], n_c, v[1], v[2], n_bed) for v in stats.values())
     peak, peak_kind = load_peaks()
     step_gbs = step_bytes / (elapsed / args.steps) / 1e9
     line = {"metric": METRIC, "value": particle_steps / elapsed, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -347,7 +348,8 @@ def run_c4(args, rank, world, local, dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ensemble generator)",
             "config": {"workload": f"c4_ensemble_{args.instances}x64cube", "instances": args.instances,
                        "particles_min": min(counts), "particles_max": max(counts), "particles_total": sum(counts),
-                       "pairs_mean": sum(v[1] for v in stats.values()) / len(stats), "residual_tol": 1e-5,
+                       "pairs_mean": sum(v[1] for v in stats.values()) / len(stats),
+                       "residual_checks_mean": sum(v[2] for v in stats.values()) / len(stats), "residual_tol": 1e-5,
                        "omega": args.omega, "timing": "CUDA events on the ensemble stream, max over ranks",
                        "l2": "not flushed: 64 resident pours' particle and grid arrays exceed the 126 MB L2 many times over"
                              if args.instances >= 16 else "not flushed",

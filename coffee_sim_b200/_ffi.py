@@ -204,7 +204,7 @@ class CsMetrics(C.Structure):
         ("nan_flag", C.c_uint32),
         ("timeout_flag", C.c_uint32),
         ("learned_used", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("residual_checks", C.c_uint32),
         ("solve_ms", C.c_double),
     ]
 

@@ -435,12 +435,16 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
     };
     sweeps = 0;
     r0 = r1 = -1.0;
+    const uint64_t evals0 = prof_.residual_evals;
     const bool refine = s.solve_mode == CS_SOLVE_RESIDUAL && s.pressure_storage != CS_PRESSURE_FIXED_POINT;
     if (refine && s.rbgs_kernel != 1 && sc_ranks_ > 0) {
         bool done = false;
         int rc = solve_cluster(sweeps, r0, r1, done);
         if (rc) return rc;
-        if (done) return CS_OK;
+        if (done) {
+            last.residual_checks = (uint32_t)(prof_.residual_evals - evals0);
+            return CS_OK;
+        }
     }
     if (refine) {
         const uint32_t ce = s.check_every ? s.check_every : 10;
@@ -484,6 +488,7 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
         sweeps = s.pressure_rbgs_pairs;
         if (s.check_every) r1 = residual();
     }
+    last.residual_checks = (uint32_t)(prof_.residual_evals - evals0);
     return check(cudaGetLastError(), "rbgs");
 }
 
@@ -506,6 +511,7 @@ int Engine::substep(float sub_dt, uint32_t P) {
     if (graph) return substep_graph(sub_dt);
     uint32_t sweeps = 0;
     double r0 = -1.0, r1 = -1.0;
+    last.residual_checks = 0;
     if ((rc = enqueue(P, false, sweeps, r0, r1))) return rc;
     total_time += sub_dt;
     last.last_sweeps = sweeps;
@@ -698,6 +704,7 @@ int Engine::collect() {
     seen_ = t;
     if (t.runs) {
         last.last_sweeps = t.last.sweeps;
+        last.residual_checks = t.last.evals;
         last.last_residual = t.last.r1;
         last.initial_residual = t.last.r0;
     }
@@ -1265,6 +1272,7 @@ int Ensemble::enqueue() {
                 continue;
             }
             e.last.last_sweeps = r.sweeps;
+            e.last.residual_checks = r.evals;
             e.last.initial_residual = r.r0;
             e.last.last_residual = r.r1;
             e.prof_.sweeps += r.sweeps;
@@ -1280,6 +1288,7 @@ int Ensemble::enqueue() {
         }
         for (Engine* e : eng) {
             e->last.last_sweeps = s.pressure_rbgs_pairs;
+            e->last.residual_checks = 0;
             e->prof_.sweeps += s.pressure_rbgs_pairs;
         }
     }

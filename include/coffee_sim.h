@@ -246,7 +246,7 @@ typedef struct CsMetrics {
     uint32_t nan_flag;             /* a non-finite particle or grid value was seen */
     uint32_t timeout_flag;         /* a bounded device wait gave up */
     uint32_t learned_used;         /* 1 if the learned guess was kept in the last solve */
-    uint32_t reserved;
+    uint32_t residual_checks;      /* FP64 residual evaluations in the last solve, the warm start's included */
     double solve_ms;               /* device time of the last pressure solve, if timed */
 } CsMetrics;
 

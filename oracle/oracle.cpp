@@ -1791,7 +1791,7 @@ struct Sim : SimBase {
             return go && cond;
         };
         double r0 = -1.0, r1 = -1.0;
-        uint32_t sweeps = 0;
+        uint32_t sweeps = 0, checks = 0;
         if (run(true)) k_metrics_clear();
         if (run(true)) k_bed_lookup_clear();
         if (run(u.num_bed > 0)) k_bed_lookup_scatter();
@@ -1804,6 +1804,7 @@ struct Sim : SimBase {
                 uint32_t ce = s.check_every ? s.check_every : 10;
                 r0 = refine_residual();
                 r1 = r0;
+                checks = 1;
                 uint32_t next = ce;
                 while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
                     uint32_t k = std::min(next, s.max_sweeps - sweeps);
@@ -1815,12 +1816,14 @@ struct Sim : SimBase {
                     refine_accumulate();
                     const double r_before = r1;
                     r1 = refine_residual();
+                    ++checks;
                     next = next_check_interval(r1, r_before, k, (double)s.residual_tol, ce);
                 }
             } else if (s.solve_mode == CS_SOLVE_RESIDUAL) {
                 uint32_t ce = s.check_every ? s.check_every : 1;
                 r0 = residual();
                 r1 = r0;
+                checks = 1;
                 if (!(r0 <= (double)s.residual_tol)) {
                     while (sweeps < s.max_sweeps) {
                         k_rbgs(0);
@@ -1828,6 +1831,7 @@ struct Sim : SimBase {
                         ++sweeps;
                         if (sweeps % ce == 0 || sweeps == s.max_sweeps) {
                             r1 = residual();
+                            ++checks;
                             if (r1 <= (double)s.residual_tol) break;
                         }
                     }
@@ -1838,7 +1842,10 @@ struct Sim : SimBase {
                     k_rbgs(1);
                 }
                 sweeps = s.pressure_rbgs_pairs;
-                if (s.check_every) r1 = residual();
+                if (s.check_every) {
+                    r1 = residual();
+                    checks = 1;
+                }
             }
             have_prev_p = true;
         }
@@ -1862,6 +1869,7 @@ struct Sim : SimBase {
         metrics_out.pressure_clamp_fires = metrics[M_P_CLAMP];
         metrics_out.mass_overflow_fires = metrics[M_OVERFLOW];
         metrics_out.last_sweeps = sweeps;
+        metrics_out.residual_checks = checks;
         metrics_out.last_residual = r1;
         metrics_out.initial_residual = r0;
         return CS_OK;

@@ -36,6 +36,7 @@ def test_ensemble_matches_independent_pours(engine):
             assert ens.counts(i) == (sim.num_water, sim.num_bed)
             me, ms = ens.metrics(i), sim.latest_metrics()
             assert me.last_sweeps == ms.last_sweeps, (k, i)
+            assert me.residual_checks == ms.residual_checks >= 2, (k, i)
             assert me.last_residual <= 1e-5
             assert mismatch(ens.read_particles(i), sim.read_particles()) == 0, (k, i)
     # the pours differ (different flows emit different amounts)

@@ -48,6 +48,11 @@ def test_oracle_int64_steps_close_to_i32(oracle):
     assert b.particle_count() == n
     assert relerr(b.read_particles(0, n)[:, :3], a.read_particles(0, n)[:, :3]) < 1e-5
     assert b.latest_metrics().last_residual <= 1e-5
+    ce = a.current_settings().check_every
+    for sim in (a, b):
+        m = sim.latest_metrics()
+        # the warm start's check plus one per cycle of 2..check_every pairs
+        assert -(-m.last_sweeps // ce) <= m.residual_checks - 1 <= -(-m.last_sweeps // 2), (m.last_sweeps, m.residual_checks)
 
 
 def test_lanes64_only_in_int64_mode(oracle):

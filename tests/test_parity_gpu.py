@@ -173,6 +173,7 @@ def test_v60_refinement_solve_matches_oracle(engine, oracle, grid, omega):
         o.step_substep(scenes.C2_DT)
         me, mo = e.latest_metrics(), o.latest_metrics()
         assert me.last_sweeps == mo.last_sweeps, (k, me.last_sweeps, mo.last_sweeps)
+        assert me.residual_checks == mo.residual_checks >= 2, (k, me.residual_checks, mo.residual_checks)
         assert abs(me.last_residual - mo.last_residual) <= 1e-9 * max(mo.last_residual, 1e-30) + 1e-15
         if omega != 1.0:
             assert me.last_residual <= 1e-5
@@ -201,6 +202,7 @@ def test_cluster_solver_matches_per_colour_launches(engine, cluster_kernel):
         # the cluster path ran: one launch in the sweep phase of each substep
         assert sims[1].profile_read().phase_launches[4] == k + 1
         assert ma.last_sweeps == mb.last_sweeps
+        assert ma.residual_checks == mb.residual_checks >= 2
         assert mb.last_residual <= 1e-5
         assert mismatch(sims[0].read_pressure(), sims[1].read_pressure()) == 0
         assert mismatch(sims[0].read_particles(), sims[1].read_particles()) == 0
