@@ -245,8 +245,12 @@ __device__ __forceinline__ bool valid_bed_solid(const Ctx& c, int32_t b) {
 __device__ __forceinline__ f3 bed_matrix_velocity(const Ctx& c, int x, int y, int z) {
     f3 sum = mk(0.0f, 0.0f, 0.0f);
     float ws = 0.0f;
+    // unrolled so the 27 lookups (and then the sample reads) are in flight together
+#pragma unroll
     for (int di = -1; di <= 1; ++di)
+#pragma unroll
         for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
             for (int dk = -1; dk <= 1; ++dk) {
                 int cx = x + di, cy = y + dj, cz = z + dk;
                 if (!in_grid(c.u, cx, cy, cz)) continue;
@@ -292,24 +296,25 @@ __device__ __forceinline__ void bed_impulse_add(const Ctx& c, uint32_t b, f3 imp
     atomicAdd(&delta_lane(c, 3)[b], to_i32(wclamp(imp.z, -cap, cap) * FP_SCALE));
 }
 __device__ __forceinline__ void bed_impulse_neighborhood(const Ctx& c, int x, int y, int z, f3 imp) {
+    // the 27 lookups and validity reads are issued together and kept for the second
+    // pass (nothing this pass writes changes them)
+    int32_t ids[27];
     float n = 0.0f;
-    for (int di = -1; di <= 1; ++di)
-        for (int dj = -1; dj <= 1; ++dj)
-            for (int dk = -1; dk <= 1; ++dk) {
-                int cx = x + di, cy = y + dj, cz = z + dk;
-                if (!in_grid(c.u, cx, cy, cz)) continue;
-                if (valid_bed_solid(c, c.lookup[cidx(c.u, cx, cy, cz)])) n += 1.0f;
-            }
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int cx = x + q / 9 - 1, cy = y + (q / 3) % 3 - 1, cz = z + q % 3 - 1;
+        ids[q] = in_grid(c.u, cx, cy, cz) ? c.lookup[cidx(c.u, cx, cy, cz)] : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        if (!valid_bed_solid(c, ids[q])) ids[q] = -1;
+        if (ids[q] >= 0) n += 1.0f;
+    }
     if (n <= 0.0f) return;
     f3 share = imp / n;
-    for (int di = -1; di <= 1; ++di)
-        for (int dj = -1; dj <= 1; ++dj)
-            for (int dk = -1; dk <= 1; ++dk) {
-                int cx = x + di, cy = y + dj, cz = z + dk;
-                if (!in_grid(c.u, cx, cy, cz)) continue;
-                int32_t b = c.lookup[cidx(c.u, cx, cy, cz)];
-                if (valid_bed_solid(c, b)) bed_impulse_add(c, (uint32_t)b, share);
-            }
+#pragma unroll
+    for (int q = 0; q < 27; ++q)
+        if (ids[q] >= 0) bed_impulse_add(c, (uint32_t)ids[q], share);
 }
 __device__ __forceinline__ void world_to_cell(const Params& u, f3 p, int& x, int& y, int& z) {
     x = (int)floorf((p.x - u.ox) * u.inv_dx);
