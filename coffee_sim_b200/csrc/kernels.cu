@@ -413,7 +413,8 @@ __device__ __forceinline__ bool open_nb(const Ctx& c, f3 cc, uint32_t x, uint32_
     return sample_sdf(c, cc + mk(ox, oy, oz)) >= 0.0f;
 }
 
-__global__ void k_classify(const Ctx* __restrict__ cp) {
+// 64 registers (4 blocks of 256 per SM) instead of 80: the kernel is latency bound
+__global__ void __launch_bounds__(256, 4) k_classify(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     // the metrics' max |div| and fluid-cell count, per thread, then one atomic per warp
