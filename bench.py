@@ -265,7 +265,17 @@ def cpu_baseline(args, steps, warm):
         sim.step_substep(scenes.C2_DT)
         sweeps += sim.latest_metrics().last_sweeps
     dt = time.perf_counter() - t
-    return {"value": particle_steps / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+    # the next two substeps on one thread (integer grid atomics make the result the same)
+    lib.lib.oracle_set_threads(1)
+    ps1, t1 = 0, time.perf_counter()
+    for _ in range(2):
+        ps1 += sim.particle_count()
+        sim.step_substep(scenes.C2_DT)
+    dt1 = time.perf_counter() - t1
+    lib.lib.oracle_set_threads(nthreads)
+    single = {"value": ps1 / dt1, "unit": UNIT, "cores": 1,
+              "sample": f"substeps {warm + steps + 1}..{warm + steps + 2} of the same pour"}
+    return {"value": particle_steps / dt, "unit": UNIT, "cores": nthreads, "kind": "port", "single_thread": single,
             "sample": f"substeps {warm + 1}..{warm + steps} of the V60 64^3 pour ({n0} samples at the start; "
                       f"{sweeps / max(steps, 1):.0f} red-black pairs per substep), the first {steps} of the GPU "
                       f"arm's timed substeps; oracle/ C++ restatement, OpenMP on {nthreads} threads, -O3",
@@ -283,7 +293,7 @@ def run_reference(args, rank):
             "config": {"workload": WORKLOAD, "particles": res["particles"], "omega": args.omega,
                        "residual_tol": 1e-5},
             "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"], "kind": "port",
-                             "sample": res["sample"]},
+                             "sample": res["sample"], "single_thread": res["single_thread"]},
             "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
