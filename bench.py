@@ -430,8 +430,9 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--grid", type=int, default=64)
     # omega chosen by cs_autotune on this scene (1.80-1.96); the check interval is the longest
-    # one: the solve predicts the pairs it still needs after each check (measured: 20 -> 330,
-    # 30 -> 340, 40 -> 351, 60 -> 358, 80 -> 358 M particle-steps/s; 80 adds pairs)
+    # one: the solve predicts the pairs it still needs after each check (measured in M
+    # particle-steps/s: 20 -> 330, 30 -> 340, 40 -> 345; with the later kernels 40 -> 351,
+    # 60 -> 358, 80 -> 358 with more pairs)
     ap.add_argument("--omega", type=float, default=1.92)
     ap.add_argument("--max-sweeps", type=int, default=4000)
     ap.add_argument("--solve-sync", default="p2p", choices=["p2p", "cluster"],
