@@ -155,6 +155,7 @@ def build_scene(lib, args, device=0, learned=False, populate=True):
     s.raw.rbgs_omega = args.omega
     s.raw.max_sweeps = args.max_sweeps
     s.raw.check_every = args.check_every
+    s.raw.first_check = args.first_check
     s.raw.rbgs_kernel = {"p2p": 2, "cluster": 3}[args.solve_sync]
     s.raw.p2g_mode = {"atomic": 0, "sorted": 1}[args.p2g]
     s.raw.device_emission = 1  # jet samples built on the device (the oracle matches this mode)
@@ -316,6 +317,8 @@ def run_c4(args, rank, world, local, dist):
         settings[i].raw.p2g_mode = 1
         settings[i].raw.rbgs_omega = args.omega
         settings[i].raw.max_sweeps = args.max_sweeps
+        settings[i].raw.check_every = args.check_every
+        settings[i].raw.first_check = args.first_check
         settings[i].raw.rbgs_kernel = {"p2p": 2, "cluster": 3}[args.solve_sync]
     ens = MpmEnsemble([settings[i] for i in mine], lib)
     for k, i in enumerate(mine):
@@ -360,7 +363,8 @@ def run_c4(args, rank, world, local, dist):
                        "particles_min": min(counts), "particles_max": max(counts), "particles_total": sum(counts),
                        "pairs_mean": sum(v[1] for v in stats.values()) / len(stats),
                        "residual_checks_mean": sum(v[2] for v in stats.values()) / len(stats), "residual_tol": 1e-5,
-                       "omega": args.omega, "timing": "CUDA events on the ensemble stream, max over ranks",
+                       "omega": args.omega, "check_every_pairs": args.check_every,
+                       "first_check_pairs": args.first_check or args.check_every, "timing": "CUDA events on the ensemble stream, max over ranks",
                        "l2": "not flushed: 64 resident pours' particle and grid arrays exceed the 126 MB L2 many times over"
                              if args.instances >= 16 else "not flushed",
                        "parallelism": f"instances sharded over {world} GPU(s)"},
@@ -439,6 +443,12 @@ def main():
                     help="colour separation inside the cluster solve: point-to-point mbarrier waits "
                          "or cluster barriers")
     ap.add_argument("--check-every", type=int, default=60)
+    # c2: just under the ~137 pairs a substep of this pour takes (0.92 of the fewest, the
+    # rule cs_autotune applies; measured 0 -> 360, 125 -> 367, 132 -> 365, 140 -> 361,
+    # 150 -> 349 M particle-steps/s); c4: 0, since its pours take different pair counts
+    ap.add_argument("--first-check", type=int, default=None,
+                    help="pairs before each solve's first FP64 residual check (0: --check-every; "
+                         "default 125 for c2, 0 for c4)")
     ap.add_argument("--p2g", default="sorted", choices=["atomic", "sorted"],
                     help="P2G accumulation: per-particle global atomics or tile-sorted shared memory")
     ap.add_argument("--cpu-steps", type=int, default=40, help="cap on the CPU baseline's timed substeps")
@@ -450,6 +460,8 @@ def main():
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.first_check is None:
+        args.first_check = 125 if args.workload == "c2" else 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -592,7 +604,8 @@ def main():
         "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "particles": n_p, "particles_mean": particle_steps / args.steps,
                    "bed_particles": n_bed, "timed_substeps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "substep_dt_s": dt, "residual_tol": 1e-5, "omega": args.omega, "warm_start": "previous substep",
-                   "check_every_pairs": args.check_every, "p2g": args.p2g,
+                   "check_every_pairs": args.check_every, "first_check_pairs": args.first_check or args.check_every,
+                   "p2g": args.p2g,
                    "solve_sync": {"p2p": "point-to-point mbarrier waits", "cluster": "cluster barriers"}[args.solve_sync],
                    "emission": "device kernel",
                    "timed_launch": "CUDA graph replay" if use_graph else "direct launches",

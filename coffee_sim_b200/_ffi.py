@@ -187,7 +187,8 @@ class CsSettings(C.Structure):
         ("flow_override_ml_s", C.c_float),
         ("exit_speed_override", C.c_float),
         ("rbgs_omega", C.c_float),
-        ("reserved", C.c_uint32 * 7),
+        ("first_check", C.c_uint32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 
@@ -235,7 +236,8 @@ class CsTuneResult(C.Structure):
         ("trials", C.c_uint32),
         ("best_ms", C.c_float),
         ("initial_ms", C.c_float),
-        ("reserved", C.c_uint32 * 2),
+        ("first_check", C.c_uint32),
+        ("reserved", C.c_uint32 * 1),
     ]
 
 

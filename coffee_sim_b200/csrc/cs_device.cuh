@@ -70,6 +70,7 @@ struct Params {
     JetPlan jet;               // device emission of this substep (count 0: none)
     uint32_t warm;             // keep last substep's pressure in fluid cells
     float omega;               // red-black over-relaxation (1 = plain Gauss-Seidel)
+    uint32_t first_check;      // pairs before a solve's first residual check (0: check_every)
 };
 
 // Device pointers of one simulation (or one ensemble member).

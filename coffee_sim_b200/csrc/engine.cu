@@ -311,6 +311,7 @@ void Engine::fill_params(Params& u, float dt) const {
     u.ntz = (u.gz + 1 + P2G_TILE - 1) / P2G_TILE;
     u.warm = (s.warm_start != CS_WARM_NONE && !u.fixed_point && have_prev_p) ? 1u : 0u;
     u.omega = s.rbgs_omega > 0.0f ? s.rbgs_omega : 1.0f;
+    u.first_check = s.first_check;
 }
 
 int Engine::upload_ctx() {
@@ -450,7 +451,7 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
         const uint32_t ce = s.check_every ? s.check_every : 10;
         r0 = refine_residual();
         r1 = r0;
-        uint32_t next = ce;
+        uint32_t next = s.first_check ? s.first_check : ce;
         while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
             uint32_t k = std::min(next, s.max_sweeps - sweeps);
             mark(CS_PHASE_SWEEPS);
@@ -1123,7 +1124,8 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
         if (t.grid_dims[0] != a.grid_dims[0] || t.grid_dims[1] != a.grid_dims[1] || t.grid_dims[2] != a.grid_dims[2] ||
             t.p2g_mode != a.p2g_mode || t.solve_mode != a.solve_mode || t.pressure_storage != a.pressure_storage ||
             t.device != a.device || t.pressure_rbgs_pairs != a.pressure_rbgs_pairs || t.max_sweeps != a.max_sweeps ||
-            t.check_every != a.check_every || t.residual_tol != a.residual_tol || t.warm_start != a.warm_start) {
+            t.check_every != a.check_every || t.first_check != a.first_check || t.residual_tol != a.residual_tol ||
+            t.warm_start != a.warm_start) {
             set_error("ensemble instances must share grid dims, device, P2G mode, warm start and solver settings");
             return CS_ERR_INVALID_ARG;
         }
@@ -1578,17 +1580,21 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    auto trial = [&](float omega, uint32_t ce, uint32_t p2g, float& ms) -> int {
+    uint32_t trial_min_pairs = 0;  // fewest pairs of one substep in the last trial
+    auto trial = [&](float omega, uint32_t ce, uint32_t p2g, uint32_t first, float& ms) -> int {
         int r = snapshot_load(state.data(), bytes);
         if (r) return r;
         s.rbgs_omega = omega;
         s.check_every = ce;
         s.p2g_mode = p2g;
+        s.first_check = first;
         bool converged = true;
+        trial_min_pairs = 0xffffffffu;
         cudaEventRecord(a, stream_);
         for (uint32_t k = 0; k < substeps; ++k) {
             if ((r = substep(sub_dt, 0xffffffffu))) return r;
             converged = converged && last.last_residual >= 0.0 && last.last_residual <= (double)s.residual_tol;
+            trial_min_pairs = std::min(trial_min_pairs, last.last_sweeps);
         }
         cudaEventRecord(b, stream_);
         if ((r = sync())) return r;
@@ -1599,34 +1605,55 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     };
     CsTuneResult res{};
     float ms = 0.0f;
-    if ((rc = trial(entry.rbgs_omega, entry.check_every, entry.p2g_mode, ms))) goto done;
+    uint32_t best_pairs = 0;
+    if ((rc = trial(entry.rbgs_omega, entry.check_every, entry.p2g_mode, entry.first_check, ms))) goto done;
     res.initial_ms = ms;
     res.best_ms = ms;
     res.omega = entry.rbgs_omega;
     res.check_every = entry.check_every;
     res.p2g_mode = entry.p2g_mode;
+    res.first_check = entry.first_check;
     res.trials = 1;
+    best_pairs = trial_min_pairs;
     // P2G mode at the entry solver settings, then the solver at the chosen mode
     for (uint32_t m : {(uint32_t)CS_P2G_ATOMIC32, (uint32_t)CS_P2G_SORTED_SHARED}) {
         if (m == entry.p2g_mode || entry.p2g_mode == CS_P2G_INT64) continue;  // int64 changes the numerics
-        if ((rc = trial(entry.rbgs_omega, entry.check_every, m, ms))) goto done;
+        if ((rc = trial(entry.rbgs_omega, entry.check_every, m, entry.first_check, ms))) goto done;
         ++res.trials;
         if (ms < res.best_ms) {
             res.best_ms = ms;
             res.p2g_mode = m;
+            best_pairs = trial_min_pairs;
         }
     }
     for (float omega : {1.80f, 1.85f, 1.88f, 1.90f, 1.92f, 1.94f, 1.96f})
         for (uint32_t ce : {10u, 20u, 40u, 60u, 80u}) {
-            if (omega == res.omega && ce == res.check_every) continue;
-            if ((rc = trial(omega, ce, res.p2g_mode, ms))) goto done;
+            if (omega == res.omega && ce == res.check_every && res.first_check == 0) continue;
+            if ((rc = trial(omega, ce, res.p2g_mode, 0u, ms))) goto done;
             ++res.trials;
             if (ms < res.best_ms) {
                 res.best_ms = ms;
                 res.omega = omega;
                 res.check_every = ce;
+                res.first_check = 0;
+                best_pairs = trial_min_pairs;
             }
         }
+    // the first check just before the fewest pairs a trial substep took (each check skipped
+    // saves an FP64 residual pass; a first interval past convergence costs extra pairs)
+    if (best_pairs != 0xffffffffu && best_pairs > 4) {
+        const uint32_t base = best_pairs;
+        for (double f : {0.85, 0.92, 0.98}) {
+            const uint32_t first = (uint32_t)(f * (double)base);
+            if (first < 2 || first == res.first_check) continue;
+            if ((rc = trial(res.omega, res.check_every, res.p2g_mode, first, ms))) goto done;
+            ++res.trials;
+            if (ms < res.best_ms) {
+                res.best_ms = ms;
+                res.first_check = first;
+            }
+        }
+    }
 done:
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -1639,6 +1666,7 @@ done:
     s.rbgs_omega = res.omega;
     s.check_every = res.check_every;
     s.p2g_mode = res.p2g_mode;
+    s.first_check = res.first_check;
     if (out) *out = res;
     return CS_OK;
 }

@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     double r0 = residual(slot);
     double r1 = r0;
     uint32_t pairs = 0, evals = 1;
-    uint32_t next = ce;  // pairs before the next check (same value on every CTA)
+    uint32_t next = u.first_check ? u.first_check : ce;  // pairs before the next check (same on every CTA)
     while (!(r1 <= (double)tol) && pairs < max_pairs && !abort_all) {
         uint32_t k = min(next, max_pairs - pairs);
         for (uint32_t j = 0; j < k; ++j) {

@@ -230,7 +230,9 @@ typedef struct CsSettings {
     float flow_override_ml_s;     /* >0: constant flow instead of the kettle-angle model */
     float exit_speed_override;    /* >0 with flow override: jet speed */
     float rbgs_omega;             /* red-black over-relaxation; 0 or 1 = plain Gauss-Seidel */
-    uint32_t reserved[7];
+    uint32_t first_check;         /* FP32 residual mode: pairs before a solve's first residual
+                                     check (0: check_every); later intervals are predicted */
+    uint32_t reserved[6];
 } CsSettings;
 
 /* Observability counters (mod.rs:50-68 / state.rs:22-28) + solver telemetry. */
@@ -447,11 +449,13 @@ typedef struct CsTuneResult {
     uint32_t trials;       /* configurations timed */
     float best_ms;         /* device ms per substep with the chosen configuration */
     float initial_ms;      /* device ms per substep with the configuration at entry */
-    uint32_t reserved[2];
+    uint32_t first_check;  /* chosen pairs before each solve's first residual check (0: check_every) */
+    uint32_t reserved[1];
 } CsTuneResult;
 
 /* Time `substeps` substeps of length sub_dt from the current state for each candidate
- * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/40/60/80),
+ * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/40/60/80,
+ * then a first-check interval of 0.85/0.92/0.98 of the fewest pairs a substep took),
  * restoring the state after every trial; keep the fastest whose every substep reached
  * the residual target.  The simulation ends in the state it had at entry with the
  * chosen configuration applied.  Residual-mode solves only (CS_ERR_UNSUPPORTED else). */

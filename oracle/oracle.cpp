@@ -1805,7 +1805,7 @@ struct Sim : SimBase {
                 r0 = refine_residual();
                 r1 = r0;
                 checks = 1;
-                uint32_t next = ce;
+                uint32_t next = s.first_check ? s.first_check : ce;
                 while (!(r1 <= (double)s.residual_tol) && sweeps < s.max_sweeps) {
                     uint32_t k = std::min(next, s.max_sweeps - sweeps);
                     for (uint32_t j = 0; j < k; ++j) {

@@ -50,7 +50,9 @@ def test_autotune_restores_state_and_applies_choice(engine):
     assert sim.particle_count() == n
     assert mismatch(sim.read_particles(0, n), before[0]) == 0
     assert mismatch(sim.read_pressure(), before[1]) == 0
+    assert r.first_check == 0 or 2 <= r.first_check <= 4000
     st = sim.current_settings()
     assert st.rbgs_omega == r.omega and st.check_every == r.check_every and st.p2g_mode == r.p2g_mode
+    assert st.first_check == r.first_check
     sim.step_substep(scenes.C2_DT)
     assert sim.latest_metrics().last_residual <= 1e-5
