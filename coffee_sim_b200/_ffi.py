@@ -279,6 +279,8 @@ PROTOTYPES = {
     "cs_get_emission": (I32, [P, PF, PF, PU32, PU32]),
     "cs_get_mass_units_per_ml": (I32, [P, PF]),
     "cs_get_metrics": (I32, [P, PM]),
+    "cs_metrics_request": (I32, [P]),
+    "cs_metrics_wait": (I32, [P, PM]),
     "cs_get_settings": (I32, [P, PS]),
     "cs_read_particles": (I32, [P, U32, U32, PF]),
     "cs_read_affine": (I32, [P, U32, U32, PF]),

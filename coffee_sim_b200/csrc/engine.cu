@@ -48,6 +48,11 @@ Engine::~Engine() {
     if (cur_event_ && spans_.empty()) cudaEventDestroy(cur_event_);
     if (t0_) cudaEventDestroy(t0_);
     if (t1_) cudaEventDestroy(t1_);
+    if (mevent_) cudaEventDestroy(mevent_);
+    if (mstage_) cudaFreeHost(mstage_);
+    for (cudaEvent_t e : ctx_ev_)
+        if (e) cudaEventDestroy(e);
+    if (ctx_pinned_) cudaFreeHost(ctx_pinned_);
     free_all();
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -316,7 +321,21 @@ void Engine::fill_params(Params& u, float dt) const {
 
 int Engine::upload_ctx() {
     prof_.h2d_bytes += sizeof(Ctx);
-    return check(cudaMemcpyAsync(d_ctx_.ptr, &ctx_, sizeof(Ctx), cudaMemcpyHostToDevice, stream_), "ctx upload");
+    int rc;
+    if (!ctx_pinned_) {
+        if ((rc = check(cudaHostAlloc((void**)&ctx_pinned_, 2 * sizeof(Ctx), cudaHostAllocDefault), "pinned context")))
+            return rc;
+        for (cudaEvent_t& e : ctx_ev_)
+            if ((rc = check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "context event"))) return rc;
+    }
+    ctx_slot_ ^= 1;
+    if (ctx_ev_used_[ctx_slot_] && (rc = check(cudaEventSynchronize(ctx_ev_[ctx_slot_]), "context slot"))) return rc;
+    std::memcpy(&ctx_pinned_[ctx_slot_], &ctx_, sizeof(Ctx));
+    if ((rc = check(cudaMemcpyAsync(d_ctx_.ptr, &ctx_pinned_[ctx_slot_], sizeof(Ctx), cudaMemcpyHostToDevice, stream_),
+                    "ctx upload")))
+        return rc;
+    ctx_ev_used_[ctx_slot_] = true;
+    return check(cudaEventRecord(ctx_ev_[ctx_slot_], stream_), "context event");
 }
 
 // inflow.rs:122-242: plan on the host, build the samples, append them.
@@ -745,6 +764,78 @@ int Engine::metrics(CsMetrics* out) {
     out->mass_overflow_fires = m[M_OVERFLOW];
     out->nan_flag = m[M_NAN];
     out->timeout_flag = m[M_TIMEOUT];
+    return CS_OK;
+}
+
+int Engine::metrics_request() {
+    if (mreq_) {
+        set_error("a metrics request is already pending");
+        return CS_ERR_INVALID_ARG;
+    }
+    mreq_ = true;
+    mreq_totals_ = false;
+    if (settings.warm_start == CS_WARM_LEARNED) return CS_OK;  // the wait reads synchronously
+    int rc;
+    if (!mstage_) {
+        if ((rc = check(cudaHostAlloc((void**)&mstage_, sizeof(MetricsStage), cudaHostAllocDefault), "pinned stage")))
+            return rc;
+        if ((rc = check(cudaEventCreateWithFlags(&mevent_, cudaEventDisableTiming), "event"))) return rc;
+    }
+    if ((rc = check(cudaMemcpyAsync(mstage_->m, metrics_.ptr, sizeof(mstage_->m), cudaMemcpyDeviceToHost, stream_),
+                    "metrics request")))
+        return rc;
+    prof_.d2h_bytes += sizeof(mstage_->m);
+    mreq_totals_ = graph_pending_;
+    if (mreq_totals_) {
+        if ((rc = check(cudaMemcpyAsync(&mstage_->t, sc_totals_.ptr, sizeof(ScTotals), cudaMemcpyDeviceToHost, stream_),
+                        "totals request")))
+            return rc;
+        prof_.d2h_bytes += sizeof(ScTotals);
+    }
+    mreq_last_ = last;
+    return check(cudaEventRecord(mevent_, stream_), "metrics event");
+}
+
+int Engine::metrics_wait(CsMetrics* out) {
+    if (!mreq_) {
+        set_error("no metrics request is pending");
+        return CS_ERR_INVALID_ARG;
+    }
+    mreq_ = false;
+    if (settings.warm_start == CS_WARM_LEARNED) return metrics(out);
+    int rc = check(cudaEventSynchronize(mevent_), "metrics wait");
+    if (rc) return rc;
+    CsMetrics r = mreq_last_;
+    if (mreq_totals_) {
+        const ScTotals t = mstage_->t;
+        bool failed = false;
+        if (t.runs >= seen_.runs) {  // not already accounted by a later synchronising call
+            prof_.sweeps += t.sweeps - seen_.sweeps;
+            prof_.residual_evals += t.evals - seen_.evals;
+            failed = t.failed != seen_.failed;
+            seen_ = t;
+        }
+        if (t.runs) {
+            r.last_sweeps = t.last.sweeps;
+            r.residual_checks = t.last.evals;
+            r.last_residual = t.last.r1;
+            r.initial_residual = t.last.r0;
+        }
+        if (failed) {
+            set_error("a replayed substep's pressure solve did not fit the thread-block cluster "
+                      "(16 x 4095 fluid cells); run this scene with use_graph = 0");
+            return CS_ERR_CAPACITY;
+        }
+    }
+    const uint32_t* m = mstage_->m;
+    r.max_abs_div = (float)m[M_MAX_DIV] * (1.0f / METRICS_DIV_FP_SCALE);
+    r.fluid_cells = m[M_FLUID];
+    r.div_clamp_fires = m[M_DIV_CLAMP];
+    r.pressure_clamp_fires = m[M_P_CLAMP];
+    r.mass_overflow_fires = m[M_OVERFLOW];
+    r.nan_flag = m[M_NAN];
+    r.timeout_flag = m[M_TIMEOUT];
+    *out = r;
     return CS_OK;
 }
 
@@ -2033,6 +2124,15 @@ int32_t cs_get_metrics(CsSim* sim, CsMetrics* out) {
     CS_SIM(sim);
     CS_PTR(out);
     return sim->e->metrics(out);
+}
+int32_t cs_metrics_request(CsSim* sim) {
+    CS_SIM(sim);
+    return sim->e->metrics_request();
+}
+int32_t cs_metrics_wait(CsSim* sim, CsMetrics* out) {
+    CS_SIM(sim);
+    CS_PTR(out);
+    return sim->e->metrics_wait(out);
 }
 int32_t cs_get_settings(const CsSim* sim, CsSettings* out) {
     CS_SIM(sim);

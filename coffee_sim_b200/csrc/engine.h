@@ -45,6 +45,8 @@ public:
     int read_sdf(float* out);
     int read_class(uint8_t* out);
     int metrics(CsMetrics* out);
+    int metrics_request();
+    int metrics_wait(CsMetrics* out);
     int add_water_block(const float lo[3], const float hi[3], uint32_t per_axis, float jitter, uint32_t seed,
                         uint32_t require_open_sdf, uint32_t* added);
     int snapshot_size(uint64_t* bytes);
@@ -112,6 +114,15 @@ private:
     bool graph_pending_ = false;   // replays whose solve totals are not yet read
     DeviceBuffer sc_totals_;
     ScTotals seen_{};              // totals at the last collect()
+    // pipelined metrics readback: device counters and solve totals staged in pinned memory
+    struct MetricsStage {
+        uint32_t m[8];
+        ScTotals t;
+    };
+    MetricsStage* mstage_ = nullptr;
+    cudaEvent_t mevent_ = nullptr;
+    bool mreq_ = false, mreq_totals_ = false;
+    CsMetrics mreq_last_{};
     // cluster-resident solver
     DeviceBuffer sc_scratch_;  // every solver scratch buffer, laid out by sc_scratch_layout
     ScBuffers sc_buf_{};
@@ -120,6 +131,13 @@ private:
     int solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done);
     DeviceBuffer flush_;    // > L2 scratch for cs_flush_l2 (allocated on first use)
     Ctx ctx_{};             // host copy of the device context
+    // two pinned staging slots for the context upload, so that the copy is asynchronous
+    // (a pageable source may make the copy wait for the stream); a slot is rewritten only
+    // after the copy that last read it has run
+    Ctx* ctx_pinned_ = nullptr;
+    cudaEvent_t ctx_ev_[2] = {nullptr, nullptr};
+    bool ctx_ev_used_[2] = {false, false};
+    int ctx_slot_ = 0;
     std::vector<float> sdf_host_;
 
 public:

@@ -230,6 +230,16 @@ class MpmSim3D:
         self.lib.call("cs_get_metrics", self._h, C.byref(m))
         return m
 
+    def metrics_request(self):
+        """Queue a copy of the latest substep's metrics without waiting for the GPU."""
+        self.lib.call("cs_metrics_request", self._h)
+
+    def metrics_wait(self):
+        """The metrics of the substep current at the last metrics_request()."""
+        m = CsMetrics()
+        self.lib.call("cs_metrics_wait", self._h, C.byref(m))
+        return m
+
     # -- readback (reference byte layouts) --
     def _read_rows(self, fn, width, first, count, dtype=np.float32):
         if count is None:

@@ -302,6 +302,13 @@ int32_t cs_get_emission(const CsSim* sim, float* frame_emitted_mass, float* tota
 int32_t cs_get_mass_units_per_ml(const CsSim* sim, float* out);
 /* refresh_metrics + metric getters (mod.rs:546-567, lib.rs:219-252); synchronises. */
 int32_t cs_get_metrics(CsSim* sim, CsMetrics* out);
+/* Pipelined readback (no reference counterpart): cs_metrics_request queues a copy of the
+ * latest substep's metrics behind the work already enqueued and returns at once;
+ * cs_metrics_wait waits for that copy only and returns the metrics as cs_get_metrics would
+ * have after that substep.  Substeps may be enqueued in between, so a host loop can read
+ * step k's result while step k+1 runs.  One request at a time (CS_ERR_INVALID_ARG else). */
+int32_t cs_metrics_request(CsSim* sim);
+int32_t cs_metrics_wait(CsSim* sim, CsMetrics* out);
 int32_t cs_get_settings(const CsSim* sim, CsSettings* out);
 
 /* ---- readback into caller buffers (physics_tests.rs:61-1083 read the same layouts) ---- */

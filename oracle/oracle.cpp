@@ -1920,6 +1920,8 @@ using namespace orc;
 
 struct CsSim {
     std::unique_ptr<SimBase> impl;
+    bool metrics_pending = false;
+    CsMetrics metrics_req{};
 };
 
 static int check_settings(const CsSettings* s) {
@@ -2126,6 +2128,21 @@ int32_t cs_get_mass_units_per_ml(const CsSim* sim, float* out) {
 int32_t cs_get_metrics(CsSim* sim, CsMetrics* out) {
     if (!sim || !out) return fail(CS_ERR_INVALID_ARG, "null");
     *out = sim->impl->metrics_out;
+    return CS_OK;
+}
+// the oracle steps synchronously: a request records the metrics, the wait returns them
+int32_t cs_metrics_request(CsSim* sim) {
+    if (!sim) return fail(CS_ERR_INVALID_ARG, "null");
+    if (sim->metrics_pending) return fail(CS_ERR_INVALID_ARG, "a metrics request is already pending");
+    sim->metrics_pending = true;
+    sim->metrics_req = sim->impl->metrics_out;
+    return CS_OK;
+}
+int32_t cs_metrics_wait(CsSim* sim, CsMetrics* out) {
+    if (!sim || !out) return fail(CS_ERR_INVALID_ARG, "null");
+    if (!sim->metrics_pending) return fail(CS_ERR_INVALID_ARG, "no metrics request is pending");
+    sim->metrics_pending = false;
+    *out = sim->metrics_req;
     return CS_OK;
 }
 int32_t cs_get_settings(const CsSim* sim, CsSettings* out) {
