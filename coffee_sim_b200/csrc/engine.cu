@@ -554,6 +554,10 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     const int cb = launch_cells_blocks();
     const int pb = launch_particle_blocks(np);
     const int bb = launch_particle_blocks(capture ? settings.max_particles : num_bed);
+    // the bed-lookup scatter (27 atomicMax per bed sample, a few thousand samples) runs in
+    // warp-sized blocks so that it spreads over the SMs (clear phase 27.7 -> 23.5 us)
+    const int bb32 = (int)std::max<size_t>(
+        1, std::min<size_t>(((size_t)(capture ? settings.max_particles : num_bed) + 31) / 32, (size_t)sms_ * 16));
     const dim3 T(kThreads);
     auto ph = [&](int phase) {
         if (!capture) mark(phase);
@@ -575,7 +579,7 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     if (settings.p2g_mode == CS_P2G_INT64) cudaMemsetAsync(lanes64_.ptr, 0, lanes64_.bytes, stream_);
     if (P > 0) cudaMemsetAsync(metrics_.ptr, 0, metrics_.bytes, stream_);
     if (P > 1) cudaMemsetAsync(lookup_.ptr, 0xff, lookup_.bytes, stream_);
-    if (P > 2 && any_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb, 1), T, 0, stream_>>>(dc));
+    if (P > 2 && any_bed) CS_LAUNCH(k_bed_lookup_scatter<<<dim3(bb32, 1), 32, 0, stream_>>>(dc));
     ph(CS_PHASE_P2G);
     if (P > 3 && any_p) {
         if (settings.p2g_mode != CS_P2G_ATOMIC32) {
