@@ -322,12 +322,11 @@ void Engine::fill_params(Params& u, float dt) const {
 int Engine::upload_ctx() {
     prof_.h2d_bytes += sizeof(Ctx);
     int rc;
-    if (!ctx_pinned_) {
-        if ((rc = check(cudaHostAlloc((void**)&ctx_pinned_, 2 * sizeof(Ctx), cudaHostAllocDefault), "pinned context")))
-            return rc;
-        for (cudaEvent_t& e : ctx_ev_)
-            if ((rc = check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "context event"))) return rc;
-    }
+    if (!ctx_pinned_ &&
+        (rc = check(cudaHostAlloc((void**)&ctx_pinned_, 2 * sizeof(Ctx), cudaHostAllocDefault), "pinned context")))
+        return rc;
+    for (cudaEvent_t& e : ctx_ev_)
+        if (!e && (rc = check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "context event"))) return rc;
     ctx_slot_ ^= 1;
     if (ctx_ev_used_[ctx_slot_] && (rc = check(cudaEventSynchronize(ctx_ev_[ctx_slot_]), "context slot"))) return rc;
     std::memcpy(&ctx_pinned_[ctx_slot_], &ctx_, sizeof(Ctx));
@@ -776,15 +775,16 @@ int Engine::metrics_request() {
         set_error("a metrics request is already pending");
         return CS_ERR_INVALID_ARG;
     }
-    mreq_ = true;
     mreq_totals_ = false;
-    if (settings.warm_start == CS_WARM_LEARNED) return CS_OK;  // the wait reads synchronously
-    int rc;
-    if (!mstage_) {
-        if ((rc = check(cudaHostAlloc((void**)&mstage_, sizeof(MetricsStage), cudaHostAllocDefault), "pinned stage")))
-            return rc;
-        if ((rc = check(cudaEventCreateWithFlags(&mevent_, cudaEventDisableTiming), "event"))) return rc;
+    if (settings.warm_start == CS_WARM_LEARNED) {  // the wait reads synchronously
+        mreq_ = true;
+        return CS_OK;
     }
+    int rc;
+    if (!mstage_ &&
+        (rc = check(cudaHostAlloc((void**)&mstage_, sizeof(MetricsStage), cudaHostAllocDefault), "pinned stage")))
+        return rc;
+    if (!mevent_ && (rc = check(cudaEventCreateWithFlags(&mevent_, cudaEventDisableTiming), "event"))) return rc;
     if ((rc = check(cudaMemcpyAsync(mstage_->m, metrics_.ptr, sizeof(mstage_->m), cudaMemcpyDeviceToHost, stream_),
                     "metrics request")))
         return rc;
@@ -797,7 +797,9 @@ int Engine::metrics_request() {
         prof_.d2h_bytes += sizeof(ScTotals);
     }
     mreq_last_ = last;
-    return check(cudaEventRecord(mevent_, stream_), "metrics event");
+    if ((rc = check(cudaEventRecord(mevent_, stream_), "metrics event"))) return rc;
+    mreq_ = true;
+    return CS_OK;
 }
 
 int Engine::metrics_wait(CsMetrics* out) {
