@@ -121,6 +121,17 @@ impl MpmSim3D {
         check(unsafe { sys::cs_get_metrics(self.raw, &mut m) })?;
         Ok(m)
     }
+    /// Queue a copy of the latest substep's metrics without waiting for the GPU
+    /// (engine extension; pair with `metrics_wait` after queuing the next step).
+    pub fn metrics_request(&mut self) -> Result<(), CsError> {
+        check(unsafe { sys::cs_metrics_request(self.raw) })
+    }
+    /// The metrics queued by the last `metrics_request`; waits for that copy only.
+    pub fn metrics_wait(&mut self) -> Result<sys::CsMetrics, CsError> {
+        let mut m = sys::CsMetrics::default();
+        check(unsafe { sys::cs_metrics_wait(self.raw, &mut m) })?;
+        Ok(m)
+    }
 }
 
 impl Drop for MpmSim3D {
