@@ -290,6 +290,7 @@ PROTOTYPES = {
     "cs_read_grid_vel": (I32, [P, PF]),
     "cs_read_pressure": (I32, [P, PF]),
     "cs_read_cell_kind": (I32, [P, PI32]),
+    "cs_read_solver_inputs": (I32, [P, PF, PF]),
     "cs_read_bed_lookup": (I32, [P, PI32]),
     "cs_read_bed_delta": (I32, [P, PI32]),
     "cs_read_render": (I32, [P, U32, U32, PF]),

@@ -89,6 +89,9 @@ struct Ctx {
     int32_t* delta;   // 4 lanes x max_p: water, impulse x/y/z
     // grid
     int32_t* lanes;   // 6 x cells, reference aliasing (shader.rs:152-164)
+    // cell kind of each cell: lane 3 of `lanes` in a simulation; the pressure solves
+    // read the kind only through this pointer, so they can run on a caller's array
+    const int32_t* kind;
     long long* lanes64;  // 6 x cells in int64 mode
     // sorted P2G (CS_P2G_SORTED_SHARED): particles counting-sorted by 4^3-cell tile
     uint32_t* p2g_key;     // max_p: tile of each particle (P2G_NO_TILE if it deposits nothing)
@@ -116,6 +119,7 @@ struct Ctx {
     uint32_t* metrics;      // 8 counters
     double* resid;          // [0] sum r^2, [1] sum b^2
     ScBuffers sb;           // cluster-resident pressure solve scratch of this instance
+    GsBuffers gs;           // grid-wide pressure solve scratch (large grids)
 };
 
 // ---------------- math with WGSL semantics ----------------

@@ -14,6 +14,7 @@
 #include "engine.h"
 #include "kernels.cu"
 #include "solver_cluster.cuh"
+#include "solver_grid.cuh"
 
 namespace cs {
 
@@ -146,6 +147,7 @@ int Engine::init() {
         ctx_.sb = sc_buf_;
         sc_ranks_ = sc_max_cluster_ranks();
     }
+    if ((rc = gs_alloc())) return rc;
 
     ctx_.pos = (float4*)pos_.ptr;
     ctx_.vel = (float4*)vel_.ptr;
@@ -158,6 +160,7 @@ int Engine::init() {
     ctx_.snap = (float4*)snap_.ptr;
     ctx_.delta = (int32_t*)delta_.ptr;
     ctx_.lanes = (int32_t*)lanes_.ptr;
+    ctx_.kind = (const int32_t*)lanes_.ptr + 3 * cells_;
     ctx_.lanes64 = (long long*)lanes64_.ptr;
     ctx_.p2g_key = (uint32_t*)p2g_key_.ptr;
     ctx_.p2g_rank = (uint32_t*)p2g_rank_.ptr;
@@ -410,6 +413,82 @@ double Engine::refine_residual() {
     return std::sqrt(h[0]) / std::sqrt(h[1]);
 }
 
+// The cluster-resident solve serves grids of at most kClusterMaxCells cells (unless the
+// per-colour launches or the grid-wide solve are asked for); larger grids use the
+// grid-wide solve, whose row segments cover only the rows that hold fluid.
+bool Engine::use_cluster_solve() const {
+    return sc_ranks_ > 0 && settings.rbgs_kernel != 1 && settings.rbgs_kernel != 4 && cells_ <= kClusterMaxCells;
+}
+
+// Grid-wide solve buffers (solver_grid.cuh), sized for the worst case: every row of
+// the grid holding fluid across its whole width.
+int Engine::gs_alloc() {
+    const uint32_t gx = settings.grid_dims[0];
+    const size_t rows = (size_t)settings.grid_dims[1] * settings.grid_dims[2];
+    const size_t units = rows * ((gx + GS_UNIT - 1) / GS_UNIT);
+    const size_t slots = units * GS_UNIT;
+    int rc;
+    if ((rc = alloc(gs_rows_, (2 * (rows + 1) + rows) * sizeof(uint32_t)))) return rc;
+    if ((rc = alloc(gs_desc_, units * sizeof(GsDesc)))) return rc;
+    if ((rc = alloc(gs_slots_, slots * (3 * sizeof(float2) + 2 * sizeof(float))))) return rc;
+    if ((rc = gs_blocks(&gs_ctas_))) return rc;
+    if ((rc = alloc(gs_misc_, sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)) + 256 +
+                                  sc_align(sizeof(ScResult))))) return rc;
+    size_t cub = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, cub, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)rows + 1, stream_);
+    if ((rc = alloc(gs_cub_, cub))) return rc;
+    GsBuffers& g = gs_buf_;
+    uint32_t* r = (uint32_t*)gs_rows_.ptr;
+    g.row_units = r;
+    g.row_start = r + rows + 1;
+    g.row_xlo = r + 2 * (rows + 1);
+    g.desc = (GsDesc*)gs_desc_.ptr;
+    unsigned char* sl = (unsigned char*)gs_slots_.ptr;
+    g.cf = (float2*)sl;
+    g.dfc = (float2*)(sl + slots * sizeof(float2));
+    g.p = (float2*)(sl + 2 * slots * sizeof(float2));
+    g.g = (float*)(sl + 3 * slots * sizeof(float2));
+    g.b = (float*)(sl + 3 * slots * sizeof(float2) + slots * sizeof(float));
+    unsigned char* m = (unsigned char*)gs_misc_.ptr;
+    g.part = (double*)m;
+    g.sync = (uint32_t*)(m + sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)));
+    g.result = (ScResult*)(m + sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)) + 256);
+    g.cub_temp = gs_cub_.ptr;
+    g.cub_bytes = cub;
+    ctx_.gs = g;
+    return CS_OK;
+}
+
+// Whole-GPU solve (solver_grid.cuh): row-segment prep, then one cooperative launch.
+// `done` is false when the launch could not run on this device or a bounded wait ran
+// out (the caller then solves with per-colour launches).
+int Engine::solve_grid(uint32_t& sweeps, double& r0, double& r1, bool& done) {
+    done = false;
+    if (gs_ctas_ <= 0) return CS_OK;
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    const CsSettings& s = settings;
+    mark(CS_PHASE_RESIDUAL);
+    int rc = gs_launch_prep(dc, &gs_buf_, s.grid_dims[1] * s.grid_dims[2], stream_, sms_);
+    if (rc) return rc;
+    count_launch(kGsPrepLaunches);
+    mark(CS_PHASE_SWEEPS);
+    if ((rc = gs_launch_solve(dc, gs_ctas_, s.residual_tol, s.max_sweeps, s.check_every, stream_))) return rc;
+    count_launch();
+    ScResult res;
+    if ((rc = check(cudaMemcpyAsync(&res, gs_buf_.result, sizeof(res), cudaMemcpyDeviceToHost, stream_),
+                    "grid solve result")))
+        return rc;
+    prof_.d2h_bytes += sizeof(res);
+    if ((rc = sync())) return rc;
+    if (res.status != 1) return CS_OK;
+    sweeps = res.sweeps;
+    r0 = res.r0;
+    r1 = res.r1;
+    prof_.residual_evals += res.evals;
+    done = true;
+    return CS_OK;
+}
+
 // One-launch solve on a thread-block cluster (solver_cluster.cuh).  `done` is false
 // when the fluid cells exceed the cluster's shared-memory capacity.
 int Engine::solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done) {
@@ -456,9 +535,18 @@ int Engine::solve_pressure(uint32_t& sweeps, double& r0, double& r1) {
     r0 = r1 = -1.0;
     const uint64_t evals0 = prof_.residual_evals;
     const bool refine = s.solve_mode == CS_SOLVE_RESIDUAL && s.pressure_storage != CS_PRESSURE_FIXED_POINT;
-    if (refine && s.rbgs_kernel != 1 && sc_ranks_ > 0) {
+    if (refine && use_cluster_solve()) {
         bool done = false;
         int rc = solve_cluster(sweeps, r0, r1, done);
+        if (rc) return rc;
+        if (done) {
+            last.residual_checks = (uint32_t)(prof_.residual_evals - evals0);
+            return CS_OK;
+        }
+    }
+    if (refine && s.rbgs_kernel != 1) {
+        bool done = false;
+        int rc = solve_grid(sweeps, r0, r1, done);
         if (rc) return rc;
         if (done) {
             last.residual_checks = (uint32_t)(prof_.residual_evals - evals0);
@@ -608,13 +696,24 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
             const CsSettings& s = settings;
             if (s.solve_mode == CS_SOLVE_RESIDUAL) {
                 if (s.warm_start == CS_WARM_LEARNED && (rc = learned_enqueue(false))) return rc;
-                if ((rc = sc_launch_prep(dc, &sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_))) return rc;
-                count_launch(kScPrepLaunches);
-                if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
-                                            stream_, s.rbgs_kernel == 3 ? 0u : 1u)))
-                    return rc;
-                count_launch();
-                CS_LAUNCH(k_sc_account<<<1, 1, 0, stream_>>>(sc_buf_.result, (ScTotals*)sc_totals_.ptr));
+                if (use_cluster_solve()) {
+                    if ((rc = sc_launch_prep(dc, &sc_buf_, (uint32_t)sc_codes_, sc_ranks_, 1, stream_, sms_)))
+                        return rc;
+                    count_launch(kScPrepLaunches);
+                    if ((rc = sc_launch_cluster(dc, sc_ranks_, 1, s.residual_tol, s.max_sweeps, s.check_every,
+                                                stream_, s.rbgs_kernel == 3 ? 0u : 1u)))
+                        return rc;
+                    count_launch();
+                    CS_LAUNCH(k_sc_account<<<1, 1, 0, stream_>>>(sc_buf_.result, (ScTotals*)sc_totals_.ptr));
+                } else {
+                    if ((rc = gs_launch_prep(dc, &gs_buf_, s.grid_dims[1] * s.grid_dims[2], stream_, sms_)))
+                        return rc;
+                    count_launch(kGsPrepLaunches);
+                    if ((rc = gs_launch_solve(dc, gs_ctas_, s.residual_tol, s.max_sweeps, s.check_every, stream_)))
+                        return rc;
+                    count_launch();
+                    CS_LAUNCH(k_sc_account<<<1, 1, 0, stream_>>>(gs_buf_.result, (ScTotals*)sc_totals_.ptr));
+                }
             } else {
                 const uint32_t half = (s.grid_dims[0] + 1) / 2;
                 const size_t ncol = (size_t)half * s.grid_dims[1] * s.grid_dims[2];
@@ -678,8 +777,9 @@ int Engine::substep_graph(float sub_dt) {
             cudaGraphExecDestroy(gexec_);
             gexec_ = nullptr;
         }
-        if (settings.solve_mode == CS_SOLVE_RESIDUAL && sc_ranks_ == 0) {
-            set_error("graph mode needs the cluster-resident solve, which this device cannot launch");
+        if (settings.solve_mode == CS_SOLVE_RESIDUAL && !use_cluster_solve() && gs_ctas_ <= 0) {
+            set_error("graph mode needs the cluster-resident or the grid-wide solve, neither of which this "
+                      "device can launch");
             return CS_ERR_UNSUPPORTED;
         }
         const uint64_t before = prof_.launches;
@@ -711,6 +811,22 @@ int Engine::substep_graph(float sub_dt) {
     return CS_OK;
 }
 
+// The error of the replayed solves counted between two readings of the totals: a solve
+// whose fluid did not fit the cluster (capacity) or one whose bounded waits ran out.
+int Engine::totals_error(const ScTotals& t, const ScTotals& before) {
+    if (t.failed != before.failed) {
+        set_error("a replayed substep's pressure solve did not fit the thread-block cluster "
+                  "(16 x 4095 fluid cells); run this scene with use_graph = 0");
+        return CS_ERR_CAPACITY;
+    }
+    if (t.timeouts != before.timeouts) {
+        set_error("a replayed substep's pressure solve gave up waiting for a neighbouring CTA "
+                  "(bounded wait ran out); the pressure of that substep is not solved");
+        return CS_ERR_TIMEOUT;
+    }
+    return CS_OK;
+}
+
 // Solve totals of the replayed substeps since the last call: sweep and residual
 // counters, the latest substep's metrics, and an error if a solve did not complete.
 int Engine::collect() {
@@ -723,7 +839,7 @@ int Engine::collect() {
     if ((rc = check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"))) return rc;
     prof_.sweeps += t.sweeps - seen_.sweeps;
     prof_.residual_evals += t.evals - seen_.evals;
-    const bool failed = t.failed != seen_.failed;
+    const int err = totals_error(t, seen_);
     seen_ = t;
     if (t.runs) {
         last.last_sweeps = t.last.sweeps;
@@ -731,11 +847,7 @@ int Engine::collect() {
         last.last_residual = t.last.r1;
         last.initial_residual = t.last.r0;
     }
-    if (failed) {
-        set_error("a replayed substep's pressure solve did not fit the thread-block cluster "
-                  "(16 x 4095 fluid cells); run this scene with use_graph = 0");
-        return CS_ERR_CAPACITY;
-    }
+    if (err) return err;
     return learned_collect();
 }
 
@@ -814,11 +926,11 @@ int Engine::metrics_wait(CsMetrics* out) {
     CsMetrics r = mreq_last_;
     if (mreq_totals_) {
         const ScTotals t = mstage_->t;
-        bool failed = false;
+        int err = 0;
         if (t.runs >= seen_.runs) {  // not already accounted by a later synchronising call
             prof_.sweeps += t.sweeps - seen_.sweeps;
             prof_.residual_evals += t.evals - seen_.evals;
-            failed = t.failed != seen_.failed;
+            err = totals_error(t, seen_);
             seen_ = t;
         }
         if (t.runs) {
@@ -827,11 +939,7 @@ int Engine::metrics_wait(CsMetrics* out) {
             r.last_residual = t.last.r1;
             r.initial_residual = t.last.r0;
         }
-        if (failed) {
-            set_error("a replayed substep's pressure solve did not fit the thread-block cluster "
-                      "(16 x 4095 fluid cells); run this scene with use_graph = 0");
-            return CS_ERR_CAPACITY;
-        }
+        if (err) return err;
     }
     const uint32_t* m = mstage_->m;
     r.max_abs_div = (float)m[M_MAX_DIV] * (1.0f / METRICS_DIV_FP_SCALE);
@@ -914,6 +1022,15 @@ int Engine::read_pressure(float* out) {
 int Engine::read_kind(int32_t* out) {
     int rc = check(cudaMemcpyAsync(out, (int32_t*)lanes_.ptr + 3 * cells_, cells_ * 4, cudaMemcpyDeviceToHost, stream_),
                    "kind");
+    return rc ? rc : sync();
+}
+int Engine::read_solver_inputs(float* fill, float* div) {
+    if (settings.pressure_storage == CS_PRESSURE_FIXED_POINT) {
+        set_error("the solver's divergence array exists in FP32 pressure storage only");
+        return CS_ERR_UNSUPPORTED;
+    }
+    int rc = check(cudaMemcpyAsync(fill, fill_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "fill");
+    if (!rc) rc = check(cudaMemcpyAsync(div, divf_.ptr, cells_ * 4, cudaMemcpyDeviceToHost, stream_), "divergence");
     return rc ? rc : sync();
 }
 int Engine::read_lookup(int32_t* out) {
@@ -1831,6 +1948,66 @@ int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ra
     return CS_OK;
 }
 
+int gs_blocks(int* ctas) {
+    *ctas = 0;
+    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CS_OK;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return CS_OK;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return CS_OK;
+    const size_t smem = (size_t)GS_DESC_SMEM * sizeof(GsDesc);
+    if (cudaFuncSetAttribute(k_gs_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return CS_OK;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_solve, GS_THREADS, smem) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return CS_OK;
+    }
+    *ctas = sms;  // one CTA per SM: fewer barrier arrivals
+    return CS_OK;
+}
+
+int gs_launch_prep(const Ctx* d_ctx, const GsBuffers* gb, uint32_t rows, cudaStream_t stream, int sms) {
+    const int wb = (int)std::max<size_t>(1, std::min<size_t>(((size_t)rows * 32 + 255) / 256, (size_t)sms * 16));
+    k_gs_rows<<<dim3(wb, 1), 256, 0, stream>>>(d_ctx);
+    size_t bytes = gb->cub_bytes;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(gb->cub_temp, bytes, gb->row_units, gb->row_start, (int)rows + 1,
+                                                  stream);
+    if (e == cudaSuccess) {
+        const int rb = (int)std::max<size_t>(1, std::min<size_t>(((size_t)rows + 255) / 256, (size_t)sms * 16));
+        k_gs_desc<<<dim3(rb, 1), 256, 0, stream>>>(d_ctx);
+        e = cudaMemsetAsync(gb->sync, 0, 4 * sizeof(uint32_t), stream);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(gb->result, 0, sizeof(ScResult), stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("grid solve prep: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+
+int gs_launch_solve(const Ctx* d_ctx, int ctas, float tol, uint32_t max_pairs, uint32_t check_every,
+                    cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctas, 1, 1);
+    cfg.blockDim = dim3(GS_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = (size_t)GS_DESC_SMEM * sizeof(GsDesc);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeCooperative;
+    attr.val.cooperative = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_gs_solve, d_ctx, tol, max_pairs, check_every);
+    if (e != cudaSuccess) {
+        set_error(std::string("grid solve launch: ") + cudaGetErrorString(e));
+        return CS_ERR_CUDA;
+    }
+    return CS_OK;
+}
+
 // The cluster solve of `instances` independent systems: one cluster of `ranks` CTAs each.
 int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,
                       uint32_t check_every, cudaStream_t stream, uint32_t p2p) {
@@ -2194,6 +2371,12 @@ int32_t cs_read_cell_kind(CsSim* s, int32_t* o) {
     CS_SIM(s);
     CS_PTR(o);
     return s->e->read_kind(o);
+}
+int32_t cs_read_solver_inputs(CsSim* s, float* fill, float* div) {
+    CS_SIM(s);
+    CS_PTR(fill);
+    CS_PTR(div);
+    return s->e->read_solver_inputs(fill, div);
 }
 int32_t cs_read_bed_lookup(CsSim* s, int32_t* o) {
     CS_SIM(s);

@@ -40,6 +40,7 @@ public:
     int read_gvel(float* out);
     int read_pressure(float* out);
     int read_kind(int32_t* out);
+    int read_solver_inputs(float* fill, float* div);
     int read_lookup(int32_t* out);
     int read_delta(int32_t* out);
     int read_sdf(float* out);
@@ -101,6 +102,7 @@ private:
     int enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, double& r1);
     int substep_graph(float sub_dt);
     int collect();          // read the solve totals of replayed substeps
+    int totals_error(const ScTotals& t, const ScTotals& before);
     struct GraphKey {
         uint32_t p2g_mode, check_every, max_sweeps, solve_mode, pressure_storage, rbgs_kernel, rbgs_pairs, warm_start;
         float residual_tol;
@@ -126,6 +128,13 @@ private:
     // cluster-resident solver
     DeviceBuffer sc_scratch_;  // every solver scratch buffer, laid out by sc_scratch_layout
     ScBuffers sc_buf_{};
+    // grid-wide solver (grids above kClusterMaxCells cells)
+    int gs_alloc();
+    int solve_grid(uint32_t& sweeps, double& r0, double& r1, bool& done);
+    bool use_cluster_solve() const;
+    DeviceBuffer gs_rows_, gs_desc_, gs_slots_, gs_misc_, gs_cub_;
+    GsBuffers gs_buf_{};
+    int gs_ctas_ = 0;          // CTAs of the cooperative launch (0: cannot launch)
     int sc_ranks_ = 0;      // cluster size usable for the solve (0 = unavailable)
     size_t sc_codes_ = 0;   // Morton codes covering the grid (power-of-two cube)
     int solve_cluster(uint32_t& sweeps, double& r0, double& r1, bool& done);

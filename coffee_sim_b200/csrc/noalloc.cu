@@ -98,6 +98,12 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
         cs::set_error("invalid argument to cs_pressure_solve_noalloc");
         return CS_ERR_INVALID_ARG;
     }
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cs::set_error("cs_pressure_solve_noalloc synchronises its stream and cannot run on a capturing stream");
+        return CS_ERR_INVALID_ARG;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cs::set_error("no CUDA device is current");
@@ -106,7 +112,6 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
     DeviceSlot* slot = nullptr;
     int rc = setup_device(dev, &slot);
     if (rc) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
     unsigned char* base = slot->base;
 
     uint32_t side = 1;
@@ -128,8 +133,9 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
     u.p_clamp = cs::FP_VALUE_LIMIT - 1.0f;
     u.p_limit = 3.0e38f;  // FP32 storage: no fixed-point range to respect
     u.fixed_point = 0;
-    // the solver reads the cell kind as lane 3 of the grid lanes
-    ctx.lanes = reinterpret_cast<int32_t*>(reinterpret_cast<uintptr_t>(kind) - 3 * (uintptr_t)cells * sizeof(int32_t));
+    // the solver reads the cell kind through ctx.kind and nothing through ctx.lanes
+    ctx.lanes = nullptr;
+    ctx.kind = kind;
     ctx.fill = const_cast<float*>(fill);
     ctx.divf = const_cast<float*>(div);
     ctx.pf = p_hi;
@@ -148,19 +154,34 @@ extern "C" int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t 
         return CS_ERR_CUDA;
     }
     if ((rc = cs::sc_launch_prep(dctx, &sb, codes, slot->ranks, 1, st, slot->sms))) return rc;
-    if ((rc = cs::sc_launch_cluster(dctx, slot->ranks, 1, residual_tol, max_pairs, check_every, st, 1u)))
-        return rc;
+    // Colours are first separated by point-to-point waits; if one of those bounded
+    // waits runs out (status 3) the solve is run again from the pressure reached so far
+    // with cluster barriers, which have no time limit to run out, as the engine does.
     cs::ScResult res;
-    e = cudaMemcpyAsync(&res, sb.result, sizeof(res), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
-        return CS_ERR_CUDA;
+    for (uint32_t p2p = 1;; p2p = 0) {
+        if ((rc = cs::sc_launch_cluster(dctx, slot->ranks, 1, residual_tol, max_pairs, check_every, st, p2p)))
+            return rc;
+        e = cudaMemcpyAsync(&res, sb.result, sizeof(res), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
+            return CS_ERR_CUDA;
+        }
+        if (res.status != 3 || p2p == 0) break;
+        e = cudaMemsetAsync(sb.result, 0, sizeof(cs::ScResult), st);
+        if (e != cudaSuccess) {
+            cs::set_error(std::string("cs_pressure_solve_noalloc: ") + cudaGetErrorString(e));
+            return CS_ERR_CUDA;
+        }
     }
     if (res.status == 2) {
         cs::set_error("the fluid cells exceed what the solver's thread-block cluster holds "
                       "(16 x 4095 cells, 4095 halo cells per CTA)");
         return CS_ERR_CAPACITY;
+    }
+    if (res.status == 3) {
+        cs::set_error("the cluster solve gave up waiting for a neighbouring CTA; p_hi/p_lo are not solved");
+        return CS_ERR_TIMEOUT;
     }
     if (res.status != 1) {
         cs::set_error("the cluster solve did not complete");

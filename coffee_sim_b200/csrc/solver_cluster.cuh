@@ -107,7 +107,7 @@ __global__ void k_sc_flags(const Ctx* __restrict__ cp, uint32_t codes) {
     const ScBuffers& sb = cp[blockIdx.y].sb;
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
-    const int32_t* kl = c.lanes + 3 * (size_t)u.cells;
+    const int32_t* kl = c.kind;
     CS_FOR(m, codes) {
         unsigned long long f = 0;
         uint32_t ci, par;
@@ -182,7 +182,7 @@ __global__ void k_sc_halo(const Ctx* __restrict__ cp) {
     const Params& u = c.u;
     const ScInfo& inf = *sb.info;
     if (inf.overflow || inf.chunk == 0) return;
-    const int32_t* kl = c.lanes + 3 * (size_t)u.cells;
+    const int32_t* kl = c.kind;
     const uint32_t sy = u.gx, sz = u.gx * u.gy;
     CS_FOR(ci, u.cells) {
         const uint16_t rc = sb.ref_of_cell[ci];
@@ -253,7 +253,8 @@ __global__ void k_sc_halo(const Ctx* __restrict__ cp) {
             sb.slot_ref[(((size_t)fq[f] * 3 + (g >> 1)) * 4096 + fj[f]) * 2 + (g & 1)] =
                 (uint16_t)(hs[f] < (uint32_t)SC_HALO ? SC_HALO0 + hs[f] : SC_DUMMY);
         }
-        const float rhs = div_load(c, ci) * sf / wmax(u.dt, 1e-6f);
+        // the cluster solve runs in FP32 pressure storage only, where the divergence is divf
+        const float rhs = c.divf[ci] * sf / wmax(u.dt, 1e-6f);
         bool sent = false;
 #pragma unroll
         for (int f = 0; f < 6; ++f) sent = sent || fq[f] != 0xffu;
@@ -596,7 +597,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 __global__ void k_sc_account(const ScResult* __restrict__ res, ScTotals* __restrict__ tot) {
     const ScResult r = *res;
     tot->runs += 1;
-    if (r.status != 1) {
+    if (r.status == 3) {
+        tot->timeouts += 1;
+    } else if (r.status != 1) {
         tot->failed += 1;
     } else {
         tot->sweeps += r.sweeps;

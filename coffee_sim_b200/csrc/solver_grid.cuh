@@ -1,0 +1,521 @@
+// solver_grid.cuh — the pressure solve of one substep in one cooperative launch over
+// the whole GPU, for grids whose fluid does not fit a thread-block cluster.
+//
+// It runs the mixed-precision red-black SOR refinement of k_refine_residual /
+// k_refine_sweep / k_refine_accumulate (pressure_update, shader.rs:1371-1453, swept
+// to an FP64 residual target) with the same per-cell arithmetic in the same face
+// order (-x,+x,-y,+y,-z,+z), so it gives the per-colour launches' pressures bit for
+// bit; only the FP64 norm sums are added in another order.  What changes is where
+// the work happens and how it is synchronised:
+//
+// Layout.  Every grid row (fixed y, z) that holds fluid keeps its cells in a row
+// segment [xlo, xlo + 64 n) with xlo a multiple of 64, n units of 64 cells.  A
+// segment stores its red cells first, then its black cells, so the 32 cells of one
+// colour of a unit are 32 consecutive slots: a warp's loads of its own cells and of
+// each neighbour row are single 128-byte rows, and a sweep touches only the rows that
+// hold fluid (the dense grid of a large pour is mostly air and solid).  Per slot:
+// (1/W, flags) and (correction, fill code) as float2, the residual g, dx^2 rhs, and
+// the pressure (hi, lo).  The flags give, per face, whether it is a fluid face with
+// weight > 0 (bits 0-5) or an air face with weight > 0 (bits 8-13), and whether all
+// fluid faces have weight 1, so neither pass recomputes a cell kind.
+//
+// Prep (k_gs_rows, a CUB scan, k_gs_desc) finds each row's fluid extent, numbers the
+// units and writes for every unit the slot offsets of its own row and of its four
+// neighbour rows for both colours (a neighbour cell's slot is offset + x / 2).
+//
+// Solve (k_gs_solve).  One CTA of 1024 threads per SM, launched cooperatively so all
+// are resident; CTA b owns a contiguous range of units, its warps take them in turn,
+// two units at a time with every load of both issued before any arithmetic.  The
+// colours of a red-black pair are separated by a grid-wide barrier (an arrival
+// counter and a generation word in global memory); neighbour values written by other
+// CTAs are read with L2 loads (ld.cg).  The last pair of a refinement cycle adds the
+// correction to the pressure as it goes (a cell's correction is final after its own
+// colour's sweep), so a residual check is one pass and one barrier: each CTA writes
+// its FP64 partial sums, and after the barrier every CTA adds all partials in CTA
+// order, so all take the same stop decision.  The check schedule is sc_next_interval,
+// the same as the oracle's.  Every barrier wait is bounded; a CTA whose wait runs out
+// raises an abort word that ends the other CTAs' waits too, and the solve reports
+// status 3 (the host then re-solves with per-colour launches).
+#pragma once
+#include <climits>
+
+#include "kernels.cuh"
+#include "solver_types.cuh"
+
+namespace cs {
+
+constexpr int GS_THREADS = 1024;
+constexpr int GS_UNIT = 64;                 // cells per unit (32 slots of each colour)
+constexpr uint32_t GS_FLUID_FACES = 0x3fu;  // bits 0-5: fluid face with weight > 0
+constexpr uint32_t GS_AIR_SHIFT = 8;        // bits 8-13: air face with weight > 0
+constexpr uint32_t GS_UNITW = 1u << 16;     // every fluid face has weight 1
+constexpr uint32_t GS_EMPTY = 1u << 17;     // no face with weight > 0, not fluid, or outside the grid
+constexpr uint32_t GS_ISFLUID = 1u << 18;   // fluid cell (its pressure is accumulated)
+constexpr long long kGsWaitCycles = 1ll << 31;  // ~1 s at 2 GHz
+constexpr int GS_DESC_SMEM = 1024;          // unit descriptors a CTA keeps in shared memory
+
+// Per unit: x of its first cell, y, z; own slot offsets for colours 0/1; neighbour row
+// offsets (colour 0/1) for y-1, y+1, z-1, z+1 (INT_MIN: the row holds no fluid).
+struct GsDesc {
+    int x0, y, z, pad;
+    int own[2];
+    int nb[4][2];
+};
+static_assert(sizeof(GsDesc) == 56, "unit descriptor layout");
+
+// Grid barrier words: [0] arrivals, [1] generation, [2] abort.
+__device__ __forceinline__ uint32_t gs_ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Returns false (on every thread of the CTA) once any CTA gave up waiting.
+__device__ __forceinline__ bool gs_grid_sync(uint32_t* sync, uint32_t nblocks, uint32_t& gen) {
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ok = 1u;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&sync[0], 1u);
+        if (arrived == nblocks - 1u) {
+            atomicExch(&sync[0], 0u);
+            __threadfence();
+            atomicExch(&sync[1], gen + 1u);
+        } else {
+            const long long t0 = clock64();
+            while (gs_ld_acquire(&sync[1]) == gen) {
+                if (gs_ld_acquire(&sync[2]) != 0u) {
+                    ok = 0u;
+                    break;
+                }
+                if (clock64() - t0 > kGsWaitCycles) {
+                    atomicExch(&sync[2], 1u);
+                    ok = 0u;
+                    break;
+                }
+            }
+        }
+        if (ok && gs_ld_acquire(&sync[2]) != 0u) ok = 0u;
+        __threadfence();
+        s_ok = ok;
+    }
+    ++gen;
+    __syncthreads();
+    return s_ok != 0u;
+}
+
+// ---------------- prep ----------------
+// Fluid extent of every row: one warp per row; units = ceil((x1 - xlo) / 64) with
+// xlo = x0 rounded down to a multiple of 64.
+__global__ void k_gs_rows(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const GsBuffers& gb = c.gs;
+    const uint32_t rows = u.gy * u.gz;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+        const int32_t* kr = c.kind + (size_t)r * u.gx;
+        int lo = INT_MAX, hi = -1;
+        for (uint32_t x0 = 0; x0 < u.gx; x0 += 32) {
+            const uint32_t x = x0 + lane;
+            const bool f = x < u.gx && is_fluid(kr[x]);
+            const uint32_t m = __ballot_sync(0xffffffffu, f);
+            if (m) {
+                lo = min(lo, (int)(x0 + __ffs(m) - 1));
+                hi = (int)(x0 + 31 - __clz(m));
+            }
+        }
+        if (lane == 0) {
+            uint32_t n = 0, xlo = 0;
+            if (hi >= 0) {
+                xlo = (uint32_t)lo & ~63u;
+                n = ((uint32_t)hi + 1u - xlo + 63u) / 64u;
+            }
+            gb.row_units[r] = n;
+            gb.row_xlo[r] = xlo;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) gb.row_units[rows] = 0u;
+}
+
+__device__ __forceinline__ void gs_row_offsets(const GsBuffers& gb, uint32_t q, int off[2]) {
+    const uint32_t n = gb.row_units[q];
+    if (n == 0) {
+        off[0] = off[1] = INT_MIN;
+        return;
+    }
+    const int base = (int)(gb.row_start[q] * (uint32_t)GS_UNIT);
+    const int xh = (int)(gb.row_xlo[q] >> 1);
+    off[0] = base - xh;
+    off[1] = base + (int)(32u * n) - xh;
+}
+
+// One descriptor per unit (threads over rows).
+__global__ void k_gs_desc(const Ctx* __restrict__ cp) {
+    const Ctx& c = cp[blockIdx.y];
+    const Params& u = c.u;
+    const GsBuffers& gb = c.gs;
+    const uint32_t rows = u.gy * u.gz;
+    CS_FOR(r, rows) {
+        const uint32_t n = gb.row_units[r];
+        if (n == 0) continue;
+        const uint32_t y = r % u.gy, z = r / u.gy;
+        GsDesc d;
+        d.y = (int)y;
+        d.z = (int)z;
+        d.pad = 0;
+        gs_row_offsets(gb, r, d.own);
+        const bool in[4] = {y > 0, y + 1 < u.gy, z > 0, z + 1 < u.gz};
+        const uint32_t q[4] = {r - 1u, r + 1u, r - u.gy, r + u.gy};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (in[k]) {
+                gs_row_offsets(gb, q[k], d.nb[k]);
+            } else {
+                d.nb[k][0] = d.nb[k][1] = INT_MIN;
+            }
+        }
+        const uint32_t u0 = gb.row_start[r];
+        for (uint32_t k = 0; k < n; ++k) {
+            d.x0 = (int)(gb.row_xlo[r] + 64u * k);
+            gb.desc[u0 + k] = d;
+        }
+    }
+}
+
+// ---------------- solve ----------------
+struct GsCell {
+    int slot;   // own slot
+    int x;      // grid x (>= gx: no cell)
+};
+
+__device__ __forceinline__ int gs_clamp_slot(int off, int x, int n_slots) {
+    if (off == INT_MIN) return 0;
+    const int s = off + (x >> 1);
+    return s < 0 ? 0 : (s >= n_slots ? n_slots - 1 : s);
+}
+
+// Slots of the six neighbours of cell x (colour c) of a unit; clamped into the arrays
+// so they can be loaded before the flags say which ones are real.
+__device__ __forceinline__ void gs_nb_slots(const GsDesc& d, int c, int x, int n_slots, int nb[6]) {
+    const int oc = c ^ 1;
+    nb[0] = gs_clamp_slot(d.own[oc], x - 1, n_slots);
+    nb[1] = gs_clamp_slot(d.own[oc], x + 1, n_slots);
+    nb[2] = gs_clamp_slot(d.nb[0][oc], x, n_slots);
+    nb[3] = gs_clamp_slot(d.nb[1][oc], x, n_slots);
+    nb[4] = gs_clamp_slot(d.nb[2][oc], x, n_slots);
+    nb[5] = gs_clamp_slot(d.nb[3][oc], x, n_slots);
+}
+
+__device__ __forceinline__ float gs_weight(float fc_i, float fc_j) {
+    return (fc_i > 1.5f || fc_j > 1.5f) ? 1.0f : fminf(fc_i, fc_j);
+}
+
+// Set-up of one slot from the dense arrays classify wrote: flags, 1/W, fill code,
+// dx^2 rhs and the starting pressure (the face weights of face_weight, shader.rs:306-323).
+__device__ __forceinline__ void gs_setup_cell(const Ctx& c, const GsBuffers& gb, const GsDesc& d, int col,
+                                              uint32_t lane) {
+    const Params& u = c.u;
+    const int s = d.own[col] + (d.x0 >> 1) + (int)lane;
+    const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+    uint32_t fl = GS_EMPTY;
+    float invW = 0.0f, fci = -1.0f, b = 0.0f;
+    float2 p = make_float2(0.0f, 0.0f);
+    if (x < (int)u.gx) {
+        const uint32_t ix = (uint32_t)x, iy = (uint32_t)d.y, iz = (uint32_t)d.z;
+        const uint32_t ci = cidx(u, ix, iy, iz);
+        const int32_t kind = c.kind[ci];
+        if (is_fluid(kind)) {
+            fl = GS_ISFLUID;
+            const float sf = c.fill[ci];
+            fci = kind == CELL_BED ? 2.0f : sf;
+            const uint32_t sy = u.gx, sz = u.gx * u.gy;
+            const bool in[6] = {ix > 0, ix + 1 < u.gx, iy > 0, iy + 1 < u.gy, iz > 0, iz + 1 < u.gz};
+            const uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
+            float W = 0.0f;
+            bool unit = true;
+#pragma unroll
+            for (int f = 0; f < 6; ++f) {
+                if (!in[f]) continue;
+                const uint32_t ni = ci + off[f];
+                const int32_t nk = c.kind[ni];
+                if (is_solid(nk)) continue;
+                const float w = face_weight(kind, sf, nk, c.fill[ni]);
+                if (!(w > 0.0f)) continue;
+                W += w;
+                if (is_fluid(nk)) {
+                    fl |= 1u << f;
+                    unit = unit && (w == 1.0f);
+                } else {
+                    fl |= 1u << (GS_AIR_SHIFT + f);
+                }
+            }
+            if (unit) fl |= GS_UNITW;
+            if (W > 0.0f) {
+                invW = 1.0f / W;
+            } else {
+                fl |= GS_EMPTY;
+            }
+            // the cluster and per-colour solves run in FP32 pressure storage only, where
+            // the divergence is divf
+            const float rhs = c.divf[ci] * sf / wmax(u.dt, 1e-6f);
+            b = u.dx * u.dx * rhs;
+            p = make_float2(c.pf[ci], c.plo[ci]);
+        }
+    }
+    gb.cf[s] = make_float2(invW, __uint_as_float(fl));
+    gb.dfc[s] = make_float2(0.0f, fci);
+    gb.g[s] = 0.0f;
+    gb.b[s] = b;
+    gb.p[s] = p;
+}
+
+// FP64 residual of one slot's cell; g <- r, d <- 0.  Returns (r^2, b^2) contributions.
+__device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDesc& d, int col, uint32_t lane,
+                                                 int n_slots, double& r2, double& b2) {
+    const int s = d.own[col] + (d.x0 >> 1) + (int)lane;
+    const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+    const float2 cf = gb.cf[s];
+    const uint32_t fl = __float_as_uint(cf.y);
+    gb.dfc[s].x = 0.0f;
+    if (fl & GS_EMPTY) {
+        gb.g[s] = 0.0f;
+        return;
+    }
+    int nb[6];
+    gs_nb_slots(d, col, x, n_slots, nb);
+    float2 pj[6];
+    float fj[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        pj[f] = __ldcg(gb.p + nb[f]);
+        fj[f] = __ldcg(&gb.dfc[nb[f]].y);
+    }
+    const float fci = gb.dfc[s].y;
+    const float sfi = fci > 1.5f ? 1.0f : fci;
+    const bool unit = (fl & GS_UNITW) != 0u;
+    double wsum = 0.0, psum = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (fl & (1u << f)) {
+            const float w = unit ? 1.0f : gs_weight(fci, fj[f]);
+            wsum += (double)w;
+            psum += (double)w * ((double)pj[f].x + (double)pj[f].y);
+        } else if (fl & (1u << (GS_AIR_SHIFT + f))) {
+            wsum += (double)sfi;
+        }
+    }
+    const float2 pi = gb.p[s];
+    const double bb = (double)gb.b[s];
+    const double r = (psum - bb) - wsum * ((double)pi.x + (double)pi.y);
+    gb.g[s] = (float)r;
+    r2 += r * r;
+    b2 += bb * bb;
+}
+
+// p <- p + d in FP64 (split back into hi/lo, clamped at the pressure limit).
+__device__ __forceinline__ void gs_accumulate(const Ctx& c, const GsBuffers& gb, int s, float dn) {
+    const float2 pi = gb.p[s];
+    double p = ((double)pi.x + (double)pi.y) + (double)dn;
+    const double lim = (double)c.u.p_limit;
+    if (p > lim || p < -lim) {
+        p = p > 0.0 ? lim : -lim;
+        atomicAdd(&c.metrics[M_P_CLAMP], 1u);
+    }
+    const float hi = (float)p;
+    gb.p[s] = make_float2(hi, (float)(p - (double)hi));
+}
+
+// One colour of one unit: the loaded inputs of a cell, then its update.
+struct GsLoad {
+    float2 cf, me;
+    float g;
+    float2 nb[6];
+    int s;
+};
+
+__device__ __forceinline__ void gs_load(const GsBuffers& gb, const GsDesc& d, int col, uint32_t lane, int n_slots,
+                                        GsLoad& L) {
+    L.s = d.own[col] + (d.x0 >> 1) + (int)lane;
+    const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+    int nb[6];
+    gs_nb_slots(d, col, x, n_slots, nb);
+    L.cf = gb.cf[L.s];
+    L.g = gb.g[L.s];
+    L.me = gb.dfc[L.s];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) L.nb[f] = __ldcg(gb.dfc + nb[f]);
+}
+
+__device__ __forceinline__ void gs_update(const Ctx& c, const GsBuffers& gb, const GsLoad& L, float omega,
+                                          bool last) {
+    const uint32_t fl = __float_as_uint(L.cf.y);
+    if (fl & GS_EMPTY) {
+        if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, L.s, L.me.x);
+        return;
+    }
+    float ds = 0.0f;
+    if (fl & GS_UNITW) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if (fl & (1u << f)) ds += L.nb[f].x;
+    } else {
+        const float fi = L.me.y;
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if (fl & (1u << f)) ds += gs_weight(fi, L.nb[f].y) * L.nb[f].x;
+    }
+    const float me = L.me.x;
+    float dn = (ds + L.g) * L.cf.x;
+    if (omega != 1.0f) dn = me + omega * (dn - me);
+    gb.dfc[L.s].x = dn;
+    if (last) gs_accumulate(c, gb, L.s, dn);
+}
+
+__global__ void __launch_bounds__(GS_THREADS, 1)
+    k_gs_solve(const Ctx* __restrict__ cp, float tol, uint32_t max_pairs, uint32_t check_every) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Ctx& c = cp[0];
+    const GsBuffers& gb = c.gs;
+    const Params& u = c.u;
+    GsDesc* sdesc = reinterpret_cast<GsDesc*>(smem);
+    __shared__ double s_red[2][32];
+    __shared__ double s_norm;
+    uint32_t* sync = gb.sync;
+    const uint32_t nb = gridDim.x;
+    uint32_t gen = 0;
+    const uint32_t rows = u.gy * u.gz;
+    const uint32_t n_units = gb.row_start[rows];
+    const int n_slots = (int)(n_units * (uint32_t)GS_UNIT) > 0 ? (int)(n_units * (uint32_t)GS_UNIT) : 1;
+    // this CTA's contiguous range of units
+    const uint32_t ua = (uint32_t)(((unsigned long long)n_units * blockIdx.x) / nb);
+    const uint32_t ue = (uint32_t)(((unsigned long long)n_units * (blockIdx.x + 1)) / nb);
+    const uint32_t nu = ue - ua;
+    const bool cached = nu <= (uint32_t)GS_DESC_SMEM;
+    if (cached)
+        for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) sdesc[k] = gb.desc[ua + k];
+    __syncthreads();
+    auto desc = [&](uint32_t k) -> GsDesc { return cached ? sdesc[k] : gb.desc[ua + k]; };
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+    // set-up of every slot of this CTA's units
+    for (uint32_t k = warp; k < nu; k += nwarps) {
+        const GsDesc d = desc(k);
+        gs_setup_cell(c, gb, d, 0, lane);
+        gs_setup_cell(c, gb, d, 1, lane);
+    }
+    bool ok = gs_grid_sync(sync, nb, gen);
+
+    // FP64 residual and the relative norm every CTA agrees on
+    auto residual = [&]() -> double {
+        double r2 = 0.0, b2 = 0.0;
+        for (uint32_t k = warp; k < nu; k += nwarps) {
+            const GsDesc d = desc(k);
+            gs_residual_cell(gb, d, 0, lane, n_slots, r2, b2);
+            gs_residual_cell(gb, d, 1, lane, n_slots, r2, b2);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            r2 += __shfl_down_sync(0xffffffffu, r2, o);
+            b2 += __shfl_down_sync(0xffffffffu, b2, o);
+        }
+        if (lane == 0) {
+            s_red[0][warp] = r2;
+            s_red[1][warp] = b2;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, bs = 0.0;
+            for (uint32_t w = 0; w < nwarps; ++w) {
+                a += s_red[0][w];
+                bs += s_red[1][w];
+            }
+            gb.part[2 * blockIdx.x] = a;
+            gb.part[2 * blockIdx.x + 1] = bs;
+        }
+        ok = ok && gs_grid_sync(sync, nb, gen);
+        if (threadIdx.x == 0) {
+            double a = 0.0, bs = 0.0;
+            for (uint32_t q = 0; q < nb; ++q) {
+                a += __ldcg(gb.part + 2 * q);
+                bs += __ldcg(gb.part + 2 * q + 1);
+            }
+            s_norm = bs <= 0.0 ? 0.0 : sqrt(a) / sqrt(bs);
+        }
+        __syncthreads();
+        return s_norm;
+    };
+
+    const float omega = u.omega;
+    // one colour over this CTA's units, two units per step with all loads in flight
+    auto sweep = [&](int col, bool last) {
+        uint32_t k = warp;
+        for (; k + nwarps < nu; k += 2 * nwarps) {
+            const GsDesc d0 = desc(k), d1 = desc(k + nwarps);
+            GsLoad a, b;
+            gs_load(gb, d0, col, lane, n_slots, a);
+            gs_load(gb, d1, col, lane, n_slots, b);
+            gs_update(c, gb, a, omega, last);
+            gs_update(c, gb, b, omega, last);
+        }
+        if (k < nu) {
+            const GsDesc d0 = desc(k);
+            GsLoad a;
+            gs_load(gb, d0, col, lane, n_slots, a);
+            gs_update(c, gb, a, omega, last);
+        }
+    };
+
+    double r0 = -1.0, r1 = -1.0;
+    uint32_t pairs = 0, evals = 0;
+    if (ok) {
+        r0 = residual();
+        r1 = r0;
+        evals = 1;
+    }
+    const uint32_t ce = check_every ? check_every : 10u;
+    uint32_t next = u.first_check ? u.first_check : ce;
+    while (ok && !(r1 <= (double)tol) && pairs < max_pairs) {
+        const uint32_t k = min(next, max_pairs - pairs);
+        for (uint32_t j = 0; j < k && ok; ++j) {
+            const bool last = j + 1 == k;
+            sweep(0, last);
+            ok = gs_grid_sync(sync, nb, gen);
+            if (!ok) break;
+            sweep(1, last);
+            ok = gs_grid_sync(sync, nb, gen);
+        }
+        if (!ok) break;
+        pairs += k;
+        const double r_before = r1;
+        r1 = residual();
+        ++evals;
+        next = sc_next_interval(r1, r_before, k, (double)tol, ce);
+    }
+    // the solved pressure back to the dense arrays
+    for (uint32_t k = warp; k < nu; k += nwarps) {
+        const GsDesc d = desc(k);
+#pragma unroll
+        for (int col = 0; col < 2; ++col) {
+            const int s = d.own[col] + (d.x0 >> 1) + (int)lane;
+            const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+            if (x >= (int)u.gx) continue;
+            if (!(__float_as_uint(gb.cf[s].y) & GS_ISFLUID)) continue;
+            const uint32_t ci = cidx(u, (uint32_t)x, (uint32_t)d.y, (uint32_t)d.z);
+            const float2 p = gb.p[s];
+            c.pf[ci] = p.x;
+            c.plo[ci] = p.y;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        gb.result->sweeps = pairs;
+        gb.result->evals = evals;
+        gb.result->r0 = r0;
+        gb.result->r1 = r1;
+        gb.result->status = ok ? 1u : 3u;
+        if (!ok) atomicOr(&c.metrics[M_TIMEOUT], 1u);
+    }
+}
+
+}  // namespace cs

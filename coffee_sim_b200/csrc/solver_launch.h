@@ -24,4 +24,14 @@ int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ra
 int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,
                       uint32_t check_every, cudaStream_t stream, uint32_t p2p);
 
+// Grid-wide solve (solver_grid.cuh) of one system.  Grids of at most kClusterMaxCells
+// cells are solved on a thread-block cluster by default, larger ones with this solve.
+constexpr size_t kClusterMaxCells = (size_t)1 << 18;
+constexpr uint32_t kGsPrepLaunches = 2;  // own kernels of gs_launch_prep per call
+// CTAs of the cooperative launch on the current device (0 if it cannot launch).
+int gs_blocks(int* ctas);
+int gs_launch_prep(const Ctx* d_ctx, const GsBuffers* gb, uint32_t rows, cudaStream_t stream, int sms);
+int gs_launch_solve(const Ctx* d_ctx, int ctas, float tol, uint32_t max_pairs, uint32_t check_every,
+                    cudaStream_t stream);
+
 }  // namespace cs

@@ -71,9 +71,11 @@ struct ScResult {
     uint32_t sweeps, evals, status, pad;
     double r0, r1;
 };
-// Running totals of the solves of replayed substeps (graph mode reads them lazily).
+// Running totals of the solves of replayed substeps (graph mode reads them lazily):
+// `failed` counts solves whose fluid did not fit (status 2), `timeouts` solves whose
+// bounded waits ran out (status 3).
 struct ScTotals {
-    unsigned long long sweeps, evals, failed, runs;
+    unsigned long long sweeps, evals, failed, runs, timeouts;
     ScResult last;
 };
 // counters: halo size per rank, send-list length per (rank, colour), then the halo
@@ -94,6 +96,25 @@ struct ScBuffers {
     ScInfo* info;
     ScResult* result;
     void* cub_temp;              // CUB scan storage (host-side launches)
+    size_t cub_bytes;
+};
+
+// Grid-wide solve (solver_grid.cuh): row segments of fluid cells, units of 64 cells.
+struct GsDesc;
+struct GsBuffers {
+    uint32_t* row_units;  // [rows + 1] units of each row (last entry 0)
+    uint32_t* row_start;  // [rows + 1] exclusive scan of row_units; row_start[rows] = units
+    uint32_t* row_xlo;    // [rows] first x of each row's segment (multiple of 64)
+    GsDesc* desc;         // [max_units] slot offsets of each unit and of its neighbour rows
+    float2* cf;           // [slots] 1/W, flags
+    float2* dfc;          // [slots] correction, fill code
+    float* g;             // [slots] FP64 residual of the cycle, rounded to fp32
+    float* b;             // [slots] dx^2 rhs
+    float2* p;            // [slots] pressure hi, lo
+    double* part;         // [2 * CTAs] per-CTA partial norms
+    uint32_t* sync;       // grid barrier: arrivals, generation, abort
+    ScResult* result;
+    void* cub_temp;
     size_t cub_bytes;
 };
 

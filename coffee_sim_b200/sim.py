@@ -289,6 +289,15 @@ class MpmSim3D:
     def read_cell_kind(self):
         return self._read_cells("cs_read_cell_kind", np.int32)
 
+    def read_solver_inputs(self):
+        """(fill, divergence) of every cell as classify wrote them for the pressure solve
+        (FP32 pressure storage)."""
+        n = self.settings.cells
+        fill, div = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.lib.call("cs_read_solver_inputs", self._h, fill.ctypes.data_as(C.POINTER(C.c_float)),
+                      div.ctypes.data_as(C.POINTER(C.c_float)))
+        return fill, div
+
     def read_bed_lookup(self):
         return self._read_cells("cs_read_bed_lookup", np.int32)
 

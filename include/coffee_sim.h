@@ -225,8 +225,11 @@ typedef struct CsSettings {
     uint32_t device_emission;     /* 1: emit jet particles with a kernel (graph-capturable) */
     uint32_t use_graph;           /* 1: capture the substep in a CUDA graph */
     int32_t device;               /* CUDA device ordinal */
-    uint32_t rbgs_kernel;         /* 0 auto, 1 per-colour launches, 2 cluster-resident solve,
-                                     3 cluster-resident with cluster barriers between colours */
+    uint32_t rbgs_kernel;         /* 0 auto (cluster-resident for grids of at most 2^18 cells,
+                                     grid-wide above), 1 per-colour launches, 2 cluster-resident
+                                     solve, 3 cluster-resident with cluster barriers between
+                                     colours, 4 grid-wide solve (one cooperative launch over
+                                     the rows that hold fluid) */
     float flow_override_ml_s;     /* >0: constant flow instead of the kettle-angle model */
     float exit_speed_override;    /* >0 with flow override: jet speed */
     float rbgs_omega;             /* red-black over-relaxation; 0 or 1 = plain Gauss-Seidel */
@@ -325,6 +328,11 @@ int32_t cs_read_bed_delta(CsSim* sim, int32_t* out);        /* 4 x max_particles
 int32_t cs_read_render(CsSim* sim, uint32_t first, uint32_t count, float* out);        /* 8 f32 each */
 int32_t cs_read_sdf(CsSim* sim, float* out);                /* 128^3 R32F texels */
 int32_t cs_read_sdf_class(CsSim* sim, uint8_t* out);        /* cells */
+/* The pressure solve's inputs as classify wrote them (no reference counterpart): the
+ * liquid fill fraction of every cell (liquid_fill_fraction, shader.rs:293-304) and the
+ * divergence the solve reads in FP32 pressure storage (CS_ERR_UNSUPPORTED with
+ * fixed-point storage).  cells f32 each. */
+int32_t cs_read_solver_inputs(CsSim* sim, float* fill, float* div);
 
 /* ---- upload from caller buffers ---- */
 int32_t cs_write_particles(CsSim* sim, uint32_t first, uint32_t count, const float* in);
@@ -482,10 +490,13 @@ int32_t cs_sync(CsSim* sim);
  * in, solution out).  Scratch lives in a static device array reserved when the
  * library is loaded (about 7.6 MB per GPU, held until exit), so grids are limited to
  * 64 cells per side and 16 x 4095 fluid cells; larger inputs return CS_ERR_CAPACITY.
- * The first call on a device looks up that array's device address; make it before
- * any stream capture.  Calls share the array: calls that overlap on the GPU race.
- * `stream` is a cudaStream_t (NULL = default stream); the call synchronises it and
- * writes the red+black pair count and the final relative residual to the host. */
+ * The first call on a device looks up that array's device address.  Calls share the
+ * array: calls that overlap on the GPU race.  `stream` is a cudaStream_t (NULL =
+ * default stream); every call synchronises it, so it must never be called on a
+ * capturing stream (CS_ERR_INVALID_ARG).  It writes the red+black pair count and the
+ * final relative residual to the host.  After a call that returns an error, p_hi and
+ * p_lo hold unspecified values (a partly solved pressure); CS_ERR_TIMEOUT means a
+ * bounded wait between CTAs ran out twice. */
 int32_t cs_pressure_solve_noalloc(uint32_t gx, uint32_t gy, uint32_t gz, float dx, float dt, float omega,
                                   float residual_tol, uint32_t max_pairs, uint32_t check_every,
                                   const int32_t* kind, const float* fill, const float* div, float* p_hi,

@@ -101,7 +101,7 @@ struct SimBase {
 };
 
 enum { RD_PART, RD_AFF, RD_BEDX, RD_LANES, RD_GVEL, RD_P, RD_KIND, RD_LOOKUP, RD_DELTA, RD_RENDER, RD_SDF, RD_CLASS, RD_LANES64,
-       RD_DIV };
+       RD_DIV, RD_FILL };
 
 template <class R>
 struct Sim : SimBase {
@@ -1898,6 +1898,9 @@ struct Sim : SimBase {
                 break;
             case RD_KIND: for (size_t c = 0; c < cells; ++c) i[c] = grid[3 * cells + c]; break;
             case RD_DIV: for (size_t c = 0; c < cells; ++c) f[c] = (float)div_load((uint32_t)c); break;
+            case RD_FILL:
+                for (size_t c = 0; c < cells; ++c) f[c] = (float)liquid_fill((uint32_t)c, grid[3 * cells + c]);
+                break;
             case RD_LOOKUP: for (size_t c = 0; c < cells; ++c) i[c] = lookup[c]; break;
             case RD_DELTA: for (size_t k = 0; k < delta.size(); ++k) i[k] = delta[k]; break;
             case RD_SDF: std::memcpy(out, sdf.data(), sdf.size() * 4); break;
@@ -2176,6 +2179,14 @@ int32_t cs_read_bed_delta(CsSim* s, int32_t* o) { return rd(s, RD_DELTA, 0, 0, o
 int32_t cs_read_render(CsSim* s, uint32_t f, uint32_t c, float* o) { return rd(s, RD_RENDER, f, c, o); }
 int32_t cs_read_sdf(CsSim* s, float* o) { return rd(s, RD_SDF, 0, 0, o); }
 int32_t cs_read_sdf_class(CsSim* s, uint8_t* o) { return rd(s, RD_CLASS, 0, 0, o); }
+int32_t cs_read_solver_inputs(CsSim* s, float* fill, float* div) {
+    if (!s || !fill || !div) return fail(CS_ERR_INVALID_ARG, "null");
+    if (s->impl->settings.pressure_storage == CS_PRESSURE_FIXED_POINT)
+        return fail(CS_ERR_UNSUPPORTED, "the solver's divergence array exists in FP32 pressure storage only");
+    s->impl->read(RD_FILL, 0, 0, fill);
+    s->impl->read(RD_DIV, 0, 0, div);
+    return CS_OK;
+}
 
 static int wr(CsSim* sim, int what, uint32_t first, uint32_t count, const void* in) {
     if (!sim || !in) return fail(CS_ERR_INVALID_ARG, "null");

@@ -300,3 +300,36 @@ def test_graph_frames_match_oracle_reference_mode(engine, oracle):
         e.step_frame(FRAME)
         o.step_frame(FRAME)
         _assert_same(_state(e, cells=False), _state(o, cells=False), f"graph frame {f}")
+
+
+def test_prepare_render_matches_oracle(engine, oracle, center_pour_state):
+    """prepare_render (shader.rs:2242-2276) into the headless render buffer: 2 x vec4
+    per sample in the layout of state.rs:136-144 (position + colour value, radius),
+    compared with the oracle's after a full substep of the centre pour, and checked
+    against the properties the shader gives it: live samples carry their position,
+    water a speed colour in [0, 2], bed samples -1 - saturation, inactive samples
+    the parked position y = -1e6 with colour -999."""
+    settings, src = center_pour_state
+    e, o = pair(settings, engine, oracle)
+    copy_state(src, e)
+    copy_state(src, o)
+    for sim in (e, o):
+        sim.set_kettle_angle(36.0)
+        sim.step_substep(FRAME / 10)
+    n = e.particle_count()
+    assert n == o.particle_count() > 12000
+    re, ro = e.read_render(0, n), o.read_render(0, n)
+    assert re.shape == (n, 8)
+    assert mismatch(re, ro) == 0, relerr(re, ro)
+    parts = e.read_particles(0, n)
+    live = re[:, 3] != -999.0
+    assert live.sum() > 12000
+    assert np.array_equal(re[live, 0:3], parts[live, 0:3])
+    water = live & (re[:, 3] >= 0.0)
+    bed = live & (re[:, 3] < 0.0)
+    assert water.sum() > 0 and bed.sum() > 0
+    assert re[water, 3].max() <= 2.0
+    assert np.all(re[bed, 3] <= -1.0)
+    assert np.all(re[live, 4] > 0.0)          # radius
+    assert np.all(re[~live, 1] == -1e6)
+    assert np.all(re[:, 5:8] == 0.0)

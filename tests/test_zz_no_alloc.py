@@ -8,8 +8,11 @@ and volume lanes right after classify - rebuilds the fill fraction and divergenc
 exactly as classify computes them (float32, same operation order), runs the
 allocation-free solve twice in a row on copies of those inputs, and compares each
 result with the pressure the engine's own solve produced from the same state, to
-the 1e-5 relative tolerance of the solver's parity tests.  Kept in its own file so
-pytest collects it last.
+the 1e-5 relative tolerance of the solver's parity tests.  A second case takes a V60
+pour at 32^3, whose pressure system has solid faces (the cone wall) and bed-coupled
+faces (the coffee bed), with the fill and divergence read back from the engine.  Both
+check that the calls allocate nothing: the device's free memory is the same before
+and after the second call.  Kept in its own file so pytest collects it last.
 """
 import ctypes as C
 
@@ -89,7 +92,7 @@ def _classify_inputs(s, kind, lanes, gvel):
 
 
 def test_noalloc_solve_matches_engine_solve(engine):
-    torch = pytest.importorskip("torch")
+    pytest.importorskip("torch")
     s = _settings(engine)
     a, b = MpmSim3D(s, engine), MpmSim3D(s, engine)
     assert _pool(a) == _pool(b) > 0
@@ -104,26 +107,71 @@ def test_noalloc_solve_matches_engine_solve(engine):
     mb = b.latest_metrics()
     assert mb.last_sweeps > 0 and np.abs(want).max() > 0
 
+    _solve_twice_and_compare(engine, s, kind, fill, div, want, mb, scenes.C1_DT, omega=1.9)
+    a.close()
+    b.close()
+
+
+def _solve_twice_and_compare(engine, s, kind, fill, div, want, mb, dt, omega):
+    """Two allocation-free solves in a row on the same inputs, each from a zero
+    pressure, against the engine's solved pressure; the device's free memory is read
+    after the first call and must be unchanged after the second."""
+    import torch
     g = [int(v) for v in s.raw.grid_dims]
     dev = torch.device("cuda", 0)
     d_kind = torch.from_numpy(kind.astype(np.int32)).to(dev)
     d_fill = torch.from_numpy(fill).to(dev)
     d_div = torch.from_numpy(div).to(dev)
+    p_hi = torch.zeros(kind.size, dtype=torch.float32, device=dev)
+    p_lo = torch.zeros(kind.size, dtype=torch.float32, device=dev)
     dx = F(s.raw.bounds_size[0]) / F(g[0])
+    free_after_first = None
     for call in range(2):
-        p_hi = torch.zeros(kind.size, dtype=torch.float32, device=dev)
-        p_lo = torch.zeros(kind.size, dtype=torch.float32, device=dev)
+        p_hi.zero_()
+        p_lo.zero_()
         torch.cuda.synchronize()
         pairs, res = C.c_uint32(), C.c_double()
-        engine.call("cs_pressure_solve_noalloc", g[0], g[1], g[2], C.c_float(dx), C.c_float(scenes.C1_DT),
-                    C.c_float(1.9), C.c_float(1e-5), 2000, 10, C.c_void_p(d_kind.data_ptr()),
+        engine.call("cs_pressure_solve_noalloc", g[0], g[1], g[2], C.c_float(dx), C.c_float(dt),
+                    C.c_float(omega), C.c_float(1e-5), 2000, int(s.raw.check_every), C.c_void_p(d_kind.data_ptr()),
                     C.c_void_p(d_fill.data_ptr()), C.c_void_p(d_div.data_ptr()), C.c_void_p(p_hi.data_ptr()),
                     C.c_void_p(p_lo.data_ptr()), None, C.byref(pairs), C.byref(res))
+        torch.cuda.synchronize()
+        if call == 0:
+            free_after_first = torch.cuda.mem_get_info(dev)[0]
+        else:
+            assert torch.cuda.mem_get_info(dev)[0] == free_after_first, "the second call allocated device memory"
         got = p_hi.cpu().numpy()
         err = np.linalg.norm(got.astype(np.float64) - want) / np.linalg.norm(want.astype(np.float64))
         assert err <= 1e-5, (call, err)
         assert res.value <= 1e-5
         assert abs(int(pairs.value) - int(mb.last_sweeps)) <= 10, (pairs.value, mb.last_sweeps)
+
+
+def test_noalloc_solve_with_solid_and_bed_faces(engine):
+    """V60 pour at 32^3 (cone wall: solid faces; coffee bed: bed-coupled faces of
+    weight 1): the allocation-free solve on the fill and divergence classify wrote
+    matches the engine's solve of the same state."""
+    pytest.importorskip("torch")
+    s = scenes.c2_v60(engine, grid=32, max_particles=60000)
+    r = s.raw
+    r.warm_start = _ffi.CS_WARM_NONE
+    r.rbgs_omega = 1.9
+    a, b = MpmSim3D(s, engine), MpmSim3D(s, engine)
+    assert scenes.populate_c2(a) == scenes.populate_c2(b) > 0
+    for _ in range(4):
+        a.step_substep(scenes.C2_DT)
+        b.step_substep(scenes.C2_DT)
+    a.step_substep_partial(scenes.C2_DT, 7)   # through classify: solver inputs
+    b.step_substep_partial(scenes.C2_DT, 8)   # through the pressure solve: reference output
+    kind = a.read_cell_kind()
+    assert (kind == 3).sum() > 0 and (kind == 4).sum() > 0  # bed-coupled and solid cells
+    fill, div = a.read_solver_inputs()
+    want = b.read_pressure()
+    mb = b.latest_metrics()
+    assert mb.last_sweeps > 0 and np.abs(want).max() > 0
+    _solve_twice_and_compare(engine, s, kind, fill, div, want, mb, scenes.C2_DT, omega=1.9)
+    a.close()
+    b.close()
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch(engine):
