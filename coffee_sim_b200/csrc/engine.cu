@@ -430,7 +430,7 @@ int Engine::gs_alloc() {
     int rc;
     if ((rc = alloc(gs_rows_, (2 * (rows + 1) + rows) * sizeof(uint32_t)))) return rc;
     if ((rc = alloc(gs_desc_, units * sizeof(GsDesc)))) return rc;
-    if ((rc = alloc(gs_slots_, slots * (3 * sizeof(float2) + 2 * sizeof(float))))) return rc;
+    if ((rc = alloc(gs_slots_, slots * (sizeof(float2) + 5 * sizeof(float) + sizeof(uint16_t))))) return rc;
     if ((rc = gs_blocks(&gs_ctas_))) return rc;
     if ((rc = alloc(gs_misc_, sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)) + 256 +
                                   sc_align(sizeof(ScResult))))) return rc;
@@ -444,11 +444,14 @@ int Engine::gs_alloc() {
     g.row_xlo = r + 2 * (rows + 1);
     g.desc = (GsDesc*)gs_desc_.ptr;
     unsigned char* sl = (unsigned char*)gs_slots_.ptr;
-    g.cf = (float2*)sl;
-    g.dfc = (float2*)(sl + slots * sizeof(float2));
-    g.p = (float2*)(sl + 2 * slots * sizeof(float2));
-    g.g = (float*)(sl + 3 * slots * sizeof(float2));
-    g.b = (float*)(sl + 3 * slots * sizeof(float2) + slots * sizeof(float));
+    g.p = (float2*)sl;
+    float* f = (float*)(sl + slots * sizeof(float2));
+    g.d = f;
+    g.g = f + slots;
+    g.invw = f + 2 * slots;
+    g.fc = f + 3 * slots;
+    g.b = f + 4 * slots;
+    g.fl = (uint16_t*)(f + 5 * slots);
     unsigned char* m = (unsigned char*)gs_misc_.ptr;
     g.part = (double*)m;
     g.sync = (uint32_t*)(m + sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)));
@@ -1954,7 +1957,7 @@ int gs_blocks(int* ctas) {
     if (cudaGetDevice(&dev) != cudaSuccess) return CS_OK;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return CS_OK;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return CS_OK;
-    const size_t smem = (size_t)GS_DESC_SMEM * sizeof(GsDesc);
+    const size_t smem = (size_t)GS_SMEM;
     if (cudaFuncSetAttribute(k_gs_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return CS_OK;
@@ -1993,7 +1996,7 @@ int gs_launch_solve(const Ctx* d_ctx, int ctas, float tol, uint32_t max_pairs, u
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ctas, 1, 1);
     cfg.blockDim = dim3(GS_THREADS, 1, 1);
-    cfg.dynamicSmemBytes = (size_t)GS_DESC_SMEM * sizeof(GsDesc);
+    cfg.dynamicSmemBytes = (size_t)GS_SMEM;
     cfg.stream = stream;
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeCooperative;
@@ -2068,7 +2071,7 @@ static int validate(const CsSettings* s) {
         return CS_ERR_INVALID_ARG;
     }
     if (s->p2g_mode > CS_P2G_INT64 || s->warm_start > CS_WARM_LEARNED || s->pressure_storage > CS_PRESSURE_FP32 ||
-        s->solve_mode > CS_SOLVE_RESIDUAL || s->rbgs_kernel > 3) {
+        s->solve_mode > CS_SOLVE_RESIDUAL || s->rbgs_kernel > 4) {
         set_error("unknown mode value in settings");
         return CS_ERR_INVALID_ARG;
     }
@@ -2076,7 +2079,7 @@ static int validate(const CsSettings* s) {
     if (s->use_graph && (!s->device_emission || (s->solve_mode == CS_SOLVE_RESIDUAL &&
                                                   (s->pressure_storage != CS_PRESSURE_FP32 || s->rbgs_kernel == 1)))) {
         set_error("use_graph needs device_emission = 1 and, in residual mode, FP32 storage with the "
-                  "cluster-resident solve");
+                  "cluster-resident or the grid-wide solve");
         return CS_ERR_INVALID_ARG;
     }
     if (s->warm_start == CS_WARM_LEARNED &&

@@ -13,29 +13,33 @@
 // segment stores its red cells first, then its black cells, so the 32 cells of one
 // colour of a unit are 32 consecutive slots: a warp's loads of its own cells and of
 // each neighbour row are single 128-byte rows, and a sweep touches only the rows that
-// hold fluid (the dense grid of a large pour is mostly air and solid).  Per slot:
-// (1/W, flags) and (correction, fill code) as float2, the residual g, dx^2 rhs, and
-// the pressure (hi, lo).  The flags give, per face, whether it is a fluid face with
-// weight > 0 (bits 0-5) or an air face with weight > 0 (bits 8-13), and whether all
-// fluid faces have weight 1, so neither pass recomputes a cell kind.
+// hold fluid (the dense grid of a large pour is mostly air and solid).  Per slot, in
+// global memory: the correction d, the residual g, 1/W, the fill code, dx^2 rhs, the
+// pressure (hi, lo) and 16 flag bits giving, per face, whether it is a fluid face
+// with weight > 0 (bits 0-5) or an air face with weight > 0 (bits 8-13), and whether
+// all fluid faces have weight 1, so no pass recomputes a cell kind.
 //
 // Prep (k_gs_rows, a CUB scan, k_gs_desc) finds each row's fluid extent, numbers the
-// units and writes for every unit the slot offsets of its own row and of its four
-// neighbour rows for both colours (a neighbour cell's slot is offset + x / 2).
+// units and writes for every unit its own row's and its four neighbour rows' first
+// slot, colour-half length and first x (a neighbour cell's slot follows from its x).
 //
 // Solve (k_gs_solve).  One CTA of 1024 threads per SM, launched cooperatively so all
-// are resident; CTA b owns a contiguous range of units, its warps take them in turn,
-// two units at a time with every load of both issued before any arithmetic.  The
-// colours of a red-black pair are separated by a grid-wide barrier (an arrival
-// counter and a generation word in global memory); neighbour values written by other
-// CTAs are read with L2 loads (ld.cg).  The last pair of a refinement cycle adds the
-// correction to the pressure as it goes (a cell's correction is final after its own
-// colour's sweep), so a residual check is one pass and one barrier: each CTA writes
-// its FP64 partial sums, and after the barrier every CTA adds all partials in CTA
-// order, so all take the same stop decision.  The check schedule is sc_next_interval,
-// the same as the oracle's.  Every barrier wait is bounded; a CTA whose wait runs out
-// raises an abort word that ends the other CTAs' waits too, and the solve reports
-// status 3 (the host then re-solves with per-colour launches).
+// are resident.  CTA b owns whole rows, about 1/148 of the units, so its slots are one
+// contiguous range; when they fit (about 190 units) the CTA keeps their d, g, 1/W,
+// fill code and flags in shared memory for the whole solve, and writes each new d to
+// global memory only for the other CTAs to read.  A warp sweeps its units two at a
+// time: first the L2 loads (ld.cg) of the neighbour values held by other CTAs (rows at
+// z +- 1, and y +- 1 at the ends of the CTA's range), all in flight together, then the
+// updates from shared memory.  The colours of a red-black pair are separated by a
+// grid-wide barrier (a monotonic arrival counter: a release add per CTA, acquire
+// polling).  The last pair of a refinement cycle adds the correction to the pressure
+// as it goes (a cell's correction is final after its own colour's sweep), so a
+// residual check is one pass and one barrier: each CTA writes its FP64 partial sums,
+// and after the barrier every CTA adds all partials in CTA order, so all take the same
+// stop decision.  The check schedule is sc_next_interval, the same as the oracle's.
+// Every barrier wait is bounded; a CTA whose wait runs out raises an abort word that
+// ends the other CTAs' waits too, and the solve reports status 3 (the host then
+// re-solves with per-colour launches).
 #pragma once
 #include <climits>
 
@@ -46,61 +50,68 @@ namespace cs {
 
 constexpr int GS_THREADS = 1024;
 constexpr int GS_UNIT = 64;                 // cells per unit (32 slots of each colour)
+constexpr int GS_BATCH = 2;                 // units a warp sweeps with their remote loads in flight together
+// per-slot flags (16 bits)
 constexpr uint32_t GS_FLUID_FACES = 0x3fu;  // bits 0-5: fluid face with weight > 0
+constexpr uint32_t GS_UNITW = 1u << 6;      // every fluid face has weight 1
+constexpr uint32_t GS_EMPTY = 1u << 7;      // no face with weight > 0, not fluid, or outside the grid
 constexpr uint32_t GS_AIR_SHIFT = 8;        // bits 8-13: air face with weight > 0
-constexpr uint32_t GS_UNITW = 1u << 16;     // every fluid face has weight 1
-constexpr uint32_t GS_EMPTY = 1u << 17;     // no face with weight > 0, not fluid, or outside the grid
-constexpr uint32_t GS_ISFLUID = 1u << 18;   // fluid cell (its pressure is accumulated)
+constexpr uint32_t GS_ISFLUID = 1u << 14;   // fluid cell (its pressure is accumulated)
 constexpr long long kGsWaitCycles = 1ll << 31;  // ~1 s at 2 GHz
-constexpr int GS_DESC_SMEM = 1024;          // unit descriptors a CTA keeps in shared memory
+constexpr int GS_SMEM = 230400;             // dynamic shared memory of a solve CTA
+constexpr int GS_SLOT_SMEM = 18;            // shared bytes per resident slot: d, g, 1/W, fill code, flags
 
-// Per unit: x of its first cell, y, z; own slot offsets for colours 0/1; neighbour row
-// offsets (colour 0/1) for y-1, y+1, z-1, z+1 (INT_MIN: the row holds no fluid).
-struct GsDesc {
-    int x0, y, z, pad;
-    int own[2];
-    int nb[4][2];
+// Per unit: x of its first cell, y, z, and for its own row and the four neighbour rows
+// (y-1, y+1, z-1, z+1) the row's first slot (INT_MIN: no fluid in it), the slots per
+// colour half and the segment's first x.  Cell x of a row holds slot
+// base + colour * half + (x - xlo) / 2.  `nonunit` bit c: a cell of colour c has a
+// fluid face of weight below 1 (written by the solve's set-up).
+struct GsRow {
+    int base, half, xlo;
 };
-static_assert(sizeof(GsDesc) == 56, "unit descriptor layout");
+struct GsDesc {
+    int x0, y, z, nonunit;
+    GsRow row[5];
+};
+static_assert(sizeof(GsDesc) == 76, "unit descriptor layout");
 
-// Grid barrier words: [0] arrivals, [1] generation, [2] abort.
+// Grid barrier words: [0] arrivals (monotonic: after the g-th barrier it is g times the
+// CTA count), [2] abort.  Thread 0 of each CTA adds its arrival with a release add after
+// the CTA barrier and polls with acquire loads, so every write a CTA made before the
+// barrier is visible to every CTA after it.
 __device__ __forceinline__ uint32_t gs_ld_acquire(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ void gs_red_release(uint32_t* p, uint32_t v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // Returns false (on every thread of the CTA) once any CTA gave up waiting.
 __device__ __forceinline__ bool gs_grid_sync(uint32_t* sync, uint32_t nblocks, uint32_t& gen) {
     __shared__ uint32_t s_ok;
     __syncthreads();
+    ++gen;
     if (threadIdx.x == 0) {
         uint32_t ok = 1u;
-        __threadfence();
-        const uint32_t arrived = atomicAdd(&sync[0], 1u);
-        if (arrived == nblocks - 1u) {
-            atomicExch(&sync[0], 0u);
-            __threadfence();
-            atomicExch(&sync[1], gen + 1u);
-        } else {
-            const long long t0 = clock64();
-            while (gs_ld_acquire(&sync[1]) == gen) {
-                if (gs_ld_acquire(&sync[2]) != 0u) {
-                    ok = 0u;
-                    break;
-                }
-                if (clock64() - t0 > kGsWaitCycles) {
-                    atomicExch(&sync[2], 1u);
-                    ok = 0u;
-                    break;
-                }
+        gs_red_release(&sync[0], 1u);
+        const uint32_t target = nblocks * gen;
+        const long long t0 = clock64();
+        while ((int)(gs_ld_acquire(&sync[0]) - target) < 0) {
+            if (gs_ld_acquire(&sync[2]) != 0u) {
+                ok = 0u;
+                break;
+            }
+            if (clock64() - t0 > kGsWaitCycles) {
+                atomicExch(&sync[2], 1u);
+                ok = 0u;
+                break;
             }
         }
         if (ok && gs_ld_acquire(&sync[2]) != 0u) ok = 0u;
-        __threadfence();
         s_ok = ok;
     }
-    ++gen;
     __syncthreads();
     return s_ok != 0u;
 }
@@ -140,16 +151,13 @@ __global__ void k_gs_rows(const Ctx* __restrict__ cp) {
     if (blockIdx.x == 0 && threadIdx.x == 0) gb.row_units[rows] = 0u;
 }
 
-__device__ __forceinline__ void gs_row_offsets(const GsBuffers& gb, uint32_t q, int off[2]) {
+__device__ __forceinline__ GsRow gs_row_info(const GsBuffers& gb, uint32_t q) {
+    GsRow r;
     const uint32_t n = gb.row_units[q];
-    if (n == 0) {
-        off[0] = off[1] = INT_MIN;
-        return;
-    }
-    const int base = (int)(gb.row_start[q] * (uint32_t)GS_UNIT);
-    const int xh = (int)(gb.row_xlo[q] >> 1);
-    off[0] = base - xh;
-    off[1] = base + (int)(32u * n) - xh;
+    r.base = n ? (int)(gb.row_start[q] * (uint32_t)GS_UNIT) : INT_MIN;
+    r.half = (int)(32u * n);
+    r.xlo = (int)gb.row_xlo[q];
+    return r;
 }
 
 // One descriptor per unit (threads over rows).
@@ -165,16 +173,18 @@ __global__ void k_gs_desc(const Ctx* __restrict__ cp) {
         GsDesc d;
         d.y = (int)y;
         d.z = (int)z;
-        d.pad = 0;
-        gs_row_offsets(gb, r, d.own);
+        d.nonunit = 0;
+        d.row[0] = gs_row_info(gb, r);
         const bool in[4] = {y > 0, y + 1 < u.gy, z > 0, z + 1 < u.gz};
         const uint32_t q[4] = {r - 1u, r + 1u, r - u.gy, r + u.gy};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (in[k]) {
-                gs_row_offsets(gb, q[k], d.nb[k]);
+                d.row[k + 1] = gs_row_info(gb, q[k]);
             } else {
-                d.nb[k][0] = d.nb[k][1] = INT_MIN;
+                d.row[k + 1].base = INT_MIN;
+                d.row[k + 1].half = 0;
+                d.row[k + 1].xlo = 0;
             }
         }
         const uint32_t u0 = gb.row_start[r];
@@ -186,40 +196,50 @@ __global__ void k_gs_desc(const Ctx* __restrict__ cp) {
 }
 
 // ---------------- solve ----------------
-struct GsCell {
-    int slot;   // own slot
-    int x;      // grid x (>= gx: no cell)
-};
-
-__device__ __forceinline__ int gs_clamp_slot(int off, int x, int n_slots) {
-    if (off == INT_MIN) return 0;
-    const int s = off + (x >> 1);
-    return s < 0 ? 0 : (s >= n_slots ? n_slots - 1 : s);
-}
-
-// Slots of the six neighbours of cell x (colour c) of a unit; clamped into the arrays
-// so they can be loaded before the flags say which ones are real.
-__device__ __forceinline__ void gs_nb_slots(const GsDesc& d, int c, int x, int n_slots, int nb[6]) {
-    const int oc = c ^ 1;
-    nb[0] = gs_clamp_slot(d.own[oc], x - 1, n_slots);
-    nb[1] = gs_clamp_slot(d.own[oc], x + 1, n_slots);
-    nb[2] = gs_clamp_slot(d.nb[0][oc], x, n_slots);
-    nb[3] = gs_clamp_slot(d.nb[1][oc], x, n_slots);
-    nb[4] = gs_clamp_slot(d.nb[2][oc], x, n_slots);
-    nb[5] = gs_clamp_slot(d.nb[3][oc], x, n_slots);
-}
-
 __device__ __forceinline__ float gs_weight(float fc_i, float fc_j) {
     return (fc_i > 1.5f || fc_j > 1.5f) ? 1.0f : fminf(fc_i, fc_j);
 }
 
+// Cell x (colour col) of row r sits in slot base + col * half + (x - xlo) / 2.
+__device__ __forceinline__ int gs_slot(const GsRow& r, int col, int x) {
+    return r.base + col * r.half + ((x - r.xlo) >> 1);
+}
+
+// The state of a CTA's own slots: in shared memory when they fit there (resident),
+// else the global arrays themselves.  Element i is slot base + i.
+struct GsView {
+    float* d;
+    float* g;
+    float* invw;
+    float* fc;
+    uint16_t* fl;
+    int base;
+};
+
+// First unit of CTA b: its share of the units rounded to a whole row, so that every
+// CTA owns whole rows and its slots are one contiguous range.
+__device__ __forceinline__ uint32_t gs_cta_first_unit(const GsBuffers& gb, uint32_t rows, uint32_t n_units,
+                                                      uint32_t b, uint32_t nb) {
+    const uint32_t target = (uint32_t)(((unsigned long long)n_units * b) / nb);
+    uint32_t lo = 0, hi = rows;  // first row r with row_start[r] >= target
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (gb.row_start[mid] >= target)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return gb.row_start[lo];
+}
+
 // Set-up of one slot from the dense arrays classify wrote: flags, 1/W, fill code,
-// dx^2 rhs and the starting pressure (the face weights of face_weight, shader.rs:306-323).
-__device__ __forceinline__ void gs_setup_cell(const Ctx& c, const GsBuffers& gb, const GsDesc& d, int col,
-                                              uint32_t lane) {
+// dx^2 rhs and the starting pressure (the face weights of face_weight,
+// shader.rs:306-323).  Returns whether the cell has a fluid face of weight below 1.
+__device__ __forceinline__ bool gs_setup_cell(const Ctx& c, const GsBuffers& gb, const GsDesc& d, int col,
+                                              uint32_t lane, const GsView& own, bool resident) {
     const Params& u = c.u;
-    const int s = d.own[col] + (d.x0 >> 1) + (int)lane;
     const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+    const int s = gs_slot(d.row[0], col, x);
     uint32_t fl = GS_EMPTY;
     float invW = 0.0f, fci = -1.0f, b = 0.0f;
     float2 p = make_float2(0.0f, 0.0f);
@@ -258,44 +278,64 @@ __device__ __forceinline__ void gs_setup_cell(const Ctx& c, const GsBuffers& gb,
             } else {
                 fl |= GS_EMPTY;
             }
-            // the cluster and per-colour solves run in FP32 pressure storage only, where
-            // the divergence is divf
+            // the refinement solves run in FP32 pressure storage only, where the
+            // divergence is divf
             const float rhs = c.divf[ci] * sf / wmax(u.dt, 1e-6f);
             b = u.dx * u.dx * rhs;
             p = make_float2(c.pf[ci], c.plo[ci]);
         }
     }
-    gb.cf[s] = make_float2(invW, __uint_as_float(fl));
-    gb.dfc[s] = make_float2(0.0f, fci);
+    gb.invw[s] = invW;
+    gb.fl[s] = (uint16_t)fl;
+    gb.fc[s] = fci;
     gb.g[s] = 0.0f;
+    gb.d[s] = 0.0f;
     gb.b[s] = b;
     gb.p[s] = p;
+    if (resident) {
+        const int i = s - own.base;
+        own.invw[i] = invW;
+        own.fl[i] = (uint16_t)fl;
+        own.fc[i] = fci;
+        own.g[i] = 0.0f;
+        own.d[i] = 0.0f;
+    }
+    return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW)) == GS_ISFLUID;
 }
 
-// FP64 residual of one slot's cell; g <- r, d <- 0.  Returns (r^2, b^2) contributions.
+// FP64 residual of one cell; g <- r, d <- 0.  Adds its (r^2, b^2) contributions.
 __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDesc& d, int col, uint32_t lane,
-                                                 int n_slots, double& r2, double& b2) {
-    const int s = d.own[col] + (d.x0 >> 1) + (int)lane;
+                                                 const GsView& own, bool resident, double& r2, double& b2) {
     const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
-    const float2 cf = gb.cf[s];
-    const uint32_t fl = __float_as_uint(cf.y);
-    gb.dfc[s].x = 0.0f;
+    const int s = gs_slot(d.row[0], col, x);
+    const int i = s - own.base;
+    const uint32_t fl = own.fl[i];
+    own.d[i] = 0.0f;
+    if (resident) gb.d[s] = 0.0f;
     if (fl & GS_EMPTY) {
-        gb.g[s] = 0.0f;
+        own.g[i] = 0.0f;
         return;
     }
+    const int oc = col ^ 1;
     int nb[6];
-    gs_nb_slots(d, col, x, n_slots, nb);
+    nb[0] = gs_slot(d.row[0], oc, x - 1);
+    nb[1] = gs_slot(d.row[0], oc, x + 1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) nb[q + 2] = gs_slot(d.row[q + 1], oc, x);
+    const bool unit = (fl & GS_UNITW) != 0u;
     float2 pj[6];
     float fj[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        pj[f] = __ldcg(gb.p + nb[f]);
-        fj[f] = __ldcg(&gb.dfc[nb[f]].y);
+        pj[f] = make_float2(0.0f, 0.0f);
+        fj[f] = 0.0f;
+        if (fl & (1u << f)) {
+            pj[f] = __ldcg(gb.p + nb[f]);
+            if (!unit) fj[f] = __ldcg(gb.fc + nb[f]);
+        }
     }
-    const float fci = gb.dfc[s].y;
+    const float fci = own.fc[i];
     const float sfi = fci > 1.5f ? 1.0f : fci;
-    const bool unit = (fl & GS_UNITW) != 0u;
     double wsum = 0.0, psum = 0.0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -310,7 +350,7 @@ __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDe
     const float2 pi = gb.p[s];
     const double bb = (double)gb.b[s];
     const double r = (psum - bb) - wsum * ((double)pi.x + (double)pi.y);
-    gb.g[s] = (float)r;
+    own.g[i] = (float)r;
     r2 += r * r;
     b2 += bb * bb;
 }
@@ -328,59 +368,12 @@ __device__ __forceinline__ void gs_accumulate(const Ctx& c, const GsBuffers& gb,
     gb.p[s] = make_float2(hi, (float)(p - (double)hi));
 }
 
-// One colour of one unit: the loaded inputs of a cell, then its update.
-struct GsLoad {
-    float2 cf, me;
-    float g;
-    float2 nb[6];
-    int s;
-};
-
-__device__ __forceinline__ void gs_load(const GsBuffers& gb, const GsDesc& d, int col, uint32_t lane, int n_slots,
-                                        GsLoad& L) {
-    L.s = d.own[col] + (d.x0 >> 1) + (int)lane;
-    const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
-    int nb[6];
-    gs_nb_slots(d, col, x, n_slots, nb);
-    L.cf = gb.cf[L.s];
-    L.g = gb.g[L.s];
-    L.me = gb.dfc[L.s];
-#pragma unroll
-    for (int f = 0; f < 6; ++f) L.nb[f] = __ldcg(gb.dfc + nb[f]);
-}
-
-__device__ __forceinline__ void gs_update(const Ctx& c, const GsBuffers& gb, const GsLoad& L, float omega,
-                                          bool last) {
-    const uint32_t fl = __float_as_uint(L.cf.y);
-    if (fl & GS_EMPTY) {
-        if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, L.s, L.me.x);
-        return;
-    }
-    float ds = 0.0f;
-    if (fl & GS_UNITW) {
-#pragma unroll
-        for (int f = 0; f < 6; ++f)
-            if (fl & (1u << f)) ds += L.nb[f].x;
-    } else {
-        const float fi = L.me.y;
-#pragma unroll
-        for (int f = 0; f < 6; ++f)
-            if (fl & (1u << f)) ds += gs_weight(fi, L.nb[f].y) * L.nb[f].x;
-    }
-    const float me = L.me.x;
-    float dn = (ds + L.g) * L.cf.x;
-    if (omega != 1.0f) dn = me + omega * (dn - me);
-    gb.dfc[L.s].x = dn;
-    if (last) gs_accumulate(c, gb, L.s, dn);
-}
-
 __global__ void __launch_bounds__(GS_THREADS, 1)
     k_gs_solve(const Ctx* __restrict__ cp, float tol, uint32_t max_pairs, uint32_t check_every) {
     extern __shared__ __align__(16) unsigned char smem[];
     const Ctx& c = cp[0];
     const GsBuffers& gb = c.gs;
     const Params& u = c.u;
-    GsDesc* sdesc = reinterpret_cast<GsDesc*>(smem);
     __shared__ double s_red[2][32];
     __shared__ double s_norm;
     uint32_t* sync = gb.sync;
@@ -388,23 +381,47 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     uint32_t gen = 0;
     const uint32_t rows = u.gy * u.gz;
     const uint32_t n_units = gb.row_start[rows];
-    const int n_slots = (int)(n_units * (uint32_t)GS_UNIT) > 0 ? (int)(n_units * (uint32_t)GS_UNIT) : 1;
-    // this CTA's contiguous range of units
-    const uint32_t ua = (uint32_t)(((unsigned long long)n_units * blockIdx.x) / nb);
-    const uint32_t ue = (uint32_t)(((unsigned long long)n_units * (blockIdx.x + 1)) / nb);
+    const uint32_t ua = gs_cta_first_unit(gb, rows, n_units, blockIdx.x, nb);
+    const uint32_t ue = gs_cta_first_unit(gb, rows, n_units, blockIdx.x + 1, nb);
     const uint32_t nu = ue - ua;
-    const bool cached = nu <= (uint32_t)GS_DESC_SMEM;
+    const int S0 = (int)(ua * (uint32_t)GS_UNIT), S1 = (int)(ue * (uint32_t)GS_UNIT);
+    const size_t desc_bytes = ((size_t)nu * sizeof(GsDesc) + 15) & ~(size_t)15;
+    const size_t n_own = (size_t)nu * GS_UNIT;
+    const bool resident = desc_bytes + n_own * GS_SLOT_SMEM <= (size_t)GS_SMEM;
+    const bool cached = desc_bytes <= (size_t)GS_SMEM;
+    GsDesc* sdesc = reinterpret_cast<GsDesc*>(smem);
     if (cached)
         for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) sdesc[k] = gb.desc[ua + k];
+    GsView own;
+    if (resident) {
+        float* f = reinterpret_cast<float*>(smem + desc_bytes);
+        own.d = f;
+        own.g = f + n_own;
+        own.invw = f + 2 * n_own;
+        own.fc = f + 3 * n_own;
+        own.fl = reinterpret_cast<uint16_t*>(f + 4 * n_own);
+        own.base = S0;
+    } else {
+        own.d = gb.d;
+        own.g = gb.g;
+        own.invw = gb.invw;
+        own.fc = gb.fc;
+        own.fl = gb.fl;
+        own.base = 0;
+    }
     __syncthreads();
-    auto desc = [&](uint32_t k) -> GsDesc { return cached ? sdesc[k] : gb.desc[ua + k]; };
+    GsDesc* const dbase = cached ? sdesc : gb.desc + ua;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
     // set-up of every slot of this CTA's units
     for (uint32_t k = warp; k < nu; k += nwarps) {
-        const GsDesc d = desc(k);
-        gs_setup_cell(c, gb, d, 0, lane);
-        gs_setup_cell(c, gb, d, 1, lane);
+        GsDesc* dp = dbase + k;
+        const bool n0 = gs_setup_cell(c, gb, *dp, 0, lane, own, resident);
+        const bool n1 = gs_setup_cell(c, gb, *dp, 1, lane, own, resident);
+        const uint32_t m0 = __ballot_sync(0xffffffffu, n0), m1 = __ballot_sync(0xffffffffu, n1);
+        __syncwarp();
+        if (lane == 0) dp->nonunit = (m0 ? 1 : 0) | (m1 ? 2 : 0);
+        __syncwarp();
     }
     bool ok = gs_grid_sync(sync, nb, gen);
 
@@ -412,9 +429,9 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     auto residual = [&]() -> double {
         double r2 = 0.0, b2 = 0.0;
         for (uint32_t k = warp; k < nu; k += nwarps) {
-            const GsDesc d = desc(k);
-            gs_residual_cell(gb, d, 0, lane, n_slots, r2, b2);
-            gs_residual_cell(gb, d, 1, lane, n_slots, r2, b2);
+            const GsDesc& d = dbase[k];
+            gs_residual_cell(gb, d, 0, lane, own, resident, r2, b2);
+            gs_residual_cell(gb, d, 1, lane, own, resident, r2, b2);
         }
         for (int o = 16; o > 0; o >>= 1) {
             r2 += __shfl_down_sync(0xffffffffu, r2, o);
@@ -448,22 +465,99 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     };
 
     const float omega = u.omega;
-    // one colour over this CTA's units, two units per step with all loads in flight
+    // A neighbour row is local when this CTA keeps it in shared memory.
+    auto local_row = [&](const GsRow& r) { return resident && r.base >= S0 && r.base < S1; };
+    // One colour over this CTA's units.  A warp takes GS_BATCH of its units at a time:
+    // first the loads of the neighbour values held by other CTAs (the only loads that go
+    // to L2), all in flight together, then the updates from shared memory.
     auto sweep = [&](int col, bool last) {
-        uint32_t k = warp;
-        for (; k + nwarps < nu; k += 2 * nwarps) {
-            const GsDesc d0 = desc(k), d1 = desc(k + nwarps);
-            GsLoad a, b;
-            gs_load(gb, d0, col, lane, n_slots, a);
-            gs_load(gb, d1, col, lane, n_slots, b);
-            gs_update(c, gb, a, omega, last);
-            gs_update(c, gb, b, omega, last);
-        }
-        if (k < nu) {
-            const GsDesc d0 = desc(k);
-            GsLoad a;
-            gs_load(gb, d0, col, lane, n_slots, a);
-            gs_update(c, gb, a, omega, last);
+        const int oc = col ^ 1;
+        for (uint32_t k0 = warp; k0 < nu; k0 += GS_BATCH * nwarps) {
+            float rv[GS_BATCH][4], rf[GS_BATCH][4];
+#pragma unroll
+            for (int b = 0; b < GS_BATCH; ++b) {
+                const uint32_t k = k0 + (uint32_t)b * nwarps;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    rv[b][q] = 0.0f;
+                    rf[b][q] = 0.0f;
+                }
+                if (k >= nu) continue;
+                const GsDesc& d = dbase[k];
+                const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+                const uint32_t fl = own.fl[gs_slot(d.row[0], col, x) - own.base];
+                const bool nu_col = (d.nonunit >> col) & 1;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const GsRow r = d.row[q + 1];
+                    if (local_row(r) || !((fl >> (q + 2)) & 1u)) continue;
+                    const int sl = gs_slot(r, oc, x);
+                    rv[b][q] = __ldcg(gb.d + sl);
+                    if (nu_col) rf[b][q] = __ldcg(gb.fc + sl);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < GS_BATCH; ++b) {
+                const uint32_t k = k0 + (uint32_t)b * nwarps;
+                if (k >= nu) continue;
+                const GsDesc& d = dbase[k];
+                const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
+                const int s = gs_slot(d.row[0], col, x);
+                const int i = s - own.base;
+                const uint32_t fl = own.fl[i];
+                const float me = own.d[i];
+                if (fl & GS_EMPTY) {
+                    if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, s, me);
+                    continue;
+                }
+                float v[6], fj[6];
+                const bool unit = (fl & GS_UNITW) != 0u;
+                // faces -x, +x: the own row
+#pragma unroll
+                for (int f = 0; f < 2; ++f) {
+                    v[f] = 0.0f;
+                    fj[f] = 0.0f;
+                    if (fl & (1u << f)) {
+                        const int sl = gs_slot(d.row[0], oc, f == 0 ? x - 1 : x + 1);
+                        if (resident) {
+                            v[f] = own.d[sl - own.base];
+                            if (!unit) fj[f] = own.fc[sl - own.base];
+                        } else {
+                            v[f] = __ldcg(gb.d + sl);
+                            if (!unit) fj[f] = __ldcg(gb.fc + sl);
+                        }
+                    }
+                }
+                // faces -y, +y, -z, +z: neighbour rows, local or fetched above
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int f = q + 2;
+                    const GsRow r = d.row[q + 1];
+                    v[f] = rv[b][q];
+                    fj[f] = rf[b][q];
+                    if ((fl & (1u << f)) && local_row(r)) {
+                        const int sl = gs_slot(r, oc, x) - own.base;
+                        v[f] = own.d[sl];
+                        if (!unit) fj[f] = own.fc[sl];
+                    }
+                }
+                float ds = 0.0f;
+                if (unit) {
+#pragma unroll
+                    for (int f = 0; f < 6; ++f)
+                        if (fl & (1u << f)) ds += v[f];
+                } else {
+                    const float fi = own.fc[i];
+#pragma unroll
+                    for (int f = 0; f < 6; ++f)
+                        if (fl & (1u << f)) ds += gs_weight(fi, fj[f]) * v[f];
+                }
+                float dn = (ds + own.g[i]) * own.invw[i];
+                if (omega != 1.0f) dn = me + omega * (dn - me);
+                own.d[i] = dn;
+                if (resident) gb.d[s] = dn;  // the copy other CTAs read
+                if (last) gs_accumulate(c, gb, s, dn);
+            }
         }
     };
 
@@ -495,13 +589,13 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     }
     // the solved pressure back to the dense arrays
     for (uint32_t k = warp; k < nu; k += nwarps) {
-        const GsDesc d = desc(k);
+        const GsDesc& d = dbase[k];
 #pragma unroll
         for (int col = 0; col < 2; ++col) {
-            const int s = d.own[col] + (d.x0 >> 1) + (int)lane;
             const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
             if (x >= (int)u.gx) continue;
-            if (!(__float_as_uint(gb.cf[s].y) & GS_ISFLUID)) continue;
+            const int s = gs_slot(d.row[0], col, x);
+            if (!(own.fl[s - own.base] & GS_ISFLUID)) continue;
             const uint32_t ci = cidx(u, (uint32_t)x, (uint32_t)d.y, (uint32_t)d.z);
             const float2 p = gb.p[s];
             c.pf[ci] = p.x;

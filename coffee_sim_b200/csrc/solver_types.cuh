@@ -106,11 +106,13 @@ struct GsBuffers {
     uint32_t* row_start;  // [rows + 1] exclusive scan of row_units; row_start[rows] = units
     uint32_t* row_xlo;    // [rows] first x of each row's segment (multiple of 64)
     GsDesc* desc;         // [max_units] slot offsets of each unit and of its neighbour rows
-    float2* cf;           // [slots] 1/W, flags
-    float2* dfc;          // [slots] correction, fill code
+    float* d;             // [slots] correction of the current refinement cycle
     float* g;             // [slots] FP64 residual of the cycle, rounded to fp32
+    float* invw;          // [slots] 1 / (sum of the face weights)
+    float* fc;            // [slots] fill code: fill fraction, 2 for bed-coupled cells
     float* b;             // [slots] dx^2 rhs
     float2* p;            // [slots] pressure hi, lo
+    uint16_t* fl;         // [slots] face flags
     double* part;         // [2 * CTAs] per-CTA partial norms
     uint32_t* sync;       // grid barrier: arrivals, generation, abort
     ScResult* result;
