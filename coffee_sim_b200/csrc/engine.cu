@@ -429,7 +429,7 @@ int Engine::gs_alloc() {
     const size_t slots = units * GS_UNIT;
     int rc;
     if ((rc = alloc(gs_rows_, (2 * (rows + 1) + rows) * sizeof(uint32_t)))) return rc;
-    if ((rc = alloc(gs_desc_, units * sizeof(GsDesc)))) return rc;
+    if ((rc = alloc(gs_desc_, units * (sizeof(GsDesc) + 16 * sizeof(int))))) return rc;
     if ((rc = alloc(gs_slots_, slots * (sizeof(float2) + 5 * sizeof(float) + sizeof(uint16_t))))) return rc;
     if ((rc = gs_blocks(&gs_ctas_))) return rc;
     if ((rc = alloc(gs_misc_, sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)) + 256 +
@@ -443,6 +443,7 @@ int Engine::gs_alloc() {
     g.row_start = r + rows + 1;
     g.row_xlo = r + 2 * (rows + 1);
     g.desc = (GsDesc*)gs_desc_.ptr;
+    g.rec = (int*)((unsigned char*)gs_desc_.ptr + units * sizeof(GsDesc));
     unsigned char* sl = (unsigned char*)gs_slots_.ptr;
     g.p = (float2*)sl;
     float* f = (float*)(sl + slots * sizeof(float2));

@@ -216,6 +216,23 @@ struct GsView {
     int base;
 };
 
+// The fields of the simulation context the solve reads, staged once per CTA in
+// shared memory: with most of the shared memory given to resident slots the L1 cache
+// is small, and loads of the context from global memory would go to L2.
+struct GsCtx {
+    const int32_t* kind;
+    const float* fill;
+    const float* divf;
+    float* pf;
+    float* plo;
+    uint32_t* metrics;
+    uint32_t gx, gy, gz, first_check;
+    float dx, dt, omega, p_limit;
+    __device__ __forceinline__ uint32_t cell(uint32_t x, uint32_t y, uint32_t z) const {
+        return z * gx * gy + y * gx + x;  // cidx
+    }
+};
+
 // First unit of CTA b: its share of the units rounded to a whole row, so that every
 // CTA owns whole rows and its slots are one contiguous range.
 __device__ __forceinline__ uint32_t gs_cta_first_unit(const GsBuffers& gb, uint32_t rows, uint32_t n_units,
@@ -235,9 +252,9 @@ __device__ __forceinline__ uint32_t gs_cta_first_unit(const GsBuffers& gb, uint3
 // Set-up of one slot from the dense arrays classify wrote: flags, 1/W, fill code,
 // dx^2 rhs and the starting pressure (the face weights of face_weight,
 // shader.rs:306-323).  Returns whether the cell has a fluid face of weight below 1.
-__device__ __forceinline__ bool gs_setup_cell(const Ctx& c, const GsBuffers& gb, const GsDesc& d, int col,
+__device__ __forceinline__ bool gs_setup_cell(const GsCtx& c, const GsBuffers& gb, const GsDesc& d, int col,
                                               uint32_t lane, const GsView& own, bool resident) {
-    const Params& u = c.u;
+    const GsCtx& u = c;
     const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
     const int s = gs_slot(d.row[0], col, x);
     uint32_t fl = GS_EMPTY;
@@ -245,7 +262,7 @@ __device__ __forceinline__ bool gs_setup_cell(const Ctx& c, const GsBuffers& gb,
     float2 p = make_float2(0.0f, 0.0f);
     if (x < (int)u.gx) {
         const uint32_t ix = (uint32_t)x, iy = (uint32_t)d.y, iz = (uint32_t)d.z;
-        const uint32_t ci = cidx(u, ix, iy, iz);
+        const uint32_t ci = c.cell(ix, iy, iz);
         const int32_t kind = c.kind[ci];
         if (is_fluid(kind)) {
             fl = GS_ISFLUID;
@@ -303,12 +320,51 @@ __device__ __forceinline__ bool gs_setup_cell(const Ctx& c, const GsBuffers& gb,
     return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW)) == GS_ISFLUID;
 }
 
+// Per unit and colour, 8 words the sweeps read instead of the row descriptors: the own
+// cells' first index ([0]), for each face f the first index of the neighbour cells
+// ([1 + f]; cell `lane` of the unit has its neighbour at that index + lane, because
+// every segment starts at an even x), and [7]: bits 0-5 face f is read from global
+// memory (its row is held by another CTA, or this CTA keeps nothing in shared memory),
+// bit 8 some cell of this colour has a fluid face of weight below 1.  Indices of
+// faces read from shared memory are relative to the CTA's first slot.
+constexpr int GS_REC = 8;
+constexpr uint32_t GS_REC_NONUNIT = 1u << 8;
+
+__device__ __forceinline__ void gs_make_rec(const GsDesc& d, int col, int S0, int S1, bool resident, int* rec,
+                                            uint32_t lane) {
+    const int t = (col + d.y + d.z) & 1;
+    const int oc = col ^ 1;
+    const int k = (d.x0 - d.row[0].xlo) >> 6;
+    int v = 0;
+    if (lane == 0) {
+        v = d.row[0].base + col * d.row[0].half + 32 * k - (resident ? S0 : 0);
+    } else if (lane >= 1 && lane <= 6) {
+        const int f = (int)lane - 1;
+        const GsRow& r = d.row[f < 2 ? 0 : f - 1];
+        const int dx = f == 0 ? -1 : (f == 1 ? 1 : 0);
+        if (r.base != INT_MIN) {
+            const int g = r.base + oc * r.half + ((d.x0 + t + dx - r.xlo) >> 1);
+            const bool local = resident && r.base >= S0 && r.base < S1;
+            v = local ? g - S0 : g;
+        }
+    }
+    // remote bits
+    uint32_t m = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const GsRow& r = d.row[f < 2 ? 0 : f - 1];
+        const bool local = resident && r.base != INT_MIN && r.base >= S0 && r.base < S1;
+        if (!local) m |= 1u << f;
+    }
+    if (lane == 7) v = (int)m;
+    if (lane < (uint32_t)GS_REC) rec[lane] = v;
+}
+
 // FP64 residual of one cell; g <- r, d <- 0.  Adds its (r^2, b^2) contributions.
-__device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDesc& d, int col, uint32_t lane,
+__device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const int* rec, uint32_t lane,
                                                  const GsView& own, bool resident, double& r2, double& b2) {
-    const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
-    const int s = gs_slot(d.row[0], col, x);
-    const int i = s - own.base;
+    const int i = rec[0] + (int)lane;
+    const int s = i + own.base;
     const uint32_t fl = own.fl[i];
     own.d[i] = 0.0f;
     if (resident) gb.d[s] = 0.0f;
@@ -316,12 +372,7 @@ __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDe
         own.g[i] = 0.0f;
         return;
     }
-    const int oc = col ^ 1;
-    int nb[6];
-    nb[0] = gs_slot(d.row[0], oc, x - 1);
-    nb[1] = gs_slot(d.row[0], oc, x + 1);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) nb[q + 2] = gs_slot(d.row[q + 1], oc, x);
+    const uint32_t rm = (uint32_t)rec[7];
     const bool unit = (fl & GS_UNITW) != 0u;
     float2 pj[6];
     float fj[6];
@@ -330,8 +381,11 @@ __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDe
         pj[f] = make_float2(0.0f, 0.0f);
         fj[f] = 0.0f;
         if (fl & (1u << f)) {
-            pj[f] = __ldcg(gb.p + nb[f]);
-            if (!unit) fj[f] = __ldcg(gb.fc + nb[f]);
+            const bool remote = (rm >> f) & 1u;
+            const int j = rec[1 + f] + (int)lane;
+            const int gj = remote ? j : j + own.base;
+            pj[f] = __ldcg(gb.p + gj);
+            if (!unit) fj[f] = remote ? __ldcg(gb.fc + j) : own.fc[j];
         }
     }
     const float fci = own.fc[i];
@@ -356,10 +410,10 @@ __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const GsDe
 }
 
 // p <- p + d in FP64 (split back into hi/lo, clamped at the pressure limit).
-__device__ __forceinline__ void gs_accumulate(const Ctx& c, const GsBuffers& gb, int s, float dn) {
+__device__ __forceinline__ void gs_accumulate(const GsCtx& c, const GsBuffers& gb, int s, float dn) {
     const float2 pi = gb.p[s];
     double p = ((double)pi.x + (double)pi.y) + (double)dn;
-    const double lim = (double)c.u.p_limit;
+    const double lim = (double)c.p_limit;
     if (p > lim || p < -lim) {
         p = p > 0.0 ? lim : -lim;
         atomicAdd(&c.metrics[M_P_CLAMP], 1u);
@@ -371,30 +425,48 @@ __device__ __forceinline__ void gs_accumulate(const Ctx& c, const GsBuffers& gb,
 __global__ void __launch_bounds__(GS_THREADS, 1)
     k_gs_solve(const Ctx* __restrict__ cp, float tol, uint32_t max_pairs, uint32_t check_every) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const Ctx& c = cp[0];
-    const GsBuffers& gb = c.gs;
-    const Params& u = c.u;
+    __shared__ GsBuffers s_gb;
+    __shared__ GsCtx s_c;
+    if (threadIdx.x == 0) {
+        const Ctx& cg = cp[0];
+        s_gb = cg.gs;
+        s_c.kind = cg.kind;
+        s_c.fill = cg.fill;
+        s_c.divf = cg.divf;
+        s_c.pf = cg.pf;
+        s_c.plo = cg.plo;
+        s_c.metrics = cg.metrics;
+        s_c.gx = cg.u.gx;
+        s_c.gy = cg.u.gy;
+        s_c.gz = cg.u.gz;
+        s_c.first_check = cg.u.first_check;
+        s_c.dx = cg.u.dx;
+        s_c.dt = cg.u.dt;
+        s_c.omega = cg.u.omega;
+        s_c.p_limit = cg.u.p_limit;
+    }
+    __syncthreads();
+    const GsBuffers& gb = s_gb;
+    const GsCtx& c = s_c;
     __shared__ double s_red[2][32];
     __shared__ double s_norm;
     uint32_t* sync = gb.sync;
     const uint32_t nb = gridDim.x;
     uint32_t gen = 0;
-    const uint32_t rows = u.gy * u.gz;
+    const uint32_t rows = c.gy * c.gz;
     const uint32_t n_units = gb.row_start[rows];
     const uint32_t ua = gs_cta_first_unit(gb, rows, n_units, blockIdx.x, nb);
     const uint32_t ue = gs_cta_first_unit(gb, rows, n_units, blockIdx.x + 1, nb);
     const uint32_t nu = ue - ua;
     const int S0 = (int)(ua * (uint32_t)GS_UNIT), S1 = (int)(ue * (uint32_t)GS_UNIT);
-    const size_t desc_bytes = ((size_t)nu * sizeof(GsDesc) + 15) & ~(size_t)15;
+    const size_t rec_bytes = (size_t)nu * 2 * GS_REC * sizeof(int);
     const size_t n_own = (size_t)nu * GS_UNIT;
-    const bool resident = desc_bytes + n_own * GS_SLOT_SMEM <= (size_t)GS_SMEM;
-    const bool cached = desc_bytes <= (size_t)GS_SMEM;
-    GsDesc* sdesc = reinterpret_cast<GsDesc*>(smem);
-    if (cached)
-        for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) sdesc[k] = gb.desc[ua + k];
+    const bool resident = rec_bytes + n_own * GS_SLOT_SMEM <= (size_t)GS_SMEM;
+    const bool cached = rec_bytes <= (size_t)GS_SMEM;
+    int* const recb = cached ? reinterpret_cast<int*>(smem) : gb.rec + (size_t)ua * 2 * GS_REC;
     GsView own;
     if (resident) {
-        float* f = reinterpret_cast<float*>(smem + desc_bytes);
+        float* f = reinterpret_cast<float*>(smem + rec_bytes);
         own.d = f;
         own.g = f + n_own;
         own.invw = f + 2 * n_own;
@@ -409,18 +481,22 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
         own.fl = gb.fl;
         own.base = 0;
     }
-    __syncthreads();
-    GsDesc* const dbase = cached ? sdesc : gb.desc + ua;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
-    // set-up of every slot of this CTA's units
+    // set-up of every slot of this CTA's units, and their index words
     for (uint32_t k = warp; k < nu; k += nwarps) {
-        GsDesc* dp = dbase + k;
-        const bool n0 = gs_setup_cell(c, gb, *dp, 0, lane, own, resident);
-        const bool n1 = gs_setup_cell(c, gb, *dp, 1, lane, own, resident);
+        const GsDesc d = gb.desc[ua + k];
+        const bool n0 = gs_setup_cell(c, gb, d, 0, lane, own, resident);
+        const bool n1 = gs_setup_cell(c, gb, d, 1, lane, own, resident);
         const uint32_t m0 = __ballot_sync(0xffffffffu, n0), m1 = __ballot_sync(0xffffffffu, n1);
+        int* r = recb + (size_t)k * 2 * GS_REC;
+        gs_make_rec(d, 0, S0, S1, resident, r, lane);
+        gs_make_rec(d, 1, S0, S1, resident, r + GS_REC, lane);
         __syncwarp();
-        if (lane == 0) dp->nonunit = (m0 ? 1 : 0) | (m1 ? 2 : 0);
+        if (lane == 0) {
+            if (m0) r[7] |= (int)GS_REC_NONUNIT;
+            if (m1) r[GS_REC + 7] |= (int)GS_REC_NONUNIT;
+        }
         __syncwarp();
     }
     bool ok = gs_grid_sync(sync, nb, gen);
@@ -429,9 +505,9 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     auto residual = [&]() -> double {
         double r2 = 0.0, b2 = 0.0;
         for (uint32_t k = warp; k < nu; k += nwarps) {
-            const GsDesc& d = dbase[k];
-            gs_residual_cell(gb, d, 0, lane, own, resident, r2, b2);
-            gs_residual_cell(gb, d, 1, lane, own, resident, r2, b2);
+            const int* r = recb + (size_t)k * 2 * GS_REC;
+            gs_residual_cell(gb, r, lane, own, resident, r2, b2);
+            gs_residual_cell(gb, r + GS_REC, lane, own, resident, r2, b2);
         }
         for (int o = 16; o > 0; o >>= 1) {
             r2 += __shfl_down_sync(0xffffffffu, r2, o);
@@ -464,81 +540,46 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
         return s_norm;
     };
 
-    const float omega = u.omega;
-    // A neighbour row is local when this CTA keeps it in shared memory.
-    auto local_row = [&](const GsRow& r) { return resident && r.base >= S0 && r.base < S1; };
+    const float omega = c.omega;
     // One colour over this CTA's units.  A warp takes GS_BATCH of its units at a time:
-    // first the loads of the neighbour values held by other CTAs (the only loads that go
-    // to L2), all in flight together, then the updates from shared memory.
+    // first the loads of the neighbour values held in global memory, all in flight
+    // together, then the updates.
     auto sweep = [&](int col, bool last) {
-        const int oc = col ^ 1;
         for (uint32_t k0 = warp; k0 < nu; k0 += GS_BATCH * nwarps) {
-            float rv[GS_BATCH][4], rf[GS_BATCH][4];
+            float rv[GS_BATCH][6];
 #pragma unroll
             for (int b = 0; b < GS_BATCH; ++b) {
                 const uint32_t k = k0 + (uint32_t)b * nwarps;
+                const bool have = k < nu;
+                const int* r = recb + ((size_t)(have ? k : 0) * 2 + col) * GS_REC;
+                const uint32_t rm = have ? (uint32_t)r[7] : 0u;
+                const uint32_t need = have ? rm & (uint32_t)own.fl[r[0] + (int)lane] : 0u;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    rv[b][q] = 0.0f;
-                    rf[b][q] = 0.0f;
-                }
-                if (k >= nu) continue;
-                const GsDesc& d = dbase[k];
-                const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
-                const uint32_t fl = own.fl[gs_slot(d.row[0], col, x) - own.base];
-                const bool nu_col = (d.nonunit >> col) & 1;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const GsRow r = d.row[q + 1];
-                    if (local_row(r) || !((fl >> (q + 2)) & 1u)) continue;
-                    const int sl = gs_slot(r, oc, x);
-                    rv[b][q] = __ldcg(gb.d + sl);
-                    if (nu_col) rf[b][q] = __ldcg(gb.fc + sl);
-                }
+                for (int f = 0; f < 6; ++f) rv[b][f] = ((need >> f) & 1u) ? __ldcg(gb.d + r[1 + f] + (int)lane) : 0.0f;
             }
 #pragma unroll
             for (int b = 0; b < GS_BATCH; ++b) {
                 const uint32_t k = k0 + (uint32_t)b * nwarps;
                 if (k >= nu) continue;
-                const GsDesc& d = dbase[k];
-                const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
-                const int s = gs_slot(d.row[0], col, x);
-                const int i = s - own.base;
+                const int* r = recb + ((size_t)k * 2 + col) * GS_REC;
+                const uint32_t rm = (uint32_t)r[7];
+                const int i = r[0] + (int)lane;
                 const uint32_t fl = own.fl[i];
                 const float me = own.d[i];
                 if (fl & GS_EMPTY) {
-                    if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, s, me);
+                    if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, i + own.base, me);
                     continue;
                 }
-                float v[6], fj[6];
                 const bool unit = (fl & GS_UNITW) != 0u;
-                // faces -x, +x: the own row
+                float v[6], fj[6];
 #pragma unroll
-                for (int f = 0; f < 2; ++f) {
-                    v[f] = 0.0f;
+                for (int f = 0; f < 6; ++f) {
+                    v[f] = rv[b][f];
                     fj[f] = 0.0f;
-                    if (fl & (1u << f)) {
-                        const int sl = gs_slot(d.row[0], oc, f == 0 ? x - 1 : x + 1);
-                        if (resident) {
-                            v[f] = own.d[sl - own.base];
-                            if (!unit) fj[f] = own.fc[sl - own.base];
-                        } else {
-                            v[f] = __ldcg(gb.d + sl);
-                            if (!unit) fj[f] = __ldcg(gb.fc + sl);
-                        }
-                    }
-                }
-                // faces -y, +y, -z, +z: neighbour rows, local or fetched above
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int f = q + 2;
-                    const GsRow r = d.row[q + 1];
-                    v[f] = rv[b][q];
-                    fj[f] = rf[b][q];
-                    if ((fl & (1u << f)) && local_row(r)) {
-                        const int sl = gs_slot(r, oc, x) - own.base;
-                        v[f] = own.d[sl];
-                        if (!unit) fj[f] = own.fc[sl];
+                    if ((fl >> f) & 1u) {
+                        const int j = r[1 + f] + (int)lane;
+                        if (!((rm >> f) & 1u)) v[f] = own.d[j];  // a face held in shared memory
+                        if (!unit) fj[f] = ((rm >> f) & 1u) ? __ldcg(gb.fc + j) : own.fc[j];
                     }
                 }
                 float ds = 0.0f;
@@ -555,8 +596,8 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
                 float dn = (ds + own.g[i]) * own.invw[i];
                 if (omega != 1.0f) dn = me + omega * (dn - me);
                 own.d[i] = dn;
-                if (resident) gb.d[s] = dn;  // the copy other CTAs read
-                if (last) gs_accumulate(c, gb, s, dn);
+                if (resident) gb.d[i + own.base] = dn;  // the copy other CTAs read
+                if (last) gs_accumulate(c, gb, i + own.base, dn);
             }
         }
     };
@@ -569,7 +610,7 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
         evals = 1;
     }
     const uint32_t ce = check_every ? check_every : 10u;
-    uint32_t next = u.first_check ? u.first_check : ce;
+    uint32_t next = c.first_check ? c.first_check : ce;
     while (ok && !(r1 <= (double)tol) && pairs < max_pairs) {
         const uint32_t k = min(next, max_pairs - pairs);
         for (uint32_t j = 0; j < k && ok; ++j) {
@@ -589,14 +630,14 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     }
     // the solved pressure back to the dense arrays
     for (uint32_t k = warp; k < nu; k += nwarps) {
-        const GsDesc& d = dbase[k];
+        const GsDesc d = gb.desc[ua + k];
 #pragma unroll
         for (int col = 0; col < 2; ++col) {
             const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
-            if (x >= (int)u.gx) continue;
+            if (x >= (int)c.gx) continue;
             const int s = gs_slot(d.row[0], col, x);
-            if (!(own.fl[s - own.base] & GS_ISFLUID)) continue;
-            const uint32_t ci = cidx(u, (uint32_t)x, (uint32_t)d.y, (uint32_t)d.z);
+            if (!(gb.fl[s] & GS_ISFLUID)) continue;
+            const uint32_t ci = c.cell((uint32_t)x, (uint32_t)d.y, (uint32_t)d.z);
             const float2 p = gb.p[s];
             c.pf[ci] = p.x;
             c.plo[ci] = p.y;

@@ -106,6 +106,8 @@ struct GsBuffers {
     uint32_t* row_start;  // [rows + 1] exclusive scan of row_units; row_start[rows] = units
     uint32_t* row_xlo;    // [rows] first x of each row's segment (multiple of 64)
     GsDesc* desc;         // [max_units] slot offsets of each unit and of its neighbour rows
+    int* rec;             // [max_units][2][8] per-colour index words of the solve (when they do not
+                          // fit in shared memory)
     float* d;             // [slots] correction of the current refinement cycle
     float* g;             // [slots] FP64 residual of the cycle, rounded to fp32
     float* invw;          // [slots] 1 / (sum of the face weights)
