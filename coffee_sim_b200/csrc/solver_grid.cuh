@@ -251,9 +251,9 @@ __device__ __forceinline__ uint32_t gs_cta_first_unit(const GsBuffers& gb, uint3
 
 // Set-up of one slot from the dense arrays classify wrote: flags, 1/W, fill code,
 // dx^2 rhs and the starting pressure (the face weights of face_weight,
-// shader.rs:306-323).  Returns whether the cell has a fluid face of weight below 1.
-__device__ __forceinline__ bool gs_setup_cell(const GsCtx& c, const GsBuffers& gb, const GsDesc& d, int col,
-                                              uint32_t lane, const GsView& own, bool resident) {
+// shader.rs:306-323).  Returns the cell's flags.
+__device__ __forceinline__ uint32_t gs_setup_cell(const GsCtx& c, const GsBuffers& gb, const GsDesc& d, int col,
+                                                  uint32_t lane, const GsView& own, bool resident) {
     const GsCtx& u = c;
     const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
     const int s = gs_slot(d.row[0], col, x);
@@ -317,7 +317,7 @@ __device__ __forceinline__ bool gs_setup_cell(const GsCtx& c, const GsBuffers& g
         own.g[i] = 0.0f;
         own.d[i] = 0.0f;
     }
-    return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW)) == GS_ISFLUID;
+    return fl;
 }
 
 // Per unit and colour, 8 words the sweeps read instead of the row descriptors: the own
@@ -329,6 +329,9 @@ __device__ __forceinline__ bool gs_setup_cell(const GsCtx& c, const GsBuffers& g
 // faces read from shared memory are relative to the CTA's first slot.
 constexpr int GS_REC = 8;
 constexpr uint32_t GS_REC_NONUNIT = 1u << 8;
+// bit 9: every cell of this colour is a fluid cell whose six faces are fluid faces of
+// weight 1 (the bulk of a pool); its update is a plain six-term sum
+constexpr uint32_t GS_REC_BULK = 1u << 9;
 
 __device__ __forceinline__ void gs_make_rec(const GsDesc& d, int col, int S0, int S1, bool resident, int* rec,
                                             uint32_t lane) {
@@ -486,16 +489,21 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     // set-up of every slot of this CTA's units, and their index words
     for (uint32_t k = warp; k < nu; k += nwarps) {
         const GsDesc d = gb.desc[ua + k];
-        const bool n0 = gs_setup_cell(c, gb, d, 0, lane, own, resident);
-        const bool n1 = gs_setup_cell(c, gb, d, 1, lane, own, resident);
-        const uint32_t m0 = __ballot_sync(0xffffffffu, n0), m1 = __ballot_sync(0xffffffffu, n1);
+        const uint32_t f0 = gs_setup_cell(c, gb, d, 0, lane, own, resident);
+        const uint32_t f1 = gs_setup_cell(c, gb, d, 1, lane, own, resident);
+        auto nonunit = [](uint32_t fl) { return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW)) == GS_ISFLUID; };
+        auto bulk = [](uint32_t fl) {
+            return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW | GS_FLUID_FACES)) == (GS_ISFLUID | GS_UNITW | GS_FLUID_FACES);
+        };
+        const uint32_t n0 = __ballot_sync(0xffffffffu, nonunit(f0)), n1 = __ballot_sync(0xffffffffu, nonunit(f1));
+        const uint32_t b0 = __ballot_sync(0xffffffffu, bulk(f0)), b1 = __ballot_sync(0xffffffffu, bulk(f1));
         int* r = recb + (size_t)k * 2 * GS_REC;
         gs_make_rec(d, 0, S0, S1, resident, r, lane);
         gs_make_rec(d, 1, S0, S1, resident, r + GS_REC, lane);
         __syncwarp();
         if (lane == 0) {
-            if (m0) r[7] |= (int)GS_REC_NONUNIT;
-            if (m1) r[GS_REC + 7] |= (int)GS_REC_NONUNIT;
+            r[7] |= (int)((n0 ? GS_REC_NONUNIT : 0u) | (b0 == 0xffffffffu ? GS_REC_BULK : 0u));
+            r[GS_REC + 7] |= (int)((n1 ? GS_REC_NONUNIT : 0u) | (b1 == 0xffffffffu ? GS_REC_BULK : 0u));
         }
         __syncwarp();
     }
@@ -564,8 +572,20 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
                 const int* r = recb + ((size_t)k * 2 + col) * GS_REC;
                 const uint32_t rm = (uint32_t)r[7];
                 const int i = r[0] + (int)lane;
-                const uint32_t fl = own.fl[i];
                 const float me = own.d[i];
+                if (rm & GS_REC_BULK) {
+                    // six fluid faces of weight 1 on every lane: the same sum in face order
+                    float ds = 0.0f;
+#pragma unroll
+                    for (int f = 0; f < 6; ++f) ds += ((rm >> f) & 1u) ? rv[b][f] : own.d[r[1 + f] + (int)lane];
+                    float dn = (ds + own.g[i]) * own.invw[i];
+                    if (omega != 1.0f) dn = me + omega * (dn - me);
+                    own.d[i] = dn;
+                    if (resident) gb.d[i + own.base] = dn;
+                    if (last) gs_accumulate(c, gb, i + own.base, dn);
+                    continue;
+                }
+                const uint32_t fl = own.fl[i];
                 if (fl & GS_EMPTY) {
                     if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, i + own.base, me);
                     continue;
