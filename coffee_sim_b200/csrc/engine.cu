@@ -430,7 +430,7 @@ int Engine::gs_alloc() {
     int rc;
     if ((rc = alloc(gs_rows_, (2 * (rows + 1) + rows) * sizeof(uint32_t)))) return rc;
     if ((rc = alloc(gs_desc_, units * (sizeof(GsDesc) + 16 * sizeof(int))))) return rc;
-    if ((rc = alloc(gs_slots_, slots * (sizeof(float2) + 5 * sizeof(float) + sizeof(uint16_t))))) return rc;
+    if ((rc = alloc(gs_slots_, slots * (3 * sizeof(float2) + 2 * sizeof(float))))) return rc;
     if ((rc = gs_blocks(&gs_ctas_))) return rc;
     if ((rc = alloc(gs_misc_, sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)) + 256 +
                                   sc_align(sizeof(ScResult))))) return rc;
@@ -444,15 +444,12 @@ int Engine::gs_alloc() {
     g.row_xlo = r + 2 * (rows + 1);
     g.desc = (GsDesc*)gs_desc_.ptr;
     g.rec = (int*)((unsigned char*)gs_desc_.ptr + units * sizeof(GsDesc));
-    unsigned char* sl = (unsigned char*)gs_slots_.ptr;
-    g.p = (float2*)sl;
-    float* f = (float*)(sl + slots * sizeof(float2));
-    g.d = f;
-    g.g = f + slots;
-    g.invw = f + 2 * slots;
-    g.fc = f + 3 * slots;
-    g.b = f + 4 * slots;
-    g.fl = (uint16_t*)(f + 5 * slots);
+    float2* f2 = (float2*)gs_slots_.ptr;
+    g.cf = f2;
+    g.dfc = f2 + slots;
+    g.p = f2 + 2 * slots;
+    g.g = (float*)(f2 + 3 * slots);
+    g.b = g.g + slots;
     unsigned char* m = (unsigned char*)gs_misc_.ptr;
     g.part = (double*)m;
     g.sync = (uint32_t*)(m + sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)));

@@ -13,33 +13,34 @@
 // segment stores its red cells first, then its black cells, so the 32 cells of one
 // colour of a unit are 32 consecutive slots: a warp's loads of its own cells and of
 // each neighbour row are single 128-byte rows, and a sweep touches only the rows that
-// hold fluid (the dense grid of a large pour is mostly air and solid).  Per slot, in
-// global memory: the correction d, the residual g, 1/W, the fill code, dx^2 rhs, the
-// pressure (hi, lo) and 16 flag bits giving, per face, whether it is a fluid face
-// with weight > 0 (bits 0-5) or an air face with weight > 0 (bits 8-13), and whether
-// all fluid faces have weight 1, so no pass recomputes a cell kind.
+// hold fluid (the dense grid of a large pour is mostly air and solid).  Per slot:
+// (1/W, flags), (correction, fill code) and the pressure (hi, lo) as float2, the
+// residual g and dx^2 rhs.  The flags give, per face, whether it is a fluid face with
+// weight > 0 (bits 0-5) or an air face with weight > 0 (bits 8-13), and whether all
+// fluid faces have weight 1, so no pass recomputes a cell kind.
 //
 // Prep (k_gs_rows, a CUB scan, k_gs_desc) finds each row's fluid extent, numbers the
 // units and writes for every unit its own row's and its four neighbour rows' first
 // slot, colour-half length and first x (a neighbour cell's slot follows from its x).
 //
 // Solve (k_gs_solve).  One CTA of 1024 threads per SM, launched cooperatively so all
-// are resident.  CTA b owns whole rows, about 1/148 of the units, so its slots are one
-// contiguous range; when they fit (about 190 units) the CTA keeps their d, g, 1/W,
-// fill code and flags in shared memory for the whole solve, and writes each new d to
-// global memory only for the other CTAs to read.  A warp sweeps its units two at a
-// time: first the L2 loads (ld.cg) of the neighbour values held by other CTAs (rows at
-// z +- 1, and y +- 1 at the ends of the CTA's range), all in flight together, then the
-// updates from shared memory.  The colours of a red-black pair are separated by a
-// grid-wide barrier (a monotonic arrival counter: a release add per CTA, acquire
-// polling).  The last pair of a refinement cycle adds the correction to the pressure
-// as it goes (a cell's correction is final after its own colour's sweep), so a
-// residual check is one pass and one barrier: each CTA writes its FP64 partial sums,
-// and after the barrier every CTA adds all partials in CTA order, so all take the same
-// stop decision.  The check schedule is sc_next_interval, the same as the oracle's.
-// Every barrier wait is bounded; a CTA whose wait runs out raises an abort word that
-// ends the other CTAs' waits too, and the solve reports status 3 (the host then
-// re-solves with per-colour launches).
+// are resident.  CTA b owns whole rows, about 1/148 of the units.  At set-up it turns
+// each unit's descriptor into eight index words per colour, kept in shared memory: the
+// slot of the unit's first cell and of that cell's six neighbours (cell `lane` then
+// sits at slot + lane), and whether the unit is bulk (all 32 cells fluid with six
+// unit-weight fluid faces, updated by a plain six-term sum).  A warp sweeps its units
+// two at a time with all nine loads of both in flight (own coefficients, residual and
+// correction, six neighbours' correction and fill code in one 8-byte load each, read
+// from L2 with ld.cg).  The colours of a red-black pair are separated by a grid-wide
+// barrier (a monotonic arrival counter: a release add per CTA, acquire polling).  The
+// last pair of a refinement cycle adds the correction to the pressure as it goes (a
+// cell's correction is final after its own colour's sweep), so a residual check is one
+// pass and one barrier: each CTA writes its FP64 partial sums, and after the barrier
+// every CTA adds all partials in CTA order, so all take the same stop decision.  The
+// check schedule is sc_next_interval, the same as the oracle's.  Every barrier wait is
+// bounded; a CTA whose wait runs out raises an abort word that ends the other CTAs'
+// waits too, and the solve reports status 3 (the host then re-solves with per-colour
+// launches).
 #pragma once
 #include <climits>
 
@@ -50,7 +51,6 @@ namespace cs {
 
 constexpr int GS_THREADS = 1024;
 constexpr int GS_UNIT = 64;                 // cells per unit (32 slots of each colour)
-constexpr int GS_BATCH = 2;                 // units a warp sweeps with their remote loads in flight together
 // per-slot flags (16 bits)
 constexpr uint32_t GS_FLUID_FACES = 0x3fu;  // bits 0-5: fluid face with weight > 0
 constexpr uint32_t GS_UNITW = 1u << 6;      // every fluid face has weight 1
@@ -58,8 +58,7 @@ constexpr uint32_t GS_EMPTY = 1u << 7;      // no face with weight > 0, not flui
 constexpr uint32_t GS_AIR_SHIFT = 8;        // bits 8-13: air face with weight > 0
 constexpr uint32_t GS_ISFLUID = 1u << 14;   // fluid cell (its pressure is accumulated)
 constexpr long long kGsWaitCycles = 1ll << 31;  // ~1 s at 2 GHz
-constexpr int GS_SMEM = 230400;             // dynamic shared memory of a solve CTA
-constexpr int GS_SLOT_SMEM = 18;            // shared bytes per resident slot: d, g, 1/W, fill code, flags
+constexpr int GS_SMEM = 64 * 1024;          // dynamic shared memory of a solve CTA: its units' index words
 
 // Per unit: x of its first cell, y, z, and for its own row and the four neighbour rows
 // (y-1, y+1, z-1, z+1) the row's first slot (INT_MIN: no fluid in it), the slots per
@@ -205,20 +204,8 @@ __device__ __forceinline__ int gs_slot(const GsRow& r, int col, int x) {
     return r.base + col * r.half + ((x - r.xlo) >> 1);
 }
 
-// The state of a CTA's own slots: in shared memory when they fit there (resident),
-// else the global arrays themselves.  Element i is slot base + i.
-struct GsView {
-    float* d;
-    float* g;
-    float* invw;
-    float* fc;
-    uint16_t* fl;
-    int base;
-};
-
 // The fields of the simulation context the solve reads, staged once per CTA in
-// shared memory: with most of the shared memory given to resident slots the L1 cache
-// is small, and loads of the context from global memory would go to L2.
+// shared memory so that the loops do not reload them from global memory.
 struct GsCtx {
     const int32_t* kind;
     const float* fill;
@@ -253,7 +240,7 @@ __device__ __forceinline__ uint32_t gs_cta_first_unit(const GsBuffers& gb, uint3
 // dx^2 rhs and the starting pressure (the face weights of face_weight,
 // shader.rs:306-323).  Returns the cell's flags.
 __device__ __forceinline__ uint32_t gs_setup_cell(const GsCtx& c, const GsBuffers& gb, const GsDesc& d, int col,
-                                                  uint32_t lane, const GsView& own, bool resident) {
+                                                  uint32_t lane) {
     const GsCtx& u = c;
     const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
     const int s = gs_slot(d.row[0], col, x);
@@ -302,97 +289,71 @@ __device__ __forceinline__ uint32_t gs_setup_cell(const GsCtx& c, const GsBuffer
             p = make_float2(c.pf[ci], c.plo[ci]);
         }
     }
-    gb.invw[s] = invW;
-    gb.fl[s] = (uint16_t)fl;
-    gb.fc[s] = fci;
+    gb.cf[s] = make_float2(invW, __uint_as_float(fl));
+    gb.dfc[s] = make_float2(0.0f, fci);
     gb.g[s] = 0.0f;
-    gb.d[s] = 0.0f;
     gb.b[s] = b;
     gb.p[s] = p;
-    if (resident) {
-        const int i = s - own.base;
-        own.invw[i] = invW;
-        own.fl[i] = (uint16_t)fl;
-        own.fc[i] = fci;
-        own.g[i] = 0.0f;
-        own.d[i] = 0.0f;
-    }
     return fl;
 }
 
-// Per unit and colour, 8 words the sweeps read instead of the row descriptors: the own
-// cells' first index ([0]), for each face f the first index of the neighbour cells
-// ([1 + f]; cell `lane` of the unit has its neighbour at that index + lane, because
-// every segment starts at an even x), and [7]: bits 0-5 face f is read from global
-// memory (its row is held by another CTA, or this CTA keeps nothing in shared memory),
-// bit 8 some cell of this colour has a fluid face of weight below 1.  Indices of
-// faces read from shared memory are relative to the CTA's first slot.
+// Per unit and colour, 8 words the sweeps read instead of the row descriptors: [0] the
+// slot of the unit's first cell of this colour; [1 + f] for face f the slot of the
+// neighbour of that first cell (cell `lane` of the unit has its neighbour at that slot
+// + lane, because every segment starts at an even x; 0 where the neighbour row holds
+// no fluid, and such faces are never fluid faces); [7] bit 8 some cell of this colour
+// has a fluid face of weight below 1, bit 9 every cell of this colour is a fluid cell
+// whose six faces are fluid faces of weight 1 (the bulk of a pool, whose update is a
+// plain six-term sum).
 constexpr int GS_REC = 8;
 constexpr uint32_t GS_REC_NONUNIT = 1u << 8;
-// bit 9: every cell of this colour is a fluid cell whose six faces are fluid faces of
-// weight 1 (the bulk of a pool); its update is a plain six-term sum
 constexpr uint32_t GS_REC_BULK = 1u << 9;
 
-__device__ __forceinline__ void gs_make_rec(const GsDesc& d, int col, int S0, int S1, bool resident, int* rec,
-                                            uint32_t lane) {
+__device__ __forceinline__ void gs_make_rec(const GsDesc& d, int col, uint32_t flags, int* rec, uint32_t lane) {
     const int t = (col + d.y + d.z) & 1;
     const int oc = col ^ 1;
     const int k = (d.x0 - d.row[0].xlo) >> 6;
-    int v = 0;
-    if (lane == 0) {
-        v = d.row[0].base + col * d.row[0].half + 32 * k - (resident ? S0 : 0);
-    } else if (lane >= 1 && lane <= 6) {
-        const int f = (int)lane - 1;
-        const GsRow& r = d.row[f < 2 ? 0 : f - 1];
-        const int dx = f == 0 ? -1 : (f == 1 ? 1 : 0);
-        if (r.base != INT_MIN) {
-            const int g = r.base + oc * r.half + ((d.x0 + t + dx - r.xlo) >> 1);
-            const bool local = resident && r.base >= S0 && r.base < S1;
-            v = local ? g - S0 : g;
-        }
-    }
-    // remote bits
-    uint32_t m = 0;
+    int v = (int)flags;
+    if (lane == 0) v = d.row[0].base + col * d.row[0].half + 32 * k;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const GsRow& r = d.row[f < 2 ? 0 : f - 1];
-        const bool local = resident && r.base != INT_MIN && r.base >= S0 && r.base < S1;
-        if (!local) m |= 1u << f;
+        if (lane != (uint32_t)(1 + f)) continue;
+        const GsRow r = d.row[f < 2 ? 0 : f - 1];
+        const int dx = f == 0 ? -1 : (f == 1 ? 1 : 0);
+        v = r.base == INT_MIN ? 0 : r.base + oc * r.half + ((d.x0 + t + dx - r.xlo) >> 1);
     }
-    if (lane == 7) v = (int)m;
     if (lane < (uint32_t)GS_REC) rec[lane] = v;
 }
 
+// Slot of the neighbour across face f of cell `lane`, clamped into the arrays so that
+// all six can be loaded before the flags say which are fluid faces.
+__device__ __forceinline__ int gs_nb(const int* rec, int f, uint32_t lane, int n_slots) {
+    const int j = rec[1 + f] + (int)lane;
+    return j < 0 ? 0 : (j < n_slots ? j : n_slots - 1);
+}
+
 // FP64 residual of one cell; g <- r, d <- 0.  Adds its (r^2, b^2) contributions.
-__device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const int* rec, uint32_t lane,
-                                                 const GsView& own, bool resident, double& r2, double& b2) {
-    const int i = rec[0] + (int)lane;
-    const int s = i + own.base;
-    const uint32_t fl = own.fl[i];
-    own.d[i] = 0.0f;
-    if (resident) gb.d[s] = 0.0f;
+__device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const int* rec, uint32_t lane, int n_slots,
+                                                 double& r2, double& b2) {
+    const int s = rec[0] + (int)lane;
+    const float2 cf = gb.cf[s];
+    const uint32_t fl = __float_as_uint(cf.y);
+    gb.dfc[s].x = 0.0f;
     if (fl & GS_EMPTY) {
-        own.g[i] = 0.0f;
+        gb.g[s] = 0.0f;
         return;
     }
-    const uint32_t rm = (uint32_t)rec[7];
-    const bool unit = (fl & GS_UNITW) != 0u;
     float2 pj[6];
     float fj[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        pj[f] = make_float2(0.0f, 0.0f);
-        fj[f] = 0.0f;
-        if (fl & (1u << f)) {
-            const bool remote = (rm >> f) & 1u;
-            const int j = rec[1 + f] + (int)lane;
-            const int gj = remote ? j : j + own.base;
-            pj[f] = __ldcg(gb.p + gj);
-            if (!unit) fj[f] = remote ? __ldcg(gb.fc + j) : own.fc[j];
-        }
+        const int j = gs_nb(rec, f, lane, n_slots);
+        pj[f] = __ldcg(gb.p + j);
+        fj[f] = __ldcg(&gb.dfc[j].y);
     }
-    const float fci = own.fc[i];
+    const float fci = gb.dfc[s].y;
     const float sfi = fci > 1.5f ? 1.0f : fci;
+    const bool unit = (fl & GS_UNITW) != 0u;
     double wsum = 0.0, psum = 0.0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -407,9 +368,29 @@ __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const int*
     const float2 pi = gb.p[s];
     const double bb = (double)gb.b[s];
     const double r = (psum - bb) - wsum * ((double)pi.x + (double)pi.y);
-    own.g[i] = (float)r;
+    gb.g[s] = (float)r;
     r2 += r * r;
     b2 += bb * bb;
+}
+
+// One colour of one unit: the loaded inputs of a cell, then its update.
+struct GsLoad {
+    float2 cf, me;
+    float g;
+    float2 nb[6];
+    int s;
+    uint32_t rf;  // the unit's flag word
+};
+
+__device__ __forceinline__ void gs_load(const GsBuffers& gb, const int* rec, uint32_t lane, int n_slots,
+                                        GsLoad& L) {
+    L.s = rec[0] + (int)lane;
+    L.rf = (uint32_t)rec[7];
+    L.cf = gb.cf[L.s];
+    L.g = gb.g[L.s];
+    L.me = gb.dfc[L.s];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) L.nb[f] = __ldcg(gb.dfc + gs_nb(rec, f, lane, n_slots));
 }
 
 // p <- p + d in FP64 (split back into hi/lo, clamped at the pressure limit).
@@ -423,6 +404,37 @@ __device__ __forceinline__ void gs_accumulate(const GsCtx& c, const GsBuffers& g
     }
     const float hi = (float)p;
     gb.p[s] = make_float2(hi, (float)(p - (double)hi));
+}
+
+__device__ __forceinline__ void gs_update(const GsCtx& c, const GsBuffers& gb, const GsLoad& L, float omega,
+                                          bool last) {
+    const float me = L.me.x;
+    float ds = 0.0f;
+    if (L.rf & GS_REC_BULK) {
+        // six fluid faces of weight 1 on every lane: the same sum in face order
+#pragma unroll
+        for (int f = 0; f < 6; ++f) ds += L.nb[f].x;
+    } else {
+        const uint32_t fl = __float_as_uint(L.cf.y);
+        if (fl & GS_EMPTY) {
+            if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, L.s, me);
+            return;
+        }
+        if (fl & GS_UNITW) {
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if (fl & (1u << f)) ds += L.nb[f].x;
+        } else {
+            const float fi = L.me.y;
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if (fl & (1u << f)) ds += gs_weight(fi, L.nb[f].y) * L.nb[f].x;
+        }
+    }
+    float dn = (ds + L.g) * L.cf.x;
+    if (omega != 1.0f) dn = me + omega * (dn - me);
+    gb.dfc[L.s].x = dn;
+    if (last) gs_accumulate(c, gb, L.s, dn);
 }
 
 __global__ void __launch_bounds__(GS_THREADS, 1)
@@ -458,39 +470,19 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     uint32_t gen = 0;
     const uint32_t rows = c.gy * c.gz;
     const uint32_t n_units = gb.row_start[rows];
+    const int n_slots = n_units ? (int)(n_units * (uint32_t)GS_UNIT) : 1;
     const uint32_t ua = gs_cta_first_unit(gb, rows, n_units, blockIdx.x, nb);
     const uint32_t ue = gs_cta_first_unit(gb, rows, n_units, blockIdx.x + 1, nb);
     const uint32_t nu = ue - ua;
-    const int S0 = (int)(ua * (uint32_t)GS_UNIT), S1 = (int)(ue * (uint32_t)GS_UNIT);
-    const size_t rec_bytes = (size_t)nu * 2 * GS_REC * sizeof(int);
-    const size_t n_own = (size_t)nu * GS_UNIT;
-    const bool resident = rec_bytes + n_own * GS_SLOT_SMEM <= (size_t)GS_SMEM;
-    const bool cached = rec_bytes <= (size_t)GS_SMEM;
+    const bool cached = (size_t)nu * 2 * GS_REC * sizeof(int) <= (size_t)GS_SMEM;
     int* const recb = cached ? reinterpret_cast<int*>(smem) : gb.rec + (size_t)ua * 2 * GS_REC;
-    GsView own;
-    if (resident) {
-        float* f = reinterpret_cast<float*>(smem + rec_bytes);
-        own.d = f;
-        own.g = f + n_own;
-        own.invw = f + 2 * n_own;
-        own.fc = f + 3 * n_own;
-        own.fl = reinterpret_cast<uint16_t*>(f + 4 * n_own);
-        own.base = S0;
-    } else {
-        own.d = gb.d;
-        own.g = gb.g;
-        own.invw = gb.invw;
-        own.fc = gb.fc;
-        own.fl = gb.fl;
-        own.base = 0;
-    }
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
     // set-up of every slot of this CTA's units, and their index words
     for (uint32_t k = warp; k < nu; k += nwarps) {
         const GsDesc d = gb.desc[ua + k];
-        const uint32_t f0 = gs_setup_cell(c, gb, d, 0, lane, own, resident);
-        const uint32_t f1 = gs_setup_cell(c, gb, d, 1, lane, own, resident);
+        const uint32_t f0 = gs_setup_cell(c, gb, d, 0, lane);
+        const uint32_t f1 = gs_setup_cell(c, gb, d, 1, lane);
         auto nonunit = [](uint32_t fl) { return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW)) == GS_ISFLUID; };
         auto bulk = [](uint32_t fl) {
             return (fl & (GS_ISFLUID | GS_EMPTY | GS_UNITW | GS_FLUID_FACES)) == (GS_ISFLUID | GS_UNITW | GS_FLUID_FACES);
@@ -498,14 +490,8 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
         const uint32_t n0 = __ballot_sync(0xffffffffu, nonunit(f0)), n1 = __ballot_sync(0xffffffffu, nonunit(f1));
         const uint32_t b0 = __ballot_sync(0xffffffffu, bulk(f0)), b1 = __ballot_sync(0xffffffffu, bulk(f1));
         int* r = recb + (size_t)k * 2 * GS_REC;
-        gs_make_rec(d, 0, S0, S1, resident, r, lane);
-        gs_make_rec(d, 1, S0, S1, resident, r + GS_REC, lane);
-        __syncwarp();
-        if (lane == 0) {
-            r[7] |= (int)((n0 ? GS_REC_NONUNIT : 0u) | (b0 == 0xffffffffu ? GS_REC_BULK : 0u));
-            r[GS_REC + 7] |= (int)((n1 ? GS_REC_NONUNIT : 0u) | (b1 == 0xffffffffu ? GS_REC_BULK : 0u));
-        }
-        __syncwarp();
+        gs_make_rec(d, 0, (n0 ? GS_REC_NONUNIT : 0u) | (b0 == 0xffffffffu ? GS_REC_BULK : 0u), r, lane);
+        gs_make_rec(d, 1, (n1 ? GS_REC_NONUNIT : 0u) | (b1 == 0xffffffffu ? GS_REC_BULK : 0u), r + GS_REC, lane);
     }
     bool ok = gs_grid_sync(sync, nb, gen);
 
@@ -514,8 +500,8 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
         double r2 = 0.0, b2 = 0.0;
         for (uint32_t k = warp; k < nu; k += nwarps) {
             const int* r = recb + (size_t)k * 2 * GS_REC;
-            gs_residual_cell(gb, r, lane, own, resident, r2, b2);
-            gs_residual_cell(gb, r + GS_REC, lane, own, resident, r2, b2);
+            gs_residual_cell(gb, r, lane, n_slots, r2, b2);
+            gs_residual_cell(gb, r + GS_REC, lane, n_slots, r2, b2);
         }
         for (int o = 16; o > 0; o >>= 1) {
             r2 += __shfl_down_sync(0xffffffffu, r2, o);
@@ -549,76 +535,20 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
     };
 
     const float omega = c.omega;
-    // One colour over this CTA's units.  A warp takes GS_BATCH of its units at a time:
-    // first the loads of the neighbour values held in global memory, all in flight
-    // together, then the updates.
+    // one colour over this CTA's units, two units per step with all loads in flight
     auto sweep = [&](int col, bool last) {
-        for (uint32_t k0 = warp; k0 < nu; k0 += GS_BATCH * nwarps) {
-            float rv[GS_BATCH][6];
-#pragma unroll
-            for (int b = 0; b < GS_BATCH; ++b) {
-                const uint32_t k = k0 + (uint32_t)b * nwarps;
-                const bool have = k < nu;
-                const int* r = recb + ((size_t)(have ? k : 0) * 2 + col) * GS_REC;
-                const uint32_t rm = have ? (uint32_t)r[7] : 0u;
-                const uint32_t need = have ? rm & (uint32_t)own.fl[r[0] + (int)lane] : 0u;
-#pragma unroll
-                for (int f = 0; f < 6; ++f) rv[b][f] = ((need >> f) & 1u) ? __ldcg(gb.d + r[1 + f] + (int)lane) : 0.0f;
-            }
-#pragma unroll
-            for (int b = 0; b < GS_BATCH; ++b) {
-                const uint32_t k = k0 + (uint32_t)b * nwarps;
-                if (k >= nu) continue;
-                const int* r = recb + ((size_t)k * 2 + col) * GS_REC;
-                const uint32_t rm = (uint32_t)r[7];
-                const int i = r[0] + (int)lane;
-                const float me = own.d[i];
-                if (rm & GS_REC_BULK) {
-                    // six fluid faces of weight 1 on every lane: the same sum in face order
-                    float ds = 0.0f;
-#pragma unroll
-                    for (int f = 0; f < 6; ++f) ds += ((rm >> f) & 1u) ? rv[b][f] : own.d[r[1 + f] + (int)lane];
-                    float dn = (ds + own.g[i]) * own.invw[i];
-                    if (omega != 1.0f) dn = me + omega * (dn - me);
-                    own.d[i] = dn;
-                    if (resident) gb.d[i + own.base] = dn;
-                    if (last) gs_accumulate(c, gb, i + own.base, dn);
-                    continue;
-                }
-                const uint32_t fl = own.fl[i];
-                if (fl & GS_EMPTY) {
-                    if (last && (fl & GS_ISFLUID)) gs_accumulate(c, gb, i + own.base, me);
-                    continue;
-                }
-                const bool unit = (fl & GS_UNITW) != 0u;
-                float v[6], fj[6];
-#pragma unroll
-                for (int f = 0; f < 6; ++f) {
-                    v[f] = rv[b][f];
-                    fj[f] = 0.0f;
-                    if ((fl >> f) & 1u) {
-                        const int j = r[1 + f] + (int)lane;
-                        if (!((rm >> f) & 1u)) v[f] = own.d[j];  // a face held in shared memory
-                        if (!unit) fj[f] = ((rm >> f) & 1u) ? __ldcg(gb.fc + j) : own.fc[j];
-                    }
-                }
-                float ds = 0.0f;
-                if (unit) {
-#pragma unroll
-                    for (int f = 0; f < 6; ++f)
-                        if (fl & (1u << f)) ds += v[f];
-                } else {
-                    const float fi = own.fc[i];
-#pragma unroll
-                    for (int f = 0; f < 6; ++f)
-                        if (fl & (1u << f)) ds += gs_weight(fi, fj[f]) * v[f];
-                }
-                float dn = (ds + own.g[i]) * own.invw[i];
-                if (omega != 1.0f) dn = me + omega * (dn - me);
-                own.d[i] = dn;
-                if (resident) gb.d[i + own.base] = dn;  // the copy other CTAs read
-                if (last) gs_accumulate(c, gb, i + own.base, dn);
-            }
+        uint32_t k = warp;
+        for (; k + nwarps < nu; k += 2 * nwarps) {
+            GsLoad a, b;
+            gs_load(gb, recb + ((size_t)k * 2 + col) * GS_REC, lane, n_slots, a);
+            gs_load(gb, recb + ((size_t)(k + nwarps) * 2 + col) * GS_REC, lane, n_slots, b);
+            gs_update(c, gb, a, omega, last);
+            gs_update(c, gb, b, omega, last);
+        }
+        if (k < nu) {
+            GsLoad a;
+            gs_load(gb, recb + ((size_t)k * 2 + col) * GS_REC, lane, n_slots, a);
+            gs_update(c, gb, a, omega, last);
         }
     };
 
@@ -656,7 +586,7 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
             const int x = d.x0 + 2 * (int)lane + ((col + d.y + d.z) & 1);
             if (x >= (int)c.gx) continue;
             const int s = gs_slot(d.row[0], col, x);
-            if (!(gb.fl[s] & GS_ISFLUID)) continue;
+            if (!(__float_as_uint(gb.cf[s].y) & GS_ISFLUID)) continue;
             const uint32_t ci = c.cell((uint32_t)x, (uint32_t)d.y, (uint32_t)d.z);
             const float2 p = gb.p[s];
             c.pf[ci] = p.x;

@@ -108,13 +108,11 @@ struct GsBuffers {
     GsDesc* desc;         // [max_units] slot offsets of each unit and of its neighbour rows
     int* rec;             // [max_units][2][8] per-colour index words of the solve (when they do not
                           // fit in shared memory)
-    float* d;             // [slots] correction of the current refinement cycle
+    float2* cf;           // [slots] 1 / (sum of the face weights), face flags
+    float2* dfc;          // [slots] correction of the refinement cycle, fill code (2: bed-coupled)
     float* g;             // [slots] FP64 residual of the cycle, rounded to fp32
-    float* invw;          // [slots] 1 / (sum of the face weights)
-    float* fc;            // [slots] fill code: fill fraction, 2 for bed-coupled cells
     float* b;             // [slots] dx^2 rhs
     float2* p;            // [slots] pressure hi, lo
-    uint16_t* fl;         // [slots] face flags
     double* part;         // [2 * CTAs] per-CTA partial norms
     uint32_t* sync;       // grid barrier: arrivals, generation, abort
     ScResult* result;
