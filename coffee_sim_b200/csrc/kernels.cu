@@ -261,11 +261,16 @@ __global__ void k_p2g_scatter(const Ctx* __restrict__ cp) {
 }
 
 // T = int32_t (reference lanes) or unsigned long long (int64 mode; two's-complement
-// sums are the same as signed ones)
+// sums are the same as signed ones).  In int64 mode the tile accumulates each lane in
+// two 32-bit words: a value v = H * 2^32 + L (L its low 32 bits) adds L to the low word
+// with an atomic that returns the old word, so a wrap past 2^32 is seen as a carry,
+// and H + carry to the high word only when that is nonzero (almost never for the
+// magnitudes of one sample's deposit).  High * 2^32 + low is then the sum of the
+// values modulo 2^64, exactly what 64-bit atomics give, at the cost of 32-bit ones.
 template <class T>
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict__ cp) {
     constexpr bool I64 = sizeof(T) == 8;
-    __shared__ T acc[6][P2G_NODES];
+    __shared__ uint32_t acc[I64 ? 12 : 6][P2G_NODES];
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     T* glanes = I64 ? reinterpret_cast<T*>(c.lanes64) : reinterpret_cast<T*>(c.lanes);
@@ -275,7 +280,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
         if (first == last) continue;  // uniform across the block
         const uint32_t tx = t % u.ntx, ty = (t / u.ntx) % u.nty, tz = t / (u.ntx * u.nty);
         const int ox = (int)(tx * P2G_TILE) - 1, oy = (int)(ty * P2G_TILE) - 1, oz = (int)(tz * P2G_TILE) - 1;
-        for (int i = threadIdx.x; i < 6 * P2G_NODES; i += blockDim.x) (&acc[0][0])[i] = 0;
+        for (int i = threadIdx.x; i < (I64 ? 12 : 6) * P2G_NODES; i += blockDim.x) (&acc[0][0])[i] = 0;
         __syncthreads();
         // Particles of one cell are mostly adjacent in the tile list; visiting each block
         // of P2G_THREADS entries in an odd-stride order gives a warp particles of
@@ -289,7 +294,16 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
                                 q.by + 2 < oy + P2G_SPAN && q.bz + 2 < oz + P2G_SPAN;
             if (inside) {
                 p2g_deposit<I64>(c, q, [&](int x, int y, int z, int l, auto v) {
-                    atomicAdd(&acc[l][((z - oz) * P2G_SPAN + (y - oy)) * P2G_SPAN + (x - ox)], (T)v);
+                    const int n = ((z - oz) * P2G_SPAN + (y - oy)) * P2G_SPAN + (x - ox);
+                    if constexpr (I64) {
+                        const unsigned long long w = (unsigned long long)v;
+                        const uint32_t lo = (uint32_t)w, hi = (uint32_t)(w >> 32);
+                        const uint32_t old = atomicAdd(&acc[l][n], lo);
+                        const uint32_t h = hi + ((uint32_t)(old + lo) < old ? 1u : 0u);
+                        if (h) atomicAdd(&acc[6 + l][n], h);
+                    } else {
+                        atomicAdd(reinterpret_cast<int32_t*>(&acc[l][n]), (int32_t)v);
+                    }
                 });
             } else {
                 p2g_deposit<I64>(c, q, [&](int x, int y, int z, int l, auto v) {
@@ -304,7 +318,11 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
             const uint32_t ci = cidx(u, x, y, z);
 #pragma unroll
             for (int l = 0; l < 6; ++l) {
-                const T v = acc[l][i];
+                T v;
+                if constexpr (I64)
+                    v = ((unsigned long long)acc[6 + l][i] << 32) | acc[l][i];
+                else
+                    v = (T)(int32_t)acc[l][i];
                 if (v != 0) atomicAdd(&glanes[(size_t)l * u.cells + ci], v);
             }
         }
