@@ -276,28 +276,43 @@ def test_fractional_free_surface_pressure_preserves_sparse_stream_velocity(engin
     assert v1.lateral_rms_speed / max(v0.rms_speed, 1e-6) < 0.20, (v0, v1)
 
 
-@pytest.mark.xfail(strict=False, reason=(
-    "fails on the restated algorithm (engine == oracle bit for bit): RMS-speed ratio 1.074 "
-    "against the reference's bound 1.06 after 45 frames; the reference's CI does not run it"))
-def test_viscosity_preserves_falling_stream_velocity(engine):
-    """viscosity_preserves_falling_stream_velocity (physics_tests.rs:2139-2190)."""
-    def run_case(visc):
-        s = MpmSettings.benchmark_free_stream(engine)
-        s.raw.viscosity = visc
-        _aim(s, engine, (0.0, 4.2, 0.0), (0.0, -2.0, 0.0))
-        sim = MpmSim3D(s, engine)
-        sim.set_kettle_angle(36.0)
-        for _ in range(45):
-            sim.step_frame(FRAME)
-        out = ps.water_velocity_snapshot(sim, s)
-        sim.close()
-        return out
+def _falling_stream_velocity(engine, visc, angle):
+    s = MpmSettings.benchmark_free_stream(engine)
+    s.raw.viscosity = visc
+    _aim(s, engine, (0.0, 4.2, 0.0), (0.0, -2.0, 0.0))
+    sim = MpmSim3D(s, engine)
+    sim.set_kettle_angle(angle)
+    for _ in range(45):
+        sim.step_frame(FRAME)
+    out = ps.water_velocity_snapshot(sim, s)
+    sim.close()
+    return out
 
-    a, b = run_case(0.0), run_case(1.2)
+
+def _check_falling_stream(a, b):
     assert a.all_finite and b.all_finite and a.active_count > 0 and b.active_count > 0
     assert _drift(a.active_mass, b.active_mass) < 0.05
     assert 0.94 < b.rms_speed / max(a.rms_speed, 1e-6) < 1.06, (a, b)
     assert 0.94 < b.mean_speed / max(a.mean_speed, 1e-6) < 1.06, (a, b)
+
+
+@pytest.mark.xfail(strict=False, reason=(
+    "fails on the restated algorithm (engine == oracle bit for bit) at exactly 36 degrees: RMS-speed "
+    "ratio 1.074 against the bound 1.06; the statistic is chaotic in the input: the oracle in FP64 "
+    "gives 1.049, and the same FP32 algorithm at 35.9 and 36.1 degrees gives 1.041 and 1.039 (both "
+    "pass, test_viscosity_falling_stream_bounds_hold_near_36_degrees); the reference's CI does not "
+    "run it"))
+def test_viscosity_preserves_falling_stream_velocity(engine):
+    """viscosity_preserves_falling_stream_velocity (physics_tests.rs:2139-2190)."""
+    _check_falling_stream(_falling_stream_velocity(engine, 0.0, 36.0), _falling_stream_velocity(engine, 1.2, 36.0))
+
+
+@pytest.mark.parametrize("angle", [35.9, 36.1])
+def test_viscosity_falling_stream_bounds_hold_near_36_degrees(engine, angle):
+    """The reference's bounds of viscosity_preserves_falling_stream_velocity
+    (physics_tests.rs:2139-2190) with the kettle 0.1 degree either side of the scenario's
+    36 degrees: viscosity leaves the sparse falling stream's RMS and mean speed within 6 %."""
+    _check_falling_stream(_falling_stream_velocity(engine, 0.0, angle), _falling_stream_velocity(engine, 1.2, angle))
 
 
 def test_slow_spout_translation_does_not_whip_free_stream(engine):
@@ -533,20 +548,37 @@ def test_fine_grind_pools_more_than_coarse_grind(engine):
             or fine_below.active_mass <= coarse_below.active_mass * 0.85), (fine_below, coarse_below)
 
 
-@pytest.mark.xfail(strict=False, reason=(
-    "fails on the restated algorithm: throughput ratio 0.45 (FP32, engine == oracle) and 0.36 "
-    "(oracle in FP64) against the bound 0.35, with the bed's exit speed above the open filter's; "
-    "the statistic moves by 25 % with the arithmetic precision alone"))
-def test_coffee_bed_slows_post_bed_downward_flow(cp, cp_open):
-    """coffee_bed_slows_post_bed_downward_flow (physics_tests.rs:2296-2345)."""
-    bed = ps.water_velocity_snapshot(cp.run((36, 150)), cp.settings, -6.2, -3.35)
-    opn = ps.water_velocity_snapshot(cp_open.run((36, 150)), cp_open.settings, -6.2, -3.35)
+def _check_bed_slows_flow(bed, opn):
     assert opn.all_finite and bed.all_finite
     assert opn.active_count > 20, opn
     open_down = max(-opn.momentum[1] / max(opn.active_mass, 1e-6), 0.0)
     bed_down = max(-bed.momentum[1] / max(bed.active_mass, 1e-6), 0.0)
     throughput = bed.active_mass / max(opn.active_mass, 1e-6)
     assert throughput < 0.35 or bed_down < open_down * 0.85, (throughput, open_down, bed_down)
+
+
+@pytest.mark.xfail(strict=False, reason=(
+    "fails on the restated algorithm at exactly 36 degrees: throughput ratio 0.45 (FP32, engine == "
+    "oracle) and 0.36 (oracle in FP64) against 0.35, with the bed's exit speed above the open "
+    "filter's; the statistic is chaotic in the input: at 35.9 and 36.1 degrees the same FP32 "
+    "algorithm passes through the exit-speed condition (0.63 and 0.66 of the open filter's, bound "
+    "0.85; test_coffee_bed_slowing_holds_near_36_degrees)"))
+def test_coffee_bed_slows_post_bed_downward_flow(cp, cp_open):
+    """coffee_bed_slows_post_bed_downward_flow (physics_tests.rs:2296-2345)."""
+    bed = ps.water_velocity_snapshot(cp.run((36, 150)), cp.settings, -6.2, -3.35)
+    opn = ps.water_velocity_snapshot(cp_open.run((36, 150)), cp_open.settings, -6.2, -3.35)
+    _check_bed_slows_flow(bed, opn)
+
+
+@pytest.mark.parametrize("angle", [35.9, 36.1])
+def test_coffee_bed_slowing_holds_near_36_degrees(cp, cp_open, angle):
+    """The reference's condition of coffee_bed_slows_post_bed_downward_flow
+    (physics_tests.rs:2296-2345) with the kettle 0.1 degree either side of the scenario's
+    36 degrees: below the bed, either much less water than under an open filter or a
+    downward speed below 0.85 of the open filter's."""
+    bed = ps.water_velocity_snapshot(cp.run((angle, 150)), cp.settings, -6.2, -3.35)
+    opn = ps.water_velocity_snapshot(cp_open.run((angle, 150)), cp_open.settings, -6.2, -3.35)
+    _check_bed_slows_flow(bed, opn)
 
 
 def test_slow_spout_translation_does_not_whip_post_bed_stream(cp):
