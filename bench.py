@@ -183,9 +183,14 @@ def make_settings(lib, key, args, device=0, learned=False):
     r.first_check = wl["first_check"] if args.first_check is None else args.first_check
     r.rbgs_kernel = {"auto": 0, "p2p": 2, "cluster": 3, "grid": 4}[args.solve_sync]
     r.p2g_mode = {"atomic": _ffi.CS_P2G_ATOMIC32, "sorted": _ffi.CS_P2G_SORTED_SHARED,
-                  "int64": _ffi.CS_P2G_INT64}[wl["p2g"]]
+                  "int64": _ffi.CS_P2G_INT64}[p2g_of(key, args)]
     r.device_emission = 1  # jet samples built on the device (the oracle matches this mode)
     return s
+
+
+def p2g_of(key, args):
+    """The P2G mode a run uses: the workload's unless --p2g overrides it."""
+    return WORKLOADS[key]["p2g"] if args.p2g == "default" else args.p2g
 
 
 def build_scene(lib, key, args, device=0, learned=False, populate=True):
@@ -288,7 +293,7 @@ def run_pour(lib, key, args, device, world, dist, barrier, with_learned, with_cp
     n_p = sim.particle_count()
     n_c = sim.settings.cells
     n_bed = sim.num_bed
-    int64 = WORKLOADS[key]["p2g"] == "int64"
+    int64 = p2g_of(key, args) == "int64"
     # warm-up substeps bring the pour to its state before the window; every timed loop
     # replays the same K substeps from a snapshot of that state
     for k in range(W):
@@ -383,7 +388,7 @@ def run_pour(lib, key, args, device, world, dist, barrier, with_learned, with_cp
                    "residual_tol": 1e-5, "omega": float(sim.settings.rbgs_omega), "warm_start": "previous substep",
                    "check_every_pairs": int(sim.settings.check_every),
                    "first_check_pairs": int(sim.settings.first_check or sim.settings.check_every),
-                   "p2g": wl["p2g"], "pressure_solve": "grid-wide cooperative solve" if n_c > (1 << 18)
+                   "p2g": p2g_of(key, args), "pressure_solve": "grid-wide cooperative solve" if n_c > (1 << 18)
                    else "thread-block-cluster solve", "emission": "device kernel",
                    "timed_launch": "CUDA graph replay" if use_graph else "direct launches",
                    "e2e_launch": ("CUDA graph replay" if use_graph else "direct launches")
@@ -681,6 +686,8 @@ def make_parser():
     ap.add_argument("--nested-steps", type=int, default=10, help="timed substeps of each nested workload")
     ap.add_argument("--grid", type=int, default=None, help="grid side override (small CPU checks of the arms)")
     ap.add_argument("--omega", type=float, default=None, help="over-relaxation (default: the workload's)")
+    ap.add_argument("--p2g", default="default", choices=["default", "atomic", "sorted", "int64"],
+                    help="P2G accumulation (default: the workload's)")
     ap.add_argument("--max-sweeps", type=int, default=12000)
     ap.add_argument("--solve-sync", default="auto", choices=["auto", "p2p", "cluster", "grid"],
                     help="pressure solve: auto (cluster-resident up to 2^18 cells, grid-wide above), the "
