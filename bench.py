@@ -211,19 +211,26 @@ def step(sim, key, k):
     sim.step_substep(DT)
 
 
-def ncu_traffic(kernel, tag):
+def ncu_traffic(kernel, tag, pairs=None):
     """DRAM bytes (read + write) per launch of `kernel` from the committed ncu summary
-    of this workload (a line `dram_bytes_per_launch = N` in profiles/<kernel>_*<tag>*.md),
-    or None."""
+    of this workload (profiles/<kernel>_*<tag>*.md): `dram_bytes_per_pair` times the
+    launch's red-black pairs when the summary gives it (the solve), else
+    `dram_bytes_per_launch`, else None."""
     for f in sorted((ROOT / "profiles").glob(f"{kernel}_*.md")):
         if tag not in f.name:
             continue
+        vals = {}
         for ln in f.read_text().splitlines():
-            if ln.strip().startswith("dram_bytes_per_launch"):
+            k, _, v = ln.partition("=")
+            if k.strip() in ("dram_bytes_per_pair", "dram_bytes_per_launch"):
                 try:
-                    return float(ln.split("=", 1)[1].strip().split()[0])
+                    vals[k.strip()] = float(v.strip().split()[0])
                 except (IndexError, ValueError):
-                    return None
+                    pass
+        if pairs is not None and "dram_bytes_per_pair" in vals:
+            return vals["dram_bytes_per_pair"] * pairs
+        if "dram_bytes_per_launch" in vals:
+            return vals["dram_bytes_per_launch"]
     return None
 
 
@@ -274,7 +281,8 @@ def roofline(key, prof, n_p, n_c, n_f, peak, peak_kind, int64):
     step_ms = sum(phase.values())
     tag = WORKLOADS[key]["name"].split("_")[-1]
     return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": ncu_traffic(kernel.split()[0], tag),
+            "frac": achieved / peak,
+            "traffic": ncu_traffic(kernel.split()[0], tag, pairs * n / launches if dom == "sweeps" else None),
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6650 GB/s", "algorithmic_bytes_per_launch": per, "bytes_model": model,
             "dense_grid_bytes_per_launch": dense, "launch_ms": ms, "launches": int(launches),
