@@ -575,7 +575,10 @@ def run_c4(args, rank, world, local, dist, steps=None, warmup=None):
         settings[i].raw.check_every = 60 if args.check_every is None else args.check_every
         settings[i].raw.first_check = 0 if args.first_check is None else args.first_check
         settings[i].raw.rbgs_kernel = {"auto": 0, "p2p": 2, "cluster": 3, "grid": 2}[args.solve_sync]
+    # the batched substep is captured once and replayed (no host synchronisation per substep)
+    settings[mine[0]].raw.use_graph = 0 if args.no_graph else 1
     ens = MpmEnsemble([settings[i] for i in mine], lib)
+    settings[mine[0]].raw.use_graph = 0
     for k, i in enumerate(mine):
         f = fills[i]
         scenes.populate_c2(ens.member(k), fill_top=f["fill_top"], pool_depth=f["pool_depth"], seed=f["seed"])
@@ -620,7 +623,9 @@ def run_c4(args, rank, world, local, dist, steps=None, warmup=None):
                        "residual_checks_mean": sum(v[2] for v in stats.values()) / len(stats), "residual_tol": 1e-5,
                        "omega": float(settings[mine[0]].raw.rbgs_omega),
                        "check_every_pairs": int(settings[mine[0]].raw.check_every),
-                       "first_check_pairs": int(settings[mine[0]].raw.first_check or settings[mine[0]].raw.check_every), "timing": "CUDA events on the ensemble stream, max over ranks",
+                       "first_check_pairs": int(settings[mine[0]].raw.first_check or settings[mine[0]].raw.check_every),
+                       "timed_launch": "direct launches" if args.no_graph else "CUDA graph replay of the batched substep",
+                       "timing": "CUDA events on the ensemble stream, max over ranks",
                        "l2": "not flushed: 64 resident pours' particle and grid arrays exceed the 126 MB L2 many times over"
                              if args.instances >= 16 else "not flushed",
                        "parallelism": f"instances sharded over {world} GPU(s)"},

@@ -119,6 +119,7 @@ struct Ctx {
     uint32_t* metrics;      // 8 counters
     double* resid;          // [0] sum r^2, [1] sum b^2
     ScBuffers sb;           // cluster-resident pressure solve scratch of this instance
+    ScTotals* totals;       // running solve totals of replayed substeps (graph mode)
     GsBuffers gs;           // grid-wide pressure solve scratch (large grids)
 };
 

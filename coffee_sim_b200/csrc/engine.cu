@@ -13,6 +13,7 @@
 
 #include "engine.h"
 #include "kernels.cu"
+#include "batch_scan.cuh"
 #include "solver_cluster.cuh"
 #include "solver_grid.cuh"
 
@@ -131,6 +132,7 @@ int Engine::init() {
     if ((rc = alloc(resid_, 4 * sizeof(double)))) return rc;
     if ((rc = alloc(sc_totals_, sizeof(ScTotals)))) return rc;
     cudaMemsetAsync(sc_totals_.ptr, 0, sizeof(ScTotals), stream_);
+    ctx_.totals = (ScTotals*)sc_totals_.ptr;
     if ((rc = alloc(d_ctx_, sizeof(Ctx)))) return rc;
     if ((rc = alloc(staging_, std::max<size_t>(mp * 12 * sizeof(float), cells_ * 6 * sizeof(int32_t))))) return rc;
     // cluster-resident solver: buffers and the largest launchable cluster size
@@ -1293,8 +1295,10 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
 Ensemble::~Ensemble() {
     if (stream) cudaStreamSynchronize(stream);
     for (Engine* e : eng) delete e;
+    if (gexec) cudaGraphExecDestroy(gexec);
     if (d_ctx) cudaFree(d_ctx);
     if (d_results) cudaFree(d_results);
+    if (d_partial) cudaFree(d_partial);
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
     if (stream) cudaStreamDestroy(stream);
@@ -1354,9 +1358,20 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
         set_error("ensembles in residual mode need FP32 storage and the cluster-resident solve");
         return CS_ERR_UNSUPPORTED;
     }
+    graph = s[0].use_graph != 0;
+    if (graph && e0.settings.solve_mode != CS_SOLVE_RESIDUAL) {
+        set_error("ensemble graph replay needs the residual-mode solve");
+        return CS_ERR_UNSUPPORTED;
+    }
+    if (graph && e0.settings.warm_start == CS_WARM_LEARNED) {
+        set_error("the learned warm start of an ensemble runs without graph replay (use_graph = 0)");
+        return CS_ERR_UNSUPPORTED;
+    }
     ranks = e0.sc_ranks_;
+    const size_t chunks = std::max<size_t>(bs_max_chunks(e0.sc_codes_), bs_max_chunks((size_t)e0.p2g_tiles_ + 1));
     if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&d_ctx, sizeof(Ctx) * n) != cudaSuccess || cudaMalloc(&d_results, sizeof(ScResult) * n) != cudaSuccess) {
+        cudaMalloc(&d_ctx, sizeof(Ctx) * n) != cudaSuccess || cudaMalloc(&d_results, sizeof(ScResult) * n) != cudaSuccess ||
+        cudaMalloc(&d_partial, sizeof(unsigned long long) * n * chunks) != cudaSuccess) {
         set_error("ensemble allocation failed");
         return CS_ERR_CUDA;
     }
@@ -1376,13 +1391,16 @@ int Ensemble::sync() {
 }
 
 // One substep of every instance: host prologues (jet plans, uniforms), one context
-// upload, then each pass as a single launch over all instances.
+// upload, then each pass as a single launch over all instances — enqueued directly, or
+// in graph mode replayed from a graph captured at the first substep.
 int Ensemble::substep(float sub_dt) {
     int rc;
     const uint32_t n = size();
     for (uint32_t i = 0; i < n; ++i) {
         Engine& e = *eng[i];
-        if ((rc = e.sync())) return rc;  // no work of its own may be in flight
+        // no work of an instance's own may be in flight (in graph mode an instance has
+        // none: its results are read after the ensemble stream synchronised)
+        if (!graph && (rc = e.sync())) return rc;
         if ((rc = e.emit(sub_dt))) return rc;
         e.fill_params(e.ctx_.u, sub_dt);
         e.ctx_.u.jet = e.jet_;
@@ -1392,17 +1410,42 @@ int Ensemble::substep(float sub_dt) {
         set_error("ensemble context upload failed");
         return CS_ERR_CUDA;
     }
-    if ((rc = enqueue())) return rc;
+    if ((rc = graph ? substep_graph() : enqueue(false))) return rc;
     for (uint32_t i = 0; i < n; ++i) {
         Engine& e = *eng[i];
         e.total_time += sub_dt;
         e.have_prev_p = true;
         e.prof_.substeps += 1;
+        if (graph) e.graph_pending_ = true;  // solve totals read at the next synchronising call
     }
     return CS_OK;
 }
 
-int Ensemble::enqueue() {
+// Graph mode: the batched substep captured once (launch shapes cover every instance's
+// max_particles) and replayed; each instance's solve result goes to its running totals.
+// An instance whose fluid overflows its cluster is reported (CS_ERR_CAPACITY) at the
+// next metrics read instead of being re-solved alone.
+int Ensemble::substep_graph() {
+    int rc;
+    if (!gexec) {
+        if ((rc = ens_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")))
+            return rc;
+        const int erc = enqueue(true);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        if (erc) {
+            if (g) cudaGraphDestroy(g);
+            return erc;
+        }
+        if ((rc = ens_check(ce, "end capture"))) return rc;
+        rc = ens_check(cudaGraphInstantiate(&gexec, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        if (rc) return rc;
+    }
+    return ens_check(cudaGraphLaunch(gexec, stream), "graph launch");
+}
+
+int Ensemble::enqueue(bool capture) {
     int rc;
     const uint32_t n = size();
     Engine& e0 = *eng[0];
@@ -1410,7 +1453,7 @@ int Ensemble::enqueue() {
     const Ctx* dc = (const Ctx*)d_ctx;
     uint32_t max_np = 0, max_bed = 0, max_jet = 0;
     for (Engine* e : eng) {
-        max_np = std::max(max_np, e->num_water + e->num_bed);
+        max_np = std::max(max_np, capture ? e->settings.max_particles : e->num_water + e->num_bed);
         max_bed = std::max(max_bed, e->num_bed);
         max_jet = std::max(max_jet, e->jet_.count);
     }
@@ -1419,17 +1462,16 @@ int Ensemble::enqueue() {
     const int bb = e0.launch_particle_blocks(max_bed);
     const dim3 T(kThreads);
     cudaStream_t st = stream;
-    if (max_jet) k_emit_jet<<<dim3(e0.launch_particle_blocks(max_jet), n), T, 0, st>>>(dc);
+    if (capture)
+        k_emit_jet<<<dim3(16, n), T, 0, st>>>(dc);
+    else if (max_jet)
+        k_emit_jet<<<dim3(e0.launch_particle_blocks(max_jet), n), T, 0, st>>>(dc);
     k_clear_batch<<<dim3(cb, n), T, 0, st>>>(dc, e0.p2g_tiles_ + 1);
     if (max_bed) k_bed_lookup_scatter<<<dim3(bb, n), T, 0, st>>>(dc);
     if (max_np) {
         if (s.p2g_mode != CS_P2G_ATOMIC32) {
             k_p2g_keys<<<dim3(pb, n), T, 0, st>>>(dc);
-            for (Engine* e : eng) {
-                size_t temp = e->tile_temp_.bytes;
-                cub::DeviceScan::ExclusiveSum(e->tile_temp_.ptr, temp, (const uint32_t*)e->tile_count_.ptr,
-                                              (uint32_t*)e->tile_start_.ptr, (int)e->p2g_tiles_ + 1, st);
-            }
+            bs_launch<uint32_t>(dc, n, e0.p2g_tiles_ + 1, (uint32_t*)d_partial, st);
             k_p2g_scatter<<<dim3(pb, n), T, 0, st>>>(dc);
             const int tb = (int)std::min<uint32_t>(e0.p2g_tiles_, (uint32_t)e0.sms_ * 16);
             if (s.p2g_mode == CS_P2G_INT64)
@@ -1457,10 +1499,15 @@ int Ensemble::enqueue() {
         }
     }
     if (s.solve_mode == CS_SOLVE_RESIDUAL) {
-        if ((rc = sc_launch_prep(dc, hsb.data(), (uint32_t)e0.sc_codes_, ranks, n, st, e0.sms_))) return rc;
+        if ((rc = sc_launch_prep(dc, hsb.data(), (uint32_t)e0.sc_codes_, ranks, n, st, e0.sms_, d_partial)))
+            return rc;
         if ((rc = sc_launch_cluster(dc, ranks, n, s.residual_tol, s.max_sweeps, s.check_every, st,
                                     s.rbgs_kernel == 3 ? 0u : 1u)))
             return rc;
+        if (capture) {
+            k_sc_account_batch<<<(n + 127) / 128, 128, 0, st>>>(dc, n);
+            goto after_solve;
+        }
         k_gather_results<<<1, 256, 0, st>>>(dc, n, (ScResult*)d_results);
         if (cudaMemcpyAsync(results.data(), d_results, sizeof(ScResult) * n, cudaMemcpyDeviceToHost, st) !=
                 cudaSuccess ||
@@ -1509,6 +1556,7 @@ int Ensemble::enqueue() {
             e->prof_.sweeps += s.pressure_rbgs_pairs;
         }
     }
+after_solve:
     k_project<<<dim3(cb, n), T, 0, st>>>(dc, 1 | 2 | 4);
     k_packing_apply<<<dim3(cb, n), T, 0, st>>>(dc, 1);
     k_viscosity_prepare<<<dim3(cb, n), T, 0, st>>>(dc);
@@ -1926,15 +1974,19 @@ size_t sc_scan_temp_bytes(uint32_t codes) {
 // `instances` solves whose scratch blocks lie back to back (kScPrepLaunches launches
 // for one instance).
 int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ranks, uint32_t instances,
-                   cudaStream_t stream, int sms) {
+                   cudaStream_t stream, int sms, void* bs_partial) {
     const int cb = (int)std::min<size_t>((codes + kThreads - 1) / kThreads, (size_t)sms * 16);
     k_sc_flags<<<dim3(cb, instances), kThreads, 0, stream>>>(d_ctx, codes);
-    for (uint32_t k = 0; k < instances; ++k) {
-        size_t temp = sb[k].cub_bytes;
-        if (cub::DeviceScan::ExclusiveSum(sb[k].cub_temp, temp, sb[k].flags, sb[k].scan, (int)codes, stream) !=
-            cudaSuccess) {
-            set_error("scan launch failed");
-            return CS_ERR_CUDA;
+    if (bs_partial) {
+        bs_launch<unsigned long long>(d_ctx, instances, codes, (unsigned long long*)bs_partial, stream);
+    } else {
+        for (uint32_t k = 0; k < instances; ++k) {
+            size_t temp = sb[k].cub_bytes;
+            if (cub::DeviceScan::ExclusiveSum(sb[k].cub_temp, temp, sb[k].flags, sb[k].scan, (int)codes, stream) !=
+                cudaSuccess) {
+                set_error("scan launch failed");
+                return CS_ERR_CUDA;
+            }
         }
     }
     k_sc_totals<<<dim3(1, instances), 1, 0, stream>>>(d_ctx, (uint32_t)ranks, codes);

@@ -202,15 +202,19 @@ public:
     uint32_t size() const { return (uint32_t)eng.size(); }
 
 private:
-    int enqueue();
+    int enqueue(bool capture);
+    int substep_graph();
     std::vector<Engine*> eng;
     cudaStream_t stream = nullptr;
     void* d_ctx = nullptr;       // n x Ctx
     void* d_results = nullptr;   // n x ScResult
+    void* d_partial = nullptr;   // chunk sums of the batched scans
     std::vector<Ctx> hctx;
     std::vector<ScBuffers> hsb;
     std::vector<ScResult> results;
     int ranks = 0;
+    bool graph = false;          // substep captured once and replayed (settings[0].use_graph)
+    cudaGraphExec_t gexec = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
 };
 

@@ -592,6 +592,24 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     }
 }
 
+// The same for every instance of a batched launch (thread i: instance i).
+__global__ void k_sc_account_batch(const Ctx* __restrict__ cp, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const ScResult r = *cp[i].sb.result;
+    ScTotals* tot = cp[i].totals;
+    tot->runs += 1;
+    if (r.status == 3) {
+        tot->timeouts += 1;
+    } else if (r.status != 1) {
+        tot->failed += 1;
+    } else {
+        tot->sweeps += r.sweeps;
+        tot->evals += r.evals;
+    }
+    tot->last = r;
+}
+
 // Adds one solve's result to the running totals (one thread; graph mode, where the
 // host does not read each substep's result).
 __global__ void k_sc_account(const ScResult* __restrict__ res, ScTotals* __restrict__ tot) {

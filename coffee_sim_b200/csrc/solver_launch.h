@@ -16,9 +16,13 @@ void set_error(const std::string& msg);
 int sc_max_cluster_ranks();
 size_t sc_scan_temp_bytes(uint32_t codes);
 // d_ctx: device array of `instances` contexts (each carrying its ScBuffers); sb: the
-// same ScBuffers on the host, for the CUB scans launched from the host.
+// same ScBuffers on the host, for the CUB scans launched from the host.  With
+// bs_partial (instances x bs_max_chunks(codes) 64-bit words of device scratch) the fluid
+// flags of all instances are scanned by the batched scan kernels instead.
 int sc_launch_prep(const Ctx* d_ctx, const ScBuffers* sb, uint32_t codes, int ranks, uint32_t instances,
-                   cudaStream_t stream, int sms);
+                   cudaStream_t stream, int sms, void* bs_partial = nullptr);
+// Chunks of the batched scan for arrays of `len` elements.
+inline uint32_t bs_max_chunks(size_t len) { return (uint32_t)((len + 4095) / 4096); }
 // p2p: 1 separates the colours with point-to-point mbarrier waits, 0 with cluster
 // barriers (rbgs_kernel = 3).
 int sc_launch_cluster(const Ctx* d_ctx, int ranks, uint32_t instances, float tol, uint32_t max_pairs,

@@ -354,7 +354,11 @@ int32_t cs_snapshot_load(CsSim* sim, const void* buffer, uint64_t bytes);
 
 /* ---- batched ensemble of independent pours (no counterpart in the reference) ----
  * n instances with their own settings (same grid dims) stepped together: one launch
- * per pass covers every instance through per-instance offset tables. */
+ * per pass covers every instance through per-instance offset tables.  With
+ * settings[0].use_graph = 1 (residual-mode solve, plain warm start) the batched substep
+ * is captured once and replayed with no host synchronisation; an instance whose fluid
+ * overflows its solve cluster is then reported as CS_ERR_CAPACITY by the next
+ * cs_ensemble_get_metrics instead of being re-solved alone. */
 int32_t cs_ensemble_create(const CsSettings* settings, uint32_t n, CsEnsemble** out);
 int32_t cs_ensemble_destroy(CsEnsemble* ens);
 int32_t cs_ensemble_step_substep(CsEnsemble* ens, float sub_dt);
