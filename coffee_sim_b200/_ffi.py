@@ -188,7 +188,8 @@ class CsSettings(C.Structure):
         ("exit_speed_override", C.c_float),
         ("rbgs_omega", C.c_float),
         ("first_check", C.c_uint32),
-        ("reserved", C.c_uint32 * 6),
+        ("reorder_every", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
     ]
 
 

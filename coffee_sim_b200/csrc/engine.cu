@@ -9,6 +9,7 @@
 #include <memory>
 #include <string>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "engine.h"
@@ -150,6 +151,15 @@ int Engine::init() {
         sc_ranks_ = sc_max_cluster_ranks();
     }
     if ((rc = gs_alloc())) return rc;
+    if (settings.reorder_every) {
+        size_t cub = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, cub, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)mp, 0, 32, stream_);
+        if ((rc = alloc(ro_keys_, (size_t)mp * 2 * sizeof(uint32_t)))) return rc;
+        if ((rc = alloc(ro_idx_, (size_t)mp * 2 * sizeof(uint32_t)))) return rc;
+        if ((rc = alloc(ro_tmp_, (size_t)mp * sizeof(float4)))) return rc;
+        if ((rc = alloc(ro_cub_, cub))) return rc;
+    }
 
     ctx_.pos = (float4*)pos_.ptr;
     ctx_.vel = (float4*)vel_.ptr;
@@ -214,6 +224,7 @@ int Engine::reset() {
     inflow.flow_override = fo;
     inflow.speed_override = so;
     have_prev_p = false;
+    substeps_done_ = 0;
     std::memset(&last, 0, sizeof(last));
     last.last_residual = last.initial_residual = -1.0;
     DeviceBuffer* zero[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_, &render_, &snap_, &delta_, &lanes_,
@@ -613,6 +624,8 @@ int Engine::substep(float sub_dt, uint32_t P) {
         set_error("training-sample capture runs with use_graph = 0");
         return CS_ERR_UNSUPPORTED;
     }
+    if (settings.reorder_every && substeps_done_ % settings.reorder_every == 0 && (rc = reorder())) return rc;
+    substeps_done_ += 1;
     if (!graph) mark(CS_PHASE_EMIT);
     if ((rc = emit(sub_dt))) return rc;
     fill_params(ctx_.u, sub_dt);
@@ -630,6 +643,45 @@ int Engine::substep(float sub_dt, uint32_t P) {
     prof_.sweeps += sweeps;
     prof_.substeps += 1;
     return CS_OK;
+}
+
+// Reorder the water samples' slots by the tile of their P2G base cell (a stable radix
+// sort of the keys, then a gather of every particle stream): samples of one tile sit in
+// consecutive slots, so the sorted P2G reads them in order and G2P's warps gather nodes
+// of neighbouring cells.  Bed samples keep their slots (bed ids index the lookup and the
+// bed deltas).  The CPU oracle applies the same stable permutation.  Launched directly
+// ahead of the substep's work (also in graph mode).
+int Engine::reorder() {
+    const uint32_t n = num_water;
+    if (n < 2) return CS_OK;
+    const Ctx* dc = (const Ctx*)d_ctx_.ptr;
+    fill_params(ctx_.u, 0.0f);
+    int rc = upload_ctx();
+    if (rc) return rc;
+    uint32_t* keys = (uint32_t*)ro_keys_.ptr;
+    uint32_t* idx = (uint32_t*)ro_idx_.ptr;
+    const size_t mp = settings.max_particles;
+    const int pb = launch_particle_blocks(n);
+    k_reorder_keys<<<dim3(pb, 1), kThreads, 0, stream_>>>(dc, keys, idx);
+    const uint32_t tiles = p2g_tiles_;
+    int end_bit = 1;
+    while (end_bit < 32 && (1u << end_bit) <= tiles) ++end_bit;
+    size_t temp = ro_cub_.bytes;
+    if ((rc = check(cub::DeviceRadixSort::SortPairs(ro_cub_.ptr, temp, keys, keys + mp, idx, idx + mp, (int)n, 0,
+                                                    end_bit, stream_),
+                    "reorder sort")))
+        return rc;
+    DeviceBuffer* streams[] = {&pos_, &vel_, &c0_, &c1_, &c2_, &bedA_, &bedB_};
+    for (DeviceBuffer* b : streams) {
+        float4* base = (float4*)b->ptr;
+        k_reorder_gather<<<dim3(pb, 1), kThreads, 0, stream_>>>(base, (float4*)ro_tmp_.ptr, idx + mp, num_bed, n);
+        if ((rc = check(cudaMemcpyAsync(base + num_bed, ro_tmp_.ptr, (size_t)n * sizeof(float4),
+                                        cudaMemcpyDeviceToDevice, stream_),
+                        "reorder copy")))
+            return rc;
+    }
+    count_launch(1 + 7);
+    return check(cudaGetLastError(), "reorder");
 }
 
 // The device work of one substep.  With `capture`, the stream is being captured into a
@@ -1202,6 +1254,7 @@ struct SnapHeader {
     uint32_t total_dropped, have_prev_p;
     host::Inflow inflow;
     CsSpout spout;  // set_spout_position / set_spout_target move it (mod.rs:452-458)
+    uint64_t substeps_done;
 };
 static const uint64_t kSnapMagic = 0x43534e4150423230ull;  // "CSNAPB20"
 
@@ -1221,7 +1274,8 @@ int Engine::snapshot_save(void* buf, uint64_t bytes) {
     SnapHeader h;
     std::memset(&h, 0, sizeof(h));
     h.magic = kSnapMagic;
-    h.version = 3;
+    h.version = 4;
+    h.substeps_done = substeps_done_;
     h.max_p = settings.max_particles;
     h.cells = cells_;
     h.num_water = num_water;
@@ -1261,7 +1315,7 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
         return CS_ERR_INVALID_ARG;
     }
     std::memcpy(&h, buf, sizeof(h));
-    if (h.magic != kSnapMagic || h.version != 3 || h.max_p != settings.max_particles || h.cells != cells_ ||
+    if (h.magic != kSnapMagic || h.version != 4 || h.max_p != settings.max_particles || h.cells != cells_ ||
         bytes < need) {
         set_error("snapshot does not match this simulation's sizes");
         return CS_ERR_INVALID_ARG;
@@ -1286,6 +1340,7 @@ int Engine::snapshot_load(const void* buf, uint64_t bytes) {
     total_emitted_mass = h.total_emitted_mass;
     total_dropped = h.total_dropped;
     have_prev_p = h.have_prev_p != 0;
+    substeps_done_ = h.substeps_done;
     inflow = h.inflow;
     settings.spout = h.spout;
     return sync();
@@ -1358,6 +1413,11 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
         set_error("ensembles in residual mode need FP32 storage and the cluster-resident solve");
         return CS_ERR_UNSUPPORTED;
     }
+    for (uint32_t i = 0; i < n; ++i)
+        if (s[i].reorder_every) {
+            set_error("ensemble instances do not reorder their samples (reorder_every must be 0)");
+            return CS_ERR_UNSUPPORTED;
+        }
     graph = s[0].use_graph != 0;
     if (graph && e0.settings.solve_mode != CS_SOLVE_RESIDUAL) {
         set_error("ensemble graph replay needs the residual-mode solve");

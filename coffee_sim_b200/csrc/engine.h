@@ -128,6 +128,10 @@ private:
     // cluster-resident solver
     DeviceBuffer sc_scratch_;  // every solver scratch buffer, laid out by sc_scratch_layout
     ScBuffers sc_buf_{};
+    // reorder of the water samples by tile (settings.reorder_every)
+    int reorder();
+    DeviceBuffer ro_keys_, ro_idx_, ro_tmp_, ro_cub_;
+    uint64_t substeps_done_ = 0;   // substeps since creation (reorder schedule; snapshotted)
     // grid-wide solver (grids above kClusterMaxCells cells)
     int gs_alloc();
     int solve_grid(uint32_t& sweeps, double& r0, double& r1, bool& done);

@@ -251,6 +251,33 @@ __global__ void k_p2g_keys(const Ctx* __restrict__ cp) {
     }
 }
 
+// ---- reorder of the water samples by tile (reorder_every) ----
+// Key of water slot num_bed + i: the tile of its P2G base cell, the tile count for a
+// sample that deposits nothing; the value is its own index, for a stable sort.
+__global__ void k_reorder_keys(const Ctx* __restrict__ cp, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+    const Ctx& c = cp[0];
+    const Params& u = c.u;
+    CS_FOR(i, u.num_water) {
+        const uint32_t pid = u.num_bed + i;
+        const float4 P = c.pos[pid], Vv = c.vel[pid];
+        uint32_t key = u.ntx * u.nty * u.ntz;
+        if (is_water_phase(c.c0[pid].w) && !(Vv.w <= inactive_mass(u))) {
+            const int bx = (int)floorf((P.x - u.ox) * u.inv_dx - 0.5f);
+            const int by = (int)floorf((P.y - u.oy) * u.inv_dx - 0.5f);
+            const int bz = (int)floorf((P.z - u.oz) * u.inv_dx - 0.5f);
+            key = (p2g_tile_axis(bz, u.ntz) * u.nty + p2g_tile_axis(by, u.nty)) * u.ntx + p2g_tile_axis(bx, u.ntx);
+        }
+        keys[i] = key;
+        idx[i] = i;
+    }
+}
+
+// out[i] = in[num_bed + perm[i]] for the water slots of one particle stream
+__global__ void k_reorder_gather(const float4* __restrict__ in, float4* __restrict__ out,
+                                 const uint32_t* __restrict__ perm, uint32_t num_bed, uint32_t n) {
+    CS_FOR(i, n) out[i] = in[num_bed + perm[i]];
+}
+
 __global__ void k_p2g_scatter(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     uint32_t n = c.u.num_water + c.u.num_bed;

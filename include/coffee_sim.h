@@ -235,7 +235,12 @@ typedef struct CsSettings {
     float rbgs_omega;             /* red-black over-relaxation; 0 or 1 = plain Gauss-Seidel */
     uint32_t first_check;         /* FP32 residual mode: pairs before a solve's first residual
                                      check (0: check_every); later intervals are predicted */
-    uint32_t reserved[6];
+    uint32_t reorder_every;       /* >0: every this many substeps (counted from creation), reorder
+                                     the water samples' slots stably by the 4^3-cell tile of their
+                                     P2G base cell (samples that deposit nothing last), so that
+                                     P2G and G2P touch neighbouring cells from neighbouring
+                                     threads; slot numbers of water samples change then.  0: off */
+    uint32_t reserved[5];
 } CsSettings;
 
 /* Observability counters (mod.rs:50-68 / state.rs:22-28) + solver telemetry. */

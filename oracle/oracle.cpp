@@ -17,6 +17,7 @@
 // Templated on the arithmetic type: float reproduces the engine bit for bit; double
 // is the FP64 reference run that errors are reported against.  OpenMP parallelises
 // the loops; integer fixed-point atomics keep the result independent of thread count.
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -140,6 +141,7 @@ struct Sim : SimBase {
     std::vector<int32_t> init_lookup;
     size_t cells = 0;
     bool have_prev_p = false;
+    uint64_t substeps_done = 0;  // substeps since creation (the reorder schedule)
 
     explicit Sim(const CsSettings& s) {
         settings = s;
@@ -189,6 +191,7 @@ struct Sim : SimBase {
         std::fill(lookup.begin(), lookup.end(), -1);
         std::fill(delta.begin(), delta.end(), 0);
         have_prev_p = false;
+        substeps_done = 0;
         if (!settings.has_bed) return;
         BedInit bi = init_bed(settings.bed, settings.grid_dims, settings.bounds_size);
         uint32_t n = (uint32_t)(bi.particles.size() / 8);
@@ -1766,8 +1769,53 @@ struct Sim : SimBase {
     }
 
     // mod.rs:271-419, one iteration; passes limits how many dispatches run.
+    // reorder_every (an engine extension, no reference counterpart): the water samples'
+    // slots reordered stably by the 4^3-cell tile of their P2G base cell, samples that
+    // deposit nothing last — the same permutation as the engine's radix sort of the keys.
+    void reorder_water() {
+        const uint32_t n = num_water;
+        if (n < 2) return;
+        const uint32_t nt[3] = {(u.gx + 1 + 3) / 4, (u.gy + 1 + 3) / 4, (u.gz + 1 + 3) / 4};
+        const uint32_t tiles = nt[0] * nt[1] * nt[2];
+        auto axis = [](int b, uint32_t ntile) {
+            int q = b + 1;
+            q = q < 0 ? 0 : q;
+            const uint32_t t = (uint32_t)q / 4u;
+            return t < ntile ? t : ntile - 1;
+        };
+        std::vector<uint32_t> key(n), perm(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t pid = num_bed + i;
+            const R* p = &part[(size_t)pid * 8];
+            const R phase = aff[(size_t)pid * 12 + 3];
+            key[i] = tiles;
+            if (is_water_phase(phase) && !(p[7] <= inactive_mass_threshold())) {
+                const V gp = (V3<R>(p[0], p[1], p[2]) - u.origin) * u.inv_dx;
+                const int bx = (int)std::floor(gp.x - R(0.5)), by = (int)std::floor(gp.y - R(0.5)),
+                          bz = (int)std::floor(gp.z - R(0.5));
+                key[i] = (axis(bz, nt[2]) * nt[1] + axis(by, nt[1])) * nt[0] + axis(bx, nt[0]);
+            }
+            perm[i] = i;
+        }
+        std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+        auto permute = [&](std::vector<R>& v, size_t width) {
+            std::vector<R> tmp((size_t)n * width);
+            for (uint32_t i = 0; i < n; ++i)
+                for (size_t k = 0; k < width; ++k) tmp[(size_t)i * width + k] = v[((size_t)num_bed + perm[i]) * width + k];
+            std::copy(tmp.begin(), tmp.end(), v.begin() + (size_t)num_bed * width);
+        };
+        permute(part, 8);
+        permute(aff, 12);
+        permute(bedx, 8);
+    }
+
     int substep(float sub_dt, uint32_t passes) override {
         const CsSettings& s = settings;
+        if (s.reorder_every && substeps_done % s.reorder_every == 0) {
+            write_uniforms(R(sub_dt));
+            reorder_water();
+        }
+        ++substeps_done;
         float pm = s.brew.water_mass_units_per_ml / s.brew.water_particles_per_ml;
         uint32_t em = 0, dr = 0;
         emit(sub_dt, pm, em, dr);
