@@ -36,20 +36,20 @@ METRIC = "particle-steps/sec & pressure-solve ms at 1e-5 residual: learned vs pl
 UNIT = "particle-steps/s"
 DT = 5.0e-4
 
-# The timed configurations.  omega is the measured optimum of each pour (cs_autotune's
-# scan 1.80-1.96); the check cap is the longest interval between FP64 residual checks
+# The timed configurations.  omega is the measured optimum of each pour (192^3: pairs per
+# substep 367/299/222/272/363 for omega 1.93..1.97; 128^3: 228/201/221/285/378); the check cap is the longest interval between FP64 residual checks
 # (after each check the solve predicts the pairs it still needs); first_check is the
 # interval before a solve's first check (0: the cap).
 WORKLOADS = {
     "c5": {"name": "c5_v60_scale_192cube", "scene": "c5_scale", "seed": 4, "omega": 1.95, "check_every": 60,
-           "first_check": 0, "p2g": "int64", "spiral": False,
+           "first_check": 0, "p2g": "int64", "spiral": False, "reorder_every": 10,
            "text": "V60 pour at 192^3 (dx 0.83 mm), two-layer bed (porosity 0.45/0.35, 10x lower permeability "
                    "below), jet 4 ml/s at 0.8 m/s 1.2 cm off centre, int64 fixed-point P2G"},
     "c3": {"name": "c3_v60_spiral_128cube", "scene": "c3_large", "seed": 2, "omega": 1.94, "check_every": 60,
-           "first_check": 0, "p2g": "sorted", "spiral": True,
+           "first_check": 0, "p2g": "sorted", "spiral": True, "reorder_every": 10,
            "text": "V60 pour at 128^3 (dx 1.25 mm), spout on the spiral path (r 1.5 cm, 0.5 Hz), tile-sorted P2G"},
     "c2": {"name": "c2_v60_midpour_64cube", "scene": "c2_v60", "seed": 1, "omega": 1.92, "check_every": 60,
-           "first_check": 125, "p2g": "sorted", "spiral": False,
+           "first_check": 125, "p2g": "sorted", "spiral": False, "reorder_every": 0,
            "text": "V60 pour at 64^3 (dx 2.5 mm), centre pour, tile-sorted P2G"},
 }
 PHASES = ["emit", "clear", "p2g", "grid", "sweeps", "residual", "project", "g2p", "bed", "render", "learned"]
@@ -185,6 +185,9 @@ def make_settings(lib, key, args, device=0, learned=False):
     r.p2g_mode = {"atomic": _ffi.CS_P2G_ATOMIC32, "sorted": _ffi.CS_P2G_SORTED_SHARED,
                   "int64": _ffi.CS_P2G_INT64}[p2g_of(key, args)]
     r.device_emission = 1  # jet samples built on the device (the oracle matches this mode)
+    # water samples reordered by P2G tile every N substeps (the oracle applies the same
+    # permutation); at 192^3 every 10 substeps: G2P 1.68 -> 1.54 ms, every 5 costs more
+    r.reorder_every = wl["reorder_every"]
     return s
 
 
@@ -396,7 +399,7 @@ def run_pour(lib, key, args, device, world, dist, barrier, with_learned, with_cp
                    "residual_tol": 1e-5, "omega": float(sim.settings.rbgs_omega), "warm_start": "previous substep",
                    "check_every_pairs": int(sim.settings.check_every),
                    "first_check_pairs": int(sim.settings.first_check or sim.settings.check_every),
-                   "p2g": p2g_of(key, args), "pressure_solve": "grid-wide cooperative solve" if n_c > (1 << 18)
+                   "p2g": p2g_of(key, args), "reorder_every": wl["reorder_every"], "pressure_solve": "grid-wide cooperative solve" if n_c > (1 << 18)
                    else "thread-block-cluster solve", "emission": "device kernel",
                    "timed_launch": "CUDA graph replay" if use_graph else "direct launches",
                    "e2e_launch": ("CUDA graph replay" if use_graph else "direct launches")
