@@ -189,7 +189,9 @@ class CsSettings(C.Structure):
         ("rbgs_omega", C.c_float),
         ("first_check", C.c_uint32),
         ("reorder_every", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("p2g_tile", C.c_uint32),
+        ("particle_threads", C.c_uint32),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 
@@ -238,7 +240,8 @@ class CsTuneResult(C.Structure):
         ("best_ms", C.c_float),
         ("initial_ms", C.c_float),
         ("first_check", C.c_uint32),
-        ("reserved", C.c_uint32 * 1),
+        ("p2g_tile", C.c_uint32),
+        ("particle_threads", C.c_uint32),
     ]
 
 

@@ -66,7 +66,8 @@ struct Params {
     // modes
     uint32_t fixed_point;      // pressure/divergence stored as i32*2^18
     uint32_t int64_grid;       // P2G accumulators are i64*2^32
-    uint32_t ntx, nty, ntz;    // P2G tile grid (tiles of P2G_TILE^3 cells over base cells -1..g-1)
+    uint32_t ntx, nty, ntz;    // P2G tile grid (tiles of p2g_tile^3 cells over base cells -1..g-1)
+    uint32_t p2g_tile;         // cells per side of a P2G tile (4 or 8)
     JetPlan jet;               // device emission of this substep (count 0: none)
     uint32_t warm;             // keep last substep's pressure in fluid cells
     float omega;               // red-black over-relaxation (1 = plain Gauss-Seidel)

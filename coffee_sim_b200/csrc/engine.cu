@@ -85,6 +85,37 @@ int Engine::launch_particle_blocks(uint32_t n) const {
     size_t b = ((size_t)n + kThreads - 1) / kThreads;
     return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sms_ * 16));
 }
+// Launch shapes the autotuner can choose: threads per block of the particle passes and
+// the P2G tile side.
+uint32_t Engine::particle_threads() const { return settings.particle_threads ? settings.particle_threads : kThreads; }
+int Engine::launch_particle_blocks_pt(uint32_t n) const {
+    const size_t t = particle_threads();
+    size_t b = ((size_t)n + t - 1) / t;
+    return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sms_ * (2048 / t)));
+}
+uint32_t Engine::p2g_tile() const { return settings.p2g_tile ? settings.p2g_tile : (uint32_t)P2G_TILE; }
+uint32_t Engine::p2g_tile_count() const {
+    const uint32_t t = p2g_tile();
+    return ((settings.grid_dims[0] + t) / t) * ((settings.grid_dims[1] + t) / t) * ((settings.grid_dims[2] + t) / t);
+}
+// The tile-sorted P2G accumulation for `instances` contexts (template by lane width and
+// tile side).
+void Engine::launch_p2g_tiles(const Ctx* dc, uint32_t instances, cudaStream_t st) const {
+    const int tb = (int)std::min<uint32_t>(p2g_tile_count(), (uint32_t)sms_ * 16);
+    const dim3 g(tb, instances);
+    const bool i64 = settings.p2g_mode == CS_P2G_INT64;
+    if (p2g_tile() == 8) {
+        if (i64)
+            k_p2g_tiles<unsigned long long, 8><<<g, P2G_THREADS, 0, st>>>(dc);
+        else
+            k_p2g_tiles<int32_t, 8><<<g, P2G_THREADS, 0, st>>>(dc);
+    } else {
+        if (i64)
+            k_p2g_tiles<unsigned long long, 4><<<g, P2G_THREADS, 0, st>>>(dc);
+        else
+            k_p2g_tiles<int32_t, 4><<<g, P2G_THREADS, 0, st>>>(dc);
+    }
+}
 
 int Engine::init() {
     int dev = settings.device;
@@ -104,6 +135,7 @@ int Engine::init() {
     if ((rc = alloc(lanes_, cells_ * 6 * sizeof(int32_t)))) return rc;
     if ((rc = alloc(lanes64_, settings.p2g_mode == CS_P2G_INT64 ? cells_ * 6 * sizeof(long long) : 0))) return rc;
     {  // sort buffers: also used when the mode is switched at run time
+        // sized for the smallest tile side (the most tiles)
         uint32_t nt[3];
         for (int a = 0; a < 3; ++a) nt[a] = (settings.grid_dims[a] + 1 + P2G_TILE - 1) / P2G_TILE;
         p2g_tiles_ = nt[0] * nt[1] * nt[2];
@@ -327,9 +359,10 @@ void Engine::fill_params(Params& u, float dt) const {
     u.bed_surface_span = g.bed_surface_span;
     u.fixed_point = s.pressure_storage == CS_PRESSURE_FIXED_POINT ? 1u : 0u;
     u.int64_grid = s.p2g_mode == CS_P2G_INT64 ? 1u : 0u;
-    u.ntx = (u.gx + 1 + P2G_TILE - 1) / P2G_TILE;
-    u.nty = (u.gy + 1 + P2G_TILE - 1) / P2G_TILE;
-    u.ntz = (u.gz + 1 + P2G_TILE - 1) / P2G_TILE;
+    u.p2g_tile = p2g_tile();
+    u.ntx = (u.gx + u.p2g_tile) / u.p2g_tile;
+    u.nty = (u.gy + u.p2g_tile) / u.p2g_tile;
+    u.ntz = (u.gz + u.p2g_tile) / u.p2g_tile;
     u.warm = (s.warm_start != CS_WARM_NONE && !u.fixed_point && have_prev_p) ? 1u : 0u;
     u.omega = s.rbgs_omega > 0.0f ? s.rbgs_omega : 1.0f;
     u.first_check = s.first_check;
@@ -694,7 +727,8 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     const uint32_t np = capture ? settings.max_particles : num_water + num_bed;
     const bool any_p = capture || np > 0, any_bed = capture || num_bed > 0;
     const int cb = launch_cells_blocks();
-    const int pb = launch_particle_blocks(np);
+    const int pb = launch_particle_blocks_pt(np);
+    const dim3 TP(particle_threads());
     const int bb = launch_particle_blocks(capture ? settings.max_particles : num_bed);
     // the bed-lookup scatter (27 atomicMax per bed sample, a few thousand samples) runs in
     // warp-sized blocks so that it spreads over the SMs (clear phase 27.7 -> 23.5 us)
@@ -726,18 +760,14 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     if (P > 3 && any_p) {
         if (settings.p2g_mode != CS_P2G_ATOMIC32) {
             cudaMemsetAsync(tile_count_.ptr, 0, tile_count_.bytes, stream_);
-            CS_LAUNCH(k_p2g_keys<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+            CS_LAUNCH(k_p2g_keys<<<dim3(pb, 1), TP, 0, stream_>>>(dc));
             size_t temp = tile_temp_.bytes;
             cub::DeviceScan::ExclusiveSum(tile_temp_.ptr, temp, (const uint32_t*)tile_count_.ptr,
-                                          (uint32_t*)tile_start_.ptr, (int)p2g_tiles_ + 1, stream_);
-            CS_LAUNCH(k_p2g_scatter<<<dim3(pb, 1), T, 0, stream_>>>(dc));
-            const int tb = (int)std::min<uint32_t>(p2g_tiles_, (uint32_t)sms_ * 16);
-            if (settings.p2g_mode == CS_P2G_INT64)
-                CS_LAUNCH(k_p2g_tiles<unsigned long long><<<dim3(tb, 1), P2G_THREADS, 0, stream_>>>(dc));
-            else
-                CS_LAUNCH(k_p2g_tiles<int32_t><<<dim3(tb, 1), P2G_THREADS, 0, stream_>>>(dc));
+                                          (uint32_t*)tile_start_.ptr, (int)p2g_tile_count() + 1, stream_);
+            CS_LAUNCH(k_p2g_scatter<<<dim3(pb, 1), TP, 0, stream_>>>(dc));
+            CS_LAUNCH(launch_p2g_tiles(dc, 1, stream_));
         } else {
-            CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+            CS_LAUNCH(k_p2g_atomic<<<dim3(pb, 1), TP, 0, stream_>>>(dc));
         }
     }
     ph(CS_PHASE_GRID);
@@ -792,13 +822,13 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
     if (P > 13) CS_LAUNCH(k_viscosity_prepare<<<dim3(cb, 1), T, 0, stream_>>>(dc));
     if (P > 14) CS_LAUNCH(k_viscosity_apply<<<dim3(cb, 1), T, 0, stream_>>>(dc, P > 15 ? 1 : 0));
     ph(CS_PHASE_G2P);
-    if (P > 16 && any_p) CS_LAUNCH(k_g2p<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    if (P > 16 && any_p) CS_LAUNCH(k_g2p<<<dim3(pb, 1), TP, 0, stream_>>>(dc));
     ph(CS_PHASE_BED);
-    if (P > 17 && any_p) CS_LAUNCH(k_bed_coupling<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    if (P > 17 && any_p) CS_LAUNCH(k_bed_coupling<<<dim3(pb, 1), TP, 0, stream_>>>(dc));
     if (P > 18 && any_bed) CS_LAUNCH(k_extraction_advect<<<dim3(bb, 1), T, 0, stream_>>>(dc));
     if (P > 19 && any_bed) CS_LAUNCH(k_bed_dynamics<<<dim3(bb, 1), T, 0, stream_>>>(dc));
     ph(CS_PHASE_RENDER);
-    if (P > 20 && any_p) CS_LAUNCH(k_prepare_render<<<dim3(pb, 1), T, 0, stream_>>>(dc));
+    if (P > 20 && any_p) CS_LAUNCH(k_prepare_render<<<dim3(pb, 1), TP, 0, stream_>>>(dc));
 #undef CS_LAUNCH
     ph(-1);
     return check(cudaGetLastError(), "substep launch");
@@ -819,6 +849,8 @@ Engine::GraphKey Engine::graph_key() const {
     k.residual_tol = s.residual_tol;
     k.num_bed = num_bed;
     k.max_particles = s.max_particles;
+    k.p2g_tile = p2g_tile();
+    k.particle_threads = particle_threads();
     return k;
 }
 
@@ -1399,7 +1431,7 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
             t.p2g_mode != a.p2g_mode || t.solve_mode != a.solve_mode || t.pressure_storage != a.pressure_storage ||
             t.device != a.device || t.pressure_rbgs_pairs != a.pressure_rbgs_pairs || t.max_sweeps != a.max_sweeps ||
             t.check_every != a.check_every || t.first_check != a.first_check || t.residual_tol != a.residual_tol ||
-            t.warm_start != a.warm_start) {
+            t.warm_start != a.warm_start || t.p2g_tile != a.p2g_tile || t.particle_threads != a.particle_threads) {
             set_error("ensemble instances must share grid dims, device, P2G mode, warm start and solver settings");
             return CS_ERR_INVALID_ARG;
         }
@@ -1428,7 +1460,7 @@ int Ensemble::init(const CsSettings* s, uint32_t n) {
         return CS_ERR_UNSUPPORTED;
     }
     ranks = e0.sc_ranks_;
-    const size_t chunks = std::max<size_t>(bs_max_chunks(e0.sc_codes_), bs_max_chunks((size_t)e0.p2g_tiles_ + 1));
+    const size_t chunks = std::max<size_t>(bs_max_chunks(e0.sc_codes_), bs_max_chunks((size_t)e0.p2g_tiles_ + 1));  // the largest tile count
     if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&d_ctx, sizeof(Ctx) * n) != cudaSuccess || cudaMalloc(&d_results, sizeof(ScResult) * n) != cudaSuccess ||
         cudaMalloc(&d_partial, sizeof(unsigned long long) * n * chunks) != cudaSuccess) {
@@ -1518,7 +1550,8 @@ int Ensemble::enqueue(bool capture) {
         max_jet = std::max(max_jet, e->jet_.count);
     }
     const int cb = e0.launch_cells_blocks();
-    const int pb = e0.launch_particle_blocks(max_np);
+    const int pb = e0.launch_particle_blocks_pt(max_np);
+    const dim3 TP(e0.particle_threads());
     const int bb = e0.launch_particle_blocks(max_bed);
     const dim3 T(kThreads);
     cudaStream_t st = stream;
@@ -1526,20 +1559,16 @@ int Ensemble::enqueue(bool capture) {
         k_emit_jet<<<dim3(16, n), T, 0, st>>>(dc);
     else if (max_jet)
         k_emit_jet<<<dim3(e0.launch_particle_blocks(max_jet), n), T, 0, st>>>(dc);
-    k_clear_batch<<<dim3(cb, n), T, 0, st>>>(dc, e0.p2g_tiles_ + 1);
+    k_clear_batch<<<dim3(cb, n), T, 0, st>>>(dc, e0.p2g_tile_count() + 1);
     if (max_bed) k_bed_lookup_scatter<<<dim3(bb, n), T, 0, st>>>(dc);
     if (max_np) {
         if (s.p2g_mode != CS_P2G_ATOMIC32) {
-            k_p2g_keys<<<dim3(pb, n), T, 0, st>>>(dc);
-            bs_launch<uint32_t>(dc, n, e0.p2g_tiles_ + 1, (uint32_t*)d_partial, st);
-            k_p2g_scatter<<<dim3(pb, n), T, 0, st>>>(dc);
-            const int tb = (int)std::min<uint32_t>(e0.p2g_tiles_, (uint32_t)e0.sms_ * 16);
-            if (s.p2g_mode == CS_P2G_INT64)
-                k_p2g_tiles<unsigned long long><<<dim3(tb, n), P2G_THREADS, 0, st>>>(dc);
-            else
-                k_p2g_tiles<int32_t><<<dim3(tb, n), P2G_THREADS, 0, st>>>(dc);
+            k_p2g_keys<<<dim3(pb, n), TP, 0, st>>>(dc);
+            bs_launch<uint32_t>(dc, n, e0.p2g_tile_count() + 1, (uint32_t*)d_partial, st);
+            k_p2g_scatter<<<dim3(pb, n), TP, 0, st>>>(dc);
+            e0.launch_p2g_tiles(dc, n, st);
         } else {
-            k_p2g_atomic<<<dim3(pb, n), T, 0, st>>>(dc);
+            k_p2g_atomic<<<dim3(pb, n), TP, 0, st>>>(dc);
         }
     }
     k_grid_update<<<dim3(cb, n), T, 0, st>>>(dc, 1);
@@ -1622,14 +1651,14 @@ after_solve:
     k_viscosity_prepare<<<dim3(cb, n), T, 0, st>>>(dc);
     k_viscosity_apply<<<dim3(cb, n), T, 0, st>>>(dc, 1);
     if (max_np) {
-        k_g2p<<<dim3(pb, n), T, 0, st>>>(dc);
-        k_bed_coupling<<<dim3(pb, n), T, 0, st>>>(dc);
+        k_g2p<<<dim3(pb, n), TP, 0, st>>>(dc);
+        k_bed_coupling<<<dim3(pb, n), TP, 0, st>>>(dc);
     }
     if (max_bed) {
         k_extraction_advect<<<dim3(bb, n), T, 0, st>>>(dc);
         k_bed_dynamics<<<dim3(bb, n), T, 0, st>>>(dc);
     }
-    if (max_np) k_prepare_render<<<dim3(pb, n), T, 0, st>>>(dc);
+    if (max_np) k_prepare_render<<<dim3(pb, n), TP, 0, st>>>(dc);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
         set_error(std::string("ensemble substep launch: ") + cudaGetErrorString(err));
@@ -1904,6 +1933,7 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     uint32_t trial_min_pairs = 0;  // fewest pairs of one substep in the last trial
+    uint32_t tile = p2g_tile(), threads = particle_threads();  // launch shapes of the next trial
     auto trial = [&](float omega, uint32_t ce, uint32_t p2g, uint32_t first, float& ms) -> int {
         int r = snapshot_load(state.data(), bytes);
         if (r) return r;
@@ -1911,6 +1941,8 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
         s.check_every = ce;
         s.p2g_mode = p2g;
         s.first_check = first;
+        s.p2g_tile = tile;
+        s.particle_threads = threads;
         bool converged = true;
         trial_min_pairs = 0xffffffffu;
         cudaEventRecord(a, stream_);
@@ -1936,6 +1968,8 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     res.check_every = entry.check_every;
     res.p2g_mode = entry.p2g_mode;
     res.first_check = entry.first_check;
+    res.p2g_tile = tile;
+    res.particle_threads = threads;
     res.trials = 1;
     best_pairs = trial_min_pairs;
     // P2G mode at the entry solver settings, then the solver at the chosen mode
@@ -1977,6 +2011,22 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
             }
         }
     }
+    // launch shapes at the chosen solver settings: threads per block of the particle
+    // passes, and the P2G tile side when P2G is tile-sorted
+    for (uint32_t t : {4u, 8u})
+        for (uint32_t th : {128u, 256u, 512u}) {
+            if (t != 4u && res.p2g_mode == CS_P2G_ATOMIC32) continue;
+            if (t == res.p2g_tile && th == res.particle_threads) continue;
+            tile = t;
+            threads = th;
+            if ((rc = trial(res.omega, res.check_every, res.p2g_mode, res.first_check, ms))) goto done;
+            ++res.trials;
+            if (ms < res.best_ms) {
+                res.best_ms = ms;
+                res.p2g_tile = t;
+                res.particle_threads = th;
+            }
+        }
 done:
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -1990,6 +2040,8 @@ done:
     s.check_every = res.check_every;
     s.p2g_mode = res.p2g_mode;
     s.first_check = res.first_check;
+    s.p2g_tile = res.p2g_tile;
+    s.particle_threads = res.particle_threads;
     if (out) *out = res;
     return CS_OK;
 }
@@ -2178,6 +2230,12 @@ static int validate(const CsSettings* s) {
     }
     if (s->num_obstacles > CS_MAX_OBSTACLES) {
         set_error("too many obstacles");
+        return CS_ERR_INVALID_ARG;
+    }
+    if (!(s->p2g_tile == 0 || s->p2g_tile == 4 || s->p2g_tile == 8) ||
+        !(s->particle_threads == 0 || s->particle_threads == 128 || s->particle_threads == 256 ||
+          s->particle_threads == 512)) {
+        set_error("p2g_tile must be 0, 4 or 8 and particle_threads 0, 128, 256 or 512");
         return CS_ERR_INVALID_ARG;
     }
     if (s->p2g_mode > CS_P2G_INT64 || s->warm_start > CS_WARM_LEARNED || s->pressure_storage > CS_PRESSURE_FP32 ||

@@ -73,6 +73,11 @@ private:
     double refine_residual();
     int launch_cells_blocks() const;
     int launch_particle_blocks(uint32_t n) const;
+    int launch_particle_blocks_pt(uint32_t n) const;  // for particle_threads() threads per block
+    uint32_t particle_threads() const;
+    uint32_t p2g_tile() const;
+    uint32_t p2g_tile_count() const;
+    void launch_p2g_tiles(const Ctx* dc, uint32_t instances, cudaStream_t st) const;
     int check(cudaError_t e, const char* what);
 
     cudaStream_t stream_ = nullptr;
@@ -106,7 +111,7 @@ private:
     struct GraphKey {
         uint32_t p2g_mode, check_every, max_sweeps, solve_mode, pressure_storage, rbgs_kernel, rbgs_pairs, warm_start;
         float residual_tol;
-        uint32_t num_bed, max_particles;
+        uint32_t num_bed, max_particles, p2g_tile, particle_threads;
         bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
     };
     GraphKey graph_key() const;

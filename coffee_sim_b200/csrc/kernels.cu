@@ -202,16 +202,16 @@ __global__ void k_p2g_atomic(const Ctx* __restrict__ cp) {
 // block covers nodes t*P2G_TILE - 1 .. t*P2G_TILE + P2G_TILE, so every node of its
 // particles lands in it.  A particle outside the domain (clamped key) falls back to
 // global atomics.
-constexpr int P2G_TILE = 4;
-constexpr int P2G_SPAN = P2G_TILE + 2;
-constexpr int P2G_NODES = P2G_SPAN * P2G_SPAN * P2G_SPAN;
+// The tile side is 4 or 8 cells (Params::p2g_tile; a template parameter of the tile
+// kernel, which sizes its shared memory by it).
+constexpr int P2G_TILE = 4;  // default tile side, and the tiles the sample reorder sorts by
 constexpr uint32_t P2G_NO_TILE = 0xffffffffu;
 constexpr int P2G_THREADS = 256;
 
-__device__ __forceinline__ uint32_t p2g_tile_axis(int b, uint32_t nt) {
+__device__ __forceinline__ uint32_t p2g_tile_axis(int b, uint32_t nt, uint32_t tile) {
     int q = b + 1;
     q = q < 0 ? 0 : q;
-    uint32_t t = (uint32_t)q / P2G_TILE;
+    uint32_t t = (uint32_t)q / tile;
     return t < nt ? t : nt - 1;
 }
 
@@ -232,8 +232,8 @@ __global__ void k_p2g_keys(const Ctx* __restrict__ cp) {
                 const int bx = (int)floorf((P.x - u.ox) * u.inv_dx - 0.5f);
                 const int by = (int)floorf((P.y - u.oy) * u.inv_dx - 0.5f);
                 const int bz = (int)floorf((P.z - u.oz) * u.inv_dx - 0.5f);
-                key = (p2g_tile_axis(bz, u.ntz) * u.nty + p2g_tile_axis(by, u.nty)) * u.ntx +
-                      p2g_tile_axis(bx, u.ntx);
+                key = (p2g_tile_axis(bz, u.ntz, u.p2g_tile) * u.nty + p2g_tile_axis(by, u.nty, u.p2g_tile)) * u.ntx +
+                      p2g_tile_axis(bx, u.ntx, u.p2g_tile);
             }
         }
         // one counter atomic per distinct tile in the warp (neighbouring particles
@@ -252,20 +252,24 @@ __global__ void k_p2g_keys(const Ctx* __restrict__ cp) {
 }
 
 // ---- reorder of the water samples by tile (reorder_every) ----
-// Key of water slot num_bed + i: the tile of its P2G base cell, the tile count for a
-// sample that deposits nothing; the value is its own index, for a stable sort.
+// Key of water slot num_bed + i: the 4^3-cell tile of its P2G base cell (whatever the
+// P2G tile size), the tile count for a sample that deposits nothing; the value is its
+// own index, for a stable sort.
 __global__ void k_reorder_keys(const Ctx* __restrict__ cp, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
     const Ctx& c = cp[0];
     const Params& u = c.u;
+    const uint32_t ntx = (u.gx + P2G_TILE) / P2G_TILE, nty = (u.gy + P2G_TILE) / P2G_TILE,
+                   ntz = (u.gz + P2G_TILE) / P2G_TILE;
     CS_FOR(i, u.num_water) {
         const uint32_t pid = u.num_bed + i;
         const float4 P = c.pos[pid], Vv = c.vel[pid];
-        uint32_t key = u.ntx * u.nty * u.ntz;
+        uint32_t key = ntx * nty * ntz;
         if (is_water_phase(c.c0[pid].w) && !(Vv.w <= inactive_mass(u))) {
             const int bx = (int)floorf((P.x - u.ox) * u.inv_dx - 0.5f);
             const int by = (int)floorf((P.y - u.oy) * u.inv_dx - 0.5f);
             const int bz = (int)floorf((P.z - u.oz) * u.inv_dx - 0.5f);
-            key = (p2g_tile_axis(bz, u.ntz) * u.nty + p2g_tile_axis(by, u.nty)) * u.ntx + p2g_tile_axis(bx, u.ntx);
+            key = (p2g_tile_axis(bz, ntz, P2G_TILE) * nty + p2g_tile_axis(by, nty, P2G_TILE)) * ntx +
+                  p2g_tile_axis(bx, ntx, P2G_TILE);
         }
         keys[i] = key;
         idx[i] = i;
@@ -294,9 +298,11 @@ __global__ void k_p2g_scatter(const Ctx* __restrict__ cp) {
 // and H + carry to the high word only when that is nonzero (almost never for the
 // magnitudes of one sample's deposit).  High * 2^32 + low is then the sum of the
 // values modulo 2^64, exactly what 64-bit atomics give, at the cost of 32-bit ones.
-template <class T>
+template <class T, int TILE>
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict__ cp) {
     constexpr bool I64 = sizeof(T) == 8;
+    constexpr int P2G_SPAN = TILE + 2;
+    constexpr int P2G_NODES = P2G_SPAN * P2G_SPAN * P2G_SPAN;
     __shared__ uint32_t acc[I64 ? 12 : 6][P2G_NODES];
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
@@ -306,7 +312,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_tiles(const Ctx* __restrict
         const uint32_t first = c.tile_start[t], last = c.tile_start[t + 1];
         if (first == last) continue;  // uniform across the block
         const uint32_t tx = t % u.ntx, ty = (t / u.ntx) % u.nty, tz = t / (u.ntx * u.nty);
-        const int ox = (int)(tx * P2G_TILE) - 1, oy = (int)(ty * P2G_TILE) - 1, oz = (int)(tz * P2G_TILE) - 1;
+        const int ox = (int)(tx * TILE) - 1, oy = (int)(ty * TILE) - 1, oz = (int)(tz * TILE) - 1;
         for (int i = threadIdx.x; i < (I64 ? 12 : 6) * P2G_NODES; i += blockDim.x) (&acc[0][0])[i] = 0;
         __syncthreads();
         // Particles of one cell are mostly adjacent in the tile list; visiting each block

@@ -240,7 +240,12 @@ typedef struct CsSettings {
                                      P2G base cell (samples that deposit nothing last), so that
                                      P2G and G2P touch neighbouring cells from neighbouring
                                      threads; slot numbers of water samples change then.  0: off */
-    uint32_t reserved[5];
+    uint32_t p2g_tile;            /* cells per side of a sorted-P2G tile: 0 or 4, or 8 (fewer tile
+                                     borders to flush, 4x the shared memory) */
+    uint32_t particle_threads;    /* threads per block of the particle passes (P2G keys and
+                                     scatter, G2P, bed coupling, render packing): 0 or 256, 128,
+                                     512 */
+    uint32_t reserved[3];
 } CsSettings;
 
 /* Observability counters (mod.rs:50-68 / state.rs:22-28) + solver telemetry. */
@@ -474,12 +479,14 @@ typedef struct CsTuneResult {
     float best_ms;         /* device ms per substep with the chosen configuration */
     float initial_ms;      /* device ms per substep with the configuration at entry */
     uint32_t first_check;  /* chosen pairs before each solve's first residual check (0: check_every) */
-    uint32_t reserved[1];
+    uint32_t p2g_tile;     /* chosen P2G tile side (4 or 8) */
+    uint32_t particle_threads;  /* chosen threads per block of the particle passes */
 } CsTuneResult;
 
 /* Time `substeps` substeps of length sub_dt from the current state for each candidate
  * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/40/60/80,
- * then a first-check interval of 0.85/0.92/0.98 of the fewest pairs a substep took),
+ * then a first-check interval of 0.85/0.92/0.98 of the fewest pairs a substep took, then
+ * the launch shapes: P2G tile side 4/8 x 128/256/512 threads per particle-pass block),
  * restoring the state after every trial; keep the fastest whose every substep reached
  * the residual target.  The simulation ends in the state it had at entry with the
  * chosen configuration applied.  Residual-mode solves only (CS_ERR_UNSUPPORTED else). */
