@@ -42,14 +42,14 @@ DT = 5.0e-4
 # interval before a solve's first check (0: the cap).
 WORKLOADS = {
     "c5": {"name": "c5_v60_scale_192cube", "scene": "c5_scale", "seed": 4, "omega": 1.95, "check_every": 60,
-           "first_check": 0, "p2g": "int64", "spiral": False, "reorder_every": 10,
+           "first_check": 0, "p2g": "int64", "spiral": False, "reorder_every": 10, "p2g_tile": 8,
            "text": "V60 pour at 192^3 (dx 0.83 mm), two-layer bed (porosity 0.45/0.35, 10x lower permeability "
                    "below), jet 4 ml/s at 0.8 m/s 1.2 cm off centre, int64 fixed-point P2G"},
     "c3": {"name": "c3_v60_spiral_128cube", "scene": "c3_large", "seed": 2, "omega": 1.94, "check_every": 60,
-           "first_check": 0, "p2g": "sorted", "spiral": True, "reorder_every": 10,
+           "first_check": 0, "p2g": "sorted", "spiral": True, "reorder_every": 10, "p2g_tile": 8,
            "text": "V60 pour at 128^3 (dx 1.25 mm), spout on the spiral path (r 1.5 cm, 0.5 Hz), tile-sorted P2G"},
     "c2": {"name": "c2_v60_midpour_64cube", "scene": "c2_v60", "seed": 1, "omega": 1.92, "check_every": 60,
-           "first_check": 125, "p2g": "sorted", "spiral": False, "reorder_every": 0,
+           "first_check": 125, "p2g": "sorted", "spiral": False, "reorder_every": 0, "p2g_tile": 4,
            "text": "V60 pour at 64^3 (dx 2.5 mm), centre pour, tile-sorted P2G"},
 }
 PHASES = ["emit", "clear", "p2g", "grid", "sweeps", "residual", "project", "g2p", "bed", "render", "learned"]
@@ -188,6 +188,9 @@ def make_settings(lib, key, args, device=0, learned=False):
     # water samples reordered by P2G tile every N substeps (the oracle applies the same
     # permutation); at 192^3 every 10 substeps: G2P 1.68 -> 1.54 ms, every 5 costs more
     r.reorder_every = wl["reorder_every"]
+    # 8^3-cell P2G tiles at 128^3 and 192^3 (cs_autotune's launch-shape trials: 192^3 P2G
+    # 1.83 -> 1.66 ms per substep; 128 or 512 threads per particle block did not help)
+    r.p2g_tile = wl["p2g_tile"]
     return s
 
 
@@ -399,7 +402,7 @@ def run_pour(lib, key, args, device, world, dist, barrier, with_learned, with_cp
                    "residual_tol": 1e-5, "omega": float(sim.settings.rbgs_omega), "warm_start": "previous substep",
                    "check_every_pairs": int(sim.settings.check_every),
                    "first_check_pairs": int(sim.settings.first_check or sim.settings.check_every),
-                   "p2g": p2g_of(key, args), "reorder_every": wl["reorder_every"], "pressure_solve": "grid-wide cooperative solve" if n_c > (1 << 18)
+                   "p2g": p2g_of(key, args), "reorder_every": wl["reorder_every"], "p2g_tile": wl["p2g_tile"], "pressure_solve": "grid-wide cooperative solve" if n_c > (1 << 18)
                    else "thread-block-cluster solve", "emission": "device kernel",
                    "timed_launch": "CUDA graph replay" if use_graph else "direct launches",
                    "e2e_launch": ("CUDA graph replay" if use_graph else "direct launches")
