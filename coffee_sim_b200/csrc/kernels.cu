@@ -1141,7 +1141,9 @@ __device__ __forceinline__ void g2p_particle(const Ctx& c, uint32_t pid) {
     c.c2[pid] = make_float4(n2.x, n2.y, n2.z, 0.0f);
 }
 
-__global__ void k_g2p(const Ctx* __restrict__ cp) {
+// 64 registers (four 256-thread blocks per SM) instead of 80: the kernel is bound by the
+// latency of its grid, lookup and SDF gathers, and more resident warps hide more of it
+__global__ void __launch_bounds__(256, 4) k_g2p(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     uint32_t n = c.u.num_water + c.u.num_bed;
     CS_FOR(pid, n) g2p_particle(c, pid);
