@@ -2014,7 +2014,7 @@ int Engine::autotune(float sub_dt, uint32_t substeps, CsTuneResult* out) {
     // launch shapes at the chosen solver settings: threads per block of the particle
     // passes, and the P2G tile side when P2G is tile-sorted
     for (uint32_t t : {4u, 8u})
-        for (uint32_t th : {128u, 256u, 512u}) {
+        for (uint32_t th : {128u, 256u}) {
             if (t != 4u && res.p2g_mode == CS_P2G_ATOMIC32) continue;
             if (t == res.p2g_tile && th == res.particle_threads) continue;
             tile = t;
@@ -2233,9 +2233,8 @@ static int validate(const CsSettings* s) {
         return CS_ERR_INVALID_ARG;
     }
     if (!(s->p2g_tile == 0 || s->p2g_tile == 4 || s->p2g_tile == 8) ||
-        !(s->particle_threads == 0 || s->particle_threads == 128 || s->particle_threads == 256 ||
-          s->particle_threads == 512)) {
-        set_error("p2g_tile must be 0, 4 or 8 and particle_threads 0, 128, 256 or 512");
+        !(s->particle_threads == 0 || s->particle_threads == 128 || s->particle_threads == 256)) {
+        set_error("p2g_tile must be 0, 4 or 8 and particle_threads 0, 128 or 256");
         return CS_ERR_INVALID_ARG;
     }
     if (s->p2g_mode > CS_P2G_INT64 || s->warm_start > CS_WARM_LEARNED || s->pressure_storage > CS_PRESSURE_FP32 ||

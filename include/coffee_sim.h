@@ -243,8 +243,8 @@ typedef struct CsSettings {
     uint32_t p2g_tile;            /* cells per side of a sorted-P2G tile: 0 or 4, or 8 (fewer tile
                                      borders to flush, 4x the shared memory) */
     uint32_t particle_threads;    /* threads per block of the particle passes (P2G keys and
-                                     scatter, G2P, bed coupling, render packing): 0 or 256, 128,
-                                     512 */
+                                     scatter, G2P, bed coupling, render packing): 0 or 256, or 128
+                                     (G2P is compiled for at most 256 threads per block) */
     uint32_t reserved[3];
 } CsSettings;
 
@@ -486,7 +486,7 @@ typedef struct CsTuneResult {
 /* Time `substeps` substeps of length sub_dt from the current state for each candidate
  * configuration (P2G mode, then over-relaxation 1.80-1.96 x check interval 10/20/40/60/80,
  * then a first-check interval of 0.85/0.92/0.98 of the fewest pairs a substep took, then
- * the launch shapes: P2G tile side 4/8 x 128/256/512 threads per particle-pass block),
+ * the launch shapes: P2G tile side 4/8 x 128/256 threads per particle-pass block),
  * restoring the state after every trial; keep the fastest whose every substep reached
  * the residual target.  The simulation ends in the state it had at entry with the
  * chosen configuration applied.  Residual-mode solves only (CS_ERR_UNSUPPORTED else). */
