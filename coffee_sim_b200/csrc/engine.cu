@@ -476,7 +476,13 @@ int Engine::gs_alloc() {
     int rc;
     if ((rc = alloc(gs_rows_, (2 * (rows + 1) + rows) * sizeof(uint32_t)))) return rc;
     if ((rc = alloc(gs_desc_, units * (sizeof(GsDesc) + 16 * sizeof(int))))) return rc;
-    if ((rc = alloc(gs_slots_, slots * (3 * sizeof(float2) + 2 * sizeof(float))))) return rc;
+    // the arrays read at neighbour slots (correction + fill code, pressure) get gx / 2 + 64
+    // slots of padding on both sides: a neighbour slot computed for a face that is not a
+    // fluid face can fall up to gx / 2 + 33 slots outside the used range, and the solve
+    // loads all six before the flags pick the real ones
+    const size_t pad = gx / 2 + 64;
+    if ((rc = alloc(gs_slots_, (slots + 2 * pad) * 2 * sizeof(float2) + slots * (sizeof(float2) + 2 * sizeof(float)))))
+        return rc;
     if ((rc = gs_blocks(&gs_ctas_))) return rc;
     if ((rc = alloc(gs_misc_, sc_align(2 * sizeof(double) * (size_t)std::max(gs_ctas_, 1)) + 256 +
                                   sc_align(sizeof(ScResult))))) return rc;
@@ -491,10 +497,10 @@ int Engine::gs_alloc() {
     g.desc = (GsDesc*)gs_desc_.ptr;
     g.rec = (int*)((unsigned char*)gs_desc_.ptr + units * sizeof(GsDesc));
     float2* f2 = (float2*)gs_slots_.ptr;
-    g.cf = f2;
-    g.dfc = f2 + slots;
-    g.p = f2 + 2 * slots;
-    g.g = (float*)(f2 + 3 * slots);
+    g.dfc = f2 + pad;
+    g.p = f2 + (slots + 2 * pad) + pad;
+    g.cf = f2 + 2 * (slots + 2 * pad);
+    g.g = (float*)(g.cf + slots);
     g.b = g.g + slots;
     unsigned char* m = (unsigned char*)gs_misc_.ptr;
     g.part = (double*)m;

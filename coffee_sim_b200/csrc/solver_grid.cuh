@@ -325,11 +325,12 @@ __device__ __forceinline__ void gs_make_rec(const GsDesc& d, int col, uint32_t f
     if (lane < (uint32_t)GS_REC) rec[lane] = v;
 }
 
-// Slot of the neighbour across face f of cell `lane`, clamped into the arrays so that
-// all six can be loaded before the flags say which are fluid faces.
+// Slot of the neighbour across face f of cell `lane`.  All six are loaded before the
+// flags say which are fluid faces; the correction and pressure arrays are padded by
+// gx / 2 + 64 slots on both sides, which covers every slot a non-fluid face can give.
 __device__ __forceinline__ int gs_nb(const int* rec, int f, uint32_t lane, int n_slots) {
-    const int j = rec[1 + f] + (int)lane;
-    return j < 0 ? 0 : (j < n_slots ? j : n_slots - 1);
+    (void)n_slots;
+    return rec[1 + f] + (int)lane;
 }
 
 // FP64 residual of one cell; g <- r, d <- 0.  Adds its (r^2, b^2) contributions.
