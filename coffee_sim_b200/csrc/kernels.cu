@@ -464,87 +464,127 @@ __device__ __forceinline__ bool open_nb(const Ctx& c, f3 cc, uint32_t x, uint32_
     return sample_sdf(c, cc + mk(ox, oy, oz)) >= 0.0f;
 }
 
-// 64 registers (4 blocks of 256 per SM) instead of 80: the kernel is latency bound
+// One cell of classify_cells, given the loads the caller made ahead for it: its grid
+// velocity and mass, its solid class (when the SDF class cache is on), its bed lookup
+// and the pressure kept from the last substep.  In the fluid path the six neighbours'
+// velocities and both volumes are loaded before the open-face tests and the kind that
+// pick from them, so the loads are in flight together.
+__device__ __forceinline__ void classify_cell(const Ctx& c, uint32_t i, float4 sv, uint8_t cls, int32_t lk,
+                                              float keep, float keep_lo, uint32_t& max_fd, uint32_t& n_fluid) {
+    const Params& u = c.u;
+    const float mass = sv.w;
+    pressure_store(c, i, 0.0f);
+    c.plo[i] = 0.0f;
+    uint32_t ix, iy, iz;
+    decompose(u, i, ix, iy, iz);
+    f3 cc = cell_center(u, ix, iy, iz);
+    bool solid = u.use_sdf_cache ? (cls != 0) : (sample_sdf(c, cc) < 0.0f);
+    int32_t* kl = lane(c, 3);
+    if (solid) {
+        kl[i] = CELL_SOLID;
+        div_store(c, i, 0.0f);
+        c.fill[i] = 0.0f;
+        c.fcode[i] = -2.0f;
+        return;
+    }
+    if (mass <= occupancy_mass(u)) {
+        kl[i] = CELL_AIR;
+        div_store(c, i, 0.0f);
+        c.fill[i] = 0.0f;
+        c.fcode[i] = -1.0f;
+        return;
+    }
+    const uint32_t sy = u.gx, sz = u.gx * u.gy;
+    const bool in[6] = {ix > 0, ix + 1 < u.gx, iy > 0, iy + 1 < u.gy, iz > 0, iz + 1 < u.gz};
+    const uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
+    float4 nv[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) nv[f] = in[f] ? c.gvel[i + off[f]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float rest = rest_vol(c, i), cur = cur_vol(c, i);
+    int32_t kind;
+    if (lk >= 0) {
+        kind = CELL_BED;
+    } else {
+        bool air = !(in[0] && in[1] && in[2] && in[3] && in[4] && in[5]);
+        if (!air) {
+            const float occ = occupancy_mass(u);
+            air = nv[0].w <= occ || nv[1].w <= occ || nv[2].w <= occ || nv[3].w <= occ || nv[4].w <= occ ||
+                  nv[5].w <= occ;
+        }
+        kind = air ? CELL_SURFACE : CELL_INTERIOR;
+    }
+    kl[i] = kind;
+    const float fill = liquid_fill_of(u, kind, rest, cur);
+    c.fill[i] = fill;
+    c.fcode[i] = kind == CELL_BED ? 2.0f : fill;
+    if (u.warm && !u.fixed_point) {
+        c.pf[i] = keep;
+        c.plo[i] = keep_lo;
+    }
+    const float d = u.dx;
+    float vxm = -sv.x, vxp = -sv.x, vym = -sv.y, vyp = -sv.y, vzm = -sv.z, vzp = -sv.z;
+    if (in[0] && open_nb(c, cc, ix - 1, iy, iz, -d, 0.0f, 0.0f)) vxm = nv[0].x;
+    if (in[1] && open_nb(c, cc, ix + 1, iy, iz, d, 0.0f, 0.0f)) vxp = nv[1].x;
+    if (in[2] && open_nb(c, cc, ix, iy - 1, iz, 0.0f, -d, 0.0f)) vym = nv[2].y;
+    if (in[3] && open_nb(c, cc, ix, iy + 1, iz, 0.0f, d, 0.0f)) vyp = nv[3].y;
+    if (in[4] && open_nb(c, cc, ix, iy, iz - 1, 0.0f, 0.0f, -d)) vzm = nv[4].z;
+    if (in[5] && open_nb(c, cc, ix, iy, iz + 1, 0.0f, 0.0f, d)) vzp = nv[5].z;
+    float div = 0.5f * u.inv_dx * (((vxp - vxm) + (vyp - vym)) + (vzp - vzm));
+    float target = volume_target(u, rest, cur);
+    if (kind == CELL_BED) {
+        int32_t b = lk;
+        if (b >= 0 && (uint32_t)b < u.num_bed) {
+            float pt = bed_pore_target(c, (uint32_t)b, cc, rest, cur);
+            float poro = wclamp(compacted_porosity(c, (uint32_t)b), 0.08f, 1.0f);
+            float sfrac = 1.0f - poro;
+            int x = ix, y = iy, z = iz;
+            float bxm = bed_velocity_at(c, x - 1, y, z).x, bxp = bed_velocity_at(c, x + 1, y, z).x;
+            float bym = bed_velocity_at(c, x, y - 1, z).y, byp = bed_velocity_at(c, x, y + 1, z).y;
+            float bzm = bed_velocity_at(c, x, y, z - 1).z, bzp = bed_velocity_at(c, x, y, z + 1).z;
+            float sdiv = 0.5f * u.inv_dx * (((bxp - bxm) + (byp - bym)) + (bzp - bzm));
+            target = (pt - sfrac * sdiv) / poro;
+        }
+    }
+    div_store(c, i, div - target);
+    uint32_t fd = to_u32(wclamp(fabsf(div) * METRICS_DIV_FP_SCALE, 0.0f, 2147483648.0f));
+    max_fd = max_fd > fd ? max_fd : fd;
+    n_fluid += 1u;
+}
+
+// classify_cells over the whole grid.  The kernel is latency bound (a chain of
+// dependent loads per fluid cell), so each thread takes CLS_CELLS cells a grid stride
+// apart and issues the first loads of all of them before working on any.  No cell
+// reads what another writes here, so the order of the loads changes nothing.  64
+// registers (4 blocks of 256 per SM).
+constexpr uint32_t CLS_CELLS = 4;
 __global__ void __launch_bounds__(256, 4) k_classify(const Ctx* __restrict__ cp) {
     const Ctx& c = cp[blockIdx.y];
     const Params& u = c.u;
     // the metrics' max |div| and fluid-cell count, per thread, then one atomic per warp
     uint32_t max_fd = 0u, n_fluid = 0u;
-    CS_FOR(i, u.cells) {
-        float mass = c.gvel[i].w;
-        float keep = (!u.fixed_point && u.warm) ? c.pf[i] : 0.0f;
-        float keep_lo = (!u.fixed_point && u.warm) ? c.plo[i] : 0.0f;
-        pressure_store(c, i, 0.0f);
-        c.plo[i] = 0.0f;
-        uint32_t ix, iy, iz;
-        decompose(u, i, ix, iy, iz);
-        f3 cc = cell_center(u, ix, iy, iz);
-        bool solid = u.use_sdf_cache ? (c.cls[i] != 0) : (sample_sdf(c, cc) < 0.0f);
-        int32_t* kl = lane(c, 3);
-        if (solid) {
-            kl[i] = CELL_SOLID;
-            div_store(c, i, 0.0f);
-            c.fill[i] = 0.0f;
-            c.fcode[i] = -2.0f;
-            continue;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const bool kept = !u.fixed_point && u.warm;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < u.cells; i0 += CLS_CELLS * stride) {
+        float4 sv[CLS_CELLS];
+        uint8_t cls[CLS_CELLS];
+        int32_t lk[CLS_CELLS];
+        float keep[CLS_CELLS], keep_lo[CLS_CELLS];
+#pragma unroll
+        for (uint32_t j = 0; j < CLS_CELLS; ++j) {
+            const uint32_t i = i0 + j * stride;
+            if (i >= u.cells) continue;
+            sv[j] = c.gvel[i];
+            cls[j] = u.use_sdf_cache ? c.cls[i] : (uint8_t)0;
+            lk[j] = c.lookup[i];
+            keep[j] = kept ? c.pf[i] : 0.0f;
+            keep_lo[j] = kept ? c.plo[i] : 0.0f;
         }
-        if (mass <= occupancy_mass(u)) {
-            kl[i] = CELL_AIR;
-            div_store(c, i, 0.0f);
-            c.fill[i] = 0.0f;
-            c.fcode[i] = -1.0f;
-            continue;
+#pragma unroll
+        for (uint32_t j = 0; j < CLS_CELLS; ++j) {
+            const uint32_t i = i0 + j * stride;
+            if (i >= u.cells) continue;
+            classify_cell(c, i, sv[j], cls[j], lk[j], keep[j], keep_lo[j], max_fd, n_fluid);
         }
-        int32_t kind;
-        if (c.lookup[i] >= 0) {
-            kind = CELL_BED;
-        } else {
-            bool air = (ix == 0) || (ix + 1 >= u.gx) || (iy == 0) || (iy + 1 >= u.gy) || (iz == 0) || (iz + 1 >= u.gz);
-            if (!air) {
-                const float occ = occupancy_mass(u);
-                air = c.gvel[i - 1].w <= occ || c.gvel[i + 1].w <= occ || c.gvel[i - u.gx].w <= occ ||
-                      c.gvel[i + u.gx].w <= occ || c.gvel[i - u.gx * u.gy].w <= occ ||
-                      c.gvel[i + u.gx * u.gy].w <= occ;
-            }
-            kind = air ? CELL_SURFACE : CELL_INTERIOR;
-        }
-        kl[i] = kind;
-        c.fill[i] = liquid_fill(c, i, kind);
-        c.fcode[i] = kind == CELL_BED ? 2.0f : c.fill[i];
-        if (u.warm && !u.fixed_point) {
-            c.pf[i] = keep;
-            c.plo[i] = keep_lo;
-        }
-        float4 sv = c.gvel[i];
-        const float d = u.dx;
-        float vxm = -sv.x, vxp = -sv.x, vym = -sv.y, vyp = -sv.y, vzm = -sv.z, vzp = -sv.z;
-        if (ix > 0 && open_nb(c, cc, ix - 1, iy, iz, -d, 0.0f, 0.0f)) vxm = c.gvel[i - 1].x;
-        if (ix + 1 < u.gx && open_nb(c, cc, ix + 1, iy, iz, d, 0.0f, 0.0f)) vxp = c.gvel[i + 1].x;
-        if (iy > 0 && open_nb(c, cc, ix, iy - 1, iz, 0.0f, -d, 0.0f)) vym = c.gvel[i - u.gx].y;
-        if (iy + 1 < u.gy && open_nb(c, cc, ix, iy + 1, iz, 0.0f, d, 0.0f)) vyp = c.gvel[i + u.gx].y;
-        if (iz > 0 && open_nb(c, cc, ix, iy, iz - 1, 0.0f, 0.0f, -d)) vzm = c.gvel[i - u.gx * u.gy].z;
-        if (iz + 1 < u.gz && open_nb(c, cc, ix, iy, iz + 1, 0.0f, 0.0f, d)) vzp = c.gvel[i + u.gx * u.gy].z;
-        float div = 0.5f * u.inv_dx * (((vxp - vxm) + (vyp - vym)) + (vzp - vzm));
-        float rest = rest_vol(c, i), cur = cur_vol(c, i);
-        float target = volume_target(u, rest, cur);
-        if (kind == CELL_BED) {
-            int32_t b = c.lookup[i];
-            if (b >= 0 && (uint32_t)b < u.num_bed) {
-                float pt = bed_pore_target(c, (uint32_t)b, cc, rest, cur);
-                float poro = wclamp(compacted_porosity(c, (uint32_t)b), 0.08f, 1.0f);
-                float sfrac = 1.0f - poro;
-                int x = ix, y = iy, z = iz;
-                float bxm = bed_velocity_at(c, x - 1, y, z).x, bxp = bed_velocity_at(c, x + 1, y, z).x;
-                float bym = bed_velocity_at(c, x, y - 1, z).y, byp = bed_velocity_at(c, x, y + 1, z).y;
-                float bzm = bed_velocity_at(c, x, y, z - 1).z, bzp = bed_velocity_at(c, x, y, z + 1).z;
-                float sdiv = 0.5f * u.inv_dx * (((bxp - bxm) + (byp - bym)) + (bzp - bzm));
-                target = (pt - sfrac * sdiv) / poro;
-            }
-        }
-        div_store(c, i, div - target);
-        uint32_t fd = to_u32(wclamp(fabsf(div) * METRICS_DIV_FP_SCALE, 0.0f, 2147483648.0f));
-        max_fd = max_fd > fd ? max_fd : fd;
-        n_fluid += 1u;
     }
     // every lane leaves the loop (blocks are whole warps and nothing returns early)
     max_fd = __reduce_max_sync(0xffffffffu, max_fd);

@@ -56,11 +56,15 @@ __device__ __forceinline__ float rest_vol(const Ctx& c, uint32_t i) { return p2g
 __device__ __forceinline__ float cur_vol(const Ctx& c, uint32_t i) { return p2g_lane(c, 5, i); }
 
 // shader.rs:293-304; evaluated once per cell by classify and stored in c.fill
-__device__ __forceinline__ float liquid_fill(const Ctx& c, uint32_t i, int32_t kind) {
+__device__ __forceinline__ float liquid_fill_of(const Params& u, int32_t kind, float rest, float cur) {
     if (kind == CELL_INTERIOR || kind == CELL_BED) return 1.0f;
     if (kind != CELL_SURFACE) return 0.0f;
-    float cv = wmax(c.u.dx * c.u.dx * c.u.dx, 1e-8f);
-    return wclamp(wmax(rest_vol(c, i), cur_vol(c, i)) / cv, 0.0f, 1.0f);
+    float cv = wmax(u.dx * u.dx * u.dx, 1e-8f);
+    return wclamp(wmax(rest, cur) / cv, 0.0f, 1.0f);
+}
+__device__ __forceinline__ float liquid_fill(const Ctx& c, uint32_t i, int32_t kind) {
+    if (kind != CELL_SURFACE) return liquid_fill_of(c.u, kind, 0.0f, 0.0f);
+    return liquid_fill_of(c.u, kind, rest_vol(c, i), cur_vol(c, i));
 }
 // shader.rs:306-323 with the neighbour's fill read from c.fill
 __device__ __forceinline__ float face_weight(int32_t sk, float sf, int32_t nk, float nfill) {

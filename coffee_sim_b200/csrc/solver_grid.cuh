@@ -87,17 +87,19 @@ __device__ __forceinline__ void gs_red_release(uint32_t* p, uint32_t v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Returns false (on every thread of the CTA) once any CTA gave up waiting.
+// Returns false (on every thread of the CTA) once any CTA gave up waiting.  The abort
+// word is read on every 16th poll only: each read is another L2 round trip in the loop.
 __device__ __forceinline__ bool gs_grid_sync(uint32_t* sync, uint32_t nblocks, uint32_t& gen) {
     __shared__ uint32_t s_ok;
     __syncthreads();
     ++gen;
     if (threadIdx.x == 0) {
-        uint32_t ok = 1u;
+        uint32_t ok = 1u, polls = 0;
         gs_red_release(&sync[0], 1u);
         const uint32_t target = nblocks * gen;
         const long long t0 = clock64();
         while ((int)(gs_ld_acquire(&sync[0]) - target) < 0) {
+            if ((++polls & 15u) != 0u) continue;
             if (gs_ld_acquire(&sync[2]) != 0u) {
                 ok = 0u;
                 break;
