@@ -408,12 +408,14 @@ __global__ void k_bed_velocity(const Ctx* __restrict__ cp) {
     CS_FOR(i, u.cells) {
         uint32_t ix, iy, iz;
         decompose(u, i, ix, iy, iz);
-        // read only at bed-coupled cells (lookup >= 0) and their six neighbours
+        // read only at bed-coupled cells (lookup >= 0) and their six neighbours; the seven
+        // lookups are loaded together (no short-circuit chain of dependent loads)
         const uint32_t sy = u.gx, sz = u.gx * u.gy;
+        const bool in[6] = {ix > 0, ix + 1 < u.gx, iy > 0, iy + 1 < u.gy, iz > 0, iz + 1 < u.gz};
+        const uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
         bool near = c.lookup[i] >= 0;
-        near = near || (ix > 0 && c.lookup[i - 1] >= 0) || (ix + 1 < u.gx && c.lookup[i + 1] >= 0);
-        near = near || (iy > 0 && c.lookup[i - sy] >= 0) || (iy + 1 < u.gy && c.lookup[i + sy] >= 0);
-        near = near || (iz > 0 && c.lookup[i - sz] >= 0) || (iz + 1 < u.gz && c.lookup[i + sz] >= 0);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) near |= in[f] && c.lookup[i + off[f]] >= 0;
         f3 v = mk(0.0f, 0.0f, 0.0f);
         if (near) v = bed_matrix_velocity(c, (int)ix, (int)iy, (int)iz);
         c.bedv[i] = make_float4(v.x, v.y, v.z, 0.0f);
