@@ -480,7 +480,7 @@ int Engine::gs_alloc() {
     // slots of padding on both sides: a neighbour slot computed for a face that is not a
     // fluid face can fall up to gx / 2 + 33 slots outside the used range, and the solve
     // loads all six before the flags pick the real ones
-    const size_t pad = gx / 2 + 64;
+    const size_t pad = (gx / 2 + 64 + 15) & ~(size_t)15;  // whole 128-byte lines of float2
     if ((rc = alloc(gs_slots_, (slots + 2 * pad) * 2 * sizeof(float2) + slots * (sizeof(float2) + 2 * sizeof(float)))))
         return rc;
     if ((rc = gs_blocks(&gs_ctas_))) return rc;
@@ -2126,6 +2126,10 @@ int gs_blocks(int* ctas) {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return CS_OK;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return CS_OK;
     const size_t smem = (size_t)GS_SMEM;
+    // the smallest shared-memory carve-out that fits: the solve reads its own rows through L1
+    if (cudaFuncSetAttribute(k_gs_solve, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxL1) !=
+        cudaSuccess)
+        cudaGetLastError();
     if (cudaFuncSetAttribute(k_gs_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return CS_OK;

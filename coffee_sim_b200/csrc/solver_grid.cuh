@@ -30,8 +30,11 @@
 // sits at slot + lane), and whether the unit is bulk (all 32 cells fluid with six
 // unit-weight fluid faces, updated by a plain six-term sum).  A warp sweeps its units
 // two at a time with all nine loads of both in flight (own coefficients, residual and
-// correction, six neighbours' correction and fill code in one 8-byte load each, read
-// from L2 with ld.cg).  The colours of a red-black pair are separated by a grid-wide
+// correction, six neighbours' correction and fill code in one 8-byte load each).  A
+// neighbour in a row of another CTA is read from L2 with ld.cg; one in a row this CTA
+// owns goes through L1: CTA ranges start at unit boundaries and the slot arrays at
+// 128-byte lines, so no other CTA writes those lines, and within the CTA its barriers
+// make its own writes visible.  The colours of a red-black pair are separated by a grid-wide
 // barrier (a monotonic arrival counter: a release add per CTA, acquire polling).  The
 // last pair of a refinement cycle adds the correction to the pressure as it goes (a
 // cell's correction is final after its own colour's sweep), so a residual check is one
@@ -58,7 +61,8 @@ constexpr uint32_t GS_EMPTY = 1u << 7;      // no face with weight > 0, not flui
 constexpr uint32_t GS_AIR_SHIFT = 8;        // bits 8-13: air face with weight > 0
 constexpr uint32_t GS_ISFLUID = 1u << 14;   // fluid cell (its pressure is accumulated)
 constexpr long long kGsWaitCycles = 1ll << 31;  // ~1 s at 2 GHz
-constexpr int GS_SMEM = 64 * 1024;          // dynamic shared memory of a solve CTA: its units' index words
+constexpr int GS_SMEM = 24 * 1024;          // dynamic shared memory of a solve CTA: its units' index words
+                                            // (384 units; small, so that the rest of the SM's 256 KB is L1)
 
 // Per unit: x of its first cell, y, z, and for its own row and the four neighbour rows
 // (y-1, y+1, z-1, z+1) the row's first slot (INT_MIN: no fluid in it), the slots per
@@ -310,6 +314,16 @@ __device__ __forceinline__ uint32_t gs_setup_cell(const GsCtx& c, const GsBuffer
 constexpr int GS_REC = 8;
 constexpr uint32_t GS_REC_NONUNIT = 1u << 8;
 constexpr uint32_t GS_REC_BULK = 1u << 9;
+// bits 10-15: the neighbour across face f lies in a row of another CTA (or in no fluid
+// row), so it is read from L2 (ld.cg); the other neighbours lie in rows this CTA owns,
+// whose cache lines no other CTA writes, and are read through L1
+constexpr uint32_t GS_REC_FOREIGN_SHIFT = 10;
+
+// Load of a neighbour slot: through L1 when its row belongs to this CTA, else from L2.
+template <class T>
+__device__ __forceinline__ T gs_ld_nb(const T* p, bool foreign) {
+    return foreign ? __ldcg(p) : *p;
+}
 
 __device__ __forceinline__ void gs_make_rec(const GsDesc& d, int col, uint32_t flags, int* rec, uint32_t lane) {
     const int t = (col + d.y + d.z) & 1;
@@ -351,8 +365,9 @@ __device__ __forceinline__ void gs_residual_cell(const GsBuffers& gb, const int*
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int j = gs_nb(rec, f, lane, n_slots);
-        pj[f] = __ldcg(gb.p + j);
-        fj[f] = __ldcg(&gb.dfc[j].y);
+        const bool foreign = ((uint32_t)rec[7] >> (GS_REC_FOREIGN_SHIFT + f)) & 1u;
+        pj[f] = gs_ld_nb(gb.p + j, foreign);
+        fj[f] = gs_ld_nb(&gb.dfc[j].y, foreign);
     }
     const float fci = gb.dfc[s].y;
     const float sfi = fci > 1.5f ? 1.0f : fci;
@@ -393,7 +408,8 @@ __device__ __forceinline__ void gs_load(const GsBuffers& gb, const int* rec, uin
     L.g = gb.g[L.s];
     L.me = gb.dfc[L.s];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) L.nb[f] = __ldcg(gb.dfc + gs_nb(rec, f, lane, n_slots));
+    for (int f = 0; f < 6; ++f)
+        L.nb[f] = gs_ld_nb(gb.dfc + gs_nb(rec, f, lane, n_slots), ((L.rf >> (GS_REC_FOREIGN_SHIFT + f)) & 1u) != 0u);
 }
 
 // p <- p + d in FP64 (split back into hi/lo, clamped at the pressure limit).
@@ -493,8 +509,18 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
         const uint32_t n0 = __ballot_sync(0xffffffffu, nonunit(f0)), n1 = __ballot_sync(0xffffffffu, nonunit(f1));
         const uint32_t b0 = __ballot_sync(0xffffffffu, bulk(f0)), b1 = __ballot_sync(0xffffffffu, bulk(f1));
         int* r = recb + (size_t)k * 2 * GS_REC;
-        gs_make_rec(d, 0, (n0 ? GS_REC_NONUNIT : 0u) | (b0 == 0xffffffffu ? GS_REC_BULK : 0u), r, lane);
-        gs_make_rec(d, 1, (n1 ? GS_REC_NONUNIT : 0u) | (b1 == 0xffffffffu ? GS_REC_BULK : 0u), r + GS_REC, lane);
+        // faces whose neighbour row is another CTA's (x faces: the unit's own row)
+        uint32_t foreign = 0;
+#pragma unroll
+        for (int f = 2; f < 6; ++f) {
+            const int base = d.row[f - 1].base;
+            const bool own = base != INT_MIN && (uint32_t)base / (uint32_t)GS_UNIT >= ua &&
+                             (uint32_t)base / (uint32_t)GS_UNIT < ue;
+            if (!own) foreign |= 1u << f;
+        }
+        foreign <<= GS_REC_FOREIGN_SHIFT;
+        gs_make_rec(d, 0, foreign | (n0 ? GS_REC_NONUNIT : 0u) | (b0 == 0xffffffffu ? GS_REC_BULK : 0u), r, lane);
+        gs_make_rec(d, 1, foreign | (n1 ? GS_REC_NONUNIT : 0u) | (b1 == 0xffffffffu ? GS_REC_BULK : 0u), r + GS_REC, lane);
     }
     bool ok = gs_grid_sync(sync, nb, gen);
 
