@@ -755,8 +755,14 @@ int Engine::enqueue(uint32_t P, bool capture, uint32_t& sweeps, double& r0, doub
         CS_LAUNCH(k_emit_jet<<<dim3(launch_particle_blocks(jet_.count), 1), T, 0, stream_>>>(dc));
     }
     ph(CS_PHASE_CLEAR);
-    // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309)
-    cudaMemsetAsync(lanes_.ptr, 0, lanes_.bytes, stream_);
+    // clear_buffer(grid), clear_buffer(grid_vel) (mod.rs:308-309).  In int64 mode (fixed at
+    // creation) P2G accumulates in lanes64, and a full substep writes every int32 lane it
+    // reads for every cell before reading it: the kind (lane 3) and, with fixed-point
+    // storage, pressure and divergence (lanes 0, 1) in classify, the packing pressure
+    // (lane 2) in project, the viscosity scratch (lanes 1-3) in viscosity_prepare; lanes
+    // 4 and 5 are written only by the int32 P2G modes.  So only a partial substep, whose
+    // lanes are compared pass by pass, clears them.
+    if (settings.p2g_mode != CS_P2G_INT64 || P <= 20) cudaMemsetAsync(lanes_.ptr, 0, lanes_.bytes, stream_);
     cudaMemsetAsync(gvel_.ptr, 0, gvel_.bytes, stream_);
     if (settings.p2g_mode == CS_P2G_INT64) cudaMemsetAsync(lanes64_.ptr, 0, lanes64_.bytes, stream_);
     if (P > 0) cudaMemsetAsync(metrics_.ptr, 0, metrics_.bytes, stream_);
