@@ -397,7 +397,7 @@ __global__ void k_boundary(const Ctx* __restrict__ cp) {
     }
 }
 
-// bed_matrix_velocity_cell (shader.rs:380-407) of every cell, once per substep: the bed
+// bed_matrix_velocity_cell (shader.rs:380-407) of every cell next to the bed, once per substep: the bed
 // samples' velocities and the cell lookup do not change between bed_lookup_scatter and
 // bed_dynamics, so classify (six neighbours of each bed-coupled cell) and project (each
 // bed-coupled cell) read these instead of rescanning 27 cells per call.
@@ -408,16 +408,17 @@ __global__ void k_bed_velocity(const Ctx* __restrict__ cp) {
     CS_FOR(i, u.cells) {
         uint32_t ix, iy, iz;
         decompose(u, i, ix, iy, iz);
-        // read only at bed-coupled cells (lookup >= 0) and their six neighbours; the seven
-        // lookups are loaded together (no short-circuit chain of dependent loads)
+        // read only at bed-coupled cells (lookup >= 0, by project) and their six
+        // neighbours (by classify), so only those cells are written; the seven lookups are
+        // loaded together (no short-circuit chain of dependent loads)
         const uint32_t sy = u.gx, sz = u.gx * u.gy;
         const bool in[6] = {ix > 0, ix + 1 < u.gx, iy > 0, iy + 1 < u.gy, iz > 0, iz + 1 < u.gz};
         const uint32_t off[6] = {(uint32_t)-1, 1u, (uint32_t)0 - sy, sy, (uint32_t)0 - sz, sz};
         bool near = c.lookup[i] >= 0;
 #pragma unroll
         for (int f = 0; f < 6; ++f) near |= in[f] && c.lookup[i + off[f]] >= 0;
-        f3 v = mk(0.0f, 0.0f, 0.0f);
-        if (near) v = bed_matrix_velocity(c, (int)ix, (int)iy, (int)iz);
+        if (!near) continue;
+        const f3 v = bed_matrix_velocity(c, (int)ix, (int)iy, (int)iz);
         c.bedv[i] = make_float4(v.x, v.y, v.z, 0.0f);
     }
 }
