@@ -476,11 +476,13 @@ int Engine::gs_alloc() {
     int rc;
     if ((rc = alloc(gs_rows_, (2 * (rows + 1) + rows) * sizeof(uint32_t)))) return rc;
     if ((rc = alloc(gs_desc_, units * (sizeof(GsDesc) + 16 * sizeof(int))))) return rc;
-    // the arrays read at neighbour slots (correction + fill code, pressure) get gx / 2 + 64
-    // slots of padding on both sides: a neighbour slot computed for a face that is not a
-    // fluid face can fall up to gx / 2 + 33 slots outside the used range, and the solve
-    // loads all six before the flags pick the real ones
-    const size_t pad = (gx / 2 + 64 + 15) & ~(size_t)15;  // whole 128-byte lines of float2
+    // the arrays read at neighbour slots (correction + fill code, pressure) get at least
+    // gx / 2 + 64 slots of padding on both sides: a neighbour slot computed for a face that
+    // is not a fluid face can fall up to gx / 2 + 33 slots outside the used range, and the
+    // solve loads all six before the flags pick the real ones.  The padding is a whole
+    // number of 128-byte lines, so every unit's slots start on a line of their own and the
+    // lines of a CTA's rows hold no other CTA's slots (the solve reads those through L1).
+    const size_t pad = (gx / 2 + 64 + 15) & ~(size_t)15;
     if ((rc = alloc(gs_slots_, (slots + 2 * pad) * 2 * sizeof(float2) + slots * (sizeof(float2) + 2 * sizeof(float)))))
         return rc;
     if ((rc = gs_blocks(&gs_ctas_))) return rc;
