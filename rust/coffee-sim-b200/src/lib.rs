@@ -132,6 +132,55 @@ impl MpmSim3D {
         check(unsafe { sys::cs_metrics_wait(self.raw, &mut m) })?;
         Ok(m)
     }
+    /// One substep of `sub_dt` seconds (engine extension: the reference steps whole
+    /// frames, split into its substeps).
+    pub fn step_substep(&mut self, sub_dt: f32) -> Result<(), CsError> {
+        check(unsafe { sys::cs_step_substep(self.raw, sub_dt) })
+    }
+    /// Jet flow in ml/s and exit speed in m/s in place of the kettle-angle flow (engine
+    /// extension, for the configurations stated in SI).
+    pub fn set_flow_override(&mut self, flow_ml_s: f32, exit_speed: f32) -> Result<(), CsError> {
+        check(unsafe { sys::cs_set_flow_override(self.raw, flow_ml_s, exit_speed) })
+    }
+    /// The settings the simulation runs with (after any `cs_set_*` or autotuner change).
+    pub fn settings(&self) -> Result<MpmSettings, CsError> {
+        let mut s = MpmSettings::default();
+        check(unsafe { sys::cs_get_settings(self.raw, &mut s) })?;
+        Ok(s)
+    }
+    /// The whole simulation state as bytes, for checkpoints (engine extension; the
+    /// reference only has `reset`).
+    pub fn snapshot(&self) -> Result<Vec<u8>, CsError> {
+        let mut n = 0u64;
+        check(unsafe { sys::cs_snapshot_size(self.raw, &mut n) })?;
+        let mut out = vec![0u8; n as usize];
+        check(unsafe { sys::cs_snapshot_save(self.raw, out.as_mut_ptr() as *mut std::ffi::c_void, n) })?;
+        Ok(out)
+    }
+    /// Resumes from the bytes of `snapshot` (taken with the same settings).
+    pub fn restore(&mut self, bytes: &[u8]) -> Result<(), CsError> {
+        check(unsafe {
+            sys::cs_snapshot_load(self.raw, bytes.as_ptr() as *const std::ffi::c_void, bytes.len() as u64)
+        })
+    }
+    /// Times candidate solver settings and launch shapes over `substeps` substeps from
+    /// the current state (restored after every trial), applies the fastest that reaches
+    /// the residual target and returns it (engine extension).
+    pub fn autotune(&mut self, sub_dt: f32, substeps: u32) -> Result<sys::CsTuneResult, CsError> {
+        let mut r = sys::CsTuneResult::default();
+        check(unsafe { sys::cs_autotune(self.raw, sub_dt, substeps, &mut r) })?;
+        Ok(r)
+    }
+    /// Fill fraction and divergence of every cell as the last classify wrote them (the
+    /// right-hand side of the pressure system), one f32 per cell each.
+    pub fn read_solver_inputs(&self) -> Result<(Vec<f32>, Vec<f32>), CsError> {
+        let s = self.settings()?;
+        let cells: usize = s.grid_dims.iter().map(|&d| d as usize).product();
+        let mut fill = vec![0.0f32; cells];
+        let mut div = vec![0.0f32; cells];
+        check(unsafe { sys::cs_read_solver_inputs(self.raw, fill.as_mut_ptr(), div.as_mut_ptr()) })?;
+        Ok((fill, div))
+    }
 }
 
 impl Drop for MpmSim3D {
