@@ -1,0 +1,230 @@
+"""The CPU oracle against a second, independent restatement of the WGSL grid passes
+(`tests/wgsl_numpy.py`), pass by pass, on the CPU.
+
+Each test takes the oracle's state after the first n dispatches of a substep
+(`cs_step_substep_partial`, the dispatch numbering of `mod.rs:317-414`), applies the
+numpy restatement of dispatch n, and compares with the oracle's state after n + 1
+dispatches.  The engine is compared with the oracle bit for bit by the GPU tests, so
+agreement here carries over to it.
+"""
+import numpy as np
+import pytest
+
+from coffee_sim_b200.sim import MpmSettings, MpmSim3D
+from helpers import copy_state
+import wgsl_numpy as W
+
+FRAME = 1.0 / 60.0
+SUB_DT = FRAME / 10
+
+# dispatch numbers of one substep (mod.rs:317-414; the oracle numbers them alike)
+P_P2G, P_GRID_UPDATE, P_BOUNDARY0, P_CLASSIFY, P_RBGS = 3, 4, 5, 6, 7
+P_PROJECT, P_BOUNDARY1, P_PACK_PREP, P_PACK_APPLY, P_BOUNDARY2 = 8, 9, 10, 11, 12
+P_VISC_PREP, P_VISC_APPLY, P_BOUNDARY3, P_G2P = 13, 14, 15, 16
+
+
+def _pour(oracle):
+    """The reference's centre-pour scene (mod.rs:107-160 preset) after 24 frames of a
+    strong pour, so that water reaches the bed."""
+    s = MpmSettings.benchmark_center_pour(oracle)
+    src = MpmSim3D(s, oracle)
+    src.set_kettle_angle(36.0)
+    src.set_flow_override(40.0, 0.0)
+    for _ in range(24):
+        src.step_frame(FRAME)
+    return s, src
+
+
+def _scatter(src, seed=5):
+    """Every third water sample of the pour moved to a random point of the domain (the
+    carafe below the cone included, where the SDF constrains the flow, and the margin of
+    the box) with a random velocity of up to 3 units/s: inputs that reach the SDF
+    contact and box branches of boundary_project."""
+    rng = np.random.default_rng(seed)
+    nb, nw = src.num_bed, src.num_water
+    p = src.read_particles(nb, nw)
+    k = np.arange(0, nw, 3)
+    lo, hi = np.array([-6.9, -9.9, -6.9]), np.array([6.9, 9.9, 6.9])
+    p[k, 0:3] = rng.uniform(lo, hi, size=(k.size, 3)).astype(np.float32)
+    d = rng.normal(size=(k.size, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    p[k, 4:7] = (d * rng.uniform(0.0, 3.0, size=(k.size, 1))).astype(np.float32)
+    src.write_particles(nb, p)
+    return src
+
+
+@pytest.fixture(scope="module", params=["pour", "scattered"])
+def source(request, oracle):
+    s, src = _pour(oracle)
+    if request.param == "scattered":
+        _scatter(src)
+    return request.param, s, src
+
+
+class Stages:
+    """Oracle states after the first n dispatches of the next substep, one simulation
+    per n, all started from the same copied state."""
+
+    def __init__(self, oracle, settings, src):
+        self.oracle, self.settings, self.src = oracle, settings, src
+        self.cache = {}
+        self.static = None
+
+    def __call__(self, n):
+        if n not in self.cache:
+            sim = MpmSim3D(self.settings, self.oracle)
+            copy_state(self.src, sim)
+            sim.set_kettle_angle(36.0)
+            sim.step_substep_partial(SUB_DT, n)
+            st = {"particles": sim.read_particles(0, sim.particle_count()),
+                  "affine": sim.read_affine(0, sim.particle_count()),
+                  "lanes": sim.read_grid_lanes(), "grid_vel": sim.read_grid_vel(),
+                  "lookup": sim.read_bed_lookup(), "bed_delta": sim.read_bed_delta(),
+                  "num_water": sim.num_water, "num_bed": sim.num_bed}
+            if sim.num_bed:
+                st["bed_extract"] = sim.read_bed_extract(0, sim.num_bed)
+            if self.static is None:
+                self.static = {"sdf": sim.read_sdf(), "sdf_class": sim.read_sdf_class()}
+            self.cache[n] = st
+            sim.close()
+        return self.cache[n]
+
+    def uniforms(self, n):
+        st = self(n)
+        return W.Uniforms(self.settings.raw, st["num_water"], st["num_bed"], SUB_DT)
+
+
+@pytest.fixture(scope="module")
+def stages(oracle, source):
+    name, s, src = source
+    st = Stages(oracle, s, src)
+    st.name = name
+    return st
+
+
+def _report(name, got, want):
+    got, want = np.asarray(got), np.asarray(want)
+    bad = np.flatnonzero(got.reshape(-1) != want.reshape(-1))
+    if bad.size:
+        i = bad[0]
+        return f"{name}: {bad.size} of {got.size} differ, first at {i}: {got.reshape(-1)[i]!r} vs {want.reshape(-1)[i]!r}"
+    return None
+
+
+def test_scene_has_water_in_the_bed(stages):
+    """The inputs reach the branches under test: water in bed-coupled and interior
+    cells (both states), grid velocities changed by the SDF contact (scattered state)."""
+    st = stages(P_CLASSIFY + 1)
+    assert st["num_water"] > 2000 and st["num_bed"] == 12000
+    kind = st["lanes"][3]
+    assert np.count_nonzero(kind == W.CELL_BED_COUPLED) > 100
+    assert np.count_nonzero(kind == W.CELL_INTERIOR_FLUID) > 100
+    if stages.name == "scattered":
+        u = stages.uniforms(P_BOUNDARY0)
+        sdf = W.Sdf(u, stages.static["sdf"])
+        px, py, pz = W.cell_centres(u)
+        live = stages(P_BOUNDARY0)["grid_vel"][:, 3] >= 1e-6
+        assert np.count_nonzero(live & (sdf.sample(px, py, pz).reshape(-1) < u.contact_offset)) > 50
+        assert np.count_nonzero(stages(P_BOUNDARY0)["grid_vel"] != stages(P_BOUNDARY0 + 1)["grid_vel"]) > 50
+
+
+def test_p2g(stages):
+    u = stages.uniforms(P_P2G)
+    before = stages(P_P2G)
+    after = stages(P_P2G + 1)
+    assert not before["lanes"].any()
+    lanes = W.p2g(u, before["particles"], before["affine"])
+    msg = _report("lanes", lanes, after["lanes"])
+    assert msg is None, msg
+
+
+def test_grid_update(stages):
+    u = stages.uniforms(P_GRID_UPDATE)
+    before = stages(P_GRID_UPDATE)
+    after = stages(P_GRID_UPDATE + 1)
+    gv = W.grid_update(u, before["lanes"])
+    msg = _report("grid_vel", gv, after["grid_vel"])
+    assert msg is None, msg
+
+
+@pytest.mark.parametrize("n", [P_BOUNDARY0, P_BOUNDARY1])
+def test_boundary_project(stages, n):
+    u = stages.uniforms(n)
+    before = stages(n)
+    after = stages(n + 1)
+    sdf = W.Sdf(u, stages.static["sdf"])
+    gv = W.boundary_project(u, sdf, before["grid_vel"])
+    msg = _report("grid_vel", gv, after["grid_vel"])
+    assert msg is None, msg
+
+
+def _bed(stages, n, u):
+    st = stages(n)
+    return W.Bed(u, st["lookup"], st["particles"], st["affine"], st.get("bed_extract", np.zeros((0, 8), np.float32)))
+
+
+def test_classify(stages):
+    u = stages.uniforms(P_CLASSIFY)
+    before, after = stages(P_CLASSIFY), stages(P_CLASSIFY + 1)
+    sdf = W.Sdf(u, stages.static["sdf"])
+    solid = stages.static["sdf_class"].reshape(u.grid_shape()) != 0
+    lanes = W.classify(u, before["lanes"], before["grid_vel"], _bed(stages, P_CLASSIFY, u), sdf, solid,
+                       bool(stages.settings.raw.use_sdf_cache))
+    for lane, name in ((3, "kind"), (1, "divergence"), (0, "pressure"), (2, "lane 2"), (4, "rest volume"), (5, "current volume")):
+        msg = _report(name, lanes[lane], after["lanes"][lane])
+        assert msg is None, msg
+
+
+def test_rbgs_fixed_pairs(stages):
+    """The reference configuration: fixed-point pressure, `pressure_rbgs_pairs` red+black
+    pairs from the cold start (mod.rs:352-357)."""
+    raw = stages.settings.raw
+    assert raw.pressure_storage == 0 and raw.solve_mode == 0 and raw.rbgs_omega in (0.0, 1.0)
+    u = stages.uniforms(P_RBGS)
+    before, after = stages(P_RBGS), stages(P_RBGS + 1)
+    lanes = W.rbgs(u, before["lanes"], int(raw.pressure_rbgs_pairs))
+    assert np.count_nonzero(after["lanes"][0]) > 100
+    msg = _report("pressure", lanes[0], after["lanes"][0])
+    assert msg is None, msg
+
+
+def test_project_with_darcy_drag(stages):
+    u = stages.uniforms(P_PROJECT)
+    before, after = stages(P_PROJECT), stages(P_PROJECT + 1)
+    gv, imp = W.project(u, before["lanes"], before["grid_vel"], _bed(stages, P_PROJECT, u))
+    kind = before["lanes"][3]
+    darcy = (kind == W.CELL_BED_COUPLED) & (before["grid_vel"][:, 3] >= 1e-6) & (before["lookup"] >= 0)
+    assert np.count_nonzero(darcy) > 50
+    msg = _report("grid_vel", gv, after["grid_vel"])
+    assert msg is None, msg
+    added = after["bed_delta"][1:4, :u.num_bed].astype(np.int64) - before["bed_delta"][1:4, :u.num_bed]
+    assert np.count_nonzero(imp) > 0
+    msg = _report("bed impulse lanes", W.wrap_i32(imp), W.wrap_i32(added))
+    assert msg is None, msg
+
+
+def test_packing(stages):
+    u = stages.uniforms(P_PACK_PREP)
+    before, mid, after = stages(P_PACK_PREP), stages(P_PACK_APPLY), stages(P_PACK_APPLY + 1)
+    lanes = W.packing_prepare(u, before["lanes"])
+    msg = _report("lanes", lanes.reshape(6, -1), mid["lanes"])
+    assert msg is None, msg
+    gv = W.packing_apply(u, mid["lanes"], mid["grid_vel"])
+    msg = _report("grid_vel", gv, after["grid_vel"])
+    assert msg is None, msg
+
+
+def test_viscosity(stages):
+    u = stages.uniforms(P_VISC_PREP)
+    assert u.viscosity > 0
+    before, mid, after = stages(P_VISC_PREP), stages(P_VISC_APPLY), stages(P_VISC_APPLY + 1)
+    solid = stages.static["sdf_class"].reshape(u.grid_shape()) != 0
+    lanes = W.viscosity_prepare(u, before["lanes"], before["grid_vel"], solid)
+    msg = _report("lanes", lanes, mid["lanes"])
+    assert msg is None, msg
+    scratch = W.lane_f32(u, mid["lanes"][1:4]).T
+    blended = np.count_nonzero(np.any(scratch != before["grid_vel"][:, :3], axis=1) & (before["grid_vel"][:, 3] > 2 * u.nominal_mass))
+    assert blended > 50
+    gv = W.viscosity_apply(u, mid["lanes"], mid["grid_vel"])
+    msg = _report("grid_vel", gv, after["grid_vel"])
+    assert msg is None, msg

@@ -1,0 +1,693 @@
+"""A second, independent restatement of grid passes of the reference's WGSL step, in
+vectorised numpy float32 — test infrastructure only.
+
+The C++ oracle (`oracle/oracle.cpp`) and the CUDA engine were written from the same
+reading of `crates/sim-wasm/src/mpm_3d/shader.rs`, so their bit-exact agreement cannot
+expose a misreading they share.  This module is a separate reading of the same WGSL,
+written directly from the shader text in a different form (whole-grid array
+expressions instead of per-cell loops), and the tests compare it with the oracle
+pass by pass.  Every function cites the shader lines it restates.
+
+Floating point: every value is an IEEE float32 array and every WGSL expression is
+evaluated in its written, left-to-right order (numpy >= 2 keeps Python scalars weak,
+so `f32_array * 0.5` stays float32).  WGSL conversions are restated explicitly:
+`i32(f)` truncates toward zero and saturates, `f32(i)` rounds to nearest, `mix(a, b, t)`
+is `a * (1 - t) + b * t`, `clamp(x, lo, hi)` is `min(max(x, lo), hi)`, `fract(x)` is
+`x - floor(x)`, `length(v)` is `sqrt(x*x + y*y + z*z)`.  Integer atomics are
+order-independent sums that wrap at 32 bits.
+"""
+import numpy as np
+
+F32 = np.float32
+
+# shader.rs:172-177 cell kinds
+CELL_AIR, CELL_SURFACE_FLUID, CELL_INTERIOR_FLUID, CELL_BED_COUPLED, CELL_SOLID = 0, 1, 2, 3, 4
+# state.rs:13-28
+FP_SCALE = F32(262144.0)
+FP_VALUE_LIMIT = F32(8192.0)
+SDF_RES = 128
+METRICS_DIV_FP_SCALE = F32(1024.0)
+# shader.rs:75-76
+BED_REACTION_ALPHA = F32(0.04)
+BED_REACTION_IMPULSE_CAP = F32(0.012)
+# neighbour order of every six-face loop in the shader (shader.rs:1114-1121, 1388-1395)
+FACES = ((-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1))
+
+
+def f32(x):
+    return np.asarray(x, dtype=np.float32)
+
+
+def to_i32(x):
+    """WGSL `i32(f32)`: truncate toward zero, saturate at the i32 range."""
+    t = np.trunc(np.asarray(x, dtype=np.float64))
+    t = np.where(np.isnan(t), 0.0, t)
+    return np.clip(t, -2147483648.0, 2147483647.0).astype(np.int32)
+
+
+def wrap_i32(x):
+    """Two's-complement wrap of an int64 sum to i32 (WGSL atomicAdd on i32)."""
+    return (np.asarray(x, dtype=np.int64) & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
+
+
+def mix(a, b, t):
+    return a * (1 - t) + b * t
+
+
+def clamp(x, lo, hi):
+    return np.minimum(np.maximum(x, lo), hi)
+
+
+def length3(x, y, z):
+    return np.sqrt(x * x + y * y + z * z)
+
+
+def smoothstep(e0, e1, x):
+    t = clamp((x - e0) / (e1 - e0), F32(0.0), F32(1.0))
+    return t * t * (3 - 2 * t)
+
+
+class Uniforms:
+    """`MpmUniforms` as `MpmSim3D::write_uniforms` fills it (mod.rs:569-660), from the
+    settings the simulation was created with and the counts of the substep."""
+
+    def __init__(self, raw, num_water, num_bed, dt):
+        gx, gy, gz = (int(v) for v in raw.grid_dims)
+        self.gx, self.gy, self.gz = gx, gy, gz
+        self.cells = gx * gy * gz
+        self.num_water, self.num_bed = int(num_water), int(num_bed)
+        self.max_particles = int(raw.max_particles)
+        bs = [F32(v) for v in raw.bounds_size]
+        self.dx = bs[0] / F32(gx)                                   # mod.rs:573
+        self.inv_dx = F32(1.0) / self.dx                            # mod.rs:574
+        brew = raw.brew
+        self.nominal_mass = F32(brew.water_mass_units_per_ml) / F32(brew.water_particles_per_ml)  # mod.rs:575
+        self.p_vol = self.dx * self.dx * self.dx * F32(raw.particle_volume_cells)                # mod.rs:576
+        self.dt = F32(dt)
+        self.gravity = F32(raw.gravity)
+        self.origin = np.array([-b * F32(0.5) for b in bs], dtype=np.float32)
+        self.bounds_max = np.array([b * F32(0.5) for b in bs], dtype=np.float32)
+        self.bulk_K = F32(raw.bulk_modulus)
+        self.viscosity = F32(raw.viscosity)
+        self.fp = FP_SCALE
+        self.inv_fp = F32(1.0) / FP_SCALE
+        self.vel_cap = F32(raw.max_velocity)
+        g = raw.geom
+        self.friction = F32(g.sdf_friction)
+        self.restitution = F32(g.sdf_restitution)
+        self.contact_offset = F32(g.contact_offset)
+        self.nu_m2s = F32(brew.water_kinematic_viscosity_m2_s)
+        self.min_perm = F32(brew.min_bed_permeability_m2)
+        self.div_clamp = np.minimum(F32(4.0) * self.vel_cap * self.inv_dx, FP_VALUE_LIMIT - F32(1.0))  # mod.rs:589-590
+        self.p_clamp = FP_VALUE_LIMIT - F32(1.0)                    # mod.rs:593
+        self.j_alpha, self.j_expand_alpha, self.max_rest_frac = F32(32.0), F32(2.0), F32(1.20)  # mod.rs:656
+        self.surface_void_scale = F32(brew.bed_surface_void_scale)
+        self.pore_capacity_scale = F32(brew.bed_pore_capacity_scale)
+        self.pore_overfill_alpha = F32(brew.bed_pore_overfill_alpha)
+
+    # shader.rs:116, 171-172
+    @property
+    def occupancy(self):
+        return self.nominal_mass * F32(0.1)
+
+    @property
+    def inactive(self):
+        return self.nominal_mass * F32(0.10)
+
+    def grid_shape(self):
+        return (self.gz, self.gy, self.gx)
+
+
+# ---------------------------------------------------------------- neighbour access
+
+def shifted(a, d, fill):
+    """b[z, y, x] = a[z + dz, y + dy, x + dx] (last three axes), `fill` off the grid."""
+    dxo, dyo, dzo = d
+    out = np.empty_like(a)
+    out[...] = fill
+    nz, ny, nx = a.shape[:3]
+
+    def rng(o, n):
+        return (slice(max(0, -o), n - max(0, o)), slice(max(0, o), n - max(0, -o)))
+
+    (zd, zs), (yd, ys), (xd, xs) = rng(dzo, nz), rng(dyo, ny), rng(dxo, nx)
+    out[zd, yd, xd] = a[zs, ys, xs]
+    return out
+
+
+def in_grid(u, d):
+    """True where the neighbour at offset d lies on the grid."""
+    return shifted(np.ones(u.grid_shape(), dtype=bool), d, False)
+
+
+def cell_centres(u):
+    """origin + (vec3(f32(i)) + 0.5) * dx for every cell (shader.rs:1645-1646)."""
+    iz, iy, ix = np.meshgrid(np.arange(u.gz, dtype=np.float32), np.arange(u.gy, dtype=np.float32),
+                             np.arange(u.gx, dtype=np.float32), indexing="ij")
+    return [u.origin[a] + (c + F32(0.5)) * u.dx for a, c in enumerate((ix, iy, iz))]
+
+
+# ---------------------------------------------------------------- p2g  (shader.rs:955-1052)
+
+def p2g(u, particles, affine):
+    """Six i32 lanes after P2G into a cleared grid: (6, cells) int32."""
+    n = u.num_water + u.num_bed
+    p = np.asarray(particles, np.float32).reshape(-1, 8)[:n]
+    a = np.asarray(affine, np.float32).reshape(-1, 12)[:n]
+    xp, J, vp, mass = p[:, 0:3], p[:, 3], p[:, 4:7], p[:, 7]
+    phase = a[:, 3]
+    live = (phase < F32(0.5)) & ~(mass <= u.inactive)               # shader.rs:966-968
+    xp, J, vp, mass, a = xp[live], J[live], vp[live], mass[live], a[live]
+    grid_pos = (xp - u.origin) * u.inv_dx                           # shader.rs:971
+    base_f = np.floor(grid_pos - F32(0.5))
+    base = to_i32(base_f)
+    fx = grid_pos - base.astype(np.float32)
+    w = [[F32(0.5) * (F32(1.5) - fx[:, c]) * (F32(1.5) - fx[:, c]),  # shader.rs:979-987
+          F32(0.75) - (fx[:, c] - F32(1.0)) * (fx[:, c] - F32(1.0)),
+          F32(0.5) * (fx[:, c] - F32(0.5)) * (fx[:, c] - F32(0.5))] for c in range(3)]
+    cols = [a[:, 0:3], a[:, 4:7], a[:, 8:11]]
+    aff = [np.stack([mass * C[:, 0], mass * C[:, 1], mass * C[:, 2]], axis=1) for C in cols]  # shader.rs:993-995
+    rest_vol = u.p_vol * mass / np.maximum(u.nominal_mass, F32(1e-6))           # shader.rs:999
+    cur_vol = rest_vol * clamp(J, F32(0.40), F32(2.00))                          # shader.rs:1000
+    mvp = mass[:, None] * vp
+    acc = np.zeros((6, u.cells), dtype=np.int64)
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                off = np.array([i, j, k], dtype=np.int32)
+                cell = base + off
+                ok = ((cell >= 0).all(axis=1) & (cell[:, 0] < u.gx) & (cell[:, 1] < u.gy) & (cell[:, 2] < u.gz))
+                wt = w[0][i] * w[1][j] * w[2][k]                                   # shader.rs:1010
+                dpos = (off.astype(np.float32) - fx) * u.dx                        # shader.rs:1011
+                dots = [c[:, 0] * dpos[:, 0] + c[:, 1] * dpos[:, 1] + c[:, 2] * dpos[:, 2] for c in aff]
+                mom = [wt * (mvp[:, q] + dots[q]) for q in range(3)]               # shader.rs:1016-1020
+                vals = [wt * mass * u.fp, mom[0] * u.fp, mom[1] * u.fp, mom[2] * u.fp,
+                        wt * rest_vol * u.fp, wt * cur_vol * u.fp]                 # shader.rs:1032-1037
+                ci = (cell[:, 2].astype(np.int64) * u.gy + cell[:, 1]) * u.gx + cell[:, 0]
+                for lane in range(6):
+                    np.add.at(acc[lane], ci[ok], to_i32(vals[lane][ok]).astype(np.int64))
+    return wrap_i32(acc)
+
+
+# ---------------------------------------------------------------- grid_update  (shader.rs:1056-1082)
+
+def grid_update(u, lanes):
+    """`grid_vel` after grid_update on a cleared `grid_vel`: (cells, 4) float32."""
+    L = np.asarray(lanes, np.int32).reshape(6, -1)
+    mass = L[0].astype(np.float32) * u.inv_fp
+    live = ~(mass < F32(1e-6))
+    m = np.where(live, mass, F32(1.0))
+    v = [L[q].astype(np.float32) * u.inv_fp / m for q in (1, 2, 3)]
+    v[1] = v[1] + u.gravity * u.dt
+    speed = length3(*v)
+    over = speed > u.vel_cap
+    s = np.where(over, u.vel_cap / np.where(over, speed, F32(1.0)), F32(1.0))
+    v = [np.where(over, c * s, c) for c in v]
+    out = np.zeros((u.cells, 4), dtype=np.float32)
+    for q in range(3):
+        out[:, q] = np.where(live, v[q], F32(0.0))
+    out[:, 3] = np.where(live, mass, F32(0.0))
+    return out
+
+
+# ---------------------------------------------------------------- SDF  (shader.rs:668-715)
+
+class Sdf:
+    """The 128^3 SDF texture read with `textureLoad` (R32F texels, x fastest)."""
+
+    def __init__(self, u, texels):
+        self.u = u
+        self.t = np.asarray(texels, np.float32).reshape(SDF_RES, SDF_RES, SDF_RES)
+
+    def load(self, cx, cy, cz):
+        m = SDF_RES - 1
+        return self.t[np.clip(cz, 0, m), np.clip(cy, 0, m), np.clip(cx, 0, m)]
+
+    def sample(self, px, py, pz):
+        """shader.rs:678-699, trilinear by `mix` in x, then y, then z."""
+        u = self.u
+        bsz = u.bounds_max * F32(2.0)
+        res = F32(SDF_RES)
+        uv = [(p + u.bounds_max[a]) / bsz[a] * res - F32(0.5) for a, p in enumerate((px, py, pz))]
+        fl = [np.floor(c) for c in uv]
+        b = [to_i32(c) for c in fl]
+        f = [c - d for c, d in zip(uv, fl)]
+        c = {}
+        for dz in (0, 1):
+            for dy in (0, 1):
+                for dx_ in (0, 1):
+                    c[(dx_, dy, dz)] = self.load(b[0] + dx_, b[1] + dy, b[2] + dz)
+        c00 = mix(c[(0, 0, 0)], c[(1, 0, 0)], f[0])
+        c10 = mix(c[(0, 1, 0)], c[(1, 1, 0)], f[0])
+        c01 = mix(c[(0, 0, 1)], c[(1, 0, 1)], f[0])
+        c11 = mix(c[(0, 1, 1)], c[(1, 1, 1)], f[0])
+        c0 = mix(c00, c10, f[1])
+        c1 = mix(c01, c11, f[1])
+        return mix(c0, c1, f[2])
+
+    def gradient(self, px, py, pz):
+        """shader.rs:701-715: central differences at +-dx, normalised."""
+        e = self.u.dx
+        g = [self.sample(px + e, py, pz) - self.sample(px - e, py, pz),
+             self.sample(px, py + e, pz) - self.sample(px, py - e, pz),
+             self.sample(px, py, pz + e) - self.sample(px, py, pz - e)]
+        ln = length3(*g)
+        small = ln < F32(1e-8)
+        d = np.where(small, F32(1.0), ln)
+        return [np.where(small, F32(0.0), c / d) for c in g]
+
+
+# ---------------------------------------------------------------- boundary_project  (shader.rs:1630-1679)
+
+def boundary_project(u, sdf, grid_vel):
+    """`grid_vel` after one boundary_project pass: (cells, 4) float32."""
+    gv = np.array(grid_vel, np.float32).reshape(u.gz, u.gy, u.gx, 4)
+    live = ~(gv[..., 3] < F32(1e-6))
+    v = [gv[..., q].copy() for q in range(3)]
+    px, py, pz = cell_centres(u)
+    sd = sdf.sample(px, py, pz)
+    near = live & (sd < u.contact_offset)
+    n = sdf.gradient(px, py, pz)
+    vn = v[0] * n[0] + v[1] * n[1] + v[2] * n[2]
+    hit = near & (vn < F32(0.0))
+    k = F32(1.0) + u.restitution
+    v2 = [v[q] - n[q] * vn * k for q in range(3)]                          # shader.rs:1653
+    d2 = v2[0] * n[0] + v2[1] * n[1] + v2[2] * n[2]
+    vt = [v2[q] - n[q] * d2 for q in range(3)]                             # shader.rs:1655
+    vtl = length3(*vt)
+    fr = hit & (vtl > F32(1e-6))
+    safe = np.where(fr, vtl, F32(1.0))
+    imp = np.minimum(u.friction * np.abs(vn), vtl)
+    v3 = [np.where(fr, v2[q] - vt[q] * (imp / safe), v2[q]) for q in range(3)]
+    v = [np.where(hit, v3[q], v[q]) for q in range(3)]
+    margin = F32(2.0) * u.dx                                               # shader.rs:1665-1667
+    for q, p in enumerate((px, py, pz)):
+        lo = u.origin[q] + margin
+        hi = u.bounds_max[q] - margin
+        v[q] = np.where((p < lo) & (v[q] < F32(0.0)), F32(0.0), v[q])
+        v[q] = np.where((p > hi) & (v[q] > F32(0.0)), F32(0.0), v[q])
+    out = gv.copy()
+    for q in range(3):
+        out[..., q] = np.where(live, v[q], gv[..., q])
+    return out.reshape(-1, 4)
+
+
+# ---------------------------------------------------------------- shared helpers of the pressure passes
+
+def is_fluid(kind):
+    """shader.rs:582-591"""
+    return (kind == CELL_INTERIOR_FLUID) | (kind == CELL_SURFACE_FLUID) | (kind == CELL_BED_COUPLED)
+
+
+def lane_f32(u, lane):
+    """`f32(atomicLoad(&grid[...])) * inv_fp_scale()` (shader.rs:198-200, 262-264, 285-291)."""
+    return lane.astype(np.float32) * u.inv_fp
+
+
+def fill_fraction(u, kind, rest, cur):
+    """liquid_fill_fraction (shader.rs:293-304)."""
+    cell_volume = np.maximum(u.dx * u.dx * u.dx, F32(1e-8))
+    dep = clamp(np.maximum(rest, cur) / cell_volume, F32(0.0), F32(1.0))
+    out = np.where(kind == CELL_SURFACE_FLUID, dep, F32(0.0))
+    return np.where((kind == CELL_INTERIOR_FLUID) | (kind == CELL_BED_COUPLED), F32(1.0), out).astype(np.float32)
+
+
+def face_weight(self_kind, self_fill, nb_kind, nb_fill):
+    """pressure_face_weight (shader.rs:306-323); nb_fill = liquid_fill_fraction(neighbour)."""
+    w = np.minimum(self_fill, nb_fill)
+    w = np.where(~is_fluid(nb_kind), self_fill, w)
+    w = np.where((self_kind == CELL_BED_COUPLED) | (nb_kind == CELL_BED_COUPLED), F32(1.0), w)
+    return np.where(nb_kind == CELL_SOLID, F32(0.0), w).astype(np.float32)
+
+
+def store_clamped(u, value, lo, hi):
+    """pressure_store / divergence_store / packing_pressure_store: clamp, then
+    `i32(clamped * fp_scale())` (shader.rs:202-221, 352-359)."""
+    return to_i32(clamp(value, lo, hi) * u.fp)
+
+
+class Bed:
+    """Bed-sample views the grid passes read: lookup per cell, the sample rows."""
+
+    def __init__(self, u, lookup, particles, affine, bed_extract):
+        self.u = u
+        self.lookup = np.asarray(lookup, np.int32).reshape(u.grid_shape())
+        nb = u.num_bed
+        self.vel = np.asarray(particles, np.float32).reshape(-1, 8)[:nb, 4:7]
+        self.pos_y = np.asarray(particles, np.float32).reshape(-1, 8)[:nb, 1]
+        self.phase = np.asarray(affine, np.float32).reshape(-1, 12)[:nb, 3]
+        self.bx = np.asarray(bed_extract, np.float32).reshape(-1, 8)[:nb] if nb else np.zeros((0, 8), np.float32)
+
+    def valid_solid(self, idx):
+        """is_valid_bed_solid_idx (shader.rs:365-370)."""
+        ok = (idx >= 0) & (idx < self.u.num_bed)
+        safe = np.where(ok, idx, 0)
+        ph = self.phase[safe] if self.u.num_bed else np.zeros(idx.shape, np.float32)
+        return ok & ~(ph < F32(0.5))
+
+    def matrix_velocity(self):
+        """bed_matrix_velocity_cell (shader.rs:380-407) of every cell: the mean velocity of
+        the valid bed samples looked up in the 3x3x3 block, summed x-offset outermost."""
+        u = self.u
+        sums = [np.zeros(u.grid_shape(), np.float32) for _ in range(3)]
+        wsum = np.zeros(u.grid_shape(), np.float32)
+        for di in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    li = shifted(self.lookup, (di, dj, dk), -1)
+                    ok = self.valid_solid(li)
+                    safe = np.where(ok, li, 0)
+                    for q in range(3):
+                        vq = self.vel[safe, q] if u.num_bed else np.zeros(li.shape, np.float32)
+                        sums[q] = np.where(ok, sums[q] + vq, sums[q])
+                    wsum = np.where(ok, wsum + F32(1.0), wsum)
+        has = ~(wsum <= F32(0.0))
+        d = np.where(has, wsum, F32(1.0))
+        return [np.where(has, s / d, F32(0.0)).astype(np.float32) for s in sums]
+
+    def compacted_porosity(self, b):
+        """bed_compacted_porosity (shader.rs:435-440)."""
+        be = self.bx[b]
+        base = clamp(be[:, 1], F32(0.18), F32(0.70))
+        comp = clamp(be[:, 3], F32(0.0), F32(2.25))
+        return clamp(base - comp * F32(0.12), F32(0.16), base)
+
+    def compacted_permeability(self, b):
+        """bed_compacted_permeability (shader.rs:442-449) with kozeny_porosity_factor
+        (shader.rs:429-433)."""
+        def kozeny(phi_in):
+            phi = clamp(phi_in, F32(0.08), F32(0.82))
+            solid = np.maximum(F32(1.0) - phi, F32(1e-4))
+            return (phi * phi * phi) / (solid * solid)
+        be = self.bx[b]
+        base = clamp(be[:, 1], F32(0.18), F32(0.70))
+        ratio = kozeny(self.compacted_porosity(b)) / np.maximum(kozeny(base), F32(1e-8))
+        return np.maximum(be[:, 2] * ratio, self.u.min_perm)
+
+
+def solid_at(u, sdf, solid_class, use_cache, d):
+    """Whether the neighbour at offset d is solid as classify_cells tests it
+    (shader.rs:1279-1326): the class texture when the SDF cache is on, else the SDF at the
+    neighbour's centre (cell centre + offset * dx) below zero."""
+    if use_cache:
+        return shifted(solid_class, d, False)
+    px, py, pz = cell_centres(u)
+    e = u.dx
+    q = [px, py, pz]
+    for a in range(3):
+        if d[a] > 0:
+            q[a] = q[a] + e
+        elif d[a] < 0:
+            q[a] = q[a] + (-e)
+    return ~(sdf.sample(*q) >= F32(0.0))
+
+
+# ---------------------------------------------------------------- classify_cells  (shader.rs:1181-1367)
+
+def volume_target(u, rest, cur):
+    """volume_projection_target_divergence (shader.rs:597-619)."""
+    cell_volume = u.dx * u.dx * u.dx
+    eps = np.maximum(cell_volume * F32(1e-5), u.p_vol * F32(1e-3))
+    small = rest <= eps
+    j = cur / np.where(small, F32(1.0), rest)
+    ce = clamp(F32(1.0) - j, F32(0.0), F32(0.75))
+    ee = clamp(j - F32(1.0), F32(0.0), F32(0.75))
+    t = ce * u.j_alpha - ee * u.j_expand_alpha
+    packed = np.maximum(rest, cur) / np.maximum(cell_volume, F32(1e-8))
+    over = np.maximum(packed - u.max_rest_frac, F32(0.0))
+    t = np.maximum(t, over * u.j_alpha)
+    return np.where(small, F32(0.0), t).astype(np.float32)
+
+
+def bed_pore_target(u, bed, b, centre_y, rest, cur):
+    """bed_pore_projection_target_divergence (shader.rs:621-666) for bed samples b."""
+    t = volume_target(u, rest, cur)
+    cell_volume = u.dx * u.dx * u.dx
+    be = bed.bx[b]
+    base = bed.compacted_porosity(b)
+    sat = clamp(be[:, 7], F32(0.0), F32(1.0))
+    comp = clamp(be[:, 3], F32(0.0), F32(2.25))
+    surface_t = smoothstep(F32(-0.25), F32(0.75), (centre_y - bed.pos_y[b]) * u.inv_dx)
+    open_pore = clamp((F32(1.0) - F32(0.65) * sat) * (F32(1.0) - F32(0.12) * comp), F32(0.20), F32(1.0))
+    opening = surface_t * clamp(u.surface_void_scale, F32(0.0), F32(1.0)) * open_pore
+    surface_por = np.minimum(base + F32(0.35), F32(0.82))
+    eff = mix(base, surface_por, opening)
+    occ = mix(F32(1.0), F32(0.35), opening)
+    sat_cap = mix(F32(1.0), F32(0.32), sat)
+    comp_cap = mix(F32(1.0), F32(0.58), clamp(comp / F32(1.5), F32(0.0), F32(1.0)))
+    cap = eff * cell_volume * np.maximum(u.pore_capacity_scale, F32(0.0)) * sat_cap * comp_cap
+    overfill = np.maximum(cur - cap, F32(0.0)) / np.maximum(cell_volume, F32(1e-8))
+    resp = u.pore_overfill_alpha * occ * mix(F32(1.0), F32(1.45), sat)
+    return np.maximum(t, overfill * resp)
+
+
+def classify(u, lanes, grid_vel, bed, sdf, solid_class, use_cache):
+    """Lanes after classify_cells: pressure (lane 0) zeroed, kind (lane 3) and the
+    divergence minus its target (lane 1) written for every cell; (6, cells) int32."""
+    L = np.array(lanes, np.int32).reshape(6, *u.grid_shape())
+    gv = np.asarray(grid_vel, np.float32).reshape(*u.grid_shape(), 4)
+    mass = gv[..., 3]
+    px, py, pz = cell_centres(u)
+    self_solid = solid_class if use_cache else (sdf.sample(px, py, pz) < F32(0.0))
+    occ = u.occupancy
+    air = mass <= occ
+    air_nb = np.zeros(u.grid_shape(), bool)
+    for d in FACES:
+        air_nb |= ~in_grid(u, d) | (shifted(mass, d, F32(0.0)) <= occ)
+    kind = np.where(air_nb, CELL_SURFACE_FLUID, CELL_INTERIOR_FLUID)
+    kind = np.where(bed.lookup >= 0, CELL_BED_COUPLED, kind)
+    kind = np.where(air, CELL_AIR, kind)
+    kind = np.where(self_solid, CELL_SOLID, kind).astype(np.int32)
+    # ghost-mirrored central differences (shader.rs:1270-1328)
+    vel = [gv[..., q] for q in range(3)]
+    faces = {}
+    for a, d in enumerate(FACES):
+        axis = a // 2
+        open_ = in_grid(u, d) & ~solid_at(u, sdf, solid_class, use_cache, d)
+        faces[a] = np.where(open_, shifted(vel[axis], d, F32(0.0)), -vel[axis])
+    div = F32(0.5) * u.inv_dx * (((faces[1] - faces[0]) + (faces[3] - faces[2])) + (faces[5] - faces[4]))
+    rest, cur = lane_f32(u, L[4]), lane_f32(u, L[5])
+    target = volume_target(u, rest, cur)
+    li = bed.lookup
+    bedc = (kind == CELL_BED_COUPLED) & (li >= 0) & (li < u.num_bed)
+    if bedc.any():
+        sel = np.nonzero(bedc)
+        b = li[sel]
+        pore = bed_pore_target(u, bed, b, py[sel], rest[sel], cur[sel])
+        porosity = clamp(bed.compacted_porosity(b), F32(0.08), F32(1.0))
+        solid_fraction = F32(1.0) - porosity
+        bmv = bed.matrix_velocity()
+        nbv = {}
+        for a, d in enumerate(FACES):
+            nbv[a] = shifted(bmv[a // 2], d, F32(0.0))[sel]
+        sdiv = F32(0.5) * u.inv_dx * (((nbv[1] - nbv[0]) + (nbv[3] - nbv[2])) + (nbv[5] - nbv[4]))
+        target[sel] = (pore - solid_fraction * sdiv) / porosity
+    fluid = is_fluid(kind)
+    out = L.copy()
+    out[0] = 0                                                          # pressure_store(idx, 0.0)
+    out[3] = kind
+    out[1] = np.where(fluid, store_clamped(u, div - target, -u.div_clamp, u.div_clamp), 0)
+    return out.reshape(6, -1)
+
+
+# ---------------------------------------------------------------- pressure_rbgs  (shader.rs:1371-1453)
+
+def rbgs(u, lanes, pairs):
+    """Lane 0 (pressure) after `pairs` red+black sweeps of pressure_update; (6, cells)."""
+    L = np.array(lanes, np.int32).reshape(6, *u.grid_shape())
+    kind = L[3]
+    fill = fill_fraction(u, kind, lane_f32(u, L[4]), lane_f32(u, L[5]))
+    div = lane_f32(u, L[1])
+    iz, iy, ix = np.meshgrid(np.arange(u.gz), np.arange(u.gy), np.arange(u.gx), indexing="ij")
+    parity = (ix + iy + iz) & 1
+    fluid = is_fluid(kind)
+    nbk = {d: shifted(kind, d, CELL_SOLID) for d in FACES}     # off-grid faces are skipped like solids
+    nbf = {d: shifted(fill, d, F32(0.0)) for d in FACES}
+    w = {d: face_weight(kind, fill, nbk[d], nbf[d]) for d in FACES}
+    use = {d: in_grid(u, d) & (nbk[d] != CELL_SOLID) & ~(w[d] <= F32(0.0)) for d in FACES}
+    rhs = div * fill / np.maximum(u.dt, F32(1e-6))
+    dx2rhs = u.dx * u.dx * rhs
+    p = L[0].copy()
+    for _ in range(pairs):
+        for colour in (0, 1):
+            pf = lane_f32(u, p)
+            cnt = np.zeros(u.grid_shape(), np.float32)
+            psum = np.zeros(u.grid_shape(), np.float32)
+            for d in FACES:
+                cnt = np.where(use[d], cnt + w[d], cnt)
+                term = w[d] * shifted(pf, d, F32(0.0))
+                psum = np.where(use[d] & is_fluid(nbk[d]), psum + term, psum)
+            none = cnt <= F32(0.0)
+            pnew = (psum - dx2rhs) / np.where(none, F32(1.0), cnt)
+            val = np.where(fluid & ~none, pnew, F32(0.0))
+            stored = store_clamped(u, val, -u.p_clamp, u.p_clamp)
+            p = np.where(parity == colour, stored, p)
+    out = L.copy()
+    out[0] = p
+    return out.reshape(6, -1)
+
+
+# ---------------------------------------------------------------- project_pressure  (shader.rs:1457-1543)
+
+def project(u, lanes, grid_vel, bed):
+    """`grid_vel` after project_pressure and the bed impulses it adds: ((cells, 4) float32,
+    (3, num_bed) int64 sums of the impulse lanes)."""
+    L = np.asarray(lanes, np.int32).reshape(6, *u.grid_shape())
+    gv = np.array(grid_vel, np.float32).reshape(*u.grid_shape(), 4)
+    kind = L[3]
+    fill = fill_fraction(u, kind, lane_f32(u, L[4]), lane_f32(u, L[5]))
+    p = lane_f32(u, L[0])
+    act = ~(gv[..., 3] < F32(1e-6)) & is_fluid(kind)
+    pn = {}
+    for d in FACES:
+        ok = in_grid(u, d)
+        nk = shifted(kind, d, CELL_SOLID)
+        mirror = ~ok | (nk == CELL_SOLID)
+        nbp = np.where(is_fluid(nk), shifted(p, d, F32(0.0)), F32(0.0))
+        wgt = face_weight(kind, fill, nk, shifted(fill, d, F32(0.0)))
+        pn[d] = np.where(mirror, p, mix(p, nbp, wgt))                    # pressure_weighted_or_mirror
+    h = F32(0.5) * u.inv_dx
+    grad = [h * (pn[FACES[1]] - pn[FACES[0]]), h * (pn[FACES[3]] - pn[FACES[2]]), h * (pn[FACES[5]] - pn[FACES[4]])]
+    v = [gv[..., q] - u.dt * grad[q] for q in range(3)]
+    imp = np.zeros((3, max(u.num_bed, 1)), np.int64)
+    li = bed.lookup
+    darcy = act & (kind == CELL_BED_COUPLED) & (li >= 0) & (li < u.num_bed)
+    if darcy.any():
+        sel = np.nonzero(darcy)
+        b = li[sel]
+        perm = bed.compacted_permeability(b)
+        rate = u.nu_m2s / perm
+        damp = F32(1.0) / (F32(1.0) + np.maximum(rate * u.dt, F32(0.0)))
+        bmv = bed.matrix_velocity()
+        before = [v[q][sel] for q in range(3)]
+        after = [bmv[q][sel] + (before[q] - bmv[q][sel]) * damp for q in range(3)]
+        water_imp = [gv[..., 3][sel] * (after[q] - before[q]) for q in range(3)]
+        share_in = [(-water_imp[q]) * BED_REACTION_ALPHA for q in range(3)]
+        for q in range(3):
+            v[q][sel] = after[q]
+        # bed_impulse_delta_add_neighborhood (shader.rs:479-515)
+        cz, cy, cx = (np.asarray(a) for a in sel)
+        count = np.zeros(cz.shape, np.float32)
+        nbr = []
+        for di in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    x, y, z = cx + di, cy + dj, cz + dk
+                    on = (x >= 0) & (y >= 0) & (z >= 0) & (x < u.gx) & (y < u.gy) & (z < u.gz)
+                    bi = np.where(on, li[np.clip(z, 0, u.gz - 1), np.clip(y, 0, u.gy - 1), np.clip(x, 0, u.gx - 1)], -1)
+                    ok = bed.valid_solid(bi)
+                    count = np.where(ok, count + F32(1.0), count)
+                    nbr.append((bi, ok))
+        has = ~(count <= F32(0.0))
+        cnt = np.where(has, count, F32(1.0))
+        share = [s / cnt for s in share_in]
+        cap = u.nominal_mass * u.vel_cap * BED_REACTION_IMPULSE_CAP
+        q_i = [to_i32(clamp(s, -cap, cap) * u.fp).astype(np.int64) for s in share]
+        for bi, ok in nbr:
+            m = ok & has
+            for q in range(3):
+                np.add.at(imp[q], bi[m], q_i[q][m])
+    speed = length3(*v)
+    over = speed > u.vel_cap
+    sc = u.vel_cap / np.where(over, speed, F32(1.0))
+    v = [np.where(over, c * sc, c) for c in v]
+    out = gv.copy()
+    for q in range(3):
+        out[..., q] = np.where(act, v[q], gv[..., q])
+    return out.reshape(-1, 4), imp[:, :u.num_bed]
+
+
+# ---------------------------------------------------------------- packing  (shader.rs:1545-1626)
+
+def packing_prepare(u, lanes):
+    """Lane 2 after packing_prepare; (6, cells)."""
+    L = np.array(lanes, np.int32).reshape(6, -1)
+    kind = L[3]
+    cell_volume = u.dx * u.dx * u.dx
+    packed = np.maximum(lane_f32(u, L[4]), lane_f32(u, L[5])) / np.maximum(cell_volume, F32(1e-8))
+    target = np.minimum(u.max_rest_frac, F32(1.0))
+    over = np.maximum(packed - target, F32(0.0))
+    val = np.where(is_fluid(kind) & (kind != CELL_BED_COUPLED), u.bulk_K * over, F32(0.0))
+    L[2] = store_clamped(u, val, F32(0.0), u.p_clamp)
+    return L
+
+
+def packing_apply(u, lanes, grid_vel):
+    """`grid_vel` after packing_apply; (cells, 4)."""
+    L = np.asarray(lanes, np.int32).reshape(6, *u.grid_shape())
+    gv = np.array(grid_vel, np.float32).reshape(*u.grid_shape(), 4)
+    kind = L[3]
+    pk = lane_f32(u, L[2])
+    act = ~(gv[..., 3] <= u.occupancy) & is_fluid(kind)
+    pn = {}
+    for d in FACES:
+        nk = shifted(kind, d, CELL_SOLID)
+        mirror = ~in_grid(u, d) | (nk == CELL_SOLID)
+        val = np.where(is_fluid(nk), shifted(pk, d, F32(0.0)), F32(0.0))
+        pn[d] = np.where(mirror, pk, val)                                  # packing_pressure_or_mirror
+    h = F32(0.5) * u.inv_dx
+    grad = [h * (pn[FACES[1]] - pn[FACES[0]]), h * (pn[FACES[3]] - pn[FACES[2]]), h * (pn[FACES[5]] - pn[FACES[4]])]
+    v = [gv[..., q] - u.dt * grad[q] for q in range(3)]
+    speed = length3(*v)
+    over = speed > u.vel_cap
+    sc = u.vel_cap / np.where(over, speed, F32(1.0))
+    v = [np.where(over, c * sc, c) for c in v]
+    out = gv.copy()
+    for q in range(3):
+        out[..., q] = np.where(act, v[q], gv[..., q])
+    return out.reshape(-1, 4)
+
+
+# ---------------------------------------------------------------- viscosity  (shader.rs:1086-1177)
+
+def scratch_store(u, v):
+    """velocity_scratch_store (shader.rs:274-283): speed cap, then i32(v * fp)."""
+    speed = length3(*v)
+    over = speed > u.vel_cap
+    sc = u.vel_cap / np.where(over, speed, F32(1.0))
+    return [to_i32(np.where(over, c * sc, c) * u.fp) for c in v]
+
+
+def viscosity_prepare(u, lanes, grid_vel, solid_class):
+    """Lanes 1-3 (velocity scratch) after viscosity_prepare; (6, cells)."""
+    L = np.array(lanes, np.int32).reshape(6, *u.grid_shape())
+    gv = np.asarray(grid_vel, np.float32).reshape(*u.grid_shape(), 4)
+    m = gv[..., 3]
+    vh = [gv[..., q] for q in range(3)]
+    plain = (m <= u.occupancy) | (u.viscosity <= F32(0.0)) | (m <= u.nominal_mass * F32(2.0))
+    alpha = clamp(u.viscosity * u.dt / np.maximum(u.dx * u.dx, F32(1e-6)), F32(0.0), F32(0.14))
+    vs = [np.zeros(u.grid_shape(), np.float32) for _ in range(3)]
+    ws = np.zeros(u.grid_shape(), np.float32)
+    cnt = np.zeros(u.grid_shape(), np.int32)
+    denom = np.maximum(np.maximum(m, u.nominal_mass), F32(1e-6))
+    for d in FACES:
+        wall = ~in_grid(u, d) | shifted(solid_class, d, False)
+        nm = shifted(m, d, F32(0.0))
+        fl = ~wall & ~(nm <= u.occupancy)
+        nw = clamp(nm / denom, F32(0.0), F32(1.0))
+        for q in range(3):
+            vs[q] = np.where(fl, vs[q] + shifted(gv[..., q], d, F32(0.0)) * nw, vs[q])
+        ws = np.where(wall, ws + F32(1.0), np.where(fl, ws + nw, ws))
+        cnt = cnt + fl
+    keep = plain | (cnt < 3) | (ws <= F32(1e-6))
+    wsd = np.where(keep, F32(1.0), ws)
+    avg = [s / wsd for s in vs]
+    blend = clamp(alpha * ws, F32(0.0), F32(0.65))
+    out_v = [np.where(keep, vh[q], mix(vh[q], avg[q], blend)) for q in range(3)]
+    st = scratch_store(u, out_v)
+    for q in range(3):
+        L[1 + q] = st[q]
+    return L.reshape(6, -1)
+
+
+def viscosity_apply(u, lanes, grid_vel):
+    """`grid_vel` after viscosity_apply; (cells, 4)."""
+    L = np.asarray(lanes, np.int32).reshape(6, -1)
+    gv = np.array(grid_vel, np.float32).reshape(-1, 4)
+    m = gv[:, 3]
+    dead = m <= u.occupancy
+    out = np.zeros_like(gv)
+    for q in range(3):
+        out[:, q] = np.where(dead, F32(0.0), lane_f32(u, L[1 + q]))
+    out[:, 3] = np.where(dead, F32(0.0), m)
+    return out
