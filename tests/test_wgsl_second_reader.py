@@ -228,3 +228,34 @@ def test_viscosity(stages):
     gv = W.viscosity_apply(u, mid["lanes"], mid["grid_vel"])
     msg = _report("grid_vel", gv, after["grid_vel"])
     assert msg is None, msg
+
+
+def test_g2p(stages):
+    """G2P with APIC, weak-support and airborne ballistic blending, porous drag with its
+    bed impulses, the J update and the particle-level contacts.  Every value is compared
+    bit for bit except J, whose exponential (shader.rs:1853) WGSL leaves to the backend
+    (within 4 ulp here, the restatement using float64 exp rounded to float32)."""
+    raw = stages.settings.raw
+    g = raw.geom
+    assert (g.cone_bot_y, g.cone_top_y, g.cup_top_y, g.cup_radius, g.cup_floor_y, g.wall_thickness) == \
+        (-3.0, 3.0, -3.5, 3.0, -8.0, np.float32(0.4))
+    assert g.cone_radius_span == np.float32(4.2634315)
+    u = stages.uniforms(P_G2P)
+    before, after = stages(P_G2P), stages(P_G2P + 1)
+    sdf = W.Sdf(u, stages.static["sdf"])
+    stats = {}
+    P, A, imp = W.g2p(u, sdf, _bed(stages, P_G2P, u), np.float32(raw.brew.dripper_outlet_radius),
+                      before["particles"], before["affine"], before["grid_vel"], stats=stats)
+    assert min(stats["weak"], stats["airborne"], stats["porous"]) > 50, stats
+    want_p, want_a = after["particles"], after["affine"]
+    cols = [c for c in range(8) if c != 3]
+    msg = _report("particles (J excluded)", P[:, cols], want_p[:, cols])
+    assert msg is None, msg
+    j_ulp = np.abs(P[:, 3].view(np.int32).astype(np.int64) - want_p[:, 3].view(np.int32).astype(np.int64))
+    assert j_ulp.max() <= 4, f"J differs by {j_ulp.max()} ulp"
+    msg = _report("affine", A, want_a)
+    assert msg is None, msg
+    added = after["bed_delta"][1:4, :u.num_bed].astype(np.int64) - before["bed_delta"][1:4, :u.num_bed]
+    msg = _report("bed impulse lanes", W.wrap_i32(imp), W.wrap_i32(added))
+    assert msg is None, msg
+    assert np.count_nonzero(imp) > 0

@@ -691,3 +691,230 @@ def viscosity_apply(u, lanes, grid_vel):
         out[:, q] = np.where(dead, F32(0.0), lane_f32(u, L[1 + q]))
     out[:, 3] = np.where(dead, F32(0.0), m)
     return out
+
+
+# ---------------------------------------------------------------- g2p  (shader.rs:1683-1881)
+
+# V60 geometry the shader writes as literals (shader.rs:101, 106-107, 749-750, 800-801)
+CONE_TOP_Y, CONE_BOT_Y, CONE_RADIUS_SPAN = F32(3.0), F32(-3.0), F32(4.2634315)
+CUP_TOP_Y, CUP_RADIUS, CUP_FLOOR_Y, WALL_THICKNESS = F32(-3.5), F32(3.0), F32(-8.0), F32(0.4)
+
+
+def radial_barrier(u, pos, vel, max_r, on):
+    """resolve_radial_barrier (shader.rs:717-742) about the y axis, where `on`."""
+    x, z = pos[0], pos[2]
+    r = np.sqrt(x * x + z * z)
+    hit = on & (r > max_r) & (r > F32(1e-6))
+    rs = np.where(hit, r, F32(1.0))
+    ox, oz = x / rs, z / rs
+    px = np.where(hit, F32(0.0) + ox * max_r, pos[0])
+    pz = np.where(hit, F32(0.0) + oz * max_r, pos[2])
+    vn = vel[0] * ox + vel[2] * oz
+    slide = hit & (vn > F32(0.0))
+    k = F32(1.0) - u.friction * F32(0.35)
+    vx = np.where(slide, (vel[0] - ox * vn) * k, vel[0])
+    vz = np.where(slide, (vel[2] - oz * vn) * k, vel[2])
+    return [px, pos[1], pz], [vx, vel[1], vz]
+
+
+def scene_obstacles_water(u, outlet_r, pos, vel):
+    """resolve_scene_obstacles (shader.rs:744-823) for water (is_bed = false): the cone's
+    radial barrier, then the carafe's wall and floor."""
+    y = pos[1]
+    in_cone = (y <= CONE_TOP_Y) & (y >= CONE_BOT_Y)
+    t = clamp((y - CONE_BOT_Y) / (CONE_TOP_Y - CONE_BOT_Y), F32(0.0), F32(1.0))
+    cone_r = mix(outlet_r, outlet_r + CONE_RADIUS_SPAN, t) - u.contact_offset
+    pos, vel = radial_barrier(u, pos, vel, cone_r, in_cone)
+    half = WALL_THICKNESS * F32(0.5)
+    in_cup = pos[1] <= CUP_TOP_Y
+    pos, vel = radial_barrier(u, pos, vel, CUP_RADIUS - half - u.contact_offset, in_cup)
+    floor_y = CUP_FLOOR_Y + half + u.contact_offset
+    below = in_cup & (pos[1] < floor_y)
+    stop = below & (vel[1] < F32(0.0))
+    k = F32(1.0) - u.friction * F32(0.55)
+    pos = [pos[0], np.where(below, floor_y, pos[1]), pos[2]]
+    vel = [np.where(stop, vel[0] * k, vel[0]), np.where(stop, F32(0.0), vel[1]), np.where(stop, vel[2] * k, vel[2])]
+    return pos, vel
+
+
+def sdf_contact_water(u, sdf, outlet_r, pos, vel):
+    """resolve_sdf_contact (shader.rs:879-903) for water."""
+    sd = sdf.sample(*pos)
+    n = sdf.gradient(*pos)
+    near = (sd < u.contact_offset) & (length3(*n) > F32(1e-6))
+    push = u.contact_offset - sd
+    pos = [np.where(near, pos[q] + n[q] * push, pos[q]) for q in range(3)]
+    vn = vel[0] * n[0] + vel[1] * n[1] + vel[2] * n[2]
+    hit = near & (vn < F32(0.0))
+    k = F32(1.0) + u.restitution
+    v2 = [vel[q] - n[q] * vn * k for q in range(3)]
+    d2 = v2[0] * n[0] + v2[1] * n[1] + v2[2] * n[2]
+    vt = [v2[q] - n[q] * d2 for q in range(3)]
+    vtl = length3(*vt)
+    fr = hit & (vtl > F32(1e-6))
+    imp = np.minimum(u.friction * np.abs(vn), vtl)
+    safe = np.where(fr, vtl, F32(1.0))
+    v3 = [np.where(fr, v2[q] - vt[q] * (imp / safe), v2[q]) for q in range(3)]
+    vel = [np.where(hit, v3[q], vel[q]) for q in range(3)]
+    return scene_obstacles_water(u, outlet_r, pos, vel)
+
+
+def g2p(u, sdf, bed, outlet_r, particles, affine, grid_vel, exp=np.exp, stats=None):
+    """Particles, affine columns and bed impulse sums after G2P.  Returns (particles
+    (n, 8), affine (n, 12), impulse sums (3, num_bed) int64).  `exp` evaluates the J
+    update's exponential (shader.rs:1853), whose precision WGSL leaves to the backend.
+    `stats`, if a dict, receives how many samples took each branch."""
+    n = u.num_water + u.num_bed
+    P = np.array(particles, np.float32).reshape(-1, 8)[:n]
+    A = np.array(affine, np.float32).reshape(-1, 12)[:n]
+    gv = np.asarray(grid_vel, np.float32).reshape(-1, 4)
+    imp = np.zeros((3, max(u.num_bed, 1)), np.int64)
+    water = A[:, 3] < F32(0.5)
+    idle = water & (P[:, 7] <= u.inactive)
+    P[idle, 7] = F32(0.0)                                                    # shader.rs:1695-1698
+    act = np.flatnonzero(water & ~idle)
+    if act.size == 0:
+        return P, A, imp[:, :u.num_bed]
+    p, a = P[act], A[act]
+    xp, J_old, vp, mass = [p[:, q] for q in range(3)], p[:, 3], [p[:, 4 + q] for q in range(3)], p[:, 7]
+    gp = [(xp[q] - u.origin[q]) * u.inv_dx for q in range(3)]
+    base = [to_i32(np.floor(c - F32(0.5))) for c in gp]
+    fx = [gp[q] - base[q].astype(np.float32) for q in range(3)]
+    w = [[F32(0.5) * (F32(1.5) - f) * (F32(1.5) - f), F32(0.75) - (f - F32(1.0)) * (f - F32(1.0)),
+          F32(0.5) * (f - F32(0.5)) * (f - F32(0.5))] for f in fx]
+    m = act.size
+    z = lambda: np.zeros(m, np.float32)  # noqa: E731
+    new_v, C = [z(), z(), z()], [[z(), z(), z()] for _ in range(3)]
+    supported, local_mass, bow, bps = z(), z(), z(), z()
+    bvs = [z(), z(), z()]
+    B = F32(4.0) * u.inv_dx * u.inv_dx
+    lookup = bed.lookup.reshape(-1)
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                cx, cy, cz = base[0] + i, base[1] + j, base[2] + k
+                ok = (cx >= 0) & (cy >= 0) & (cz >= 0) & (cx < u.gx) & (cy < u.gy) & (cz < u.gz)
+                ci = np.where(ok, (cz.astype(np.int64) * u.gy + cy) * u.gx + cx, 0)
+                wt = w[0][i] * w[1][j] * w[2][k]
+                g = gv[ci]
+                dpos = [(F32(o) - fx[q]) * u.dx for q, o in enumerate((i, j, k))]
+                sup = ok & (g[:, 3] > F32(1e-6))
+                for q in range(3):
+                    new_v[q] = np.where(sup, new_v[q] + wt * g[:, q], new_v[q])
+                wB = wt * B
+                for col in range(3):
+                    for q in range(3):
+                        C[col][q] = np.where(sup, C[col][q] + wB * g[:, q] * dpos[col], C[col][q])
+                supported = np.where(sup, supported + wt, supported)
+                local_mass = np.where(sup, local_mass + wt * g[:, 3], local_mass)
+                bi = np.where(ok, lookup[ci], -1)
+                vb = ok & (u.num_bed > 0) & bed.valid_solid(bi)
+                sb = np.where(vb, bi, 0)
+                bow = np.where(vb, bow + wt, bow)
+                for q in range(3):
+                    bvs[q] = np.where(vb, bvs[q] + wt * bed.vel[sb, q], bvs[q]) if u.num_bed else bvs[q]
+                if u.num_bed:
+                    bps = np.where(vb, bps + wt * bed.compacted_permeability(sb), bps)
+    support_ratio = clamp(supported, F32(0.0), F32(1.0))
+    jus = support_ratio
+    has = supported > F32(1e-6)
+    inv = F32(1.0) / np.where(has, supported, F32(1.0))
+    new_v = [np.where(has, c * inv, c) for c in new_v]
+    C = [[np.where(has, c * inv, c) for c in col] for col in C]
+    co = u.contact_offset
+    cupr = F32(3.0) + co
+    in_cup = (xp[1] < F32(-3.5)) & ((xp[0] * xp[0] + xp[2] * xp[2]) < cupr * cupr)
+    dense = clamp(local_mass / np.maximum(u.nominal_mass * F32(4.0), F32(1e-6)), F32(0.0), F32(1.0))
+    porous = clamp(bow, F32(0.0), F32(1.0))
+    hb = bow > F32(1e-6)
+    invb = F32(1.0) / np.where(hb, bow, F32(1.0))
+    pbv = [np.where(hb, c * invb, F32(0.0)) for c in bvs]
+    pbp = np.where(hb, np.maximum(bps * invb, u.min_perm), u.min_perm)
+    ballistic = [vp[0], vp[1] + u.gravity * u.dt, vp[2]]
+    # weak stencil support (shader.rs:1778-1792)
+    weak = support_ratio < F32(0.999)
+    pg = mix(np.where(in_cup, F32(1.15), F32(1.35)), F32(0.18), porous)
+    pc = mix(np.where(in_cup, F32(0.95), F32(0.995)), F32(0.16), porous)
+    dpd = mix(F32(1.0), F32(0.12), dense)
+    keep = clamp((F32(1.0) - support_ratio) * pg * dpd, F32(0.0), pc)
+    new_v = [np.where(weak, mix(new_v[q], ballistic[q], keep), new_v[q]) for q in range(3)]
+    ad = F32(1.0) - keep * F32(0.75)
+    C = [[np.where(weak, c * ad, c) for c in col] for col in C]
+    # airborne (shader.rs:1798-1812)
+    airborne = (porous <= F32(0.05)) & (sdf.sample(*xp) > co * F32(2.0))
+    dr = clamp(local_mass / np.maximum(u.nominal_mass * F32(4.0), F32(1e-6)), F32(0.0), F32(1.0))
+    jus = np.where(airborne, np.minimum(jus, dr), jus)
+    pg = np.where(in_cup, F32(0.72), F32(0.98))
+    pc = np.where(in_cup, F32(0.88), F32(0.98))
+    keep = clamp((F32(1.0) - dr) * pg, F32(0.0), pc)
+    new_v = [np.where(airborne, mix(new_v[q], ballistic[q], keep), new_v[q]) for q in range(3)]
+    ad = F32(1.0) - keep * F32(0.65)
+    C = [[np.where(airborne, c * ad, c) for c in col] for col in C]
+    # porous drag (shader.rs:1814-1834)
+    por = porous > F32(1e-4)
+    rel = [new_v[q] - pbv[q] for q in range(3)]
+    rate = u.nu_m2s / pbp
+    dd = F32(1.0) / (F32(1.0) + np.maximum(rate * u.dt * porous, F32(0.0)))
+    rs = length3(*rel)
+    idmp = F32(1.0) / (F32(1.0) + np.maximum(rs * u.dt * u.inv_dx * porous * F32(0.35), F32(0.0)))
+    dragged = [pbv[q] + rel[q] * dd * idmp for q in range(3)]
+    wimp = [mass * (dragged[q] - new_v[q]) for q in range(3)]
+    new_v = [np.where(por, dragged[q], new_v[q]) for q in range(3)]
+    ad = mix(F32(1.0), dd * idmp, porous)
+    C = [[np.where(por, c * ad, c) for c in col] for col in C]
+    jus = np.where(por, np.maximum(jus, porous), jus)
+    if stats is not None:
+        stats.update(active=int(act.size), weak=int(weak.sum()), airborne=int(airborne.sum()), porous=int(por.sum()))
+    if por.any() and u.num_bed:
+        sel = np.flatnonzero(por)
+        cell = [to_i32(np.floor((xp[q][sel] - u.origin[q]) * u.inv_dx)) for q in range(3)]   # world_to_cell
+        share_in = [(-wimp[q][sel]) * BED_REACTION_ALPHA for q in range(3)]
+        _impulse_neighbourhood(u, bed, cell, share_in, imp)
+    # J update (shader.rs:1836-1840)
+    trace = C[0][0] + C[1][1] + C[2][2]
+    jc = clamp(np.where(J_old > F32(0.0), J_old, F32(1.0)), F32(0.40), F32(2.00))
+    ex = exp(clamp(u.dt * trace, F32(-0.35), F32(0.35)).astype(np.float64)).astype(np.float32)
+    j_apic = clamp(jc * ex, F32(0.40), F32(2.00))
+    jb = smoothstep(F32(0.35), F32(0.85), clamp(jus, F32(0.0), F32(1.0)))
+    j_new = clamp(mix(jc, j_apic, jb), F32(0.40), F32(2.00))
+    # advection and particle-level contact (shader.rs:1842-1869)
+    new_pos = [xp[q] + new_v[q] * u.dt for q in range(3)]
+    mid = [mix(xp[q], new_pos[q], F32(0.5)) for q in range(3)]
+    _, new_v = sdf_contact_water(u, sdf, outlet_r, mid, new_v)
+    new_pos, new_v = sdf_contact_water(u, sdf, outlet_r, new_pos, new_v)
+    margin = u.dx * F32(0.5)
+    new_pos = [clamp(new_pos[q], u.origin[q] + margin, u.bounds_max[q] - margin) for q in range(3)]
+    for q in range(3):
+        P[act, q] = new_pos[q]
+        P[act, 4 + q] = new_v[q]
+        for col in range(3):
+            A[act, 4 * col + q] = C[col][q]
+    P[act, 3] = j_new
+    A[act, 7] = F32(0.0)
+    A[act, 11] = F32(0.0)
+    return P, A, imp[:, :u.num_bed]
+
+
+def _impulse_neighbourhood(u, bed, cell, share_in, imp):
+    """bed_impulse_delta_add_neighborhood (shader.rs:479-515) for a batch of home cells."""
+    cx, cy, cz = cell
+    count = np.zeros(cx.shape, np.float32)
+    lk = bed.lookup
+    nbr = []
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                x, y, z = cx + di, cy + dj, cz + dk
+                on = (x >= 0) & (y >= 0) & (z >= 0) & (x < u.gx) & (y < u.gy) & (z < u.gz)
+                bi = np.where(on, lk[np.clip(z, 0, u.gz - 1), np.clip(y, 0, u.gy - 1), np.clip(x, 0, u.gx - 1)], -1)
+                ok = bed.valid_solid(bi)
+                count = np.where(ok, count + F32(1.0), count)
+                nbr.append((bi, ok))
+    has = ~(count <= F32(0.0))
+    cnt = np.where(has, count, F32(1.0))
+    cap = u.nominal_mass * u.vel_cap * BED_REACTION_IMPULSE_CAP
+    q_i = [to_i32(clamp(s / cnt, -cap, cap) * u.fp).astype(np.int64) for s in share_in]
+    for bi, ok in nbr:
+        mk = ok & has
+        for q in range(3):
+            np.add.at(imp[q], bi[mk], q_i[q][mk])
