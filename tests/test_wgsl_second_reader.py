@@ -259,3 +259,50 @@ def test_g2p(stages):
     msg = _report("bed impulse lanes", W.wrap_i32(imp), W.wrap_i32(added))
     assert msg is None, msg
     assert np.count_nonzero(imp) > 0
+
+
+P_LOOKUP_CLEAR, P_COUPLING, P_EXTRACTION, P_RENDER = 1, 17, 18, 20
+
+
+def test_bed_lookup(stages):
+    u = stages.uniforms(P_LOOKUP_CLEAR)
+    before, after = stages(P_LOOKUP_CLEAR), stages(P_LOOKUP_CLEAR + 2)
+    look = W.bed_lookup(u, before["particles"], before["affine"])
+    assert np.count_nonzero(look >= 0) > 1000
+    msg = _report("lookup", look, after["lookup"])
+    assert msg is None, msg
+
+
+def test_bed_coupling(stages):
+    u = stages.uniforms(P_COUPLING)
+    before, after = stages(P_COUPLING), stages(P_COUPLING + 1)
+    P, add = W.bed_coupling(u, _bed(stages, P_COUPLING, u), before["particles"], before["affine"])
+    assert np.count_nonzero(add) > 20
+    msg = _report("particles", P, after["particles"])
+    assert msg is None, msg
+    got = after["bed_delta"][0, :u.num_bed].astype(np.int64) - before["bed_delta"][0, :u.num_bed]
+    msg = _report("bed water lane", W.wrap_i32(add), W.wrap_i32(got))
+    assert msg is None, msg
+
+
+def test_extraction_advect(stages):
+    u = stages.uniforms(P_EXTRACTION)
+    before, after = stages(P_EXTRACTION), stages(P_EXTRACTION + 1)
+    be = W.extraction_advect(u, before["bed_extract"], before["bed_delta"][0])
+    assert np.count_nonzero(before["bed_delta"][0, :u.num_bed]) > 20
+    msg = _report("bed_extract", be, after["bed_extract"])
+    assert msg is None, msg
+    assert not after["bed_delta"][0, :u.num_bed].any()
+
+
+def test_prepare_render(stages):
+    u = stages.uniforms(P_RENDER)
+    before = stages(P_RENDER)
+    sim = MpmSim3D(stages.settings, stages.oracle)
+    copy_state(stages.src, sim)
+    sim.set_kettle_angle(36.0)
+    sim.step_substep_partial(SUB_DT, P_RENDER + 1)
+    want = sim.read_render(0, sim.particle_count())
+    got = W.prepare_render(u, before["particles"], before["affine"], before.get("bed_extract"))
+    msg = _report("render", got, want)
+    assert msg is None, msg

@@ -104,6 +104,13 @@ class Uniforms:
         self.surface_void_scale = F32(brew.bed_surface_void_scale)
         self.pore_capacity_scale = F32(brew.bed_pore_capacity_scale)
         self.pore_overfill_alpha = F32(brew.bed_pore_overfill_alpha)
+        self.absorption_rate = F32(brew.bed_absorption_rate)
+        self.filter_absorption = F32(brew.filter_absorption_rate_s)
+        self.water_r_dx, self.bed_r_dx = F32(brew.water_sample_radius_dx), F32(brew.bed_sample_radius_dx)
+        self.extraction_rate = F32(0.01)                            # mod.rs:643
+        # bed_capacity_per_particle (mod.rs:578-582)
+        self.max_saturation = (F32(brew.target_bed_retention_ml) * F32(brew.water_mass_units_per_ml) / F32(num_bed)
+                               if num_bed > 0 else F32(0.7))
 
     # shader.rs:116, 171-172
     @property
@@ -918,3 +925,142 @@ def _impulse_neighbourhood(u, bed, cell, share_in, imp):
         mk = ok & has
         for q in range(3):
             np.add.at(imp[q], bi[mk], q_i[q][mk])
+
+
+# ---------------------------------------------------------------- bed lookup  (shader.rs:2289-2335)
+
+def world_to_cell(u, pos):
+    """shader.rs:668-671 for rows of positions: (n, 3) int32."""
+    return np.stack([to_i32(np.floor((pos[:, q] - u.origin[q]) * u.inv_dx)) for q in range(3)], axis=1)
+
+
+def bed_lookup(u, particles, affine):
+    """bed_lookup_clear then bed_lookup_scatter: every solid-phase bed sample stamps its
+    id over the 3x3x3 cells around its cell, the highest id winning (atomicMax)."""
+    look = np.full(u.cells, -1, np.int64)
+    nb = u.num_bed
+    if nb == 0:
+        return look.astype(np.int32)
+    p = np.asarray(particles, np.float32).reshape(-1, 8)[:nb]
+    ph = np.asarray(affine, np.float32).reshape(-1, 12)[:nb, 3]
+    ids = np.flatnonzero(~(ph < F32(0.5)))
+    cell = world_to_cell(u, p[ids, 0:3])
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                c = cell + np.array([di, dj, dk])
+                ok = (c >= 0).all(axis=1) & (c[:, 0] < u.gx) & (c[:, 1] < u.gy) & (c[:, 2] < u.gz)
+                ci = (c[ok, 2].astype(np.int64) * u.gy + c[ok, 1]) * u.gx + c[ok, 0]
+                np.maximum.at(look, ci, ids[ok])
+    return look.astype(np.int32)
+
+
+# ---------------------------------------------------------------- bed_coupling  (shader.rs:1885-1957)
+
+def bed_coupling(u, bed, particles, affine):
+    """Particles after bed_coupling and the water-lane additions it makes: (particles
+    (n, 8), (num_bed,) int64 sums).  The paper-absorption branch (shader.rs:1906-1911)
+    runs only with a positive filter absorption rate; the default brew has none."""
+    assert not u.filter_absorption > 0, "the restatement leaves out paper absorption"
+    n = u.num_water + u.num_bed
+    P = np.array(particles, np.float32).reshape(-1, 8)[:n]
+    ph = np.asarray(affine, np.float32).reshape(-1, 12)[:n, 3]
+    add = np.zeros(max(u.num_bed, 1), np.int64)
+    cand = np.flatnonzero(ph < F32(0.5))
+    cell = world_to_cell(u, P[cand, 0:3])
+    on = (cell >= 0).all(axis=1) & (cell[:, 0] < u.gx) & (cell[:, 1] < u.gy) & (cell[:, 2] < u.gz)
+    cand, cell = cand[on], cell[on]
+    ci = (cell[:, 2].astype(np.int64) * u.gy + cell[:, 1]) * u.gx + cell[:, 0]
+    bi = bed.lookup.reshape(-1)[ci]
+    ok = (bi >= 0) & (bi < u.num_bed)
+    cand, cell, bi = cand[ok], cell[ok], bi[ok]
+    be = bed.bx[bi]
+    mass = P[cand, 7]
+    sat = be[:, 7]
+    capacity = np.maximum(u.max_saturation - be[:, 0], F32(0.0))
+    go = ~(capacity <= F32(1e-6))
+    abs_rate = u.absorption_rate * (F32(1.0) - sat) * u.dt
+    v = P[cand, 4:7]
+    speed = length3(v[:, 0], v[:, 1], v[:, 2])
+    absorbed = np.minimum(np.minimum(mass * clamp(abs_rate, F32(0.0), F32(0.25)), mass * F32(0.5)), capacity)
+    rem = mass - absorbed
+    retire = (rem > F32(0.0)) & (rem <= u.nominal_mass * F32(0.22))
+    almost = np.minimum(mass, capacity)
+    wet = ~retire & (sat > F32(0.55)) & (speed < F32(1.35)) & ((mass - almost) <= u.nominal_mass * F32(0.35))
+    absorbed = np.where(retire | wet, almost, absorbed)
+    remnant = ((mass - absorbed) <= u.inactive) & (absorbed < mass)
+    absorbed = np.where(remnant, np.maximum(mass - u.inactive * F32(1.05), F32(0.0)), absorbed)
+    go &= ~(absorbed <= F32(1e-6))
+    cand, cell, bi, mass, absorbed = cand[go], cell[go], bi[go], mass[go], absorbed[go]
+    remaining = mass - absorbed
+    gone = remaining <= u.inactive
+    P[cand[gone], 4:8] = F32(0.0)
+    P[cand[~gone], 7] = remaining[~gone]
+    # deposit_absorbed_bed_water (shader.rs:524-576)
+    nshare = absorbed * F32(0.35)
+    home = absorbed - nshare
+
+    def water_add(ids, amount):
+        pos = ~(amount <= F32(0.0))
+        np.add.at(add, ids[pos], to_i32(amount[pos] * u.fp).astype(np.int64))
+
+    water_add(bi, home)
+    nbr = np.full((bi.size, 6), -1, np.int64)
+    lk = bed.lookup
+    for f, d in enumerate(FACES):
+        c = cell + np.array(d)
+        on = (c >= 0).all(axis=1) & (c[:, 0] < u.gx) & (c[:, 1] < u.gy) & (c[:, 2] < u.gz)
+        nid = np.where(on, lk[np.clip(c[:, 2], 0, u.gz - 1), np.clip(c[:, 1], 0, u.gy - 1), np.clip(c[:, 0], 0, u.gx - 1)], -1)
+        keep = (nid >= 0) & (nid != bi) & (nid < u.num_bed)
+        for g in range(f):
+            keep &= nbr[:, g] != nid
+        nbr[:, f] = np.where(keep, nid, -1)
+    count = (nbr >= 0).sum(axis=1)
+    lone = count == 0
+    water_add(bi[lone], nshare[lone])
+    each = nshare / np.where(lone, 1, count).astype(np.float32)
+    for f in range(6):
+        has = ~lone & (nbr[:, f] >= 0)
+        water_add(nbr[has, f], each[has])
+    return P, add[:u.num_bed]
+
+
+# ---------------------------------------------------------------- extraction_advect  (shader.rs:1961-1987)
+
+def extraction_advect(u, bed_extract, water_lane):
+    """bed_extract rows after extraction_advect, given the water lane it exchanges to 0."""
+    be = np.array(bed_extract, np.float32).reshape(-1, 8)[:u.num_bed]
+    absorbed = np.asarray(water_lane, np.int32)[:u.num_bed].astype(np.float32) * u.inv_fp
+    got = absorbed > F32(0.0)
+    be[:, 0] = np.where(got, be[:, 0] + absorbed, be[:, 0])
+    be[:, 7] = np.where(got, clamp(be[:, 0] / np.maximum(u.max_saturation, F32(1e-6)), F32(0.0), F32(1.0)), be[:, 7])
+    sat = be[:, 7]
+    ex = sat > F32(0.01)
+    flux = u.extraction_rate * be[:, 4] * sat * u.dt
+    be[:, 4] = np.where(ex, np.maximum(be[:, 4] - flux, F32(0.0)), be[:, 4])
+    be[:, 5] = np.where(ex, be[:, 5] + flux, be[:, 5])
+    return be
+
+
+# ---------------------------------------------------------------- prepare_render  (shader.rs:2242-2276)
+
+def prepare_render(u, particles, affine, bed_extract):
+    """Render rows (n, 8): position and colour parameter, then radius."""
+    n = u.num_water + u.num_bed
+    p = np.asarray(particles, np.float32).reshape(-1, 8)[:n]
+    ph = np.asarray(affine, np.float32).reshape(-1, 12)[:n, 3]
+    out = np.zeros((n, 8), np.float32)
+    dead = p[:, 7] <= u.inactive
+    water = ph < F32(0.5)
+    speed = length3(p[:, 4], p[:, 5], p[:, 6])
+    sat = np.zeros(n, np.float32)
+    isbed = np.arange(n) < u.num_bed
+    if u.num_bed:
+        sat[:u.num_bed] = np.asarray(bed_extract, np.float32).reshape(-1, 8)[:u.num_bed, 7]
+    colour = np.where(water, clamp(speed / F32(10.0), F32(0.0), F32(2.0)), F32(-1.0) - np.where(isbed, sat, F32(0.0)))
+    radius = np.where(~water & isbed, u.dx * u.bed_r_dx, u.dx * u.water_r_dx)
+    out[:, 0:3] = p[:, 0:3]
+    out[:, 3] = colour
+    out[:, 4] = radius
+    out[dead] = np.array([0.0, -1e6, 0.0, -999.0, 0, 0, 0, 0], np.float32)
+    return out
