@@ -50,6 +50,14 @@ def _scatter(src, seed=5):
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     p[k, 4:7] = (d * rng.uniform(0.0, 3.0, size=(k.size, 1))).astype(np.float32)
     src.write_particles(nb, p)
+    # bed grains: every 7th suspended (phase 2), every 3rd nearly saturated, so that the
+    # suspended-grain, redeposit and detach branches of bed_dynamics are reached
+    a = src.read_affine(0, nb)
+    a[::7, 3] = 2.0
+    src.write_affine(0, a)
+    be = src.read_bed_extract(0, nb)
+    be[::3, 7] = 0.9
+    src.write_bed_extract(0, be)
     return src
 
 
@@ -306,3 +314,34 @@ def test_prepare_render(stages):
     got = W.prepare_render(u, before["particles"], before["affine"], before.get("bed_extract"))
     msg = _report("render", got, want)
     assert msg is None, msg
+
+
+P_BED_DYNAMICS = 19
+
+
+def test_bed_dynamics(stages):
+    """bed_dynamics with the other samples' positions read from before the dispatch (the
+    WGSL reads them while they are written; the oracle and the engine read a snapshot)."""
+    raw = stages.settings.raw
+    g = raw.geom
+    assert (g.filter_center_y, g.filter_top_rel, g.filter_bot_rel) == (np.float32(-0.35), np.float32(2.75), np.float32(3.02))
+    assert (g.filter_top_radius, g.filter_thickness) == (np.float32(4.10), np.float32(0.08))
+    assert (g.bed_surface_ref_y, g.bed_surface_span) == (3.0, 3.5)
+    u = stages.uniforms(P_BED_DYNAMICS)
+    before, after = stages(P_BED_DYNAMICS), stages(P_BED_DYNAMICS + 1)
+    sdf = W.Sdf(u, stages.static["sdf"])
+    nb = u.num_bed
+    P, A, BE = W.bed_dynamics(u, sdf, np.float32(raw.brew.dripper_outlet_radius), before["lanes"],
+                              before["grid_vel"], before["lookup"], before["particles"], before["affine"],
+                              before["bed_extract"], before["bed_delta"][1:4])
+    moved = np.count_nonzero(np.any(before["particles"][:nb, 0:3] != after["particles"][:nb, 0:3], axis=1))
+    assert moved > 1000
+    if stages.name == "scattered":
+        suspended = before["affine"][:nb, 3] >= 1.5
+        assert suspended.sum() > 1000
+        assert np.count_nonzero(before["affine"][:nb, 3] != after["affine"][:nb, 3]) > 1000
+    for name, got, want in (("bed particles", P, after["particles"][:nb]), ("bed affine", A, after["affine"][:nb]),
+                            ("bed_extract", BE, after["bed_extract"])):
+        msg = _report(name, got, want)
+        assert msg is None, msg
+    assert not after["bed_delta"][1:4, :nb].any()

@@ -108,6 +108,8 @@ class Uniforms:
         self.filter_absorption = F32(brew.filter_absorption_rate_s)
         self.water_r_dx, self.bed_r_dx = F32(brew.water_sample_radius_dx), F32(brew.bed_sample_radius_dx)
         self.extraction_rate = F32(0.01)                            # mod.rs:643
+        self.compaction_rate = F32(brew.bed_compaction_rate)
+        self.bed_impact = F32(brew.bed_impact_rate)
         # bed_capacity_per_particle (mod.rs:578-582)
         self.max_saturation = (F32(brew.target_bed_retention_ml) * F32(brew.water_mass_units_per_ml) / F32(num_bed)
                                if num_bed > 0 else F32(0.7))
@@ -724,28 +726,61 @@ def radial_barrier(u, pos, vel, max_r, on):
     return [px, pos[1], pz], [vx, vel[1], vz]
 
 
-def scene_obstacles_water(u, outlet_r, pos, vel):
-    """resolve_scene_obstacles (shader.rs:744-823) for water (is_bed = false): the cone's
-    radial barrier, then the carafe's wall and floor."""
+# paper filter literals (shader.rs:137-141, 765-769)
+FILTER_CENTER_Y, FILTER_TOP_REL, FILTER_BOT_REL = F32(-0.35), F32(2.75), F32(3.02)
+FILTER_TOP_RADIUS, FILTER_THICKNESS = F32(4.10), F32(0.08)
+
+
+def coffee_filter_floor_y(u):
+    """shader.rs:136-146"""
+    top = FILTER_CENTER_Y + FILTER_TOP_REL
+    bot = FILTER_CENTER_Y - FILTER_BOT_REL
+    bco = np.maximum(u.contact_offset, u.dx * u.bed_r_dx)
+    height = np.maximum(top - bot, F32(1e-6))
+    slope = FILTER_TOP_RADIUS / height
+    return bot + (bco + FILTER_THICKNESS) / np.maximum(slope, F32(1e-6))
+
+
+def scene_obstacles(u, outlet_r, pos, vel, is_bed):
+    """resolve_scene_obstacles (shader.rs:744-823): the cone's radial barrier; for bed
+    samples the paper filter's barrier and the apex floor; then the carafe's wall and
+    floor."""
     y = pos[1]
     in_cone = (y <= CONE_TOP_Y) & (y >= CONE_BOT_Y)
     t = clamp((y - CONE_BOT_Y) / (CONE_TOP_Y - CONE_BOT_Y), F32(0.0), F32(1.0))
     cone_r = mix(outlet_r, outlet_r + CONE_RADIUS_SPAN, t) - u.contact_offset
     pos, vel = radial_barrier(u, pos, vel, cone_r, in_cone)
+    k = F32(1.0) - u.friction * F32(0.55)
+    if is_bed:
+        top = FILTER_CENTER_Y + FILTER_TOP_REL
+        bot = FILTER_CENTER_Y - FILTER_BOT_REL
+        bco = np.maximum(u.contact_offset, u.dx * u.bed_r_dx)
+        y = pos[1]
+        in_f = (y <= top) & (y >= bot)
+        ft = clamp((y - bot) / (top - bot), F32(0.0), F32(1.0))
+        outer = mix(F32(0.0), FILTER_TOP_RADIUS, ft)
+        fr = np.maximum(outer - FILTER_THICKNESS, F32(0.0)) - bco
+        pos, vel = radial_barrier(u, pos, vel, np.maximum(fr, F32(0.0)), in_f)
+        fl = coffee_filter_floor_y(u)
+        at = pos[1] <= fl
+        stop = at & (vel[1] < F32(0.0))
+        pos = [np.where(at, F32(0.0), pos[0]), np.where(at, fl, pos[1]), np.where(at, F32(0.0), pos[2])]
+        vx = np.where(stop, vel[0] * k, vel[0])
+        vz = np.where(stop, vel[2] * k, vel[2])
+        vel = [np.where(at, vx * k, vel[0]), np.where(stop, F32(0.0), vel[1]), np.where(at, vz * k, vel[2])]
     half = WALL_THICKNESS * F32(0.5)
     in_cup = pos[1] <= CUP_TOP_Y
     pos, vel = radial_barrier(u, pos, vel, CUP_RADIUS - half - u.contact_offset, in_cup)
     floor_y = CUP_FLOOR_Y + half + u.contact_offset
     below = in_cup & (pos[1] < floor_y)
     stop = below & (vel[1] < F32(0.0))
-    k = F32(1.0) - u.friction * F32(0.55)
     pos = [pos[0], np.where(below, floor_y, pos[1]), pos[2]]
     vel = [np.where(stop, vel[0] * k, vel[0]), np.where(stop, F32(0.0), vel[1]), np.where(stop, vel[2] * k, vel[2])]
     return pos, vel
 
 
-def sdf_contact_water(u, sdf, outlet_r, pos, vel):
-    """resolve_sdf_contact (shader.rs:879-903) for water."""
+def sdf_contact(u, sdf, outlet_r, pos, vel, is_bed=False):
+    """resolve_sdf_contact (shader.rs:879-903)."""
     sd = sdf.sample(*pos)
     n = sdf.gradient(*pos)
     near = (sd < u.contact_offset) & (length3(*n) > F32(1e-6))
@@ -763,7 +798,7 @@ def sdf_contact_water(u, sdf, outlet_r, pos, vel):
     safe = np.where(fr, vtl, F32(1.0))
     v3 = [np.where(fr, v2[q] - vt[q] * (imp / safe), v2[q]) for q in range(3)]
     vel = [np.where(hit, v3[q], vel[q]) for q in range(3)]
-    return scene_obstacles_water(u, outlet_r, pos, vel)
+    return scene_obstacles(u, outlet_r, pos, vel, is_bed)
 
 
 def g2p(u, sdf, bed, outlet_r, particles, affine, grid_vel, exp=np.exp, stats=None):
@@ -887,8 +922,8 @@ def g2p(u, sdf, bed, outlet_r, particles, affine, grid_vel, exp=np.exp, stats=No
     # advection and particle-level contact (shader.rs:1842-1869)
     new_pos = [xp[q] + new_v[q] * u.dt for q in range(3)]
     mid = [mix(xp[q], new_pos[q], F32(0.5)) for q in range(3)]
-    _, new_v = sdf_contact_water(u, sdf, outlet_r, mid, new_v)
-    new_pos, new_v = sdf_contact_water(u, sdf, outlet_r, new_pos, new_v)
+    _, new_v = sdf_contact(u, sdf, outlet_r, mid, new_v)
+    new_pos, new_v = sdf_contact(u, sdf, outlet_r, new_pos, new_v)
     margin = u.dx * F32(0.5)
     new_pos = [clamp(new_pos[q], u.origin[q] + margin, u.bounds_max[q] - margin) for q in range(3)]
     for q in range(3):
@@ -1064,3 +1099,221 @@ def prepare_render(u, particles, affine, bed_extract):
     out[:, 4] = radius
     out[dead] = np.array([0.0, -1e6, 0.0, -999.0, 0, 0, 0, 0], np.float32)
     return out
+
+
+# ---------------------------------------------------------------- bed_dynamics  (shader.rs:1991-2238)
+
+def _pressure_gradient_at(u, lanes, cell):
+    """pressure_gradient_at_cell (shader.rs:238-260) at rows of cells (n, 3): the pressure
+    lane and whatever lane 3 holds when it runs (the kind test is `== CELL_SOLID`)."""
+    L = np.asarray(lanes, np.int32).reshape(6, -1)
+    p = lane_f32(u, L[0])
+    kind = L[3]
+    cx, cy, cz = cell[:, 0], cell[:, 1], cell[:, 2]
+
+    def on(x, y, z):
+        return (x >= 0) & (y >= 0) & (z >= 0) & (x < u.gx) & (y < u.gy) & (z < u.gz)
+
+    def idx(x, y, z):
+        return (np.clip(z, 0, u.gz - 1).astype(np.int64) * u.gy + np.clip(y, 0, u.gy - 1)) * u.gx + np.clip(x, 0, u.gx - 1)
+
+    here_on = on(cx, cy, cz)
+    ph = p[idx(cx, cy, cz)]
+    nbp = []
+    for d in FACES:
+        x, y, z = cx + d[0], cy + d[1], cz + d[2]
+        i = idx(x, y, z)
+        mirror = ~on(x, y, z) | (kind[i] == CELL_SOLID)
+        nbp.append(np.where(mirror, ph, p[i]))
+    h = F32(0.5) * u.inv_dx
+    g = [h * (nbp[1] - nbp[0]), h * (nbp[3] - nbp[2]), h * (nbp[5] - nbp[4])]
+    return [np.where(here_on, c, F32(0.0)) for c in g]
+
+
+def _coffee_packing(u, bed_pos, lookup, pos, vel, bids):
+    """resolve_coffee_particle_packing (shader.rs:825-877).  Other samples' positions are
+    read from `bed_pos`, the positions before the dispatch."""
+    cell = world_to_cell(u, np.stack(pos, axis=1))
+    m = bids.size
+    best = np.full(m, F32(1e9), np.float32)
+    bd = [np.zeros(m, np.float32) for _ in range(3)]
+    found = np.zeros(m, bool)
+    lk = lookup.reshape(-1)
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                x, y, z = cell[:, 0] + di, cell[:, 1] + dj, cell[:, 2] + dk
+                ok = (x >= 0) & (y >= 0) & (z >= 0) & (x < u.gx) & (y < u.gy) & (z < u.gz)
+                ci = (np.clip(z, 0, u.gz - 1).astype(np.int64) * u.gy + np.clip(y, 0, u.gy - 1)) * u.gx + np.clip(x, 0, u.gx - 1)
+                o = np.where(ok, lk[ci], -1)
+                ok &= (o >= 0) & (o != bids) & (o < u.num_bed)
+                so = np.where(ok, o, 0)
+                d = [pos[q] - bed_pos[so, q] for q in range(3)]
+                dist = length3(*d)
+                better = ok & (dist < best)
+                best = np.where(better, dist, best)
+                bd = [np.where(better, d[q], bd[q]) for q in range(3)]
+                found |= better
+    min_sep = u.dx * u.bed_r_dx * F32(1.78)
+    hit = found & (best < min_sep)
+    far = best > F32(1e-5)
+    sb = np.where(far, best, F32(1.0))
+    n = [np.where(far, bd[0] / sb, F32(0.0)), np.where(far, bd[1] / sb, F32(1.0)), np.where(far, bd[2] / sb, F32(0.0))]
+    push = np.minimum((min_sep - best) * F32(0.65), u.dx * F32(0.22))
+    pos = [np.where(hit, pos[q] + n[q] * push, pos[q]) for q in range(3)]
+    vn = vel[0] * n[0] + vel[1] * n[1] + vel[2] * n[2]
+    back = hit & (vn < F32(0.0))
+    vel = [np.where(back, vel[q] - n[q] * vn, vel[q]) for q in range(3)]
+    return pos, vel
+
+
+def bed_dynamics(u, sdf, outlet_r, lanes, grid_vel, lookup, particles, affine, bed_extract, impulse_lanes,
+                 bed_damping=F32(8.5), surface_ref_y=F32(3.0), surface_span=F32(3.5)):
+    """Bed samples after bed_dynamics: (particles (num_bed, 8), affine (num_bed, 12),
+    bed_extract (num_bed, 8)).  `impulse_lanes` are the three i32 impulse lanes that
+    bed_impulse_delta_exchange (shader.rs:517-522) reads and clears.  Another sample's
+    position (the packing contact) is its position before the dispatch."""
+    nb = u.num_bed
+    P = np.array(particles, np.float32).reshape(-1, 8)[:nb].copy()
+    A = np.array(affine, np.float32).reshape(-1, 12)[:nb].copy()
+    BE = np.array(bed_extract, np.float32).reshape(-1, 8)[:nb].copy()
+    gv = np.asarray(grid_vel, np.float32).reshape(-1, 4)
+    lk = np.asarray(lookup, np.int32).reshape(-1)
+    bed_pos = P[:, 0:3].copy()
+    bids = np.arange(nb)
+    pos = [P[:, q] for q in range(3)]
+    v0 = [P[:, 4 + q] for q in range(3)]
+    mass = P[:, 7]
+    phase = A[:, 3].copy()
+    rest = [A[:, 4 + q].copy() for q in range(3)]
+    imp = [np.asarray(impulse_lanes[q], np.int32)[:nb].astype(np.float32) * u.inv_fp for q in range(3)]
+    den = np.maximum(mass, u.nominal_mass * F32(0.25))
+    brv = [c / den for c in imp]
+    max_rs = np.minimum(u.vel_cap * F32(0.012), u.dx / np.maximum(u.dt, F32(1e-6)) * F32(0.02))
+    rs = length3(*brv)
+    over = (rs > max_rs) & (rs > F32(1e-6))
+    sc = max_rs / np.where(over, rs, F32(1.0))
+    brv = [np.where(over, c * sc, c) for c in brv]
+    gp = [(pos[q] - u.origin[q]) * u.inv_dx for q in range(3)]
+    base = [to_i32(np.floor(c - F32(0.5))) for c in gp]
+    fx = [gp[q] - base[q].astype(np.float32) for q in range(3)]
+    w = [[F32(0.5) * (F32(1.5) - f) * (F32(1.5) - f), F32(0.75) - (f - F32(1.0)) * (f - F32(1.0)),
+          F32(0.5) * (f - F32(0.5)) * (f - F32(0.5))] for f in fx]
+    z = lambda: np.zeros(nb, np.float32)  # noqa: E731
+    wv, wm, asw, lasw = [z(), z(), z()], z(), z(), z()
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                cx, cy, cz = base[0] + i, base[1] + j, base[2] + k
+                ok = (cx >= 0) & (cy >= 0) & (cz >= 0) & (cx < u.gx) & (cy < u.gy) & (cz < u.gz)
+                ci = np.where(ok, (cz.astype(np.int64) * u.gy + cy) * u.gx + cx, 0)
+                wt = w[0][i] * w[1][j] * w[2][k]
+                g = gv[ci]
+                wv = [np.where(ok, wv[q] + wt * g[:, q], wv[q]) for q in range(3)]
+                wm = np.where(ok, wm + wt * g[:, 3], wm)
+                sb = np.where(ok, lk[ci], -1)
+                sup = ok & (sb >= 0) & (sb != bids)
+                asw = np.where(sup, asw + wt, asw)
+                ccy = u.origin[1] + (cy.astype(np.float32) + F32(0.5)) * u.dx
+                lower = sup & (ccy <= pos[1] + u.dx * F32(0.25))
+                lasw = np.where(lower, lasw + wt, lasw)
+    floor_y = coffee_filter_floor_y(u)
+    out_pos, out_vel = [c.copy() for c in pos], [c.copy() for c in v0]
+    # suspended grains (shader.rs:2064-2105)
+    sus = phase >= F32(1.5)
+    ws = clamp(wm / np.maximum(u.nominal_mass * F32(2.0), F32(1e-6)), F32(0.0), F32(1.0))
+    drag = clamp((F32(8.0) + F32(18.0) * ws) * u.dt, F32(0.0), F32(1.0))
+    unsup = [v0[0] + brv[0] + F32(0.0), v0[1] + brv[1] + u.gravity * u.dt * F32(0.85), v0[2] + brv[2] + F32(0.0)]
+    settle = mix(F32(1.10), F32(0.32), ws)
+    carried = [wv[0] + F32(0.0), wv[1] + (-settle), wv[2] + F32(0.0)]
+    sv = [mix(unsup[q], carried[q], drag) for q in range(3)]
+    sp = length3(*sv)
+    o = sp > u.vel_cap
+    f = u.vel_cap / np.where(o, sp, F32(1.0))
+    sv = [np.where(o, c * f, c) for c in sv]
+    spos = [pos[q] + sv[q] * u.dt for q in range(3)]
+    spos, sv = sdf_contact(u, sdf, outlet_r, spos, sv, True)
+    anchored = (lasw > F32(0.06)) | (asw > F32(0.20))
+    dense = asw > F32(0.42)
+    redeposit = ((spos[1] <= floor_y + u.dx * F32(0.35)) & (ws < F32(0.35))) | \
+        (anchored & (sv[1] <= F32(0.20)) & ((ws < F32(0.55)) | dense))
+    # anchored grains (shader.rs:2107-2237)
+    sat = BE[:, 7]
+    wl = clamp(wm / np.maximum(u.nominal_mass * F32(1.5), F32(1e-6)), F32(0.0), F32(1.0))
+    mob = clamp((F32(0.30) + wl * F32(0.62)) * (F32(1.0) + sat * F32(0.40)), F32(0.0), F32(1.0))
+    sf = clamp((rest[1] + surface_ref_y) / surface_span, F32(0.12), F32(1.0))
+    damping = clamp(F32(1.0) - bed_damping * u.dt, F32(0.0), F32(1.0))
+    vel = [v0[q] + brv[q] for q in range(3)]
+    sr = clamp(F32(1.0) - asw / F32(0.55), F32(0.0), F32(1.0))
+    entr = clamp((F32(2.0) + F32(5.0) * sat) * wl * sr * u.dt, F32(0.0), F32(0.08))
+    gs = -mix(F32(0.95), F32(0.35), wl)
+    tgt = [wv[0] + F32(0.0), wv[1] + gs, wv[2] + F32(0.0)]
+    vel = [mix(vel[q], tgt[q], entr) for q in range(3)]
+    lsp = np.sqrt(wv[0] * wv[0] + wv[2] * wv[2])
+    lon = lsp > F32(1e-6)
+    ls = np.where(lon, lsp, F32(1.0))
+    ldx, ldz = np.where(lon, wv[0] / ls, F32(0.0)), np.where(lon, wv[2] / ls, F32(0.0))
+    down = np.minimum(wv[1], F32(0.0))
+    lss = np.minimum(lsp, np.abs(down) * F32(0.18))
+    impact = [ldx * lss * F32(0.08), down * F32(0.62), ldz * lss * F32(0.08)]
+    bi_ = u.bed_impact
+    vel = [vel[q] + impact[q] * bi_ * mob * sf * u.dt for q in range(3)]
+    pg = _pressure_gradient_at(u, lanes, world_to_cell(u, np.stack(pos, axis=1)))
+    sx, sz = -pg[0], -pg[2]
+    ssp = np.sqrt(sx * sx + sz * sz)
+    son = ssp > F32(1e-6)
+    sss = np.where(son, ssp, F32(1.0))
+    sdx, sdz = np.where(son, sx / sss, F32(0.0)), np.where(son, sz / sss, F32(0.0))
+    drive = np.minimum(ssp, u.vel_cap / np.maximum(u.dt, F32(1e-6)))
+    pl = clamp(wm * (F32(0.25) + sat), F32(0.0), F32(1.0))
+    slx, slz = sdx * drive * pl * F32(0.08), sdz * drive * pl * F32(0.08)
+    vel[0] = vel[0] + slx * bi_ * mob * sf * u.dt
+    vel[2] = vel[2] + slz * bi_ * mob * sf * u.dt
+    vel = [c * damping for c in vel]
+    npos = [pos[q] + vel[q] * u.dt for q in range(3)]
+    off = [npos[q] - rest[q] for q in range(3)]
+    ll = np.sqrt(off[0] * off[0] + off[2] * off[2])
+    lpt = u.dx * F32(0.22)
+    lat = (ll > lpt) & (ll > F32(1e-6))
+    lls = np.where(lat, ll, F32(1.0))
+    ldx2, ldz2 = off[0] / lls, off[2] / lls
+    lex = ll - lpt
+    lplast = clamp((F32(0.04) + sat * F32(0.35) + mob * F32(0.45) + pl * F32(0.25)) * sf * u.compaction_rate * u.dt,
+                   F32(0.0), F32(0.18))
+    rest = [np.where(lat, rest[0] + ldx2 * lex * lplast, rest[0]), rest[1],
+            np.where(lat, rest[2] + ldz2 * lex * lplast, rest[2])]
+    off = [np.where(lat, npos[q] - rest[q], off[q]) for q in range(3)]
+    cll = np.sqrt(off[0] * off[0] + off[2] * off[2])
+    max_lat = u.dx * F32(0.9) * sf
+    cap = (cll > max_lat) & (cll > F32(1e-6))
+    cls = np.where(cap, cll, F32(1.0))
+    off[0] = np.where(cap, off[0] / cls * max_lat, off[0])
+    off[2] = np.where(cap, off[2] / cls * max_lat, off[2])
+    vel[0] = np.where(cap, vel[0] * F32(0.4), vel[0])
+    vel[2] = np.where(cap, vel[2] * F32(0.4), vel[2])
+    off[1] = clamp(off[1], (-u.dx) * (F32(1.75) * sf + F32(0.2)), u.dx * F32(0.04))
+    npos = [rest[q] + off[q] for q in range(3)]
+    npos, vel = _coffee_packing(u, bed_pos, lk, npos, vel, bids)
+    comp = np.maximum(rest[1] - npos[1], F32(0.0))
+    pt = u.dx * F32(0.18)
+    plast = clamp((F32(0.05) + sat * F32(0.35) + mob * F32(0.55)) * sf * u.compaction_rate * u.dt, F32(0.0), F32(0.18))
+    rest[1] = np.where(comp > pt, rest[1] - (comp - pt) * plast, rest[1])
+    hyd = (sat > F32(0.82)) & (pl > F32(0.65)) & (wl > F32(0.65)) & (sr > F32(0.35)) & \
+        ((comp > u.dx * F32(0.65)) | (cll > u.dx * F32(0.65)))
+    flow = (sat > F32(0.58)) & (wl > F32(0.74)) & (sr > F32(0.55)) & (length3(*wv) > F32(0.95)) & \
+        (npos[1] > floor_y + u.dx * F32(0.70))
+    iso = (sat > F32(0.55)) & (wm < u.nominal_mass * F32(0.75)) & (asw < F32(0.04)) & (lasw < F32(0.03)) & \
+        (npos[1] > floor_y + u.dx * F32(0.50))
+    detach = hyd | flow | iso
+    rest = [np.where(detach, npos[q], rest[q]) for q in range(3)]
+    anchored_phase = np.where(detach, F32(2.0), phase)
+    npos, vel = sdf_contact(u, sdf, outlet_r, npos, vel, True)
+    gc = np.maximum((rest[1] - npos[1]) / np.maximum(u.dx, F32(1e-6)), F32(0.0))
+    for q in range(3):
+        P[:, q] = np.where(sus, spos[q], npos[q])
+        P[:, 4 + q] = np.where(sus, sv[q], vel[q])
+        A[:, 4 + q] = np.where(sus, spos[q], rest[q])
+    A[:, 7] = F32(0.0)
+    A[:, 3] = np.where(sus, np.where(redeposit, F32(1.0), phase), anchored_phase)
+    BE[:, 3] = np.where(sus, BE[:, 3] * F32(0.985), np.maximum(BE[:, 3] * F32(0.995), gc))
+    return P, A, BE
