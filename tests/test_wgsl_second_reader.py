@@ -345,3 +345,29 @@ def test_bed_dynamics(stages):
         msg = _report(name, got, want)
         assert msg is None, msg
     assert not after["bed_delta"][1:4, :nb].any()
+
+
+def _scene(name, oracle):
+    from coffee_sim_b200 import scenes
+    if name == "center_pour":
+        return MpmSettings.benchmark_center_pour(oracle)
+    return scenes.c2_v60(oracle, grid=64, max_particles=1000)
+
+
+@pytest.mark.parametrize("name", ["center_pour", "v60_si_64cube"])
+def test_sdf_texture_and_solid_class(oracle, name):
+    """The static SDF texture and the per-cell solid class the simulation is created with
+    (state.rs:206-344), for the reference's scene and for an SI-unit V60 scene (whose wall
+    thickness is its own, in its units)."""
+    s = _scene(name, oracle)
+    sim = MpmSim3D(s, oracle)
+    if name == "center_pour":
+        assert s.raw.geom.wall_thickness == np.float32(0.4)
+    sdf = W.generate_sdf(s.raw, s.raw.geom.wall_thickness)
+    assert np.count_nonzero(sdf < 900) > 1000
+    msg = _report("sdf", sdf, sim.read_sdf())
+    assert msg is None, msg
+    cls = W.generate_sdf_class(s.raw, sdf)
+    assert cls.any() and not cls.all()
+    msg = _report("sdf class", cls, sim.read_sdf_class())
+    assert msg is None, msg

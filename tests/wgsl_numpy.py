@@ -1317,3 +1317,75 @@ def bed_dynamics(u, sdf, outlet_r, lanes, grid_vel, lookup, particles, affine, b
     A[:, 3] = np.where(sus, np.where(redeposit, F32(1.0), phase), anchored_phase)
     BE[:, 3] = np.where(sus, BE[:, 3] * F32(0.985), np.maximum(BE[:, 3] * F32(0.995), gc))
     return P, A, BE
+
+
+# ---------------------------------------------------------------- SDF texture and solid class  (state.rs:206-344)
+
+SDF_NO_CONSTRAINT = F32(999.0)      # state.rs:30
+
+
+def generate_sdf(raw, wall_thickness=WALL_THICKNESS):
+    """generate_sdf_data (state.rs:250-275) with sdf_interior (state.rs:206-248): the
+    max-union of the obstacles' interior distances, inset by half the wall thickness, at
+    the centres of a 128^3 lattice over the bounds; (128^3,) float32, x fastest.  The
+    reference's wall is OBSTACLE_WALL_THICKNESS = 0.4 scene units; scenes in other units
+    pass their own."""
+    n = SDF_RES
+    b = [F32(v) for v in raw.bounds_size]
+    iz, iy, ix = np.meshgrid(np.arange(n, dtype=np.float32), np.arange(n, dtype=np.float32),
+                             np.arange(n, dtype=np.float32), indexing="ij")
+    p = [(-b[a]) * F32(0.5) + (c + F32(0.5)) * b[a] / F32(n) for a, c in enumerate((ix, iy, iz))]
+    data = np.full((n, n, n), SDF_NO_CONSTRAINT, np.float32)
+    half = F32(wall_thickness) * F32(0.5)
+    for ob in raw.obstacles[:raw.num_obstacles]:
+        c = [F32(v) for v in ob.center]
+        ly = p[1] - c[1]
+        ddx, ddz = p[0] - c[0], p[2] - c[2]
+        r = np.sqrt(ddx * ddx + ddz * ddz)
+        top, bot = F32(ob.top_y), F32(ob.bot_y)
+        if ob.kind == 0:                                            # truncated cone
+            height = top - bot
+            if height < F32(1e-10):
+                sd = np.full_like(ly, SDF_NO_CONSTRAINT)
+            else:
+                t = (ly - bot) / height
+                cone_r = F32(ob.bot_radius) + (F32(ob.top_radius) - F32(ob.bot_radius)) * t
+                sd = np.where((ly > top) | (ly < bot), SDF_NO_CONSTRAINT, cone_r - r)
+        else:                                                       # cylinder
+            sd = np.where(ly > top, SDF_NO_CONSTRAINT, np.minimum(F32(ob.radius) - r, ly - bot))
+        sd = sd - half
+        fresh = data >= SDF_NO_CONSTRAINT - F32(1.0)
+        data = np.where(fresh, sd, np.maximum(data, sd))
+    return data.reshape(-1)
+
+
+def generate_sdf_class(raw, sdf):
+    """generate_sdf_class_data (state.rs:323-344): 1 where the host-side trilinear sample
+    (state.rs:285-321, lerps written `a + (b - a) * f`) at the cell centre is below 0."""
+    gx, gy, gz = (int(v) for v in raw.grid_dims)
+    b = [F32(v) for v in raw.bounds_size]
+    dx = b[0] / F32(gx)
+    iz, iy, ix = np.meshgrid(np.arange(gz, dtype=np.float32), np.arange(gy, dtype=np.float32),
+                             np.arange(gx, dtype=np.float32), indexing="ij")
+    cc = [(-b[a] * F32(0.5)) + (c + F32(0.5)) * dx for a, c in enumerate((ix, iy, iz))]
+    t = np.asarray(sdf, np.float32).reshape(SDF_RES, SDF_RES, SDF_RES)
+    res = F32(SDF_RES)
+    uv = [(cc[a] + b[a] * F32(0.5)) / b[a] * res - F32(0.5) for a in range(3)]
+    fl = [np.floor(c) for c in uv]
+    base = [to_i32(c) for c in fl]
+    f = [c - d for c, d in zip(uv, fl)]
+    m = SDF_RES - 1
+
+    def ld(dx_, dy, dz):
+        return t[np.clip(base[2] + dz, 0, m), np.clip(base[1] + dy, 0, m), np.clip(base[0] + dx_, 0, m)]
+
+    def lerp(a, b_, s):
+        return a + (b_ - a) * s
+
+    c00 = lerp(ld(0, 0, 0), ld(1, 0, 0), f[0])
+    c10 = lerp(ld(0, 1, 0), ld(1, 1, 0), f[0])
+    c01 = lerp(ld(0, 0, 1), ld(1, 0, 1), f[0])
+    c11 = lerp(ld(0, 1, 1), ld(1, 1, 1), f[0])
+    c0 = lerp(c00, c10, f[1])
+    c1 = lerp(c01, c11, f[1])
+    return (lerp(c0, c1, f[2]) < F32(0.0)).astype(np.uint8).reshape(-1)
