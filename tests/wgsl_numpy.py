@@ -1389,3 +1389,100 @@ def generate_sdf_class(raw, sdf):
     c0 = lerp(c00, c10, f[1])
     c1 = lerp(c01, c11, f[1])
     return (lerp(c0, c1, f[2]) < F32(0.0)).astype(np.uint8).reshape(-1)
+
+
+# ---------------------------------------------------------------- inflow emission  (inflow.rs:108-293)
+
+def _normalized(v):
+    """Vec3::normalized with the ZERO guards of `/` (crates/sim-core/src/math.rs:41-92)."""
+    ln = np.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    if ln <= F32(1e-6):
+        return [F32(0.0)] * 3
+    return [c / ln for c in v]
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+class Inflow:
+    """InflowState (inflow.rs:68-242): kettle angle -> head -> exit speed and flow rate,
+    and the golden-angle disk emission with back-dated ages.  cos/sin of the golden
+    angle are evaluated in float64 and rounded (Rust's f32 functions leave the last bit to
+    the platform's libm)."""
+
+    def __init__(self, raw, angle_deg):
+        self.raw = raw
+        self.angle = F32(angle_deg)
+        self.accumulator = F32(0.0)
+        self.sequence = 0
+
+    def update(self):
+        sp, raw = self.raw.spout, self.raw
+        a, act, full = self.angle, F32(sp.activation_angle_deg), F32(sp.full_flow_angle_deg)
+        if a <= act:
+            s = F32(0.0)
+        elif a >= full:
+            s = F32(1.0)
+        else:
+            t = (a - act) / (full - act)
+            s = t * t * (F32(3.0) - F32(2.0) * t)
+        if a <= act:
+            head = F32(0.0)
+        elif a >= full:
+            head = F32(sp.head_at_full_angle)
+        else:
+            head = F32(sp.head_at_activation) + s * (F32(sp.head_at_full_angle) - F32(sp.head_at_activation))
+        cap = F32(sp.gentle_exit_speed) + s * (F32(sp.max_exit_speed) - F32(sp.gentle_exit_speed))
+        if head < F32(1e-6):
+            speed = F32(0.0)
+        else:
+            speed = np.minimum(np.sqrt(F32(2.0) * F32(raw.standard_gravity_m_s2) * F32(raw.sim_units_per_meter) * head), cap)
+        if speed < F32(1e-6):
+            flow = F32(0.0)
+        else:
+            r = F32(sp.nozzle_radius)
+            area = F32(np.pi) * r * r
+            flow = np.minimum(F32(sp.discharge_coeff) * area * speed * F32(sp.volume_to_ml), F32(sp.max_flow_rate_ml_s))
+        self.exit_speed, self.flow_rate = F32(speed), F32(flow)
+
+    def emit(self, dt, current_total, max_particles):
+        """New sample rows (count, 8) of one substep."""
+        self.update()
+        brew = self.raw.brew
+        if self.flow_rate < F32(1e-6):
+            self.accumulator = F32(0.0)
+            return np.zeros((0, 8), np.float32)
+        self.accumulator = self.accumulator + self.flow_rate * F32(brew.water_particles_per_ml) * F32(dt)
+        count = int(self.accumulator)
+        if count == 0:
+            return np.zeros((0, 8), np.float32)
+        self.accumulator = self.accumulator - F32(count)
+        count = min(count, max(max_particles - current_total, 0))
+        if count == 0:
+            return np.zeros((0, 8), np.float32)
+        sp = self.raw.spout
+        d = [F32(c) for c in sp.direction]
+        up = [F32(0.0), F32(1.0), F32(0.0)] if abs(d[1]) < F32(0.9) else [F32(1.0), F32(0.0), F32(0.0)]
+        t1 = _normalized(_cross(d, up))
+        t2 = _normalized(_cross(d, t1))
+        vel = [c * self.exit_speed for c in d]
+        eo = [F32(sp.origin[q]) + d[q] * F32(0.18) for q in range(3)]
+        jet_r = F32(sp.nozzle_radius) * F32(0.58)
+        i = np.arange(count, dtype=np.int64)
+        sf = ((self.sequence + i) & 0xFFFFFFFF).astype(np.float32)
+        x = (sf + F32(0.5)) * F32(0.7548777)
+        radial_u = x - np.trunc(x)
+        r = jet_r * np.sqrt(radial_u)
+        theta = sf * F32(2.399963)
+        c, s = np.cos(theta.astype(np.float64)).astype(np.float32), np.sin(theta.astype(np.float64)).astype(np.float32)
+        age = ((i.astype(np.float32) + F32(0.5)) / F32(count)) * F32(dt)
+        rows = np.zeros((count, 8), np.float32)
+        for q in range(3):
+            off = t1[q] * r * c + t2[q] * r * s
+            rows[:, q] = eo[q] + off - vel[q] * age
+            rows[:, 4 + q] = vel[q]
+        rows[:, 3] = F32(1.0)
+        rows[:, 7] = F32(brew.water_mass_units_per_ml) / F32(brew.water_particles_per_ml)
+        self.sequence = (self.sequence + count) & 0xFFFFFFFF
+        return rows
