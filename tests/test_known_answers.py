@@ -335,3 +335,53 @@ def test_sdf_class_matches_live_cell_center_sampling(oracle):
     c1 = c01 + (c11 - c01) * fr[1]
     live = (c0 + (c1 - c0) * fr[2]) < 0
     assert (live.reshape(-1).astype(np.uint8) == cls).all()
+
+
+def _filter_radius_at_y(f, y):
+    """FilterConfig::radius_at_y (filter.rs:29-33) in float32."""
+    height = max(F(f.top_y) - F(f.bot_y), F(1e-6))
+    t = min(max((F(y) - F(f.bot_y)) / height, F(0.0)), F(1.0))
+    return F(f.bot_radius) + (F(f.top_radius) - F(f.bot_radius)) * t
+
+
+def _filter_inner_radius_at_y(f, y):
+    """FilterConfig::inner_radius_at_y (filter.rs:35-37)."""
+    return max(_filter_radius_at_y(f, y) - F(f.thickness), F(f.hole_radius))
+
+
+def test_filter_preset_is_the_reference_default(oracle):
+    """filter.rs:14-26: the V60 preset's paper filter is FilterConfig::default()."""
+    f = MpmSettings.default_v60(oracle).filter
+    assert (list(f.center), f.top_y, f.bot_y) == ([0.0, F(-0.35), 0.0], F(2.75), F(-3.02))
+    assert (f.top_radius, f.bot_radius, f.thickness, f.hole_radius) == (F(4.10), 0.0, F(0.08), 0.0)
+
+
+def test_filter_radius_decreases_toward_the_apex(oracle):
+    """filter.rs:62-66."""
+    f = MpmSettings.default_v60(oracle).filter
+    assert _filter_radius_at_y(f, f.top_y) > _filter_radius_at_y(f, f.bot_y)
+
+
+def test_default_filter_paper_comes_to_a_tip(oracle):
+    """filter.rs:68-74."""
+    f = MpmSettings.default_v60(oracle).filter
+    assert f.hole_radius == 0.0
+    assert _filter_radius_at_y(f, f.bot_y) == 0.0
+    assert _filter_inner_radius_at_y(f, f.bot_y) == 0.0
+
+
+def test_filter_contains_shell_points_on_the_cone_band(oracle):
+    """filter.rs:76-92: a point midway through the paper at mid height is in the shell,
+    one 0.5 outside the outer radius is not."""
+    f = MpmSettings.default_v60(oracle).filter
+
+    def in_shell(x, y, z):
+        if y < f.bot_y or y > f.top_y:
+            return False
+        r = math.sqrt((x - f.center[0]) ** 2 + (z - f.center[2]) ** 2)
+        return _filter_inner_radius_at_y(f, y) <= r <= _filter_radius_at_y(f, y)
+
+    mid_y = (F(f.top_y) + F(f.bot_y)) * F(0.5)
+    outer, inner = _filter_radius_at_y(f, mid_y), _filter_inner_radius_at_y(f, mid_y)
+    assert in_shell(f.center[0] + (outer + inner) * F(0.5), mid_y, f.center[2])
+    assert not in_shell(f.center[0] + outer + F(0.5), mid_y, f.center[2])
