@@ -269,13 +269,14 @@ class Sdf:
 # ---------------------------------------------------------------- boundary_project  (shader.rs:1630-1679)
 
 def boundary_project(u, sdf, grid_vel):
-    """`grid_vel` after one boundary_project pass: (cells, 4) float32."""
-    gv = np.array(grid_vel, np.float32).reshape(u.gz, u.gy, u.gx, 4)
-    live = ~(gv[..., 3] < F32(1e-6))
-    v = [gv[..., q].copy() for q in range(3)]
-    px, py, pz = cell_centres(u)
+    """`grid_vel` after one boundary_project pass: (cells, 4) float32.  Cells below the
+    mass threshold return at once (shader.rs:1636), so only the others are evaluated."""
+    gv = np.array(grid_vel, np.float32).reshape(-1, 4)
+    live = np.flatnonzero(~(gv[:, 3] < F32(1e-6)))
+    v = [gv[live, q] for q in range(3)]
+    px, py, pz = (c.reshape(-1)[live] for c in cell_centres(u))
     sd = sdf.sample(px, py, pz)
-    near = live & (sd < u.contact_offset)
+    near = sd < u.contact_offset
     n = sdf.gradient(px, py, pz)
     vn = v[0] * n[0] + v[1] * n[1] + v[2] * n[2]
     hit = near & (vn < F32(0.0))
@@ -297,8 +298,8 @@ def boundary_project(u, sdf, grid_vel):
         v[q] = np.where((p > hi) & (v[q] > F32(0.0)), F32(0.0), v[q])
     out = gv.copy()
     for q in range(3):
-        out[..., q] = np.where(live, v[q], gv[..., q])
-    return out.reshape(-1, 4)
+        out[live, q] = v[q]
+    return out
 
 
 # ---------------------------------------------------------------- shared helpers of the pressure passes
@@ -1486,3 +1487,44 @@ class Inflow:
         rows[:, 7] = F32(brew.water_mass_units_per_ml) / F32(brew.water_particles_per_ml)
         self.sequence = (self.sequence + count) & 0xFFFFFFFF
         return rows
+
+
+# ---------------------------------------------------------------- one whole substep  (mod.rs:271-419)
+
+def substep(raw, sdf_texels, sdf_class, inflow, particles, affine, bed_extract, num_water, num_bed, dt):
+    """One substep of the reference configuration (fixed-point pressure, fixed pairs):
+    emission, then every dispatch in the order of mod.rs:305-414, with the lanes passed
+    from dispatch to dispatch as the shader aliases them.  Returns the sample rows,
+    affine rows and bed_extract rows after it, and the new water count."""
+    outlet_r = F32(raw.brew.dripper_outlet_radius)
+    P = np.array(particles, np.float32).reshape(-1, 8)[:num_water + num_bed]
+    A = np.array(affine, np.float32).reshape(-1, 12)[:num_water + num_bed]
+    BE = np.array(bed_extract, np.float32).reshape(-1, 8)[:num_bed]
+    new = inflow.emit(dt, num_water + num_bed, int(raw.max_particles))
+    if new.shape[0]:
+        P = np.concatenate([P, new])
+        A = np.concatenate([A, np.zeros((new.shape[0], 12), np.float32)])
+        num_water += new.shape[0]
+    u = Uniforms(raw, num_water, num_bed, dt)
+    sdf = Sdf(u, sdf_texels)
+    solid = np.asarray(sdf_class).reshape(u.grid_shape()) != 0
+    lookup = bed_lookup(u, P, A)
+    lanes = p2g(u, P, A)
+    gv = boundary_project(u, sdf, grid_update(u, lanes))
+    bed = Bed(u, lookup, P, A, BE)
+    lanes = classify(u, lanes, gv, bed, sdf, solid, bool(raw.use_sdf_cache))
+    lanes = rbgs(u, lanes, int(raw.pressure_rbgs_pairs))
+    gv, imp = project(u, lanes, gv, bed)
+    gv = boundary_project(u, sdf, gv)
+    lanes = packing_prepare(u, lanes)
+    gv = boundary_project(u, sdf, packing_apply(u, lanes, gv))
+    lanes = viscosity_prepare(u, lanes, gv, solid)
+    gv = boundary_project(u, sdf, viscosity_apply(u, lanes, gv))
+    P, A, imp_g2p = g2p(u, sdf, bed, outlet_r, P, A, gv)
+    imp = imp + imp_g2p
+    P, water = bed_coupling(u, Bed(u, lookup, P, A, BE), P, A)
+    if num_bed:
+        BE = extraction_advect(u, BE, wrap_i32(water))
+        Pb, Ab, BE = bed_dynamics(u, sdf, outlet_r, lanes, gv, lookup, P, A, BE, wrap_i32(imp))
+        P[:num_bed], A[:num_bed] = Pb, Ab
+    return P, A, BE, num_water
