@@ -17,6 +17,14 @@
 // Templated on the arithmetic type: float reproduces the engine bit for bit; double
 // is the FP64 reference run that errors are reported against.  OpenMP parallelises
 // the loops; integer fixed-point atomics keep the result independent of thread count.
+//
+// Parity unpinned: the reference runs its step only as WGSL through wgpu (a graphics
+// API) from a Rust crate, neither of which can run here, and its tests hold no golden
+// vectors for the step.  What pins this restatement: the reference's host-side known
+// answers (tests/test_known_answers.py), its scenario tests run on the engine
+// (tests/test_physics_gpu.py), and a second restatement of every dispatch written
+// independently in numpy (tests/wgsl_numpy.py), which agrees with this one bit for
+// bit except for the backend-defined exp of the J update.
 #include <algorithm>
 #include <array>
 #include <cmath>
