@@ -424,3 +424,35 @@ def test_whole_substeps_chained(stages):
         msg = _report(name, got, want)
         assert msg is None, msg
     sim.close()
+
+
+def test_int64_p2g_and_grid_update(oracle, pour_state_int64):
+    """The engine's 64-bit P2G mode (the headline workload's): lanes as i64 * 2^32 with a
+    wrapping 64-bit sum, and grid_update reading them back as f32(lane) * 2^-32."""
+    s, src = pour_state_int64
+    sims = []
+    for n in (P_P2G, P_P2G + 1, P_GRID_UPDATE + 1):
+        sim = MpmSim3D(s, oracle)
+        copy_state(src, sim)
+        sim.set_kettle_angle(36.0)
+        sim.step_substep_partial(SUB_DT, n)
+        sims.append(sim)
+    before, after_p2g, after_gu = sims
+    u = W.Uniforms(s.raw, before.num_water, before.num_bed, SUB_DT)
+    n = before.particle_count()
+    lanes64 = W.p2g(u, before.read_particles(0, n), before.read_affine(0, n), int64=True)
+    assert np.count_nonzero(lanes64[0]) > 1000
+    msg = _report("int64 lanes", lanes64, after_p2g.read_grid_lanes64())
+    assert msg is None, msg
+    gv = W.grid_update(u, after_p2g.read_grid_lanes64())
+    msg = _report("grid_vel", gv, after_gu.read_grid_vel())
+    assert msg is None, msg
+
+
+@pytest.fixture(scope="module")
+def pour_state_int64(oracle):
+    from coffee_sim_b200 import _ffi
+    s, src = _pour(oracle)
+    s = s.copy()
+    s.raw.p2g_mode = _ffi.CS_P2G_INT64
+    return s, src

@@ -158,8 +158,26 @@ def cell_centres(u):
 
 # ---------------------------------------------------------------- p2g  (shader.rs:955-1052)
 
-def p2g(u, particles, affine):
-    """Six i32 lanes after P2G into a cleared grid: (6, cells) int32."""
+def to_i64(x):
+    """Truncate toward zero and saturate at the i64 range (NaN to 0)."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.zeros(x.shape, np.int64)
+    ok = ~np.isnan(x)
+    big, small = x >= 9223372036854775807.0, x <= -9223372036854775808.0
+    mid = ok & ~big & ~small
+    out[mid] = np.trunc(x[mid]).astype(np.int64)
+    out[big] = np.iinfo(np.int64).max
+    out[small] = np.iinfo(np.int64).min
+    return out
+
+
+INT64_SCALE = F32(4294967296.0)
+
+
+def p2g(u, particles, affine, int64=False):
+    """Six i32 lanes after P2G into a cleared grid: (6, cells) int32.  With `int64`, the
+    engine's 64-bit mode (no reference counterpart): every contribution scaled by 2^32
+    instead of 2^18, truncated to i64 and summed with 64-bit wrap; (6, cells) int64."""
     n = u.num_water + u.num_bed
     p = np.asarray(particles, np.float32).reshape(-1, 8)[:n]
     a = np.asarray(affine, np.float32).reshape(-1, 12)[:n]
@@ -190,23 +208,27 @@ def p2g(u, particles, affine):
                 dpos = (off.astype(np.float32) - fx) * u.dx                        # shader.rs:1011
                 dots = [c[:, 0] * dpos[:, 0] + c[:, 1] * dpos[:, 1] + c[:, 2] * dpos[:, 2] for c in aff]
                 mom = [wt * (mvp[:, q] + dots[q]) for q in range(3)]               # shader.rs:1016-1020
-                vals = [wt * mass * u.fp, mom[0] * u.fp, mom[1] * u.fp, mom[2] * u.fp,
-                        wt * rest_vol * u.fp, wt * cur_vol * u.fp]                 # shader.rs:1032-1037
+                fp = INT64_SCALE if int64 else u.fp
+                vals = [wt * mass * fp, mom[0] * fp, mom[1] * fp, mom[2] * fp,
+                        wt * rest_vol * fp, wt * cur_vol * fp]                     # shader.rs:1032-1037
                 ci = (cell[:, 2].astype(np.int64) * u.gy + cell[:, 1]) * u.gx + cell[:, 0]
                 for lane in range(6):
-                    np.add.at(acc[lane], ci[ok], to_i32(vals[lane][ok]).astype(np.int64))
-    return wrap_i32(acc)
+                    q = to_i64(vals[lane][ok]) if int64 else to_i32(vals[lane][ok]).astype(np.int64)
+                    np.add.at(acc[lane], ci[ok], q)
+    return acc if int64 else wrap_i32(acc)
 
 
 # ---------------------------------------------------------------- grid_update  (shader.rs:1056-1082)
 
 def grid_update(u, lanes):
-    """`grid_vel` after grid_update on a cleared `grid_vel`: (cells, 4) float32."""
-    L = np.asarray(lanes, np.int32).reshape(6, -1)
-    mass = L[0].astype(np.float32) * u.inv_fp
+    """`grid_vel` after grid_update on a cleared `grid_vel`: (cells, 4) float32.  Int64
+    lanes (the 64-bit mode) are read as f32(lane) * 2^-32."""
+    L = np.asarray(lanes).reshape(6, -1)
+    inv = F32(1.0) / INT64_SCALE if L.dtype == np.int64 else u.inv_fp
+    mass = L[0].astype(np.float32) * inv
     live = ~(mass < F32(1e-6))
     m = np.where(live, mass, F32(1.0))
-    v = [L[q].astype(np.float32) * u.inv_fp / m for q in (1, 2, 3)]
+    v = [L[q].astype(np.float32) * inv / m for q in (1, 2, 3)]
     v[1] = v[1] + u.gravity * u.dt
     speed = length3(*v)
     over = speed > u.vel_cap
