@@ -456,3 +456,27 @@ def pour_state_int64(oracle):
     s = s.copy()
     s.raw.p2g_mode = _ffi.CS_P2G_INT64
     return s, src
+
+
+def test_reorder_permutation(oracle, stages):
+    """The engine's sample reorder (`reorder_every`): the oracle's permutation of the water
+    slots equals a stable sort by the tile key described in the header.  With no dispatch
+    run, the state after the substep is the reordered state plus the new jet samples."""
+    s = stages.settings.copy()
+    s.raw.reorder_every = 1
+    sim = MpmSim3D(s, oracle)
+    copy_state(stages.src, sim)
+    sim.set_kettle_angle(36.0)
+    nw, nb = sim.num_water, sim.num_bed
+    P, A = sim.read_particles(0, nw + nb), sim.read_affine(0, nw + nb)
+    u = W.Uniforms(s.raw, nw, nb, SUB_DT)
+    perm = W.reorder_permutation(u, P, A)
+    assert np.count_nonzero(perm != np.arange(nw)) > nw // 2
+    sim.step_substep_partial(SUB_DT, 0)
+    got_p = sim.read_particles(nb, nw)
+    got_a = sim.read_affine(nb, nw)
+    msg = _report("reordered samples", P[nb:][perm], got_p)
+    assert msg is None, msg
+    msg = _report("reordered affine", A[nb:][perm], got_a)
+    assert msg is None, msg
+    sim.close()

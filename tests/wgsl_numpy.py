@@ -1550,3 +1550,24 @@ def substep(raw, sdf_texels, sdf_class, inflow, particles, affine, bed_extract, 
         Pb, Ab, BE = bed_dynamics(u, sdf, outlet_r, lanes, gv, lookup, P, A, BE, wrap_i32(imp))
         P[:num_bed], A[:num_bed] = Pb, Ab
     return P, A, BE, num_water
+
+
+# ---------------------------------------------------------------- sample reorder (engine extension)
+
+def reorder_permutation(u, particles, affine, tile=4):
+    """The engine's `reorder_every` permutation of the water slots (no reference
+    counterpart): each water sample keyed by the tile of its P2G base cell (tiles of
+    `tile`^3 over the (g + 1)-node lattice, base index + 1 clamped to the tiles), samples
+    that deposit nothing keyed after every tile, then a stable sort.  Returns, for each
+    new water slot, the old water slot."""
+    nb, nw = u.num_bed, u.num_water
+    p = np.asarray(particles, np.float32).reshape(-1, 8)[nb:nb + nw]
+    ph = np.asarray(affine, np.float32).reshape(-1, 12)[nb:nb + nw, 3]
+    nt = [(g + 1 + tile - 1) // tile for g in (u.gx, u.gy, u.gz)]
+    live = (ph < F32(0.5)) & ~(p[:, 7] <= u.inactive)
+    t = []
+    for q in range(3):
+        b = to_i32(np.floor((p[:, q] - u.origin[q]) * u.inv_dx - F32(0.5))).astype(np.int64)
+        t.append(np.minimum(np.maximum(b + 1, 0) // tile, nt[q] - 1))
+    key = np.where(live, (t[2] * nt[1] + t[1]) * nt[0] + t[0], nt[0] * nt[1] * nt[2])
+    return np.argsort(key, kind="stable")
