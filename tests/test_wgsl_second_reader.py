@@ -480,3 +480,35 @@ def test_reorder_permutation(oracle, stages):
     msg = _report("reordered affine", A[nb:][perm], got_a)
     assert msg is None, msg
     sim.close()
+
+
+@pytest.mark.parametrize("grid,omega,cap,first", [(32, 1.9, 20, 0), (64, 1.92, 60, 125)])
+def test_refinement_solve_cold_start(oracle, grid, omega, cap, first):
+    """The engine's residual-mode solve (FP32 pressure words, FP64 residual checks,
+    over-relaxed correction sweeps, predicted check intervals) restated in numpy from the
+    solver inputs the oracle's classify wrote, on the SI-unit V60 pour from a cold start
+    (at 64^3 with the bench's omega, check cap and first check): same pair and check
+    counts, the pressure's high word bit for bit, and the residuals within 1e-9 relative
+    (the oracle sums its FP64 norms per thread)."""
+    from coffee_sim_b200 import _ffi, scenes
+    s = scenes.c2_v60(oracle, grid=grid, max_particles=340000)
+    r = s.raw
+    r.warm_start = _ffi.CS_WARM_NONE
+    r.rbgs_omega, r.check_every, r.first_check, r.max_sweeps = omega, cap, first, 3000
+    sims = []
+    for n in (P_CLASSIFY + 1, P_RBGS + 1):
+        sim = MpmSim3D(s, oracle)
+        assert scenes.populate_c2(sim) > 10000
+        sim.step_substep_partial(scenes.C2_DT, n)
+        sims.append(sim)
+    a, b = sims
+    u = W.Uniforms(r, a.num_water, a.num_bed, scenes.C2_DT)
+    fill, div = a.read_solver_inputs()
+    hi, lo, pairs, checks, r0, r1 = W.refine_solve(u, a.read_cell_kind(), fill, div, r.rbgs_omega,
+                                                   r.residual_tol, r.check_every, r.first_check, r.max_sweeps)
+    m = b.latest_metrics()
+    assert 20 < pairs < r.max_sweeps and r1 <= 1e-5
+    assert (pairs, checks) == (m.last_sweeps, m.residual_checks)
+    assert abs(r0 - m.initial_residual) <= 1e-9 * r0 and abs(r1 - m.last_residual) <= 1e-9 * r1
+    msg = _report("pressure (high word)", hi, b.read_pressure())
+    assert msg is None, msg

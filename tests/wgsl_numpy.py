@@ -1571,3 +1571,99 @@ def reorder_permutation(u, particles, affine, tile=4):
         t.append(np.minimum(np.maximum(b + 1, 0) // tile, nt[q] - 1))
     key = np.where(live, (t[2] * nt[1] + t[1]) * nt[0] + t[0], nt[0] * nt[1] * nt[2])
     return np.argsort(key, kind="stable")
+
+
+# ---------------------------------------------------------------- FP32 refinement solve (engine extension)
+
+def next_check_interval(r_new, r_old, k, tol, ce):
+    """Pairs until the next FP64 residual check: the pairs the last cycle's decay predicts,
+    ceil(k log(tol / r_new) / log(r_new / r_old)), at least 2 and at most ce; ce when no
+    decay was measured."""
+    import math
+    if not (r_old > 0.0) or not (r_new > tol) or not (r_new < r_old) or k == 0:
+        return ce
+    n = math.ceil(k * math.log(tol / r_new) / math.log(r_new / r_old))
+    if not (n < ce):
+        return ce
+    return 2 if n < 2 else int(n)
+
+
+def refine_solve(u, kind, fill, div, omega, tol, check_every, first_check, max_sweeps):
+    """The engine's residual-mode pressure solve from a cold start (no reference
+    counterpart; its operator is pressure_update's, shader.rs:1371-1439): the pressure
+    kept as two float32 words (hi + lo); each cycle evaluates the FP64 residual
+    r = (sum_f w_f p_f - dx^2 rhs) - W p, relaxes the float32 correction d of W d = r
+    (over-relaxed red-black sweeps), and adds it back in FP64.  Returns (hi, lo, pairs,
+    checks, r0, r1) over all cells."""
+    shp = u.grid_shape()
+    kind = np.asarray(kind, np.int32).reshape(shp)
+    fill = np.asarray(fill, np.float32).reshape(shp)
+    div = np.asarray(div, np.float32).reshape(shp)
+    fl = np.flatnonzero(is_fluid(kind).reshape(-1))
+    iz, iy, ix = np.unravel_index(fl, shp)
+    par = ((ix + iy + iz) & 1)[:]
+    nbi, w, wf = [], [], []
+    for d in FACES:
+        x, y, z = ix + d[0], iy + d[1], iz + d[2]
+        on = (x >= 0) & (y >= 0) & (z >= 0) & (x < u.gx) & (y < u.gy) & (z < u.gz)
+        ni = np.where(on, (np.clip(z, 0, u.gz - 1) * u.gy + np.clip(y, 0, u.gy - 1)) * u.gx + np.clip(x, 0, u.gx - 1), 0)
+        nk = np.where(on, kind.reshape(-1)[ni], CELL_SOLID)
+        wt = face_weight(kind.reshape(-1)[fl], fill.reshape(-1)[fl], nk, fill.reshape(-1)[ni])
+        use = on & (nk != CELL_SOLID) & ~(wt <= F32(0.0))
+        nbi.append(ni)
+        w.append(np.where(use, wt, F32(0.0)))
+        wf.append(use & is_fluid(nk))
+    sf = fill.reshape(-1)[fl]
+    rhs = div.reshape(-1)[fl] * sf / np.maximum(u.dt, F32(1e-6))
+    b = (u.dx * u.dx * rhs).astype(np.float64)
+    nc = np.zeros(fl.size, np.float32)
+    wsum = np.zeros(fl.size)
+    for q in range(6):
+        nc = nc + w[q]                      # zero weights add exactly nothing
+        wsum = wsum + w[q].astype(np.float64)
+    solvable = ~(nc <= F32(0.0))
+    hi = np.zeros(u.cells, np.float32)
+    lo = np.zeros(u.cells, np.float32)
+    pd = np.zeros(u.cells, np.float32)
+    omega = F32(omega)
+
+    def residual():
+        p = hi.astype(np.float64) + lo.astype(np.float64)
+        psum = np.zeros(fl.size)
+        for q in range(6):
+            psum = psum + np.where(wf[q], w[q].astype(np.float64) * p[nbi[q]], 0.0)
+        r = (psum - b) - wsum * p[fl]
+        r = np.where(wsum > 0.0, r, 0.0)
+        bb = np.where(wsum > 0.0, b, 0.0)
+        b2 = float(np.sum(bb * bb))
+        return r.astype(np.float32), (0.0 if b2 <= 0.0 else float(np.sqrt(np.sum(r * r)) / np.sqrt(b2)))
+
+    def sweep(parity, g):
+        sel = solvable & (par == parity)
+        ds = np.zeros(fl.size, np.float32)
+        for q in range(6):
+            ds = np.where(wf[q], ds + w[q] * pd[nbi[q]], ds)
+        dn = (ds + g) * (F32(1.0) / np.where(solvable, nc, F32(1.0)))
+        if omega != F32(1.0):
+            dn = pd[fl] + omega * (dn - pd[fl])
+        pd[fl[sel]] = dn[sel]
+
+    ce = check_every if check_every else 10
+    g, r1 = residual()
+    r0, checks, sweeps = r1, 1, 0
+    nxt = first_check if first_check else ce
+    while not (r1 <= tol) and sweeps < max_sweeps:
+        k = min(nxt, max_sweeps - sweeps)
+        pd[:] = F32(0.0)
+        for _ in range(k):
+            sweep(0, g)
+            sweep(1, g)
+        sweeps += k
+        p = (hi[fl].astype(np.float64) + lo[fl].astype(np.float64)) + pd[fl].astype(np.float64)
+        hi[fl] = p.astype(np.float32)
+        lo[fl] = (p - hi[fl].astype(np.float64)).astype(np.float32)
+        before = r1
+        g, r1 = residual()
+        checks += 1
+        nxt = next_check_interval(r1, before, k, tol, ce)
+    return hi, lo, sweeps, checks, r0, r1
