@@ -1,11 +1,12 @@
-"""The CPU oracle against a second, independent restatement of the WGSL grid passes
-(`tests/wgsl_numpy.py`), pass by pass, on the CPU.
+"""The CPU oracle against a second, independent restatement of the WGSL step
+(`tests/wgsl_numpy.py`), on the CPU.
 
-Each test takes the oracle's state after the first n dispatches of a substep
-(`cs_step_substep_partial`, the dispatch numbering of `mod.rs:317-414`), applies the
-numpy restatement of dispatch n, and compares with the oracle's state after n + 1
-dispatches.  The engine is compared with the oracle bit for bit by the GPU tests, so
-agreement here carries over to it.
+Most tests take the oracle's state after the first n dispatches of a substep
+(`cs_step_substep_partial`, the dispatch numbering of `mod.rs:317-414`), apply the
+numpy restatement of dispatch n, and compare with the oracle's state after n + 1
+dispatches; one chains the restated dispatches over three whole substeps.  The engine
+is compared with the oracle bit for bit by the GPU tests, so agreement here carries
+over to it.
 """
 import numpy as np
 import pytest

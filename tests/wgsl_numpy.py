@@ -1,12 +1,15 @@
-"""A second, independent restatement of grid passes of the reference's WGSL step, in
-vectorised numpy float32 — test infrastructure only.
+"""A second, independent restatement of the reference's WGSL step, in vectorised numpy
+float32 — test infrastructure only.
 
 The C++ oracle (`oracle/oracle.cpp`) and the CUDA engine were written from the same
 reading of `crates/sim-wasm/src/mpm_3d/shader.rs`, so their bit-exact agreement cannot
 expose a misreading they share.  This module is a separate reading of the same WGSL,
-written directly from the shader text in a different form (whole-grid array
-expressions instead of per-cell loops), and the tests compare it with the oracle
-pass by pass.  Every function cites the shader lines it restates.
+written directly from the shader text in a different form (whole-grid and whole-sample
+array expressions with masks instead of per-cell loops), and the tests compare it with
+the oracle dispatch by dispatch and over whole substeps.  It covers every dispatch of
+the step, the uniforms (mod.rs:569-660), the SDF texture and solid class (state.rs),
+jet emission (inflow.rs), and three engine extensions: the int64 P2G lanes, the sample
+reorder and the residual-mode pressure solve.  Every function cites what it restates.
 
 Floating point: every value is an IEEE float32 array and every WGSL expression is
 evaluated in its written, left-to-right order (numpy >= 2 keeps Python scalars weak,
