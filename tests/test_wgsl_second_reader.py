@@ -513,3 +513,24 @@ def test_refinement_solve_cold_start(oracle, grid, omega, cap, first):
     assert abs(r0 - m.initial_residual) <= 1e-9 * r0 and abs(r1 - m.last_residual) <= 1e-9 * r1
     msg = _report("pressure (high word)", hi, b.read_pressure())
     assert msg is None, msg
+
+
+def test_bed_seeding(oracle):
+    """The seeded bed of the reference's scene: BedConfig::seated_in_filter (bed.rs:41-82),
+    the lattice with its rounded bottom and the downsampling to the target count
+    (bed.rs:107-226), and the initial cell lookup (bed.rs:228-314), against the
+    simulation the oracle creates."""
+    s = MpmSettings.benchmark_center_pour(oracle)
+    b = s.raw.bed
+    assert b.log_perm_sigma == 0.0 and b.lower_porosity_scale in (0.0, 1.0)
+    seat = W.seated_in_filter(s.raw.filter)
+    assert tuple(np.float32(v) for v in (b.center[1], b.top_y, b.bot_y, b.top_radius, b.bot_radius)) == seat
+    sim = MpmSim3D(s, oracle)
+    P, A, BE, look = W.init_bed(b, s.raw.grid_dims, s.raw.bounds_size)
+    nb = sim.num_bed
+    assert nb == P.shape[0] == 12000
+    for name, got, want in (("bed samples", P, sim.read_particles(0, nb)), ("bed affine", A, sim.read_affine(0, nb)),
+                            ("bed_extract", BE, sim.read_bed_extract(0, nb)), ("lookup", look, sim.read_bed_lookup())):
+        msg = _report(name, got, want)
+        assert msg is None, msg
+    sim.close()

@@ -1670,3 +1670,142 @@ def refine_solve(u, kind, fill, div, omega, tol, check_every, first_check, max_s
         checks += 1
         nxt = next_check_interval(r1, before, k, tol, ce)
     return hi, lo, sweeps, checks, r0, r1
+
+
+# ---------------------------------------------------------------- bed seeding  (bed.rs:41-314)
+
+def _order_bounds(lo, hi):
+    """bed.rs:84-91"""
+    if lo <= hi:
+        return lo, hi
+    mid = (lo + hi) * F32(0.5)
+    return mid, mid
+
+
+def seated_in_filter(filt):
+    """BedConfig::seated_in_filter (bed.rs:41-82) of the default BedConfig (bed.rs:20-38)
+    in a paper filter: (center_y, top_y, bot_y, top_radius, bot_radius), the y values
+    relative to the filter's centre."""
+    cy = F32(filt.center[1])
+    ftop, fbot = F32(filt.top_y), F32(filt.bot_y)
+    thick, hole, frad = F32(filt.thickness), F32(filt.hole_radius), F32(filt.top_radius)
+
+    def radius_at(y):
+        height = np.maximum(ftop - fbot, F32(1e-6))
+        t = clamp((y - fbot) / height, F32(0.0), F32(1.0))
+        return F32(filt.bot_radius) + (frad - F32(filt.bot_radius)) * t
+
+    def inner_at(y):
+        return np.maximum(radius_at(y) - thick, hole)
+
+    fbot_abs, ftop_abs = cy + fbot, cy + ftop
+    tlo, thi = _order_bounds(fbot_abs + F32(0.6), ftop_abs - F32(0.35))
+    top_abs = clamp(cy + F32(0.45), tlo, thi)
+    blo, bhi = _order_bounds(fbot_abs + F32(0.4), top_abs - F32(1.4))
+    bot_abs = clamp(cy + F32(-2.70), blo, bhi)
+    top_y, bot_y = top_abs - cy, bot_abs - cy
+    rlo, rhi = _order_bounds(hole + F32(0.8), frad - thick - F32(0.1))
+    top_r = clamp(inner_at(top_abs - cy) - F32(0.18), rlo, rhi)
+    blo2, bhi2 = _order_bounds(hole + F32(0.14), top_r - F32(0.25))
+    bot_r = clamp(inner_at(bot_abs - cy) - F32(0.12), blo2, bhi2)
+    return cy, top_y, bot_y, top_r, bot_r
+
+
+def init_bed(bed, grid_dims, bounds_size):
+    """init_bed_particles (bed.rs:107-226) and build_cell_lookup (bed.rs:228-314) for a
+    bed whose per-sample permeability is uniform.  Returns (particles (n, 8), affine
+    (n, 12), bed_extract (n, 8), lookup (cells,))."""
+    import math
+    c = [F32(v) for v in bed.center]
+    top_y, bot_y = F32(bed.top_y), F32(bed.bot_y)
+    top_r, bot_r = F32(bed.top_radius), F32(bed.bot_radius)
+    gx, gy, gz = (int(v) for v in grid_dims)
+    height = top_y - bot_y
+    if height < F32(1e-6):
+        return (np.zeros((0, 8), np.float32), np.zeros((0, 12), np.float32), np.zeros((0, 8), np.float32),
+                np.full(gx * gy * gz, -1, np.int32))
+    avg = (top_r + bot_r) * F32(0.5)
+    q = bot_r / avg
+    volume = F32(np.pi) * avg * avg * height / F32(3.0) * (F32(1.0) + bot_r / avg + q * q)
+    # f32::cbrt leaves the last bit to the platform's libm: evaluated in float64 and
+    # rounded (numpy's own float32 cbrt is one ulp off the rounded cube root here)
+    spacing = F32(np.cbrt(np.float64(volume / F32(max(int(bed.num_particles), 1)))))
+    nx = int(math.ceil(float((top_r * F32(2.0)) / spacing)))
+    ny = int(math.ceil(float(height / spacing)))
+    nz = nx
+    rows, keys = [], []
+    for iy in range(ny):
+        base_y = c[1] + bot_y + (F32(iy) + F32(0.5)) * spacing
+        t = (base_y - (c[1] + bot_y)) / height
+        max_r = bot_r + (top_r - bot_r) * t
+        ix = np.repeat(np.arange(nx), nz)
+        iz = np.tile(np.arange(nz), nx)
+        x = c[0] - max_r + (ix.astype(np.float32) + F32(0.5)) * spacing
+        z = c[2] - max_r + (iz.astype(np.float32) + F32(0.5)) * spacing
+        ddx, ddz = x - c[0], z - c[2]
+        r = np.sqrt(ddx * ddx + ddz * ddz)
+        keep = ~(r > max_r)
+        cap_t = clamp(t / F32(0.16), F32(0.0), F32(1.0))
+        radial_t = r / max_r if max_r > F32(1e-6) else np.zeros_like(r)
+        one = F32(1.0) - cap_t
+        lift = spacing * F32(0.75) * (one * one) * (radial_t * radial_t)
+        y = base_y + lift
+        for k in np.flatnonzero(keep):
+            rows.append((x[k], y[k], z[k]))
+            keys.append((int(ix[k]), iy, int(iz[k])))
+    n_src = len(rows)
+    src = list(range(n_src))
+    target = int(bed.num_particles)
+    if n_src > target:
+        src = [int(min(math.floor(float((F32(o) + F32(0.5)) * F32(n_src) / F32(target))), float(n_src - 1)))
+               for o in range(target)]
+    P = np.zeros((len(src), 8), np.float32)
+    A = np.zeros((len(src), 12), np.float32)
+    BE = np.zeros((len(src), 8), np.float32)
+    lattice = {}
+    for o, i in enumerate(src):
+        x, y, z = rows[i]
+        P[o] = (x, y, z, 1.0, 0.0, 0.0, 0.0, 1.0)
+        A[o] = (0.0, 0.0, 0.0, 1.0, x, y, z, 0.0, y, 0.0, 0.0, 0.0)
+        BE[o] = (0.0, bed.initial_porosity, bed.initial_permeability, 0.0, bed.extractable_mass, 0.0, 93.0, 0.0)
+        lattice[keys[i]] = o
+    # build_cell_lookup
+    bs = [F32(v) for v in bounds_size]
+    org = [-b * F32(0.5) for b in bs]
+    dx = bs[0] / F32(gx)
+    bottom = c[1] + bot_y
+    look = np.full(gx * gy * gz, -1, np.int32)
+    iz_, iy_, ix_ = np.meshgrid(np.arange(gz), np.arange(gy), np.arange(gx), indexing="ij")
+    px = org[0] + (ix_.astype(np.float32) + F32(0.5)) * dx
+    py = org[1] + (iy_.astype(np.float32) + F32(0.5)) * dx
+    pz = org[2] + (iz_.astype(np.float32) + F32(0.5)) * dx
+    inside = ~((py < bottom) | (py > c[1] + top_y))
+    t = clamp((py - bottom) / height, F32(0.0), F32(1.0))
+    mr = bot_r + (top_r - bot_r) * t
+    ddx, ddz = px - c[0], pz - c[2]
+    inside &= ~(np.sqrt(ddx * ddx + ddz * ddz) > mr)
+    for flat in np.flatnonzero(inside.reshape(-1)):
+        k3 = np.unravel_index(flat, inside.shape)
+        x, y, z, m = px[k3], py[k3], pz[k3], mr[k3]
+        gy_ = int(np.rint((y - bottom) / spacing - F32(0.5)))
+        gx_ = int(np.rint((x - (c[0] - m)) / spacing - F32(0.5)))
+        gz_ = int(np.rint((z - (c[2] - m)) / spacing - F32(0.5)))
+        best, best_d2 = -1, F32(np.inf)
+        for dy in (-1, 0, 1):
+            for dxi in (-1, 0, 1):
+                for dzi in (-1, 0, 1):
+                    key = (min(max(gx_ + dxi, 0), max(nx - 1, 0)), min(max(gy_ + dy, 0), max(ny - 1, 0)),
+                           min(max(gz_ + dzi, 0), max(nz - 1, 0)))
+                    if key not in lattice:
+                        continue
+                    ly = bottom + (F32(key[1]) + F32(0.5)) * spacing
+                    lt = clamp((ly - bottom) / height, F32(0.0), F32(1.0))
+                    lr = bot_r + (top_r - bot_r) * lt
+                    lx = c[0] - lr + (F32(key[0]) + F32(0.5)) * spacing
+                    lz = c[2] - lr + (F32(key[2]) + F32(0.5)) * spacing
+                    a, b_, e = x - lx, y - ly, z - lz
+                    d2 = a * a + b_ * b_ + e * e
+                    if d2 < best_d2:
+                        best_d2, best = d2, lattice[key]
+        look[flat] = best
+    return P, A, BE, look
