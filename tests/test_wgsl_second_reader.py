@@ -534,3 +534,40 @@ def test_bed_seeding(oracle):
         msg = _report(name, got, want)
         assert msg is None, msg
     sim.close()
+
+
+@pytest.mark.parametrize("name", ["default_v60", "benchmark_free_stream", "benchmark_center_pour"])
+def test_reference_presets(oracle, name):
+    """The reference's scene presets (mod.rs:105-177) with the spout defaults and aim
+    (inflow.rs:27-59), units (units.rs:9-33) and brew constants (brew_config.rs:38-96),
+    restated as float32 arithmetic, against the settings the oracle's preset fills."""
+    want = W.reference_presets()[name]
+    s = getattr(MpmSettings, name)(oracle).raw
+    f = np.float32
+    assert [f(v) for v in s.bounds_size] == want["bounds_size"]
+    assert list(s.grid_dims) == want["grid_dims"]
+    assert (s.max_particles, s.substeps, s.pressure_rbgs_pairs, s.use_sdf_cache) == \
+        (want["max_particles"], want["substeps"], want["pressure_rbgs_pairs"], want["use_sdf_cache"])
+    for k in ("gravity", "bulk_modulus", "viscosity", "render_radius", "initial_kettle_angle_deg"):
+        assert f(getattr(s, k)) == want[k], k
+    u = want["units"]
+    assert (f(s.sim_units_per_meter), f(s.max_velocity)) == (u["sim_units_per_meter"], u["max_velocity"])
+    cone, cup = s.obstacles[0], s.obstacles[1]
+    assert s.num_obstacles == 2 and list(cone.center) == [0.0, 0.0, 0.0] and list(cup.center) == [0.0, 0.0, 0.0]
+    for k, v in want["cone"].items():
+        assert f(getattr(cone, k)) == v, k
+    for k, v in want["cup"].items():
+        assert f(getattr(cup, k)) == v, k
+    sp = want["spout"]
+    for k, v in sp.items():
+        got = getattr(s.spout, k)
+        got = [f(x) for x in got] if isinstance(v, list) else f(got)
+        assert got == v, (k, got, v)
+    for k, v in want["brew"].items():
+        if hasattr(s.brew, k):
+            assert f(getattr(s.brew, k)) == v, k
+    assert s.has_bed == want["has_bed"]
+    if s.has_bed:
+        assert f(s.bed.initial_permeability) == want["bed_permeability"]
+        assert f(s.bed.initial_porosity) == want["brew"]["bed_porosity"]
+        assert s.bed.num_particles == want["brew"]["bed_particle_samples"]

@@ -1809,3 +1809,64 @@ def init_bed(bed, grid_dims, bounds_size):
                         best_d2, best = d2, lattice[key]
         look[flat] = best
     return P, A, BE, look
+
+
+# ---------------------------------------------------------------- presets  (mod.rs:105-177, inflow.rs:27-58, units.rs, brew_config.rs)
+
+def reference_presets():
+    """MpmSettings::default_v60 / benchmark_free_stream / benchmark_center_pour as plain
+    float32 values, with the units, brew constants and spout defaults they use."""
+    brew = dict(bed_porosity=F32(0.40), bed_particle_samples=12000, water_particles_per_ml=F32(320.0),
+                water_mass_units_per_ml=F32(80.0), water_sample_radius_dx=F32(0.18), bed_sample_radius_dx=F32(0.62),
+                max_flow_rate_ml_s=F32(12.0), initial_kettle_angle_deg=F32(9.0), water_viscosity=F32(1.2),
+                water_kinematic_viscosity_m2_s=F32(1.0e-6), min_bed_permeability_m2=F32(1.0e-12),
+                bed_absorption_rate=F32(1.6), target_bed_retention_ml=F32(42.0), bed_pore_capacity_scale=F32(1.0),
+                bed_pore_overfill_alpha=F32(18.0), bed_surface_void_scale=F32(1.0), dripper_outlet_radius=F32(0.42),
+                filter_absorption_rate_s=F32(0.0), bed_compaction_rate=F32(5.5), bed_impact_rate=F32(8.0))
+    # brew_config.rs:92-96 kozeny_carman_permeability_m2(450 um, 0.40)
+    d = F32(450.0) * F32(1.0e-6)
+    phi = brew["bed_porosity"]
+    solid = F32(1.0) - phi
+    perm = d * d * phi * phi * phi / (F32(180.0) * solid * solid)
+    # units.rs:9-33
+    upm = (F32(2.75) - F32(-3.02)) / F32(0.10)
+    mpu = F32(1.0) / upm
+    units = dict(sim_units_per_meter=upm, ml_per_unit3=mpu * mpu * mpu * F32(1000000.0),
+                 gravity=-F32(9.80665) * upm, max_velocity=F32(1.5) * upm,
+                 gentle=F32(0.12) * upm, high=F32(0.45) * upm)
+    bounds = [F32(14.0), F32(20.0), F32(14.0)]
+    dx = bounds[0] / F32(80)
+    gy = int(np.ceil(bounds[1] / dx))
+    # filter.rs:14-26 and the support cone (mod.rs:163-177)
+    ftop, fbot, frad = F32(2.75), F32(-3.02), F32(4.10)
+    slope = (frad - F32(0.0)) / np.maximum(ftop - fbot, F32(1e-6))
+    outlet = brew["dripper_outlet_radius"]
+    cone = dict(top_radius=outlet + slope * (F32(3.0) - F32(-3.0)), bot_radius=outlet, top_y=F32(3.0), bot_y=F32(-3.0))
+
+    def spout(origin=None, target=None):
+        o = [F32(-3.4), F32(7.3), F32(0.9)]
+        dvec = _normalized([F32(0.36), F32(-0.92), F32(-0.12)])
+        t = [F32(-0.7), F32(0.4), F32(0.0)]
+        if origin is not None:
+            o = [F32(v) for v in origin]
+        if target is not None:                  # SpoutSettings::aim_at (inflow.rs:50-59)
+            t = [F32(v) for v in target]
+            delta = [t[q] - o[q] for q in range(3)]
+            if np.sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]) > F32(1e-5):
+                dvec = _normalized(delta)
+        return dict(origin=o, direction=dvec, target=t, nozzle_radius=F32(0.18), stem_radius=F32(0.24),
+                    activation_angle_deg=F32(8.0), full_flow_angle_deg=F32(56.0), head_at_activation=F32(0.04),
+                    head_at_full_angle=F32(24.0), discharge_coeff=F32(0.92), volume_to_ml=units["ml_per_unit3"],
+                    max_flow_rate_ml_s=brew["max_flow_rate_ml_s"], gentle_exit_speed=units["gentle"],
+                    max_exit_speed=units["high"], stem_length=F32(1.9))
+
+    base = dict(bounds_size=bounds, grid_dims=[80, gy, 80], max_particles=220000, substeps=10,
+                gravity=units["gravity"], bulk_modulus=F32(900.0), viscosity=brew["water_viscosity"],
+                render_radius=dx * F32(0.7), pressure_rbgs_pairs=40, use_sdf_cache=1, cone=cone,
+                cup=dict(radius=F32(3.0), top_y=F32(-3.5), bot_y=F32(-8.0)),
+                initial_kettle_angle_deg=brew["initial_kettle_angle_deg"], brew=brew, units=units,
+                bed_permeability=perm, has_bed=1)
+    presets = {"default_v60": dict(base, spout=spout()),
+               "benchmark_free_stream": dict(base, has_bed=0, spout=spout((0.0, 6.8, 0.0), (0.0, -6.8, 0.0))),
+               "benchmark_center_pour": dict(base, spout=spout((0.0, 7.1, 0.0), (0.0, 0.4, 0.0)))}
+    return presets
