@@ -9,9 +9,9 @@ configuration: fixed-point pressure, 40 pairs), in both P2G lane formats:
 * Sample count and total mass are equal.
 * int64 lanes (i64 * 2^32, the headline workload's mode), 64^3 pour: pressure 5e-8,
   grid momentum 4.4e-6, water-sample velocity 1.7e-6 relative; every water sample's
-  position within 4.8e-7 of the FP64 one (one float32 ulp).  Two of the 3000 bed grains take the other side
-  of a threshold in bed_dynamics and move by a few hundredths of a unit, which alone sets
-  the relative position error of all samples (1.8e-5).
+  position within 4.8e-7 of the FP64 one (one float32 ulp).  Two of the 3000 bed grains
+  take the other side of a threshold in bed_dynamics and move by a few hundredths of a
+  unit, which alone sets the relative position error of all samples (1.8e-5).
 * i32 lanes (i32 * 2^18, the reference's format): grid momentum 1e-4 (64^3) and 2.2e-4
   (water block), velocity 4e-5 and 1e-4.  Each deposit is truncated to a 2^-18 quantum;
   evaluated in float or in double, the same deposit truncates to a different quantum in
