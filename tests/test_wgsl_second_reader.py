@@ -401,7 +401,7 @@ def test_whole_substeps_chained(stages):
     """Three whole substeps of the restatement, each dispatch fed by the previous one
     (the dispatch order and lane aliasing of mod.rs:305-414 included), against three
     whole substeps of the oracle from the same state: every sample, affine column and
-    bed_extract value bit for bit, except J (the backend's exp, within a few ulp)."""
+    bed_extract value bit for bit, except J (the backend's exp; 2 ulp at most measured)."""
     raw = stages.settings.raw
     stages(P_P2G)                      # loads the static SDF texture and solid class
     sim = MpmSim3D(stages.settings, stages.oracle)
@@ -420,7 +420,7 @@ def test_whole_substeps_chained(stages):
     msg = _report("particles (J excluded)", P[:, cols], want_p[:, cols])
     assert msg is None, msg
     j_ulp = np.abs(P[:, 3].view(np.int32).astype(np.int64) - want_p[:, 3].view(np.int32))
-    assert j_ulp.max() <= 8, j_ulp.max()
+    assert j_ulp.max() <= 4, j_ulp.max()
     for name, got, want in (("affine", A, want_a), ("bed_extract", BE, sim.read_bed_extract(0, nb))):
         msg = _report(name, got, want)
         assert msg is None, msg
