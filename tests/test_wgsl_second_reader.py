@@ -571,3 +571,29 @@ def test_reference_presets(oracle, name):
         assert f(s.bed.initial_permeability) == want["bed_permeability"]
         assert f(s.bed.initial_porosity) == want["brew"]["bed_porosity"]
         assert s.bed.num_particles == want["brew"]["bed_particle_samples"]
+
+
+def test_classify_without_sdf_cache(oracle, stages):
+    """classify_cells with `use_sdf_cache` off: the solid tests sample the SDF texture at
+    the cell centre and at the six neighbour centres (shader.rs:1203-1207, 1279-1326)."""
+    s = stages.settings.copy()
+    s.raw.use_sdf_cache = 0
+    sims = []
+    for n in (P_CLASSIFY, P_CLASSIFY + 1):
+        sim = MpmSim3D(s, oracle)
+        copy_state(stages.src, sim)
+        sim.set_kettle_angle(36.0)
+        sim.step_substep_partial(SUB_DT, n)
+        sims.append(sim)
+    before, after = sims
+    u = W.Uniforms(s.raw, before.num_water, before.num_bed, SUB_DT)
+    sdf = W.Sdf(u, before.read_sdf())
+    n = before.particle_count()
+    bed = W.Bed(u, before.read_bed_lookup(), before.read_particles(0, n), before.read_affine(0, n),
+                before.read_bed_extract(0, before.num_bed))
+    lanes = W.classify(u, before.read_grid_lanes(), before.read_grid_vel(), bed, sdf, None, False)
+    want = after.read_grid_lanes()
+    assert np.count_nonzero(want[3] == W.CELL_SOLID) > 1000
+    for lane in (3, 1, 0):
+        msg = _report(f"lane {lane}", lanes[lane], want[lane])
+        assert msg is None, msg
